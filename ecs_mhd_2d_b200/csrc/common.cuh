@@ -1,0 +1,90 @@
+// Common device helpers for the ECS-MHD-2D B200 kernels.
+//
+// Spectral "box" layout (all hot kernels):
+//   The 2/3 dealiasing mask of the reference (jax_scripts/lib/mhd_jax.py:65-70)
+//   keeps |kx| < n/3 and |ky| < n/3.  Every hot-path state lives only on those
+//   modes, so the state is stored compactly as
+//       V[b][c][ky][slot]      c in {omega, j}, ky in [0, K), slot in [0, M)
+//   with kmax = (n-1)/3, K = kmax+1, M = 2*kmax+1 and
+//       kx(slot) = slot (slot <= kmax),  slot - M (slot > kmax).
+//   A column (fixed ky) is contiguous, which is what the column kernels read.
+//   FFT position p (fftfreq order, length n) <-> slot: p = kx mod n.
+//
+// Intermediate layouts (per batch element):
+//   G[b][field][ky][x]   column-inverse-transformed fields (complex, x contiguous)
+//   H[b][field][ky][x]   row-forward-transformed fields      (complex, x contiguous)
+//   Phys[x][field][pos]  physical rows in warp-FFT position order (primal record)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ecs {
+
+template <typename R> struct CplxT;
+template <> struct CplxT<double> { using type = double2; };
+template <> struct CplxT<float>  { using type = float2; };
+template <typename R> using cplx = typename CplxT<R>::type;
+
+template <typename R> __host__ __device__ __forceinline__ cplx<R> mk(R x, R y) { cplx<R> c; c.x = x; c.y = y; return c; }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { a.x *= s; a.y *= s; return a; }
+// (i*mu) * z for real mu, written exactly as the reference's `1j * mu * z`.
+template <typename C, typename R> __device__ __forceinline__ C cimul(C z, R mu) {
+  C r; r.x = -mu * z.y; r.y = mu * z.x; return r;
+}
+template <typename C, typename R> __device__ __forceinline__ C cdiv_r(C a, R s) { a.x = a.x / s; a.y = a.y / s; return a; }
+
+template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_c(cplx<R> v, int m) {
+  v.x = __shfl_xor_sync(0xffffffffu, v.x, m);
+  v.y = __shfl_xor_sync(0xffffffffu, v.y, m);
+  return v;
+}
+template <typename R> __device__ __forceinline__ cplx<R> shfl_c(cplx<R> v, int src) {
+  v.x = __shfl_sync(0xffffffffu, v.x, src);
+  v.y = __shfl_sync(0xffffffffu, v.y, src);
+  return v;
+}
+
+// Box geometry for a grid side n.
+struct Geom {
+  int n, kmax, K, M;
+};
+__host__ __device__ inline Geom make_geom(int n) {
+  Geom g; g.n = n; g.kmax = (n - 1) / 3; g.K = g.kmax + 1; g.M = 2 * g.kmax + 1; return g;
+}
+// FFT position -> slot (or -1 when outside the box).
+__host__ __device__ __forceinline__ int pos_to_slot(int p, int n, int kmax, int M) {
+  if (p <= kmax) return p;
+  if (p >= n - kmax) return p - n + M;
+  return -1;
+}
+__host__ __device__ __forceinline__ int slot_to_kx(int s, int kmax, int M) { return s <= kmax ? s : s - M; }
+__host__ __device__ __forceinline__ int pos_to_k(int p, int n) { return p <= n / 2 ? p : p - n; }
+
+template <int N> __device__ __forceinline__ int bitrev(int e) {
+  constexpr int B = (N == 64) ? 6 : (N == 128) ? 7 : (N == 256) ? 8 : (N == 32) ? 5 : 0;
+  static_assert(B > 0, "unsupported N");
+  return (int)(__brev((unsigned)e) >> (32 - B));
+}
+
+// Per-batch-element control block for the fixed-step and adaptive steppers.
+struct StepCtl {
+  double t;        // integration time of the call (Lawson-RK43: the horizon T)
+  double h;        // current step (Lawson-RK4: (T/nc)/ms)
+  double s;        // Lawson-RK43 pseudo-time in [0, 1]
+  double err;      // last error estimate (Lawson-RK43)
+  int accepted, rejected, fevals, done;
+  int pending_accept;   // last attempt accepted, state not yet promoted
+  int attempts;         // attempts recorded
+  unsigned long long err_bits;  // atomicMax scratch for |err| (non-negative doubles)
+  unsigned int err_blocks;      // blocks that have reported their error partial
+  int pad;
+};
+
+}  // namespace ecs

@@ -1,0 +1,710 @@
+// Hot-path kernels of the pseudo-spectral MHD right-hand side and the Lawson
+// steppers.  One right-hand-side evaluation (reference: state_vel,
+// jax_scripts/lib/mhd_jax.py:105-175) is split into two passes around the two
+// transposes of a 2D FFT:
+//
+//   column pass (one warp per (batch, ky) column, x contiguous):
+//     [forward FFT along x of the two product fields of the previous RHS]
+//     -> spectral epilogue (dealias mask, k^2, forcing, stepper stage algebra)
+//     -> stage input -> 4 spectral multipliers per channel (i kx, i ky,
+//        i ky/k^2, -i kx/k^2) -> 8 inverse FFTs along x -> G
+//   row pass (one warp per physical row x, CTA = XT rows staged in shared memory):
+//     8 half-spectra rows of G -> 4 complex inverse FFTs (two real fields
+//     packed per transform) -> pointwise products (advection, induction,
+//     mean field) -> 1 forward FFT (two products packed) -> split -> H
+//
+// The box layout and intermediate layouts are documented in common.cuh.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace ecs {
+
+// ---------------------------------------------------------------------------
+// spectral helpers
+// ---------------------------------------------------------------------------
+
+// Multiplier mu for field m in {0:x, 1:y, 2:u, 3:v} at integer (kx, ky) inside
+// the box, matching mhd_jax.py:83-90 (to_u = ky/k^2, to_v = -kx/k^2, masked).
+template <typename R>
+__device__ __forceinline__ R spectral_mu(int m, int kx, int ky) {
+  if (kx == 0 && ky == 0) return R(0);
+  const R rkx = (R)kx, rky = (R)ky;
+  const R ksq = rkx * rkx + rky * rky;
+  switch (m) {
+    case 0: return rkx;
+    case 1: return rky;
+    case 2: return rky / ksq;
+    default: return (-rkx) / ksq;
+  }
+}
+
+// (kx^2 + ky^2) * mask with masked kx, ky (mhd_jax.py:154).
+template <typename R>
+__device__ __forceinline__ R ksq_masked(int kx, int ky) {
+  if (kx == 0 && ky == 0) return R(0);
+  const R rkx = (R)kx, rky = (R)ky;
+  return rkx * rkx + rky * rky;
+}
+
+// Dissipation L = -(kx^2+ky^2) * coeff (mhd_jax.py:97-102), zero at (0,0).
+template <typename R>
+__device__ __forceinline__ R diss_L(int kx, int ky, R coeff) {
+  return (-ksq_masked<R>(kx, ky)) * coeff;
+}
+
+// ---------------------------------------------------------------------------
+// column-pass building blocks (one warp per (batch, ky) column)
+// ---------------------------------------------------------------------------
+
+// Load the two product columns H[b][0..1][ky][:] and transform them along x
+// (forward, natural -> bit-reversed order).
+template <typename R, int N>
+__device__ __forceinline__ void col_load_fwd(const cplx<R>* __restrict__ H, int b, int ky, int lane,
+                                             const cplx<R>* s_tw, cplx<R> (&r0)[N / 32], cplx<R> (&r1)[N / 32]) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const cplx<R>* h0 = H + ((size_t)(b * 2 + 0) * K + ky) * N;
+  const cplx<R>* h1 = H + ((size_t)(b * 2 + 1) * K + ky) * N;
+#pragma unroll
+  for (int j = 0; j < E; ++j) { r0[j] = h0[lane + 32 * j]; r1[j] = h1[lane + 32 * j]; }
+  fft_dif<R, N, false>(r0, s_tw, lane);
+  fft_dif<R, N, false>(r1, s_tw, lane);
+}
+
+// Nonlinear time derivative at one box mode from the transformed products:
+// v_omega = mask*(rfft2(P1) + rfft2(forcing)), v_j = k^2 mask rfft2(P2)  (mhd_jax.py:159-164).
+template <typename R>
+__device__ __forceinline__ void rhs_vals(cplx<R> r0, cplx<R> r1, int kx, int ky, cplx<R> fh, cplx<R>& v0,
+                                         cplx<R>& v1) {
+  const bool in_mask = !(kx == 0 && ky == 0);
+  v0 = in_mask ? cadd(r0, fh) : mk<R>(0, 0);
+  v1 = cscale(r1, ksq_masked<R>(kx, ky));
+}
+
+// Stage input (x0, x1 in bit-reversed slot order) -> the 8 multiplied inverse
+// transforms along x of state_vel (mhd_jax.py:136-141), scaled by 1/n^2.
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse8(const cplx<R> (&x0)[N / 32], const cplx<R> (&x1)[N / 32],
+                                             cplx<R>* __restrict__ G, int b, int ky, int lane,
+                                             const cplx<R>* s_tw) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const R inv_n2 = R(1) / (R(N) * R(N));
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      cplx<R> w[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+        const cplx<R> xv = c == 0 ? x0[j] : x1[j];
+        w[j] = cscale(cimul(xv, spectral_mu<R>(m, kx, ky)), inv_n2);
+      }
+      fft_dit<R, N, true>(w, s_tw, lane);
+      cplx<R>* gout = G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
+#pragma unroll
+      for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+    }
+  }
+}
+
+// Plain inverse transforms along x of two box columns, scaled 1/n^2, written to
+// fields 0 and 1 of G[b] (pitch `nf` fields per batch element).
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse2(const cplx<R> (&x0)[N / 32], const cplx<R> (&x1)[N / 32],
+                                             cplx<R>* __restrict__ G, int nf, int b, int ky, int lane,
+                                             const cplx<R>* s_tw) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const R inv_n2 = R(1) / (R(N) * R(N));
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    cplx<R> w[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) w[j] = cscale(c == 0 ? x0[j] : x1[j], inv_n2);
+    fft_dit<R, N, true>(w, s_tw, lane);
+    cplx<R>* gout = G + ((size_t)(b * nf + c) * K + ky) * N;
+#pragma unroll
+    for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass of the forward RHS fused with the Lawson-RK4 stage algebra
+// (reference: timestepping.lawson_rk4, jax_scripts/lib/timestepping.py:69-80).
+// ---------------------------------------------------------------------------
+
+enum ColStage : int {
+  COL_START = 0,     // no RHS input; stage input = F (start of a step)
+  COL_RK4_S1 = 1,    // finish k1, stage input X2
+  COL_RK4_S2 = 2,    // finish k2, stage input X3
+  COL_RK4_S3 = 3,    // finish k3, stage input X4
+  COL_RK4_S4 = 4,    // finish k4 (state update), stage input X1 of next step
+  COL_PLAIN = 5,     // finish RHS: OUT = v (+ L f0 if diss)   [state_vel]
+};
+
+template <typename R>
+struct ColParams {
+  const cplx<R>* H;      // [B][2][K][N]
+  cplx<R>* G;            // [B][8][K][N]
+  cplx<R>* F;            // [B][2][K][M]   state / accumulator
+  cplx<R>* A1;           // [B][2][K][M]   e*k1
+  cplx<R>* K2;           // [B][2][K][M]   k2
+  cplx<R>* OUT;          // [B][2][K][M]   COL_PLAIN output
+  const R* Etab;         // [B][2][K][M]   exp(h/2 L) * mask
+  const StepCtl* ctl;    // [B]
+  const cplx<R>* fhat;   // [K][M] box spectrum of the forcing (omega only)
+  const cplx<R>* tw;     // [N/2]
+  R nu, eta;
+  int B;
+  int stage;
+  int produce;           // write G for the stage input
+  int diss;              // COL_PLAIN: add L f (f = F)
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * K) return;
+  const int b = col / K, ky = col - b * K;
+
+  cplx<R> r0[E], r1[E];
+  if (p.stage != COL_START) {
+    const cplx<R>* h0 = p.H + ((size_t)(b * 2 + 0) * K + ky) * N;
+    const cplx<R>* h1 = p.H + ((size_t)(b * 2 + 1) * K + ky) * N;
+#pragma unroll
+    for (int j = 0; j < E; ++j) { r0[j] = h0[lane + 32 * j]; r1[j] = h1[lane + 32 * j]; }
+    fft_dif<R, N, false>(r0, s_tw, lane);
+    fft_dif<R, N, false>(r1, s_tw, lane);
+  }
+  const R h = (R)p.ctl[b].h;
+  cplx<R> x0[E], x1[E];
+  const size_t base0 = ((size_t)(b * 2 + 0) * K + ky) * M;
+  const size_t base1 = ((size_t)(b * 2 + 1) * K + ky) * M;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int pos = bitrev<N>(lane + 32 * j);
+    const int slot = pos_to_slot(pos, N, KMAX, M);
+    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    if (slot < 0) continue;
+    const int kx = slot_to_kx(slot, KMAX, M);
+    const bool in_mask = !(kx == 0 && ky == 0);
+    cplx<R> v0 = mk<R>(0, 0), v1 = mk<R>(0, 0);
+    if (p.stage != COL_START) {
+      if (in_mask) v0 = cadd(r0[j], p.fhat[ky * M + slot]);   // mask * rfft2(-adv0+adv1+forcing)
+      v1 = cscale(r1[j], ksq_masked<R>(kx, ky));                // k^2 mask * rfft2(u x B)
+    }
+    const size_t i0 = base0 + slot, i1 = base1 + slot;
+    switch (p.stage) {
+      case COL_START: {
+        x0[j] = p.F[i0]; x1[j] = p.F[i1];
+      } break;
+      case COL_RK4_S1: {   // k1 = h v(f); f = e f; k1 = e k1; X2 = f + k1/2
+        const R e0 = p.Etab[i0], e1 = p.Etab[i1];
+        cplx<R> k10 = cscale(v0, h), k11 = cscale(v1, h);
+        cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
+        k10 = cscale(k10, e0); k11 = cscale(k11, e1);
+        p.F[i0] = f0; p.F[i1] = f1; p.A1[i0] = k10; p.A1[i1] = k11;
+        x0[j] = cadd(f0, cscale(k10, R(0.5))); x1[j] = cadd(f1, cscale(k11, R(0.5)));
+      } break;
+      case COL_RK4_S2: {   // k2 = h v(X2); X3 = f + k2/2
+        cplx<R> k20 = cscale(v0, h), k21 = cscale(v1, h);
+        p.K2[i0] = k20; p.K2[i1] = k21;
+        x0[j] = cadd(p.F[i0], cscale(k20, R(0.5))); x1[j] = cadd(p.F[i1], cscale(k21, R(0.5)));
+      } break;
+      case COL_RK4_S3: {   // k3; f,k1,k2,k3 *= e; X4 = f + k3; acc = f + k1/6 + k2/3 + k3/3
+        const R e0 = p.Etab[i0], e1 = p.Etab[i1];
+        cplx<R> k30 = cscale(v0, h), k31 = cscale(v1, h);
+        cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
+        cplx<R> a0 = cscale(p.A1[i0], e0), a1 = cscale(p.A1[i1], e1);
+        cplx<R> c0 = cscale(p.K2[i0], e0), c1 = cscale(p.K2[i1], e1);
+        k30 = cscale(k30, e0); k31 = cscale(k31, e1);
+        x0[j] = cadd(f0, k30); x1[j] = cadd(f1, k31);
+        cplx<R> s0 = cadd(cadd(cadd(f0, cdiv_r(a0, R(6))), cdiv_r(c0, R(3))), cdiv_r(k30, R(3)));
+        cplx<R> s1 = cadd(cadd(cadd(f1, cdiv_r(a1, R(6))), cdiv_r(c1, R(3))), cdiv_r(k31, R(3)));
+        p.F[i0] = s0; p.F[i1] = s1;
+      } break;
+      case COL_RK4_S4: {   // k4; f = acc + k4/6
+        cplx<R> k40 = cscale(v0, h), k41 = cscale(v1, h);
+        cplx<R> f0 = cadd(p.F[i0], cdiv_r(k40, R(6))), f1 = cadd(p.F[i1], cdiv_r(k41, R(6)));
+        p.F[i0] = f0; p.F[i1] = f1;
+        x0[j] = f0; x1[j] = f1;
+      } break;
+      default: {           // COL_PLAIN: state_vel output
+        if (p.diss) {
+          v0 = cadd(v0, cscale(p.F[i0], diss_L<R>(kx, ky, p.nu)));
+          v1 = cadd(v1, cscale(p.F[i1], diss_L<R>(kx, ky, p.eta)));
+        }
+        p.OUT[i0] = v0; p.OUT[i1] = v1;
+      } break;
+    }
+  }
+  if (!p.produce) return;
+  // stage input -> 8 multiplied inverse transforms along x (irfft2 over kx, scaled 1/n^2)
+  const R inv_n2 = R(1) / (R(N) * R(N));
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      cplx<R> w[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int pos = bitrev<N>(lane + 32 * j);
+        const int kx = pos_to_k(pos, N);
+        const cplx<R> xv = c == 0 ? x0[j] : x1[j];
+        const R mu = spectral_mu<R>(m, kx, ky);
+        w[j] = cscale(cimul(xv, mu), inv_n2);
+      }
+      fft_dit<R, N, true>(w, s_tw, lane);
+      cplx<R>* gout = p.G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
+#pragma unroll
+      for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row pass of the forward RHS: products in physical space.
+// ---------------------------------------------------------------------------
+
+template <typename R>
+struct RowParams {
+  const cplx<R>* G;   // [B][8][K][N]
+  cplx<R>* H;         // [B][2][K][N]
+  R* phys;            // optional record of the 8 physical fields, see phys_row()
+  long phys_bstride;  // elements per batch element in phys
+  int rec_index;      // record slot (attempt); < 0: ctl[b].attempts
+  int phys_stage;     // stage slot 0..3 within the record
+  const StepCtl* ctl; // per-batch control (done flags, attempt counters) or null
+  const cplx<R>* tw;
+  R b0x, b0y;
+  int B;
+};
+
+// Physical-field record: phys[b][rec][stage(4)][x][field(8)][pos] with pos the
+// warp-FFT position order (see fft.cuh), so that readers with the same
+// transform structure use identical indexing.
+template <typename R, int N>
+__device__ __forceinline__ R* phys_row(R* base, long bstride, int b, int rec, int stage, int x) {
+  return base + (size_t)b * bstride + (((size_t)rec * 4 + stage) * N + x) * 8 * N;
+}
+
+// Load a [nf][K][XT] tile of a [B][nf][K][N] array into shared memory with row pitch XT+1.
+template <typename R, int N, int XT>
+__device__ __forceinline__ void load_tile(cplx<R>* s, const cplx<R>* __restrict__ g, int nfK, int x0) {
+  for (int i = threadIdx.x; i < nfK * XT; i += blockDim.x) {
+    const int xt = i % XT, r = i / XT;
+    s[r * (XT + 1) + xt] = g[(size_t)r * N + x0 + xt];
+  }
+}
+template <typename R, int N, int XT>
+__device__ __forceinline__ void store_tile(cplx<R>* __restrict__ g, const cplx<R>* s, int nfK, int x0) {
+  for (int i = threadIdx.x; i < nfK * XT; i += blockDim.x) {
+    const int xt = i % XT, r = i / XT;
+    g[(size_t)r * N + x0 + xt] = s[r * (XT + 1) + xt];
+  }
+}
+
+// Full Hermitian spectrum value at position q (natural order) of the packed
+// pair A + iB, from half-spectrum rows sA, sB (pitch XT+1, column w).  The ky=0
+// entries contribute only their real parts, as irfft does.
+template <typename R, int N, int XT>
+__device__ __forceinline__ cplx<R> packed_pair(const cplx<R>* sA, const cplx<R>* sB, int q, int w) {
+  constexpr int K = (N - 1) / 3 + 1;
+  if (q < K) {
+    cplx<R> a = sA[q * (XT + 1) + w], bb = sB[q * (XT + 1) + w];
+    if (q == 0) { a.y = 0; bb.y = 0; }
+    return mk<R>(a.x - bb.y, a.y + bb.x);
+  }
+  if (q > N - K) {
+    const int qq = N - q;
+    cplx<R> a = sA[qq * (XT + 1) + w], bb = sB[qq * (XT + 1) + w];
+    return mk<R>(a.x + bb.y, bb.x - a.y);
+  }
+  return mk<R>(0, 0);
+}
+
+// Split a natural-order forward transform W of (P1 + i P2) into the half
+// spectra of P1 and P2 and write ky < K into shared rows s1, s2.
+template <typename R, int N, int XT>
+__device__ __forceinline__ void split_store(const cplx<R> (&W)[N / 32], cplx<R>* s1, cplx<R>* s2, int w, int lane) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    cplx<R> t = shfl_c<R>(W[E - 1 - j], (32 - lane) & 31);
+    const cplx<R> P = (lane == 0) ? W[(E - j) % E] : t;
+    const int q = lane + 32 * j;
+    if (q < K) {
+      const cplx<R> Wq = W[j];
+      s1[q * (XT + 1) + w] = mk<R>((Wq.x + P.x) * R(0.5), (Wq.y - P.y) * R(0.5));
+      s2[q * (XT + 1) + w] = mk<R>((Wq.y + P.y) * R(0.5), (P.x - Wq.x) * R(0.5));
+    }
+  }
+}
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_H = s_G + 8 * K * (XT + 1);
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  if (p.ctl && p.ctl[b].done) return;   // whole block belongs to one batch element
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 8 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  R* ph = nullptr;
+  if (p.phys) {
+    const int rec = p.rec_index >= 0 ? p.rec_index : p.ctl[b].attempts;
+    ph = phys_row<R, N>(p.phys, p.phys_bstride, b, rec, p.phys_stage, x);
+  }
+
+  // pairs: (fx0,fy0) (fu0,fv0) (fx1,fy1) (fu1,fv1)
+  cplx<R> xy0[E], uv0[E], xy1[E], uv1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int q = lane + 32 * j;
+    xy0[j] = packed_pair<R, N, XT>(s_G + 0 * K * (XT + 1), s_G + 1 * K * (XT + 1), q, w);
+    uv0[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), q, w);
+    xy1[j] = packed_pair<R, N, XT>(s_G + 4 * K * (XT + 1), s_G + 5 * K * (XT + 1), q, w);
+    uv1[j] = packed_pair<R, N, XT>(s_G + 6 * K * (XT + 1), s_G + 7 * K * (XT + 1), q, w);
+  }
+  fft_dif<R, N, true>(xy0, s_tw, lane);
+  fft_dif<R, N, true>(uv0, s_tw, lane);
+  fft_dif<R, N, true>(xy1, s_tw, lane);
+  fft_dif<R, N, true>(uv1, s_tw, lane);
+  cplx<R> W[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const R fx0 = xy0[j].x, fy0 = xy0[j].y, fu0 = uv0[j].x, fv0 = uv0[j].y;
+    const R fx1 = xy1[j].x, fy1 = xy1[j].y;
+    const R fu1 = uv1[j].x + p.b0x, fv1 = uv1[j].y + p.b0y;   // mhd_jax.py:145-149
+    const R adv0 = fu0 * fx0 + fv0 * fy0;                      // :152
+    const R adv1 = fu1 * fx1 + fv1 * fy1;
+    const R P1 = -adv0 + adv1;                                 // :159 (forcing added spectrally)
+    const R P2 = fu0 * fv1 - fv0 * fu1;                        // :163
+    W[j] = mk<R>(P1, P2);
+    if (ph) {
+      const int e = lane + 32 * j;
+      ph[0 * N + e] = fx0; ph[1 * N + e] = fy0; ph[2 * N + e] = fu0; ph[3 * N + e] = fv0;
+      ph[4 * N + e] = fx1; ph[5 * N + e] = fy1; ph[6 * N + e] = fu1; ph[7 * N + e] = fv1;
+    }
+  }
+  fft_dit<R, N, false>(W, s_tw, lane);
+  split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * 2 * K * N, s_H, 2 * K, x0);
+}
+
+// ---------------------------------------------------------------------------
+// Boundary transforms between real fields [B][2][N][N] and the box spectrum.
+// ---------------------------------------------------------------------------
+
+// Row pass of rfft2 restricted to ky < K: real rows of both channels -> H[B][2][K][N].
+template <typename R>
+struct RowFwdParams {
+  const R* fields;    // [B][2][N][N]
+  cplx<R>* H;         // [B][2][K][N]
+  const cplx<R>* tw;
+  int B;
+};
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_to_box(RowFwdParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_H = s_tw + N / 2;
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  const R* u0 = p.fields + ((size_t)(b * 2 + 0) * N + x) * N;
+  const R* u1 = p.fields + ((size_t)(b * 2 + 1) * N + x) * N;
+  cplx<R> W[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int y = bitrev<N>(lane + 32 * j);
+    W[j] = mk<R>(u0[y], u1[y]);
+  }
+  fft_dit<R, N, false>(W, s_tw, lane);
+  split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * 2 * K * N, s_H, 2 * K, x0);
+}
+
+// Column pass of rfft2: H columns -> box spectrum V (raw rfft2 values, no mask).
+template <typename R>
+struct ColBoxParams {
+  const cplx<R>* H;   // [B][nf][K][N]
+  cplx<R>* V;         // [B][nf][K][M] with batch stride vstride (elements)
+  const cplx<R>* tw;
+  long vstride;
+  int B, nf;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_to_box(ColBoxParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * p.nf * K) return;   // col = (b*nf + f)*K + ky
+  const cplx<R>* hin = p.H + (size_t)col * N;
+  cplx<R> v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = hin[lane + 32 * j];
+  fft_dif<R, N, false>(v, s_tw, lane);
+  const int b = col / (p.nf * K), fk = col - b * p.nf * K;
+  cplx<R>* vout = p.V + (size_t)b * p.vstride + (size_t)fk * M;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    if (slot >= 0) vout[slot] = v[j];
+  }
+}
+
+// Symmetry group action applied to a box spectrum value at (kx, ky) of channel c
+// (reference: symmetry.shift_x / shift_reflect / rot180, jax_scripts/lib/symmetry.py:4-25).
+// The source value must be read at kx_src = odd_ny ? -kx : kx.
+struct SymOp {
+  double sx;   // x shift
+  double sy;   // y shift = ny * 2 pi / 8
+  int odd;     // ny odd: reflect x and negate
+  int rot;     // rot180: conj, channel signs [1, -1]
+};
+
+template <typename R>
+__device__ __forceinline__ cplx<R> apply_sym(cplx<R> g, int kx_src, int ky, int c, const SymOp& s) {
+  // masked wavenumbers: (0,0) is masked out, so both phases are 1 there
+  const bool m = !(kx_src == 0 && ky == 0);
+  double sn, cs;
+  sincos(m ? (double)kx_src * s.sx : 0.0, &sn, &cs);
+  cplx<R> a = cmul(mk<R>((R)cs, (R)sn), g);
+  sincos(m ? (double)ky * s.sy : 0.0, &sn, &cs);   // ky is unchanged by the x reflection
+  a = cmul(mk<R>((R)cs, (R)sn), a);
+  if (s.odd) { a.x = -a.x; a.y = -a.y; }
+  if (s.rot) { a.y = -a.y; if (c == 1) { a.x = -a.x; a.y = -a.y; } }
+  return a;
+}
+
+// Column inverse from a box spectrum (2 channels) -> G2[B][2][K][N], with an
+// optional symmetry action, optional scaling and optional multiplier (i kx).
+template <typename R>
+struct ColFromBoxParams {
+  const cplx<R>* V;   // [B][2][K][M]
+  cplx<R>* G;         // [B][2][K][N]
+  const cplx<R>* tw;
+  const double* sx;   // [B] or null
+  double sy;
+  int odd, rot, use_sym;
+  int mult_ikx;       // multiply by i kx (masked) before the inverse
+  int B;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * 2 * K) return;   // col = (b*2 + c)*K + ky
+  const int ky = col % K, bc = col / K, c = bc & 1, b = bc >> 1;
+  const cplx<R>* vin = p.V + (size_t)col * M;
+  SymOp so; so.sx = p.sx ? p.sx[b] : 0.0; so.sy = p.sy; so.odd = p.odd; so.rot = p.rot;
+  const R inv_n2 = R(1) / (R(N) * R(N));
+  cplx<R> v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int pos = bitrev<N>(lane + 32 * j);
+    const int slot = pos_to_slot(pos, N, KMAX, M);
+    v[j] = mk<R>(0, 0);
+    if (slot < 0) continue;
+    const int kx = slot_to_kx(slot, KMAX, M);
+    cplx<R> val;
+    if (p.use_sym) {
+      const int ksrc = so.odd ? -kx : kx;
+      const int ssrc = ksrc >= 0 ? ksrc : ksrc + M;
+      val = apply_sym<R>(vin[ssrc], ksrc, ky, c, so);
+    } else {
+      val = vin[slot];
+    }
+    if (p.mult_ikx) val = cimul(val, (kx == 0 && ky == 0) ? R(0) : (R)kx);
+    v[j] = cscale(val, inv_n2);
+  }
+  fft_dit<R, N, true>(v, s_tw, lane);
+  cplx<R>* gout = p.G + (size_t)col * N;
+#pragma unroll
+  for (int j = 0; j < E; ++j) gout[lane + 32 * j] = v[j];
+}
+
+// Row c2r of the two channels G2[B][2][K][N] -> real fields.
+//   mode 0: out = u
+//   mode 1: out = base - u   (objective residual irfft2(f0 - f) with irfft2(f0) = base)
+// Optionally accumulates per-row sums of out^2 (loss) into rowsq[B][N].
+template <typename R>
+struct RowFromBoxParams {
+  const cplx<R>* G;   // [B][2][K][N]
+  R* out;             // [B][2][N][N]
+  const R* base;      // [B][2][N][N] or null
+  double* rowsq;      // [B][N] or null
+  const cplx<R>* tw;
+  int B, mode;
+};
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_from_box(RowFromBoxParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 2 * K * N, 2 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  cplx<R> z[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int q = bitrev<N>(lane + 32 * j);
+    z[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), q, w);
+  }
+  fft_dit<R, N, true>(z, s_tw, lane);
+  R* o0 = p.out + ((size_t)(b * 2 + 0) * N + x) * N;
+  R* o1 = p.out + ((size_t)(b * 2 + 1) * N + x) * N;
+  const R* b0 = p.base ? p.base + ((size_t)(b * 2 + 0) * N + x) * N : nullptr;
+  const R* b1 = p.base ? p.base + ((size_t)(b * 2 + 1) * N + x) * N : nullptr;
+  double sq = 0.0;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int y = lane + 32 * j;
+    R a = z[j].x, c = z[j].y;
+    if (p.mode == 1) { a = b0[y] - a; c = b1[y] - c; }
+    o0[y] = a; o1[y] = c;
+    sq += (double)a * (double)a + (double)c * (double)c;
+  }
+  if (p.rowsq) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if (lane == 0) p.rowsq[(size_t)b * N + x] = sq;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small elementwise kernels
+// ---------------------------------------------------------------------------
+
+// Full rfft2 layout [B][2][N][N/2+1] <-> box [B][2][K][M].
+template <typename R>
+__global__ void k_gather_box(const cplx<R>* full, cplx<R>* box, int n, int B) {
+  const Geom g = make_geom(n);
+  const int nh = n / 2 + 1;
+  const long total = (long)B * 2 * g.K * g.M;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int slot = i % g.M; const long r = i / g.M; const int ky = r % g.K; const long bc = r / g.K;
+    const int kx = slot_to_kx(slot, g.kmax, g.M);
+    const int pos = kx >= 0 ? kx : kx + n;
+    box[i] = full[(bc * n + pos) * nh + ky];
+  }
+}
+
+template <typename R>
+__global__ void k_scatter_box(const cplx<R>* box, cplx<R>* full, int n, int B) {
+  const Geom g = make_geom(n);
+  const int nh = n / 2 + 1;
+  const long total = (long)B * 2 * n * nh;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ky = i % nh; const long r = i / nh; const int pos = r % n; const long bc = r / n;
+    const int slot = (ky < g.K) ? pos_to_slot(pos, n, g.kmax, g.M) : -1;
+    full[i] = slot >= 0 ? box[(bc * g.K + ky) * g.M + slot] : mk<R>(0, 0);
+  }
+}
+
+// Lawson-RK4 setup: h = (T/nc)/ms and e = exp(h/2 L) * mask per batch element.
+template <typename R>
+__global__ void k_rk4_setup(const double* T, int nc, int ms, StepCtl* ctl, R* Etab, int n, double nu, double eta, int B) {
+  const Geom g = make_geom(n);
+  const long per = 2L * g.K * g.M;
+  const long total = (long)B * per;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / per);
+    const double tseg = T[b] / (double)nc;          // loss_functions.py:63 T/num_checkpoints
+    const R h = (R)(tseg / (double)ms);              // timestepping.py:69 h = t/steps
+    if (i % per == 0) { ctl[b].t = tseg; ctl[b].h = (double)h; }
+    const int slot = i % g.M; const long r = i / g.M; const int ky = r % g.K; const int c = (r / g.K) & 1;
+    const int kx = slot_to_kx(slot, g.kmax, g.M);
+    const R L = diss_L<R>(kx, ky, (R)(c == 0 ? nu : eta));
+    const bool msk = !(kx == 0 && ky == 0);
+    Etab[i] = msk ? exp(h / R(2) * L) : R(0);        // timestepping.py:70-72
+  }
+}
+
+// out -= P_sym(rest): the symmetry action on modes outside the box, which in
+// real space is x -> -x with negation (odd ny) and a 180 degree rotation with
+// channel signs [1, -1] (rot); shift_x and the y-phase of shift_reflect use
+// masked wavenumbers and leave these modes unchanged (symmetry.py:4-25).
+template <typename R>
+__global__ void k_sub_sym_phys(R* out, const R* rest, int odd, int rot, int n, int B) {
+  const long total = (long)B * 2 * n * n;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int y = i % n; const long r = i / n; const int x = r % n; const long bc = r / n; const int c = bc & 1;
+    const int sx = (odd ? -1 : 1) * (rot ? -1 : 1), sy = rot ? -1 : 1;
+    const int xs = ((sx * x) % n + n) % n, ys = ((sy * y) % n + n) % n;
+    R f = rest[(bc * n + xs) * n + ys];
+    if (odd) f = -f;
+    if (rot && c == 1) f = -f;
+    out[i] -= f;
+  }
+}
+
+// Per-row sums of squares of real fields [B][2][N][N]: rowsq[b][x] (one warp per (b, x)).
+template <typename R>
+__global__ void k_rowsq(const R* f, double* rowsq, int n) {
+  const int bx = blockIdx.x, b = bx / n, x = bx % n;
+  double s = 0.0;
+  for (int c = 0; c < 2; ++c) {
+    const R* row = f + ((size_t)(b * 2 + c) * n + x) * n;
+    for (int y = threadIdx.x; y < n; y += 32) s += (double)row[y] * (double)row[y];
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) rowsq[bx] = s;
+}
+
+// Deterministic per-batch reduction of row partials: out[b] = scale * sum_x rowsq[b][x].
+static __global__ void k_reduce_rows(const double* rowsq, double* out, int n, int B, double scale) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double s = 0.0;
+  for (int x = 0; x < n; ++x) s += rowsq[(size_t)b * n + x];
+  out[b] = s * scale;
+}
+
+}  // namespace ecs

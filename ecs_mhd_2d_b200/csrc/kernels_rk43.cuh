@@ -1,0 +1,259 @@
+// Adaptive Lawson-RK4(3) ("EARK43") stepper, device resident.
+//
+// Reference: lawson_rk43 (jax_scripts/lib/timestepping.py:151-335).  One
+// attempted step is five column launches (A..E) interleaved with four RHS row
+// launches and one error row launch; the error reduction's last block performs
+// the accept/reject decision and the step-size update on the device, so no host
+// round trip happens per attempt.  Candidates that completed (|s-1| < 1e-10)
+// skip all work, as the reference's lax.cond(complete, identity, do_step) does.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace ecs {
+
+// Per-candidate state slots of the stepper, each a box vector [2][K][M].
+enum Rk43Slot { S_X0 = 0, S_K1, S_XE, S_K1E, S_K2, S_K3, S_X2, S_K4, S_XF, S_K5, S_NSLOT };
+// Trajectory record slots per attempt (primal values needed by tangent/adjoint).
+enum Rk43Rec { R_X0 = 0, R_K1, R_K2, R_K3, R_K4, R_K5, R_NREC };
+
+enum Rk43Stage : int {
+  R43_START = 6,  // no RHS input; inverse transforms of x0
+  R43_INIT = 0,   // RHS of x0 finished: k1 = t v(x0)
+  R43_A = 1,      // start of an attempt: promote accepted state, twiddle, input Y2
+  R43_B = 2,      // k2 finished, input Y3
+  R43_C = 3,      // k3 finished, twiddles, input Y4
+  R43_D = 4,      // k4 finished, xf, input xf
+  R43_E = 5,      // k5 finished, error field d = h (k5 - k4)/6 -> 2 inverse columns
+};
+
+template <typename R>
+struct Col43Params {
+  const cplx<R>* H;     // [B][2][K][N]
+  cplx<R>* G;           // [B][8][K][N]
+  cplx<R>* S;           // [B][S_NSLOT][2][K][M]
+  StepCtl* ctl;         // [B]
+  const cplx<R>* fhat;  // [K][M]
+  const cplx<R>* tw;
+  cplx<R>* rec;         // optional [B][cap][R_NREC][2][K][M]
+  int cap;
+  R nu, eta;
+  int B, stage;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * K) return;
+  const int b = col / K, ky = col - b * K;
+  const StepCtl& c = p.ctl[b];
+  if (c.done) return;
+  const R t = (R)c.t, h = (R)c.h;
+  const int pend = c.pending_accept;
+  cplx<R>* S = p.S + (size_t)b * S_NSLOT * VEC;
+  cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * R_NREC * VEC
+                       : nullptr;
+
+  const bool has_rhs = p.stage != R43_A && p.stage != R43_START;
+  cplx<R> r0[E], r1[E];
+  if (has_rhs) col_load_fwd<R, N>(p.H, b, ky, lane, s_tw, r0, r1);
+  cplx<R> x0[E], x1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    if (slot < 0) continue;
+    const int kx = slot_to_kx(slot, KMAX, M);
+    cplx<R> v[2];
+    v[0] = mk<R>(0, 0); v[1] = mk<R>(0, 0);
+    if (has_rhs) rhs_vals<R>(r0[j], r1[j], kx, ky, p.fhat[ky * M + slot], v[0], v[1]);
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+      const size_t o = ((size_t)ch * K + ky) * M + slot;
+      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
+      const cplx<R> kv = cscale(v[ch], t);                 // mod_vel_fn = t * vel_fn (:243)
+      cplx<R> xin = mk<R>(0, 0);
+      switch (p.stage) {
+        case R43_START: {
+          xin = S[S_X0 * VEC + o];
+        } break;
+        case R43_INIT: {
+          S[S_K1 * VEC + o] = kv;
+        } break;
+        case R43_A: {                                      // :266-270
+          cplx<R> xs = pend ? S[S_XF * VEC + o] : S[S_X0 * VEC + o];
+          cplx<R> ks = pend ? S[S_K5 * VEC + o] : S[S_K1 * VEC + o];
+          if (pend) { S[S_X0 * VEC + o] = xs; S[S_K1 * VEC + o] = ks; }
+          if (rec) { rec[R_X0 * VEC + o] = xs; rec[R_K1 * VEC + o] = ks; }
+          const R e = exp((t * L) * h / R(2));             // e = exp(mod_L * h/2), not masked (:263)
+          const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
+          S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
+          xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
+        } break;
+        case R43_B: {                                      // :270-271
+          S[S_K2 * VEC + o] = kv;
+          if (rec) rec[R_K2 * VEC + o] = kv;
+          xin = cadd(S[S_XE * VEC + o], cscale(cscale(kv, h), R(0.5)));
+        } break;
+        case R43_C: {                                      // :271-280
+          if (rec) rec[R_K3 * VEC + o] = kv;
+          const R e = exp((t * L) * h / R(2));
+          const cplx<R> x2 = cscale(S[S_XE * VEC + o], e);
+          const cplx<R> k1ee = cscale(S[S_K1E * VEC + o], e);
+          const cplx<R> k2e = cscale(S[S_K2 * VEC + o], e);
+          const cplx<R> k3e = cscale(kv, e);
+          S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
+          S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
+          xin = cadd(x2, cscale(k3e, h));
+        } break;
+        case R43_D: {                                      // :280-281
+          S[S_K4 * VEC + o] = kv;
+          if (rec) rec[R_K4 * VEC + o] = kv;
+          cplx<R> acc = cadd(cadd(cadd(cdiv_r(S[S_K1 * VEC + o], R(6)), cdiv_r(S[S_K2 * VEC + o], R(3))),
+                                  cdiv_r(S[S_K3 * VEC + o], R(3))), cdiv_r(kv, R(6)));
+          xin = cadd(S[S_X2 * VEC + o], cscale(acc, h));
+          S[S_XF * VEC + o] = xin;
+        } break;
+        default: {                                         // R43_E: :282, :288
+          S[S_K5 * VEC + o] = kv;
+          if (rec) rec[R_K5 * VEC + o] = kv;
+          xin = cdiv_r(cscale(csub(kv, S[S_K4 * VEC + o]), h), R(6));
+        } break;
+      }
+      if (ch == 0) x0[j] = xin; else x1[j] = xin;
+    }
+  }
+  if (p.stage == R43_INIT) return;
+  if (p.stage == R43_E) col_inverse2<R, N>(x0, x1, p.G, 8, b, ky, lane, s_tw);
+  else col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
+}
+
+// Error norm max|irfft2(d)| of the two channels (timestepping.py:288-291) with
+// the accept/reject decision and h update done by the last block of each
+// candidate (timestepping.py:294-310).
+template <typename R>
+struct RowErrParams {
+  const cplx<R>* G;     // [B][8][K][N], fields 0,1 hold the inverse columns of d
+  StepCtl* ctl;
+  const cplx<R>* tw;
+  double atol;
+  double* rec_h;        // optional [B][cap] attempted step sizes ("hs", :239,:294)
+  int* rec_acc;         // optional [B][cap] accept flags
+  int cap;
+  int B;
+};
+
+__device__ __forceinline__ void rk43_control(StepCtl& c, double atol, double err, double* rec_h, int* rec_acc) {
+  const int a = c.attempts;
+  const bool accept = err < atol;                          // :297 (false for NaN)
+  if (rec_h) rec_h[a] = c.h;                               // :294
+  if (rec_acc) rec_acc[a] = accept ? 1 : 0;
+  if (accept) { c.s = c.s + c.h; c.accepted += 1; c.pending_accept = 1; }
+  else { c.rejected += 1; c.pending_accept = 0; }
+  c.fevals += 4;                                           // :285
+  double hn = isnan(err) ? c.h / 2 : c.h * 0.9 * pow(atol / err, 0.25);   // :300-302
+  const double ov = c.s + hn - 1.0;                        // :304-307 h - relu(s + h - 1)
+  hn = hn - (isnan(ov) ? ov : (ov > 0.0 ? ov : 0.0));
+  c.h = hn;
+  c.err = err;
+  c.attempts = a + 1;
+  c.done = fabs(c.s - 1.0) < 1e-10 ? 1 : 0;                // :313
+}
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  __shared__ double s_max[XT];
+  __shared__ int s_last;
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  StepCtl& c = p.ctl[b];
+  if (c.done) return;
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 2 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  cplx<R> z[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) z[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), lane + 32 * j, w);
+  fft_dif<R, N, true>(z, s_tw, lane);
+  double m = 0.0;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const double a = fabs((double)z[j].x), bb = fabs((double)z[j].y);
+    m = (a > m || isnan(a)) ? a : m;
+    m = (bb > m || isnan(bb)) ? bb : m;
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const double q = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (q > m || isnan(q)) ? q : m;
+  }
+  if (lane == 0) s_max[w] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bm = s_max[0];
+    for (int i = 1; i < XT; ++i) bm = (s_max[i] > bm || isnan(s_max[i])) ? s_max[i] : bm;
+    // non-negative doubles (and NaN with the sign bit clear) order like their bit patterns
+    atomicMax(&c.err_bits, (unsigned long long)__double_as_longlong(fabs(bm)));
+    __threadfence();
+    const unsigned prev = atomicAdd(&c.err_blocks, 1u);
+    s_last = (prev == (unsigned)(tiles - 1));
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    const double err = __longlong_as_double((long long)atomicAdd(&c.err_bits, 0ull));
+    const int a = c.attempts;
+    rk43_control(c, p.atol, err, p.rec_h && a < p.cap ? p.rec_h + (size_t)b * p.cap : nullptr,
+                 p.rec_acc && a < p.cap ? p.rec_acc + (size_t)b * p.cap : nullptr);
+    c.err_bits = 0ull;
+    c.err_blocks = 0u;
+  }
+}
+
+// Initial control state: t = T, h = h0, s = 0 (timestepping.py:255).
+static __global__ void k_rk43_setup(const double* T, double h0, StepCtl* ctl, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  StepCtl c;
+  c.t = T[b]; c.h = h0; c.s = 0.0; c.err = 0.0;
+  c.accepted = 0; c.rejected = 0; c.fevals = 1; c.done = 0;
+  c.pending_accept = 0; c.attempts = 0; c.err_bits = 0ull; c.err_blocks = 0u; c.pad = 0;
+  ctl[b] = c;
+}
+
+// Final state = x carried by the loop: xf if the last attempt was accepted.
+template <typename R>
+__global__ void k_rk43_resolve(cplx<R>* S, const StepCtl* ctl, cplx<R>* out, int n, int B) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const long total = (long)B * VEC;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / VEC);
+    const size_t o = i - (size_t)b * VEC;
+    const cplx<R>* Sb = S + (size_t)b * S_NSLOT * VEC;
+    out[i] = ctl[b].pending_accept ? Sb[S_XF * VEC + o] : Sb[S_X0 * VEC + o];
+  }
+}
+
+static __global__ void k_count_done(const StepCtl* ctl, int* count, int B) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int s = 0;
+    for (int b = 0; b < B; ++b) s += ctl[b].done;
+    *count = s;
+  }
+}
+
+}  // namespace ecs

@@ -1,0 +1,113 @@
+/*
+ * ecs_mhd.h -- C ABI of the B200-native hot path of mgolden30/ECS_MHD_2D.
+ *
+ * All array arguments are DEVICE pointers owned by the caller (e.g. torch
+ * tensors' data_ptr()).  The library never frees caller memory.  Every call is
+ * ordered on the caller's cudaStream_t (passed as void*; NULL = legacy default
+ * stream) and returns an ecs_status; ecs_last_error() gives the message.
+ * A context is not thread-safe: use one context per host thread.
+ *
+ * Layouts (C order, `real` = double for ECS_F64, float for ECS_F32):
+ *   fields   real  [batch][2][n][n]          (omega, j) in real space, x then y
+ *   f_hat    cplx  [batch][2][n][n/2+1]      jnp.fft.rfft2 layout (kx fftfreq, ky >= 0)
+ *   box      cplx  [batch][2][K][M]          dealiased modes only, see ecs_box_dims
+ *   T, sx    double[batch]
+ * Flat vectors follow jax.flatten_util.ravel_pytree order of the reference's
+ * {"T","fields","sx"} dicts: [T, fields(2*n*n), sx].
+ *
+ * Each entry point names the reference function it replaces (paths relative to
+ * the reference project root).
+ */
+#ifndef ECS_MHD_H
+#define ECS_MHD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ecs_ctx ecs_ctx;
+
+enum { ECS_F64 = 0, ECS_F32 = 1 };
+
+enum {
+  ECS_OK = 0,
+  ECS_ERR_INVALID = 1,       /* bad argument */
+  ECS_ERR_CUDA = 2,          /* CUDA runtime error */
+  ECS_ERR_BAD_MODE = 3,      /* unknown integration mode (loss_functions.py:86-88) */
+  ECS_ERR_NOT_COMPLETED = 4, /* adaptive integration hit its step cap (timestepping.py:313,327) */
+  ECS_ERR_OOM = 5,           /* device allocation failed */
+  ECS_ERR_UNSUPPORTED = 6    /* grid size / dtype not built */
+};
+
+/* Integration modes of mismatch_RPO (jax_scripts/lib/loss_functions.py:48-88). */
+enum { ECS_MODE_LAWSON_RK4 = 1, ECS_MODE_LAWSON_RK43 = 2 };
+
+typedef struct {
+  double nu, eta;          /* param_dict["nu"], ["eta"] */
+  double b0x, b0y;         /* param_dict["b0"] mean magnetic field */
+  const double* forcing;   /* HOST real [n][n] forcing on the grid of construct_domain, or NULL */
+  double kolmogorov_amp;   /* used when forcing == NULL: amp * cos(kolmogorov_k * y) */
+  int kolmogorov_k;
+} ecs_params;
+
+typedef struct {
+  int mode;                /* ECS_MODE_* */
+  int num_checkpoints;     /* Lawson_RK4: param_dict["num_checkpoints"] */
+  int ministeps;           /* Lawson_RK4: param_dict["ministeps"] */
+  int shift_reflect_ny;    /* param_dict["shift_reflect_ny"] */
+  int rot;                 /* param_dict["rot"] */
+  double atol;             /* Lawson_RK43: adaptive_dict["atol"] */
+  double h0;               /* Lawson_RK43: initial step (loss_functions.py:77 uses 1e-2) */
+  int max_steps_per_checkpoint; /* Lawson_RK43: adaptive_dict["max_steps_per_checkpoint"] */
+  int checkpoints;         /* Lawson_RK43: adaptive_dict["checkpoints"] */
+} ecs_shoot_cfg;
+
+typedef struct {
+  int completed;           /* |s - 1| < 1e-10 (timestepping.py:313) */
+  double s;
+  int accepted, rejected, fevals;
+} ecs_info;
+
+/* Library version string. */
+const char* ecs_version(void);
+
+/* Context with grid tables and workspace for grids n in {64,128,256}
+ * (replaces mhd_jax.construct_domain, jax_scripts/lib/mhd_jax.py:20-94, and
+ * dictionaryIO.recompute_grid_information, jax_scripts/lib/dictionaryIO.py:64-78).
+ * Uses the current CUDA device. */
+int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ecs_ctx** out);
+int ecs_ctx_destroy(ecs_ctx* ctx);
+const char* ecs_last_error(const ecs_ctx* ctx);
+/* K = ky columns kept, M = kx slots kept by the 2/3 mask (mhd_jax.py:65-70). */
+int ecs_box_dims(const ecs_ctx* ctx, int* K, int* M);
+
+/* rfft2 restricted to the dealiased box (jnp.fft.rfft2 at loss_functions.py:45). */
+int ecs_to_box(ecs_ctx* ctx, const void* fields, void* box, int batch, void* stream);
+/* irfft2 of a box spectrum (jnp.fft.irfft2, e.g. loss_functions.py:107). */
+int ecs_from_box(ecs_ctx* ctx, const void* box, void* fields, int batch, void* stream);
+/* irfft2(mask * rfft2(fields)) (newton.py:211-214, adjoint_descent.py:111-114). */
+int ecs_dealias(ecs_ctx* ctx, const void* fields, void* out, int batch, void* stream);
+
+/* state_vel (jax_scripts/lib/mhd_jax.py:105-175) on the full rfft2 layout. */
+int ecs_state_vel(ecs_ctx* ctx, const void* f_hat, void* dfdt_hat, int batch,
+                  int include_dissipation, void* stream);
+
+/* lawson_rk4 with the mask (jax_scripts/lib/timestepping.py:46-81) on the full
+ * rfft2 layout, in place; L_diag = dissipation(param_dict). */
+int ecs_lawson_rk4(ecs_ctx* ctx, void* f_hat, double t, int steps, int batch, void* stream);
+
+/* objective_RPO (jax_scripts/lib/loss_functions.py:132-148):
+ * out_fields = irfft2(f0 - g.Phi_T(f0)), out_T = pt, out_sx = px (both 0 in value). */
+int ecs_objective(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
+                  const double* sx, void* out_fields, double* out_T, double* out_sx,
+                  ecs_info* info, int batch, void* stream);
+
+/* loss_RPO (jax_scripts/lib/loss_functions.py:99-111): mean(irfft2(f - f0)^2) per batch element. */
+int ecs_loss(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
+             const double* sx, double* loss, ecs_info* info, int batch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ECS_MHD_H */

@@ -1,0 +1,196 @@
+"""Parity of the CUDA path (through the C-ABI) against the CPU oracle.
+
+Tolerances: FP64 results must match the oracle to <= 1e-12 relative L2 after
+64 Lawson-RK4 steps (and to ~1e-13 for single right-hand sides); FP32 results
+to <= 5e-5 relative L2.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import ecs_mhd_2d_b200 as E
+from ecs_mhd_2d_b200.synthetic import initial_condition
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_RHS = 1e-13
+TOL_64 = 1e-12
+TOL_F32 = 5e-5
+
+
+def pds(n, nu=1 / 40, eta=1 / 40, forcing="kolmogorov+", **kw):
+    return (O.make_param_dict(n, nu, eta, forcing=forcing, **kw),
+            E.make_param_dict(n, nu, eta, forcing=forcing, **kw))
+
+
+def box_mask(n):
+    k = np.fft.fftfreq(n, 1 / n)
+    return (np.abs(k)[:, None] < n / 3) & (np.abs(k[: n // 2 + 1])[None, :] < n / 3)
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_box_transforms(cuda, n):
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal((3, 2, n, n))
+    _, pd = pds(n)
+    from ecs_mhd_2d_b200 import context as C
+    ctx = C.get_context(pd, n, torch.float64, 3)
+    ut = torch.as_tensor(u, device="cuda")
+    box = torch.empty(3, 2, ctx.K, ctx.M, dtype=torch.complex128, device="cuda")
+    ctx.call("ecs_to_box", C.ptr(ut), C.ptr(box), 3, C.stream_ptr())
+    ref = np.fft.rfft2(u)
+    kmax = (n - 1) // 3
+    rows = list(range(0, kmax + 1)) + list(range(n - kmax, n))
+    want = ref[:, :, rows, : kmax + 1].transpose(0, 1, 3, 2)
+    got = box.cpu().numpy()
+    assert rel_l2(got, want) < 1e-14
+    back = torch.empty_like(ut)
+    ctx.call("ecs_from_box", C.ptr(box), C.ptr(back), 3, C.stream_ptr())
+    proj = np.fft.irfft2(ref * box_mask(n), s=(n, n))
+    assert rel_l2(back.cpu().numpy(), proj) < 1e-14
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_dealias(cuda, n):
+    u = np.random.default_rng(2).standard_normal((2, n, n))
+    opd, pd = pds(n)
+    got = E.dealias(torch.as_tensor(u, device="cuda"), pd).cpu().numpy()
+    want = np.fft.irfft2(opd["mask"] * np.fft.rfft2(u), s=(n, n))
+    assert rel_l2(got, want) < 1e-14
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("diss", [False, True])
+def test_state_vel(cuda, n, diss):
+    rng = np.random.default_rng(3)
+    u = initial_condition(5, n) + 0.01 * rng.standard_normal((2, n, n))   # aliased modes nonzero too
+    opd, pd = pds(n)
+    f = np.fft.rfft2(u)
+    want = O.state_vel(f, opd, diss)
+    got = E.state_vel(torch.as_tensor(f, device="cuda"), pd, diss).cpu().numpy()
+    assert rel_l2(got, want) < TOL_RHS
+
+
+def test_state_vel_golden(cuda):
+    g = np.load("tests/golden/synthetic_n64.npz")
+    _, pd = pds(64)
+    f = torch.as_tensor(np.fft.rfft2(g["u0"]), device="cuda")
+    assert rel_l2(E.state_vel(f, pd, False).cpu().numpy(), g["state_vel"]) < TOL_RHS
+    assert rel_l2(E.state_vel(f, pd, True).cpu().numpy(), g["state_vel_diss"]) < TOL_RHS
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_lawson_rk4_64_steps(cuda, n):
+    u0 = initial_condition(0, n)
+    opd, pd = pds(n)
+    f0 = np.fft.rfft2(u0)
+    v_fn = lambda f: O.state_vel(f, opd, False)
+    want = O.lawson_rk4(f0, 64 * 0.005, 64, v_fn, O.dissipation(opd), mask=opd["mask"])
+    got = E.lawson_rk4(torch.as_tensor(f0, device="cuda"), 64 * 0.005, 64, pd).cpu().numpy()
+    assert rel_l2(np.fft.irfft2(got, s=(n, n)), np.fft.irfft2(want, s=(n, n))) < TOL_64
+
+
+def test_lawson_rk4_golden(cuda):
+    g = np.load("tests/golden/synthetic_n64.npz")
+    _, pd = pds(64)
+    f = torch.as_tensor(np.fft.rfft2(g["u0"]), device="cuda")
+    got = E.lawson_rk4(f, 64 * 0.005, 64, pd).cpu().numpy()
+    assert rel_l2(np.fft.irfft2(got, s=(64, 64)), g["rk4_64"]) < TOL_64
+
+
+def test_lawson_rk4_fp32(cuda):
+    n = 128
+    u0 = initial_condition(0, n)
+    opd, _ = pds(n)
+    pd32 = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", data_type=torch.float32)
+    f0 = np.fft.rfft2(u0)
+    v_fn = lambda f: O.state_vel(f, opd, False)
+    want = O.lawson_rk4(f0, 64 * 0.005, 64, v_fn, O.dissipation(opd), mask=opd["mask"])
+    got = E.lawson_rk4(torch.as_tensor(f0.astype(np.complex64), device="cuda"), 64 * 0.005, 64, pd32)
+    assert rel_l2(np.fft.irfft2(got.cpu().numpy().astype(np.complex128), s=(n, n)),
+                  np.fft.irfft2(want, s=(n, n))) < TOL_F32
+
+
+@pytest.mark.parametrize("ny,rot", [(0, False), (1, True), (6, True), (3, False)])
+def test_objective_and_loss(cuda, ny, rot):
+    n = 64
+    u0 = initial_condition(1, n)
+    kw = dict(num_checkpoints=2, ministeps=32, shift_reflect_ny=ny, rot=rot)
+    opd, pd = pds(n, **kw)
+    inp = {"fields": u0, "T": 0.32, "sx": 0.7}
+    want = O.objective_RPO(inp, opd, "Lawson_RK4")
+    got = E.objective_RPO({"fields": torch.as_tensor(u0, device="cuda"), "T": 0.32, "sx": 0.7}, pd, "Lawson_RK4")
+    assert rel_l2(got["fields"].cpu().numpy(), want["fields"]) < TOL_64
+    assert float(got["T"]) == 0.0 and float(got["sx"]) == 0.0
+    wl, _ = O.loss_RPO(inp, opd, "Lawson_RK4")
+    gl, info = E.loss_RPO({"fields": torch.as_tensor(u0, device="cuda"), "T": 0.32, "sx": 0.7}, pd, "Lawson_RK4")
+    assert abs(float(gl) - float(wl)) <= TOL_64 * abs(float(wl))
+
+
+def test_objective_golden(cuda):
+    g = np.load("tests/golden/synthetic_n64.npz")
+    _, pd = pds(64, num_checkpoints=2, ministeps=32, shift_reflect_ny=1, rot=True)
+    inp = {"fields": torch.as_tensor(g["u0"], device="cuda"), "T": 0.32, "sx": 0.3}
+    got = E.objective_RPO(inp, pd, "Lawson_RK4")
+    assert rel_l2(got["fields"].cpu().numpy(), g["objective"]) < TOL_64
+    gl, _ = E.loss_RPO(inp, pd, "Lawson_RK4")
+    assert abs(float(gl) - float(g["loss"])) <= TOL_64 * float(g["loss"])
+
+
+def test_batch_equals_single(cuda):
+    n = 64
+    us = np.stack([initial_condition(s, n) for s in range(3)])
+    _, pd = pds(n, num_checkpoints=1, ministeps=16, shift_reflect_ny=1, rot=False)
+    T = torch.tensor([0.1, 0.2, 0.15], dtype=torch.float64)
+    sx = torch.tensor([0.0, 0.5, -1.0], dtype=torch.float64)
+    batch = E.objective_RPO({"fields": torch.as_tensor(us, device="cuda"), "T": T, "sx": sx}, pd, "Lawson_RK4")
+    for b in range(3):
+        one = E.objective_RPO({"fields": torch.as_tensor(us[b], device="cuda"), "T": float(T[b]),
+                               "sx": float(sx[b])}, pd, "Lawson_RK4")
+        assert torch.equal(one["fields"], batch["fields"][b])
+
+
+@pytest.mark.parametrize("name", ["Re40_RPO6", "Re40_RPO5"])
+def test_reference_solution_closes(cuda, name):
+    d = np.load(f"tests/golden/solution_{name}.npz")
+    n = d["fields"].shape[-1]
+    pd = E.make_param_dict(n, float(d["nu"]), float(d["eta"]), b0=d["b0"], forcing="kolmogorov",
+                           num_checkpoints=int(d["num_checkpoints"]), ministeps=int(d["ministeps"]),
+                           shift_reflect_ny=int(d["shift_reflect_ny"]), rot=bool(d["rot"]))
+    out = E.objective_RPO({"fields": torch.as_tensor(d["fields"], device="cuda"), "T": float(d["T"]),
+                           "sx": float(d["sx"])}, pd, "Lawson_RK4")
+    r = float(torch.linalg.norm(out["fields"]) / np.linalg.norm(d["fields"]))
+    # the oracle closes these to d["closure"]; the GPU path must agree to the 1e-12 budget
+    assert r < float(d["closure"]) + 1e-12, (r, float(d["closure"]))
+
+
+@pytest.mark.parametrize("ny,rot,dealiased", [(0, False, True), (1, True, True), (3, True, False)])
+def test_objective_rk43(cuda, ny, rot, dealiased):
+    n = 64
+    u0 = initial_condition(2, n)
+    if not dealiased:   # aliased modes are carried unchanged by the unmasked integrating factor
+        u0 = u0 + 1e-3 * np.random.default_rng(9).standard_normal(u0.shape)
+    ad = {"atol": 1e-6, "checkpoints": 8, "max_steps_per_checkpoint": 32}
+    kw = dict(shift_reflect_ny=ny, rot=rot, adaptive_dict=ad)
+    opd, pd = pds(n, **kw)
+    inp = {"fields": u0, "T": 0.5, "sx": 0.4}
+    want = O.objective_RPO(inp, opd, "Lawson_RK43")
+    f0, fT, oinfo = O.mismatch_RPO(inp, opd, "Lawson_RK43")
+    got = E.objective_RPO({"fields": torch.as_tensor(u0, device="cuda"), "T": 0.5, "sx": 0.4}, pd, "Lawson_RK43")
+    assert rel_l2(got["fields"].cpu().numpy(), want["fields"]) < TOL_64
+    gl, info = E.loss_RPO({"fields": torch.as_tensor(u0, device="cuda"), "T": 0.5, "sx": 0.4}, pd, "Lawson_RK43")
+    wl, _ = O.loss_RPO(inp, opd, "Lawson_RK43")
+    assert abs(float(gl) - float(wl)) <= TOL_64 * abs(float(wl))
+    assert info["completed"] and oinfo["completed"]
+    assert (info["accepted"], info["rejected"], info["fevals"]) == (oinfo["accepted"], oinfo["rejected"], oinfo["fevals"])
+
+
+def test_rk43_not_completed_reports_info(cuda):
+    n = 64
+    u0 = initial_condition(3, n)
+    ad = {"atol": 1e-10, "checkpoints": 1, "max_steps_per_checkpoint": 4}   # cap too small on purpose
+    _, pd = pds(n, adaptive_dict=ad)
+    gl, info = E.loss_RPO({"fields": torch.as_tensor(u0, device="cuda"), "T": 1.0, "sx": 0.0}, pd, "Lawson_RK43")
+    assert not info["completed"] and info["accepted"] + info["rejected"] == 4 and info["s"] < 1.0
