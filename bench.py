@@ -1,0 +1,329 @@
+"""Headline benchmark: Newton-GMRES matvec batch at 128^2 in FP64.
+
+Workload (one bench step): linearise objective_RPO of mgolden30/ECS_MHD_2D in
+Lawson_RK43 mode at a seeded base point (n=128, Re=Rm=50, Kolmogorov forcing
++4cos(4y), b0=[0,0.1], T=4.6, sx=0.12, atol=1e-8, cap 64x64 attempts) and push a
+batch of 64 seeded unit-norm tangents [T, fields, sx] through the hand-written
+tangent kernels: 64 JVP matvecs (jax_scripts/newton.py:165; jax.jvp at
+jax_scripts/lib/utils.py:108).  The primal adaptive solve with its trajectory
+record is inside every timed step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU
+(no data-path collective; weak scaling); the step time is the max over ranks.
+`--impl reference` times the reference algorithm's CPU restatement (the oracle,
+torch-CPU forward-mode AD as jax.jvp) on the host cores for a bounded sample of
+the same workload; only rank 0 runs it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 128
+BATCH = 64
+RE = 50.0
+T0, SX0 = 4.6, 0.12
+ATOL = 1e-8
+CAP = (64, 64)
+IC_SEED, IC_AMP = 0, 2.0
+METRIC = "GMRES matvecs/s (JVP of objective_RPO, Lawson_RK43 atol 1e-8, T=4.6) at 128^2 FP64"
+UNIT = "matvec/s"
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "newton_gmres_matvec_batch", "n": N, "dtype": "f64", "Re": RE, "forcing": "+4cos(4y)",
+           "b0": [0.0, 0.1], "T": T0, "sx": SX0, "mode": "Lawson_RK43", "atol": ATOL,
+           "checkpoints_x_max_steps": list(CAP), "tangents_per_step": BATCH, "ic": f"seed {IC_SEED}, amp {IC_AMP}",
+           "l2": "flushed (256 MiB write) between timed steps", "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def param_dict(E):
+    ad = {"atol": ATOL, "checkpoints": CAP[0], "max_steps_per_checkpoint": CAP[1]}
+    return E.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", shift_reflect_ny=0, rot=False,
+                             adaptive_dict=ad)
+
+
+def host_inputs(seed):
+    from ecs_mhd_2d_b200.synthetic import initial_condition, unit_tangents
+    u0 = initial_condition(IC_SEED + seed, N, amp=IC_AMP)
+    tv = unit_tangents(seed, N, BATCH)
+    return u0, tv
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.samples, self._stop, self._t = index, [], threading.Event(), None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(target_s=12.0, attempts_full=None):
+    """The oracle (torch-CPU restatement, torch.func.jvp) on the host cores for a
+    bounded sample: the first k attempts of the same adaptive JVP, scaled to one
+    full matvec by the attempt count of the full solve."""
+    import torch
+    from torch.func import jvp
+    import oracle as O
+    torch.set_num_threads(os.cpu_count() or 1)
+    u0, tv = host_inputs(0)
+
+    def run(cap):
+        ad = {"atol": ATOL, "checkpoints": 1, "max_steps_per_checkpoint": cap}
+        pdt = O.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", xp=O.TORCH, shift_reflect_ny=0,
+                                rot=False, adaptive_dict=ad)
+        prim = {"fields": torch.from_numpy(u0), "T": torch.tensor(T0, dtype=torch.float64),
+                "sx": torch.tensor(SX0, dtype=torch.float64)}
+        tan = {"fields": torch.from_numpy(tv[0, 1:-1].reshape(2, N, N)), "T": torch.tensor(tv[0, 0]),
+               "sx": torch.tensor(tv[0, -1])}
+        f = lambda d: O.objective_RPO(d, pdt, "Lawson_RK43", xp=O.TORCH)
+        t0 = time.perf_counter()
+        jvp(f, (prim,), (tan,))
+        return time.perf_counter() - t0
+
+    run(4)                                   # warm-up of the CPU FFT plans
+    t_small = run(10)
+    per = t_small / 10
+    k = int(max(10, min(400, target_s / max(per, 1e-6))))
+    t = run(k)
+    per = t / k
+    full = attempts_full or 1
+    return {"value": 1.0 / (per * full), "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"first {k} attempts of one JVP (1 tangent) of the same workload, {t:.1f} s; "
+                      f"scaled by {full} attempts per full matvec; restated oracle on CPU (torch.func.jvp), not JAX"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    ref_attempts = 1988   # attempts of this workload's adaptive solve (accepted + rejected), see DESIGN.md
+    cb = cpu_baseline(attempts_full=ref_attempts)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": BATCH / cb["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded initial condition and tangents)", "config": workload_config(),
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--T", type=float, default=None, help="profiling only: shorter horizon (small ncu case)")
+    ap.add_argument("--cap", type=int, nargs=2, default=None, help="profiling only: checkpoints max_steps")
+    args = ap.parse_args()
+    global T0, CAP
+    if args.T is not None:
+        T0 = args.T
+    if args.cap is not None:
+        CAP = tuple(args.cap)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import ecs_mhd_2d_b200 as E
+    from ecs_mhd_2d_b200 import build as _build, context as C
+    _build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    pd = param_dict(E)
+    u0h, tvh = host_inputs(rank)
+    dev = torch.device("cuda", local)
+    prim = {"fields": torch.as_tensor(u0h, device=dev), "T": T0, "sx": SX0}
+    tan = {"fields": torch.as_tensor(tvh[:, 1:-1].reshape(BATCH, 2, N, N), device=dev).contiguous(),
+           "T": torch.as_tensor(tvh[:, 0]), "sx": torch.as_tensor(tvh[:, -1])}
+    obj = E.Objective(pd, "Lawson_RK43")
+
+    def step():
+        obj.linearize(prim, force=True, batch=BATCH)
+        return obj.jvp(prim, tan)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    info = dict(obj.last_info)
+    ctx = obj._ctx
+    lib = ctx.lib
+    n_launch0 = lib.ecs_launch_count(ctx.handle)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    launches = lib.ecs_launch_count(ctx.handle) - n_launch0
+    t_total = sum(times)
+    if world > 1:
+        t = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t)
+    ms_per_step = t_total / args.steps
+    value = world * BATCH * args.steps / (t_total / 1e3)
+
+    # end to end through the public API from pinned host buffers
+    u0_pin = torch.as_tensor(u0h).pin_memory()
+    tf_pin = torch.as_tensor(tvh[:, 1:-1].reshape(BATCH, 2, N, N)).contiguous().pin_memory()
+    tT_pin, tsx_pin = torch.as_tensor(tvh[:, 0]).pin_memory(), torch.as_tensor(tvh[:, -1]).pin_memory()
+    out_pin = torch.empty((BATCH, 2, N, N), dtype=torch.float64).pin_memory()
+    oT_pin = torch.empty(BATCH, dtype=torch.float64).pin_memory()
+    h2d = u0_pin.numel() * 8 + tf_pin.numel() * 8 + 2 * BATCH * 8 + 16
+    d2h = out_pin.numel() * 8 + 2 * BATCH * 8
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        p = {"fields": u0_pin.to(dev, non_blocking=True), "T": T0, "sx": SX0}
+        tg = {"fields": tf_pin.to(dev, non_blocking=True), "T": tT_pin.to(dev, non_blocking=True),
+              "sx": tsx_pin.to(dev, non_blocking=True)}
+        obj.linearize(p, force=True, batch=BATCH)
+        o = obj.jvp(p, tg)
+        out_pin.copy_(o["fields"], non_blocking=True)
+        oT_pin.copy_(o["T"], non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    te = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([te], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t)
+    e2e_value = world * BATCH * args.steps / (te / 1e3)
+
+    # roofline of the dominant kernel, timed live on this stream
+    step()
+    torch.cuda.synchronize()
+    import ctypes
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kern = []
+    for which, name in ((0, "k_row_tan"), (1, "k_col_tan")):
+        ms, by = ctypes.c_float(), ctypes.c_double()
+        ctx.call("ecs_bench_kernel", which, BATCH, 20, ctypes.byref(ms), ctypes.byref(by), C.stream_ptr())
+        kern.append((name, ms.value, by.value))
+    acc = info.get("accepted", 0)
+    # launches per step: 4 row + 5 column tangent kernels per accepted attempt
+    shares = {name: ms * (4 if name == "k_row_tan" else 5) * acc for name, ms, _ in kern}
+    dom = max(kern, key=lambda k: shares[k[0]])
+    achieved = dom[2] / (dom[1] / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(dom[0])
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": dom[2], "ms_per_launch": dom[1],
+                "kernel_ms": {k[0]: k[1] for k in kern},
+                "share_of_step_est": {k: v / ms_per_step for k, v in shares.items()}}
+
+    if rank == 0:
+        clocks = clk.summary()
+        cb = None
+        if not args.no_cpu_baseline:
+            try:
+                cb = cpu_baseline(attempts_full=info.get("accepted", 0) + info.get("rejected", 0))
+            except Exception as ex:  # the oracle is test infrastructure; report why it is missing
+                cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+        extra = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
+                 "tangent_rk_steps_per_s": value * info.get("accepted", 0)}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial condition and tangents)",
+                "config": workload_config(extra),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline, "cpu_baseline": cb}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

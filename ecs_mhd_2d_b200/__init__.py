@@ -10,5 +10,7 @@ from .mhd import construct_domain, dissipation, make_param_dict, state_vel  # no
 from .timestepping import lawson_rk4  # noqa: F401
 from .loss_functions import objective_RPO, loss_RPO, dealias  # noqa: F401
 from .synthetic import initial_condition, unit_tangents  # noqa: F401
+from .autodiff import (Objective, compile_objective_and_Jacobian, vjp, loss_and_grad,  # noqa: F401
+                       loss_rpo_autograd)
 
 __version__ = "0.1.0"

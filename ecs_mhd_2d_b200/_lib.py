@@ -58,6 +58,8 @@ SIGNATURES = {
     "ecs_ctx_create": (_I, [_I, _I, ctypes.POINTER(EcsParams), _I, ctypes.POINTER(_VP)]),
     "ecs_ctx_destroy": (_I, [_VP]),
     "ecs_last_error": (ctypes.c_char_p, [_VP]),
+    "ecs_launch_count": (ctypes.c_longlong, [_VP]),
+    "ecs_bench_kernel": (_I, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), _VP]),
     "ecs_box_dims": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ecs_to_box": (_I, [_VP, _VP, _VP, _I, _VP]),
     "ecs_from_box": (_I, [_VP, _VP, _VP, _I, _VP]),
@@ -68,6 +70,9 @@ SIGNATURES = {
                            ctypes.POINTER(EcsInfo), _I, _VP]),
     "ecs_loss": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP,
                       ctypes.POINTER(EcsInfo), _I, _VP]),
+    "ecs_linearize": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, ctypes.POINTER(EcsInfo), _VP]),
+    "ecs_jvp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
+    "ecs_vjp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
 }
 
 _lib = None

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "../../include/ecs_mhd.h"
 
 struct ecs_ctx {
   int n = 0, dtype = 0, max_batch = 0;
@@ -32,6 +33,29 @@ struct ecs_ctx {
   double* rowsq = nullptr;
   double* Tbuf = nullptr;
   std::vector<void*> allocs;
+  long long launches = 0;           // kernels launched through this context
+  // linearisation (primal trajectory record) shared by JVP / VJP calls
+  struct Lin {
+    int valid = 0, mode = 0;
+    ecs_shoot_cfg cfg{};
+    double T = 0, sx = 0, h = 0;
+    long nrec = 0;                  // Lawson-RK4: steps; Lawson-RK4(3): attempts
+    std::vector<int> acc;           // Lawson-RK4(3) accept flags
+    std::vector<double> hs;         // Lawson-RK4(3) attempted step sizes
+    void* rec = nullptr; size_t rec_bytes = 0;
+    void* phi = nullptr;            // final primal box state
+    void* f0box = nullptr;          // box(rfft2(fields))
+    void* vt = nullptr;             // irfft2(state_vel(f0, dissipation)) [2][N][N]
+    void* vx = nullptr;             // irfft2(i kx f0)                    [2][N][N]
+    double* dsx = nullptr;          // primal sx on the device
+    double* dT = nullptr;           // primal T on the device
+    double* rec_h = nullptr; int* rec_acc = nullptr; size_t cap = 0;
+  } lin;
+  // tangent / adjoint workspace (grown on demand)
+  void* D = nullptr; size_t D_bytes = 0;          // tangent or adjoint slots
+  void* Greg = nullptr; void* Phys = nullptr; size_t reg_items = 0;   // regenerated primal fields
+  long* items = nullptr; size_t items_cap = 0;
+  double* hacc = nullptr; size_t hacc_bytes = 0;   // adjoint dL/dh accumulators [B][K]
   std::string err;
 };
 
@@ -46,6 +70,8 @@ template <int N> struct Geomc {
 int set_err(ecs_ctx* c, int code, const std::string& msg);
 int cuda_err(ecs_ctx* c, cudaError_t e, const char* where);
 void* dev_alloc(ecs_ctx* c, size_t bytes, int* st);
+// (re)allocate a growable device buffer owned by the context (not in allocs)
+int grow(ecs_ctx* c, void** p, size_t* have, size_t need);
 
 static __global__ void k_fill(double* p, double v, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;

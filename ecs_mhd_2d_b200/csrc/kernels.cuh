@@ -137,6 +137,10 @@ __device__ __forceinline__ void col_inverse2(const cplx<R> (&x0)[N / 32], const 
 // (reference: timestepping.lawson_rk4, jax_scripts/lib/timestepping.py:69-80).
 // ---------------------------------------------------------------------------
 
+// Lawson-RK4 record per step (box vectors): stage input X1 = F, stage
+// derivatives k1..k4 (before twiddles) and stage inputs X2..X4.
+enum Rk4Rec { Q_F = 0, Q_K1, Q_K2, Q_K3, Q_K4, Q_X2, Q_X3, Q_X4, Q_NREC };
+
 enum ColStage : int {
   COL_START = 0,     // no RHS input; stage input = F (start of a step)
   COL_RK4_S1 = 1,    // finish k1, stage input X2
@@ -163,6 +167,8 @@ struct ColParams {
   int stage;
   int produce;           // write G for the stage input
   int diss;              // COL_PLAIN: add L f (f = F)
+  cplx<R>* rec;          // optional record of this step: [Q_NREC][2][K][M] per batch element
+  long rec_bstride;      // elements between batch elements in rec
 };
 
 template <typename R, int N>
@@ -204,6 +210,12 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
       v1 = cscale(r1[j], ksq_masked<R>(kx, ky));                // k^2 mask * rfft2(u x B)
     }
     const size_t i0 = base0 + slot, i1 = base1 + slot;
+    cplx<R>* rb = p.rec ? p.rec + (size_t)b * p.rec_bstride : nullptr;
+    const size_t VEC = (size_t)2 * K * M;
+    const size_t o0 = (size_t)ky * M + slot, o1 = (size_t)(K + ky) * M + slot;
+    auto put = [&](int q, cplx<R> a0, cplx<R> a1) {
+      if (rb) { rb[q * VEC + o0] = a0; rb[q * VEC + o1] = a1; }
+    };
     switch (p.stage) {
       case COL_START: {
         x0[j] = p.F[i0]; x1[j] = p.F[i1];
@@ -211,30 +223,38 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
       case COL_RK4_S1: {   // k1 = h v(f); f = e f; k1 = e k1; X2 = f + k1/2
         const R e0 = p.Etab[i0], e1 = p.Etab[i1];
         cplx<R> k10 = cscale(v0, h), k11 = cscale(v1, h);
+        put(Q_F, p.F[i0], p.F[i1]);
+        put(Q_K1, k10, k11);
         cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
         k10 = cscale(k10, e0); k11 = cscale(k11, e1);
         p.F[i0] = f0; p.F[i1] = f1; p.A1[i0] = k10; p.A1[i1] = k11;
         x0[j] = cadd(f0, cscale(k10, R(0.5))); x1[j] = cadd(f1, cscale(k11, R(0.5)));
+        put(Q_X2, x0[j], x1[j]);
       } break;
       case COL_RK4_S2: {   // k2 = h v(X2); X3 = f + k2/2
         cplx<R> k20 = cscale(v0, h), k21 = cscale(v1, h);
         p.K2[i0] = k20; p.K2[i1] = k21;
         x0[j] = cadd(p.F[i0], cscale(k20, R(0.5))); x1[j] = cadd(p.F[i1], cscale(k21, R(0.5)));
+        put(Q_K2, k20, k21);
+        put(Q_X3, x0[j], x1[j]);
       } break;
       case COL_RK4_S3: {   // k3; f,k1,k2,k3 *= e; X4 = f + k3; acc = f + k1/6 + k2/3 + k3/3
         const R e0 = p.Etab[i0], e1 = p.Etab[i1];
         cplx<R> k30 = cscale(v0, h), k31 = cscale(v1, h);
+        put(Q_K3, k30, k31);
         cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
         cplx<R> a0 = cscale(p.A1[i0], e0), a1 = cscale(p.A1[i1], e1);
         cplx<R> c0 = cscale(p.K2[i0], e0), c1 = cscale(p.K2[i1], e1);
         k30 = cscale(k30, e0); k31 = cscale(k31, e1);
         x0[j] = cadd(f0, k30); x1[j] = cadd(f1, k31);
+        put(Q_X4, x0[j], x1[j]);
         cplx<R> s0 = cadd(cadd(cadd(f0, cdiv_r(a0, R(6))), cdiv_r(c0, R(3))), cdiv_r(k30, R(3)));
         cplx<R> s1 = cadd(cadd(cadd(f1, cdiv_r(a1, R(6))), cdiv_r(c1, R(3))), cdiv_r(k31, R(3)));
         p.F[i0] = s0; p.F[i1] = s1;
       } break;
       case COL_RK4_S4: {   // k4; f = acc + k4/6
         cplx<R> k40 = cscale(v0, h), k41 = cscale(v1, h);
+        put(Q_K4, k40, k41);
         cplx<R> f0 = cadd(p.F[i0], cdiv_r(k40, R(6))), f1 = cadd(p.F[i1], cdiv_r(k41, R(6)));
         p.F[i0] = f0; p.F[i1] = f1;
         x0[j] = f0; x1[j] = f1;
@@ -517,6 +537,7 @@ struct ColFromBoxParams {
   cplx<R>* G;         // [B][2][K][N]
   const cplx<R>* tw;
   const double* sx;   // [B] or null
+  int sx_shared;      // sx[0] applies to every batch element
   double sy;
   int odd, rot, use_sym;
   int mult_ikx;       // multiply by i kx (masked) before the inverse
@@ -535,7 +556,7 @@ __global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
   if (col >= p.B * 2 * K) return;   // col = (b*2 + c)*K + ky
   const int ky = col % K, bc = col / K, c = bc & 1, b = bc >> 1;
   const cplx<R>* vin = p.V + (size_t)col * M;
-  SymOp so; so.sx = p.sx ? p.sx[b] : 0.0; so.sy = p.sy; so.odd = p.odd; so.rot = p.rot;
+  SymOp so; so.sx = p.sx ? p.sx[p.sx_shared ? 0 : b] : 0.0; so.sy = p.sy; so.odd = p.odd; so.rot = p.rot;
   const R inv_n2 = R(1) / (R(N) * R(N));
   cplx<R> v[E];
 #pragma unroll
@@ -565,6 +586,7 @@ __global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
 // Row c2r of the two channels G2[B][2][K][N] -> real fields.
 //   mode 0: out = u
 //   mode 1: out = base - u   (objective residual irfft2(f0 - f) with irfft2(f0) = base)
+//   mode 2: out = base + u
 // Optionally accumulates per-row sums of out^2 (loss) into rowsq[B][N].
 template <typename R>
 struct RowFromBoxParams {
@@ -607,6 +629,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_from_box(RowFromBoxParams<R> p)
     const int y = lane + 32 * j;
     R a = z[j].x, c = z[j].y;
     if (p.mode == 1) { a = b0[y] - a; c = b1[y] - c; }
+    else if (p.mode == 2) { a = b0[y] + a; c = b1[y] + c; }
     o0[y] = a; o1[y] = c;
     sq += (double)a * (double)a + (double)c * (double)c;
   }
@@ -696,6 +719,11 @@ __global__ void k_rowsq(const R* f, double* rowsq, int n) {
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if (threadIdx.x == 0) rowsq[bx] = s;
+}
+
+template <typename R>
+__global__ void k_axpy(R* y, const R* x, R a, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 
 // Deterministic per-batch reduction of row partials: out[b] = scale * sum_x rowsq[b][x].

@@ -1,0 +1,432 @@
+// Adjoint (reverse-mode) kernels of the shooting map: the VJP used by
+// adjoint descent (reference: jax.value_and_grad of loss_RPO,
+// jax_scripts/adjoint_descent.py:90-91) and as the transpose preconditioner
+// of Newton-GMRES (jax.vjp of objective_RPO, jax_scripts/newton.py:168-170).
+//
+// Inner products: box vectors use <X, Y> = Re sum conj(X) Y, real fields the
+// Euclidean dot.  With these, the transposes of the box transforms are
+//   to_box^T(Y)   = n^2 irfft2(Y / c_ky)        (c_ky = 1 for ky = 0, else 2)
+//   from_box^T(w) = (c_ky / n^2) rfft2(w)
+// so one adjoint right-hand side is again a column pass and a row pass:
+//   lambda -> P1bar = Re sum mask lambda_w e^{ik.x},  P2bar = Re sum k^2 mask lambda_j e^{ik.x}
+//   -> product adjoints with the primal fields -> 8 forward transforms
+//   -> Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_mc).
+#pragma once
+
+#include "kernels.cuh"
+#include "kernels_rk43.cuh"
+#include "kernels_tan.cuh"
+
+namespace ecs {
+
+// ---------------------------------------------------------------------------
+// Adjoint row pass
+// ---------------------------------------------------------------------------
+template <typename R>
+struct RowAdjParams {
+  const cplx<R>* G;     // [B][8][K][N]: fields 0,1 hold the inverse columns of (mask lam_w, k^2 mask lam_j)/c
+  cplx<R>* H;           // [B][8][K][N]: rfft2 rows of the 8 adjoint fields
+  const R* phys;        // primal physical fields of this stage [N][8][N]
+  const cplx<R>* tw;
+  int B;
+};
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_H = s_G + 2 * K * (XT + 1);
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 2 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  const R* ph = p.phys + ((size_t)x * 8) * N;
+  cplx<R> P[E];   // (P1bar, P2bar) in position order
+#pragma unroll
+  for (int j = 0; j < E; ++j) P[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), lane + 32 * j, w);
+  fft_dif<R, N, true>(P, s_tw, lane);
+  // primal fields: 0 fx0 1 fy0 2 fu0 3 fv0 4 fx1 5 fy1 6 fu1 7 fv1 (fu1, fv1 with b0)
+  // P1 = -(fu0 fx0 + fv0 fy0) + (fu1 fx1 + fv1 fy1),  P2 = fu0 fv1 - fv0 fu1   (mhd_jax.py:152-163)
+#pragma unroll
+  for (int pr = 0; pr < 4; ++pr) {
+    cplx<R> z[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = lane + 32 * j;
+      const R p1 = P[j].x, p2 = P[j].y;
+      R a, c;
+      if (pr == 0) {          // (fx0bar, fy0bar)
+        a = -ph[2 * N + e] * p1; c = -ph[3 * N + e] * p1;
+      } else if (pr == 1) {   // (fu0bar, fv0bar)
+        a = -ph[0 * N + e] * p1 + ph[7 * N + e] * p2;
+        c = -ph[1 * N + e] * p1 - ph[6 * N + e] * p2;
+      } else if (pr == 2) {   // (fx1bar, fy1bar)
+        a = ph[6 * N + e] * p1; c = ph[7 * N + e] * p1;
+      } else {                // (fu1bar, fv1bar)
+        a = ph[4 * N + e] * p1 - ph[3 * N + e] * p2;
+        c = ph[5 * N + e] * p1 + ph[2 * N + e] * p2;
+      }
+      z[j] = mk<R>(a, c);
+    }
+    fft_dit<R, N, false>(z, s_tw, lane);
+    split_store<R, N, XT>(z, s_H + (2 * pr) * K * (XT + 1), s_H + (2 * pr + 1) * K * (XT + 1), w, lane);
+  }
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * 8 * K * N, s_H, 8 * K, x0);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint column pass
+// ---------------------------------------------------------------------------
+enum AdjStage : int {
+  AJ_PRE = 0,                        // Lawson-RK4: seed the step adjoint from obar
+  AJ_S4 = 4, AJ_S3 = 3, AJ_S2 = 2, AJ_S1 = 1,
+  AJ43_INIT = 10,                    // Lawson-RK4(3): adjoint of the initial k1 = t v(x0)
+  AJ43_PRE = 11,                     // seed an accepted attempt from (xbar_f, k5bar)
+  AJ43_S5 = 15, AJ43_S4 = 14, AJ43_S3 = 13, AJ43_S2 = 12,
+  AJ43_IPRE = 16,                    // seed the adjoint RHS of the initial k1
+};
+// Adjoint slots. Lawson-RK4: OB (obar / fbar), F2, A1, K2, B3.
+enum AdjSlot4 { J_OB = 0, J_F2, J_A1, J_K2, J_B3, J_NS4 };
+// Lawson-RK4(3): X0 (x0bar carried), K1 (k1bar carried), XF, X2, XB, K1P (k1'bar), K2, K3P (k3'bar), K2P (k2'bar), K1PP
+enum AdjSlot43 { JJ_X0 = 0, JJ_K1, JJ_X2, JJ_XB, JJ_K1P, JJ_K1PP, JJ_K2, JJ_K2P, JJ_K3P, JJ_NS43 };
+
+template <typename R>
+struct ColAdjParams {
+  const cplx<R>* H;     // [B][8][K][N]
+  cplx<R>* G;           // [B][8][K][N] (fields 0,1 written)
+  cplx<R>* J;           // adjoint slots [B][nslot][2][K][M]
+  int nslot;
+  const cplx<R>* rec;   // primal record of this step / attempt
+  const cplx<R>* rec_prev;   // Lawson-RK4 AJ_S1: record of the previous step (null at the first step)
+  double* hacc;         // [B][K] accumulators of dL/dh (RK4) or dL/dt (RK4(3))
+  double t, h;
+  const cplx<R>* tw;
+  R nu, eta;
+  int B, stage;
+};
+
+__device__ __forceinline__ double rdot2(double ax, double ay, double bx, double by) { return ax * bx + ay * by; }
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * K) return;
+  const int b = col / K, ky = col - b * K;
+  cplx<R>* J = p.J + (size_t)b * p.nslot * VEC;
+  const cplx<R>* Q = p.rec;
+  const R h = (R)p.h, t = (R)p.t;
+  const bool rk43 = p.stage >= AJ43_INIT;
+  const bool has_rhs = !(p.stage == AJ_PRE || p.stage == AJ43_PRE || p.stage == AJ43_IPRE);
+  const R cky = ky == 0 ? R(1) : R(2);
+  const R inv_n2 = R(1) / (R(N) * R(N));
+
+  // Xbar_c = (c/n^2) sum_m (-i mu_m) rfft2(fbar_mc)
+  cplx<R> xb0[E], xb1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) { xb0[j] = mk<R>(0, 0); xb1[j] = mk<R>(0, 0); }
+  if (has_rhs) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const cplx<R>* hin = p.H + ((size_t)(b * 8 + 4 * c + m) * K + ky) * N;
+        cplx<R> v[E];
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = hin[lane + 32 * j];
+        fft_dif<R, N, false>(v, s_tw, lane);
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+          const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+          const cplx<R> tmul = cimul(v[j], -spectral_mu<R>(m, kx, ky));
+          if (c == 0) xb0[j] = cadd(xb0[j], tmul); else xb1[j] = cadd(xb1[j], tmul);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < E; ++j) { xb0[j] = cscale(xb0[j], cky * inv_n2); xb1[j] = cscale(xb1[j], cky * inv_n2); }
+  }
+
+  double hpart = 0.0;
+  cplx<R> lam0[E], lam1[E];   // next adjoint-RHS input (mask lam_w / c, k^2 mask lam_j / c), unscaled inverse
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    lam0[j] = mk<R>(0, 0); lam1[j] = mk<R>(0, 0);
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    if (slot < 0) continue;
+    const int kx = slot_to_kx(slot, KMAX, M);
+    const bool in_mask = !(kx == 0 && ky == 0);
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+      const size_t o = ((size_t)ch * K + ky) * M + slot;
+      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
+      const cplx<R> Xb = ch == 0 ? xb0[j] : xb1[j];
+      cplx<R> kb = mk<R>(0, 0);   // cotangent k-bar fed to the next adjoint RHS (before the h or t factor)
+      bool feed = true;
+      if (!rk43) {
+        const R e = in_mask ? exp(h / R(2) * L) : R(0);
+        const R dedh = e * L / R(2);
+        auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
+        switch (p.stage) {
+          case AJ_PRE: {
+            const cplx<R> ob = J[J_OB * VEC + o];
+            J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_r(ob, R(6));
+            J[J_K2 * VEC + o] = cdiv_r(ob, R(3)); J[J_B3 * VEC + o] = cdiv_r(ob, R(3));
+            kb = cdiv_r(ob, R(6));                                   // k4bar
+            hpart += ip(kb, Q[Q_K4 * VEC + o]) / (double)h;
+          } break;
+          case AJ_S4: {
+            const cplx<R> f2b = cadd(J[J_F2 * VEC + o], Xb), b3b = cadd(J[J_B3 * VEC + o], Xb);
+            const cplx<R> b2b = J[J_K2 * VEC + o], b1b = J[J_A1 * VEC + o];
+            const cplx<R> f = Q[Q_F * VEC + o], k1 = Q[Q_K1 * VEC + o];
+            const double eb = ip(b3b, Q[Q_K3 * VEC + o]) + ip(b2b, Q[Q_K2 * VEC + o]) + ip(b1b, cscale(k1, e)) +
+                              ip(f2b, cscale(f, e));
+            hpart += eb * (double)dedh;
+            kb = cscale(b3b, e);                                     // k3bar
+            hpart += ip(kb, Q[Q_K3 * VEC + o]) / (double)h;
+            J[J_F2 * VEC + o] = cscale(f2b, e);                      // f1bar
+            J[J_A1 * VEC + o] = cscale(b1b, e);                      // a1bar
+            J[J_K2 * VEC + o] = cscale(b2b, e);                      // k2bar
+          } break;
+          case AJ_S3: {
+            J[J_F2 * VEC + o] = cadd(J[J_F2 * VEC + o], Xb);
+            kb = cadd(J[J_K2 * VEC + o], cscale(Xb, R(0.5)));        // k2bar final
+            hpart += ip(kb, Q[Q_K2 * VEC + o]) / (double)h;
+          } break;
+          case AJ_S2: {
+            const cplx<R> f1b = cadd(J[J_F2 * VEC + o], Xb);
+            const cplx<R> a1b = cadd(J[J_A1 * VEC + o], cscale(Xb, R(0.5)));
+            const double eb = ip(a1b, Q[Q_K1 * VEC + o]) + ip(f1b, Q[Q_F * VEC + o]);
+            hpart += eb * (double)dedh;
+            kb = cscale(a1b, e);                                     // k1bar
+            hpart += ip(kb, Q[Q_K1 * VEC + o]) / (double)h;
+            J[J_OB * VEC + o] = cscale(f1b, e);                      // fbar (without the RHS1 term)
+          } break;
+          default: {   // AJ_S1: fbar += X1bar; then seed the previous step (if any)
+            const cplx<R> fb = cadd(J[J_OB * VEC + o], Xb);
+            J[J_OB * VEC + o] = fb;
+            if (p.rec_prev) {
+              J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_r(fb, R(6));
+              J[J_K2 * VEC + o] = cdiv_r(fb, R(3)); J[J_B3 * VEC + o] = cdiv_r(fb, R(3));
+              kb = cdiv_r(fb, R(6));
+              hpart += ip(kb, p.rec_prev[Q_K4 * VEC + o]) / (double)h;
+            } else {
+              feed = false;
+            }
+          } break;
+        }
+        kb = cscale(kb, h);
+      } else {
+        const R e = exp((t * L) * h / R(2));
+        const R dedt = e * (L * h / R(2));
+        auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
+        switch (p.stage) {
+          case AJ43_PRE:      // from (xbar_f, k5bar) in (X0, K1) slots: RHS5 input = k5bar
+          case AJ43_IPRE: {   // initial k1 = t v(x0): input = k1bar
+            kb = J[JJ_K1 * VEC + o];
+            hpart += ip(kb, Q[(p.stage == AJ43_PRE ? RR_K5 : RR_K1) * VEC + o]) / (double)t;
+          } break;
+          case AJ43_S5: {     // xbar_f += Xbar5; distribute to x2, k1'', k2', k3', k4
+            const cplx<R> xfb = cadd(J[JJ_X0 * VEC + o], Xb);
+            J[JJ_X2 * VEC + o] = xfb;
+            J[JJ_K1PP * VEC + o] = cdiv_r(cscale(xfb, h), R(6));
+            J[JJ_K2P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
+            J[JJ_K3P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
+            kb = cdiv_r(cscale(xfb, h), R(6));                       // k4bar
+            hpart += ip(kb, Q[RR_K4 * VEC + o]) / (double)t;
+          } break;
+          case AJ43_S4: {     // Y4 = x2 + h k3'
+            const cplx<R> x2b = cadd(J[JJ_X2 * VEC + o], Xb);
+            const cplx<R> k3pb = cadd(J[JJ_K3P * VEC + o], cscale(Xb, h));
+            const cplx<R> k2pb = J[JJ_K2P * VEC + o], k1ppb = J[JJ_K1PP * VEC + o];
+            const cplx<R> x0 = Q[RR_X0 * VEC + o], k1 = Q[RR_K1 * VEC + o];
+            const double eb = ip(k3pb, Q[RR_K3 * VEC + o]) + ip(k2pb, Q[RR_K2 * VEC + o]) +
+                              ip(k1ppb, cscale(k1, e)) + ip(x2b, cscale(x0, e));
+            hpart += eb * (double)dedt;
+            kb = cscale(k3pb, e);                                    // k3bar
+            hpart += ip(kb, Q[RR_K3 * VEC + o]) / (double)t;
+            J[JJ_K2 * VEC + o] = cscale(k2pb, e);                    // k2bar (partial)
+            J[JJ_K1P * VEC + o] = cscale(k1ppb, e);                  // k1'bar (partial)
+            J[JJ_XB * VEC + o] = cscale(x2b, e);                     // xbar (partial)
+          } break;
+          case AJ43_S3: {     // Y3 = x + h k2/2
+            J[JJ_XB * VEC + o] = cadd(J[JJ_XB * VEC + o], Xb);
+            kb = cadd(J[JJ_K2 * VEC + o], cscale(cscale(Xb, h), R(0.5)));   // k2bar final
+            hpart += ip(kb, Q[RR_K2 * VEC + o]) / (double)t;
+          } break;
+          default: {          // AJ43_S2: Y2 = x + h k1'/2; then x0bar, k1bar of this attempt
+            const cplx<R> xbb = cadd(J[JJ_XB * VEC + o], Xb);
+            const cplx<R> k1pb = cadd(J[JJ_K1P * VEC + o], cscale(cscale(Xb, h), R(0.5)));
+            const double eb = ip(k1pb, Q[RR_K1 * VEC + o]) + ip(xbb, Q[RR_X0 * VEC + o]);
+            hpart += eb * (double)dedt;
+            J[JJ_X0 * VEC + o] = cscale(xbb, e);
+            J[JJ_K1 * VEC + o] = cscale(k1pb, e);
+            feed = false;
+          } break;
+          case AJ43_INIT: {   // initial k1 = t v(x0): x0bar += Xbar
+            J[JJ_X0 * VEC + o] = cadd(J[JJ_X0 * VEC + o], Xb);
+            feed = false;
+          } break;
+        }
+        kb = cscale(kb, t);
+      }
+      if (feed) {
+        // lambda = kb (the cotangent of v); next inverse input (mask lam_w, k^2 mask lam_j) / c
+        const cplx<R> lin = ch == 0 ? (in_mask ? kb : mk<R>(0, 0)) : cscale(kb, ksq_masked<R>(kx, ky));
+        if (ch == 0) lam0[j] = cdiv_r(lin, cky); else lam1[j] = cdiv_r(lin, cky);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) hpart += __shfl_xor_sync(0xffffffffu, hpart, o);
+  if (lane == 0) p.hacc[(size_t)b * K + ky] += hpart;
+  const bool produce = (p.stage == AJ_PRE || p.stage == AJ_S4 || p.stage == AJ_S3 || p.stage == AJ_S2 ||
+                        (p.stage == AJ_S1 && p.rec_prev) || p.stage == AJ43_PRE || p.stage == AJ43_S5 ||
+                        p.stage == AJ43_S4 || p.stage == AJ43_S3 || p.stage == AJ43_IPRE);
+  if (!produce) return;
+  // unscaled inverse: Re sum lam e^{ik.x} after the row pass doubles ky > 0
+  const R n2 = R(N) * R(N);
+#pragma unroll
+  for (int j = 0; j < E; ++j) { lam0[j] = cscale(lam0[j], n2); lam1[j] = cscale(lam1[j], n2); }
+  col_inverse2<R, N>(lam0, lam1, p.G, 8, b, ky, lane, s_tw);
+}
+
+// Rejected Lawson-RK4(3) attempt in reverse: k1_next = e (e k1).
+template <typename R>
+__global__ void k_adj_reject(cplx<R>* J, int nslot, const cplx<R>* rec, double* hacc, double t, double h, R nu, R eta,
+                             int n, int B) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  // one warp per (b, ky) column so that hacc[b][ky] has a single writer
+  const int lane = threadIdx.x & 31;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= B * g.K) return;
+  const int b = colid / g.K, ky = colid - b * g.K;
+  cplx<R>* Jb = J + (size_t)b * nslot * VEC;
+  double part = 0.0;
+  for (int ch = 0; ch < 2; ++ch)
+    for (int slot = lane; slot < g.M; slot += 32) {
+      const size_t o = ((size_t)ch * g.K + ky) * g.M + slot;
+      const int kx = slot_to_kx(slot, g.kmax, g.M);
+      const R L = diss_L<R>(kx, ky, ch == 0 ? nu : eta);
+      const R e = exp(((R)t * L) * (R)h / R(2));
+      const R dedt = e * (L * (R)h / R(2));
+      const cplx<R> k1 = rec[RR_K1 * VEC + o], k1e = cscale(k1, e);
+      const cplx<R> kppb = Jb[JJ_K1 * VEC + o];
+      const cplx<R> kpb = cscale(kppb, e);
+      part += (rdot2(kppb.x, kppb.y, k1e.x, k1e.y) + rdot2(kpb.x, kpb.y, k1.x, k1.y)) * (double)dedt;
+      Jb[JJ_K1 * VEC + o] = cscale(kpb, e);
+    }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if (lane == 0) hacc[(size_t)b * g.K + ky] += part;
+}
+
+// Head of the adjoint: from Ybar = cotangent of sym(Phi) (box, already
+// -(c/n^2) rfft2(c_out)), Phibar = sym^T(Ybar) and sxbar = <Phibar, i kx Phi>
+// (symmetry.py:4-25; shift_x uses masked kx).  One block per batch element.
+template <typename R>
+__global__ void k_adj_head(const cplx<R>* Ybar, const cplx<R>* phi, const double* sx, int sx_shared, double sy,
+                           int odd, int rot, cplx<R>* Phibar, long pb_stride, double* sxbar, int n) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const int b = blockIdx.x;
+  const double s = sx[sx_shared ? 0 : b];
+  const cplx<R>* Y = Ybar + (size_t)b * VEC;
+  cplx<R>* P = Phibar + (size_t)b * pb_stride;
+  double part = 0.0;
+  for (size_t i = threadIdx.x; i < VEC; i += blockDim.x) {
+    // i indexes the SOURCE mode kappa (the mode of Phi); its image is kx_out
+    const int slot = i % g.M; const int ky = (i / g.M) % g.K; const int c = (int)(i / ((size_t)g.K * g.M));
+    const int kap = slot_to_kx(slot, g.kmax, g.M);
+    const int kout = odd ? -kap : kap;
+    const int sout = kout >= 0 ? kout : kout + g.M;
+    cplx<R> y = Y[((size_t)c * g.K + ky) * g.M + sout];
+    if (rot) { y.y = -y.y; if (c == 1) { y.x = -y.x; y.y = -y.y; } }   // R^T = sign_c conj
+    if (odd) { y.x = -y.x; y.y = -y.y; }
+    const bool m = !(kap == 0 && ky == 0);
+    double sn, cs;
+    sincos(m ? (double)ky * sy : 0.0, &sn, &cs);
+    y = cmul(mk<R>((R)cs, (R)-sn), y);
+    sincos(m ? (double)kap * s : 0.0, &sn, &cs);
+    y = cmul(mk<R>((R)cs, (R)-sn), y);
+    P[i] = y;
+    const cplx<R> ph = phi[i];
+    const R km = m ? (R)kap : R(0);
+    // <y, i kap phi> = Re(conj(y) * i kap phi)
+    part += (double)y.x * (double)(-km * ph.y) + (double)y.y * (double)(km * ph.x);
+  }
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w];
+    sxbar[b] = a;
+  }
+}
+
+// Ybar = -(c_ky/n^2) * box  (transpose of out = base - irfft2(.))
+template <typename R>
+__global__ void k_box_scale_c(cplx<R>* v, long stride, int n, int B, R sign_over_n2) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const long total = (long)B * VEC;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / VEC); const size_t o = i - (size_t)b * VEC;
+    const int ky = (o / g.M) % g.K;
+    cplx<R>* q = v + (size_t)b * stride + o;
+    *q = cscale(*q, (ky == 0 ? R(1) : R(2)) * sign_over_n2);
+  }
+}
+
+// Z = fbar0 * n^2 / c_ky (so that from_box(Z) = to_box^T(fbar0)).
+template <typename R>
+__global__ void k_box_to_fields_adj(const cplx<R>* fb, long stride, cplx<R>* Z, int n, int B) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const long total = (long)B * VEC;
+  const R n2 = R(n) * R(n);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / VEC); const size_t o = i - (size_t)b * VEC;
+    const int ky = (o / g.M) % g.K;
+    Z[i] = cscale(fb[(size_t)b * stride + o], n2 / (ky == 0 ? R(1) : R(2)));
+  }
+}
+
+// g += cT vt / (2n^2) + csx vx / (2n^2)  (phase-condition transposes, loss_functions.py:124-129)
+template <typename R>
+__global__ void k_adj_phase(R* gfields, const R* vt, const R* vx, const double* cT, const double* csx, int n, int B) {
+  const long per = 2L * n * n;
+  const long total = (long)B * per;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / per); const long o = i - (long)b * per;
+    gfields[i] += (R)((cT[b] * (double)vt[o] + csx[b] * (double)vx[o]) / (double)per);
+  }
+}
+
+// Deterministic reduction of the [B][K] accumulators: out[b] = scale * sum_ky hacc.
+static __global__ void k_reduce_hacc(const double* hacc, int K, double scale, double* out, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double s = 0.0;
+  for (int k = 0; k < K; ++k) s += hacc[(size_t)b * K + k];
+  out[b] = s * scale;
+}
+
+}  // namespace ecs

@@ -14,8 +14,9 @@ namespace ecs {
 
 // Per-candidate state slots of the stepper, each a box vector [2][K][M].
 enum Rk43Slot { S_X0 = 0, S_K1, S_XE, S_K1E, S_K2, S_K3, S_X2, S_K4, S_XF, S_K5, S_NSLOT };
-// Trajectory record slots per attempt (primal values needed by tangent/adjoint).
-enum Rk43Rec { R_X0 = 0, R_K1, R_K2, R_K3, R_K4, R_K5, R_NREC };
+// Trajectory record per attempt (primal values needed by tangent/adjoint):
+// start state, carried k1 (before twiddles), k2..k5 and the stage inputs.
+enum Rk43Rec { RR_X0 = 0, RR_K1, RR_K2, RR_K3, RR_K4, RR_K5, RR_Y2, RR_Y3, RR_Y4, RR_XF, RR_NREC };
 
 enum Rk43Stage : int {
   R43_START = 6,  // no RHS input; inverse transforms of x0
@@ -35,7 +36,7 @@ struct Col43Params {
   StepCtl* ctl;         // [B]
   const cplx<R>* fhat;  // [K][M]
   const cplx<R>* tw;
-  cplx<R>* rec;         // optional [B][cap][R_NREC][2][K][M]
+  cplx<R>* rec;         // optional [B][cap][RR_NREC][2][K][M]
   int cap;
   R nu, eta;
   int B, stage;
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   const R t = (R)c.t, h = (R)c.h;
   const int pend = c.pending_accept;
   cplx<R>* S = p.S + (size_t)b * S_NSLOT * VEC;
-  cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * R_NREC * VEC
+  cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * RR_NREC * VEC
                        : nullptr;
 
   const bool has_rhs = p.stage != R43_A && p.stage != R43_START;
@@ -91,19 +92,21 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
           cplx<R> xs = pend ? S[S_XF * VEC + o] : S[S_X0 * VEC + o];
           cplx<R> ks = pend ? S[S_K5 * VEC + o] : S[S_K1 * VEC + o];
           if (pend) { S[S_X0 * VEC + o] = xs; S[S_K1 * VEC + o] = ks; }
-          if (rec) { rec[R_X0 * VEC + o] = xs; rec[R_K1 * VEC + o] = ks; }
+          if (rec) { rec[RR_X0 * VEC + o] = xs; rec[RR_K1 * VEC + o] = ks; }
           const R e = exp((t * L) * h / R(2));             // e = exp(mod_L * h/2), not masked (:263)
           const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
           S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
           xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
+          if (rec) rec[RR_Y2 * VEC + o] = xin;
         } break;
         case R43_B: {                                      // :270-271
           S[S_K2 * VEC + o] = kv;
-          if (rec) rec[R_K2 * VEC + o] = kv;
+          if (rec) rec[RR_K2 * VEC + o] = kv;
           xin = cadd(S[S_XE * VEC + o], cscale(cscale(kv, h), R(0.5)));
+          if (rec) rec[RR_Y3 * VEC + o] = xin;
         } break;
         case R43_C: {                                      // :271-280
-          if (rec) rec[R_K3 * VEC + o] = kv;
+          if (rec) rec[RR_K3 * VEC + o] = kv;
           const R e = exp((t * L) * h / R(2));
           const cplx<R> x2 = cscale(S[S_XE * VEC + o], e);
           const cplx<R> k1ee = cscale(S[S_K1E * VEC + o], e);
@@ -112,18 +115,20 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
           S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
           S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
           xin = cadd(x2, cscale(k3e, h));
+          if (rec) rec[RR_Y4 * VEC + o] = xin;
         } break;
         case R43_D: {                                      // :280-281
           S[S_K4 * VEC + o] = kv;
-          if (rec) rec[R_K4 * VEC + o] = kv;
+          if (rec) rec[RR_K4 * VEC + o] = kv;
           cplx<R> acc = cadd(cadd(cadd(cdiv_r(S[S_K1 * VEC + o], R(6)), cdiv_r(S[S_K2 * VEC + o], R(3))),
                                   cdiv_r(S[S_K3 * VEC + o], R(3))), cdiv_r(kv, R(6)));
           xin = cadd(S[S_X2 * VEC + o], cscale(acc, h));
           S[S_XF * VEC + o] = xin;
+          if (rec) rec[RR_XF * VEC + o] = xin;
         } break;
         default: {                                         // R43_E: :282, :288
           S[S_K5 * VEC + o] = kv;
-          if (rec) rec[R_K5 * VEC + o] = kv;
+          if (rec) rec[RR_K5 * VEC + o] = kv;
           xin = cdiv_r(cscale(csub(kv, S[S_K4 * VEC + o]), h), R(6));
         } break;
       }

@@ -1,0 +1,376 @@
+// Tangent (forward-mode) kernels of the shooting map: the JVP used as the
+// Newton-GMRES matvec (reference: jax.jvp of objective_RPO, jax_scripts/lib/utils.py:108).
+//
+// A batch of B tangents shares one primal trajectory.  The primal solve records,
+// per step (Lawson-RK4) or attempt (Lawson-RK4(3)), the compact stage inputs and
+// stage derivatives; the tangent pass regenerates the primal's 8 physical
+// fields for a chunk of stages in one batched launch pair (shared by all
+// tangents) and then advances the tangents with linearised products
+//   d(u.grad w) = du.grad w + u.grad dw, ...
+// and the product rule through the integrating factor, e' = e L h'/2.
+#pragma once
+
+#include "kernels.cuh"
+#include "kernels_rk43.cuh"
+
+namespace ecs {
+
+
+// ---------------------------------------------------------------------------
+// Regeneration of primal physical fields for a list of recorded stage inputs.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct ColRegenParams {
+  const cplx<R>* rec;     // record base
+  const long* items;      // [nitems] offsets (in box vectors) of the stage inputs in rec
+  cplx<R>* G;             // [nitems][8][K][N]
+  const cplx<R>* tw;
+  int nitems;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_regen(ColRegenParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.nitems * K) return;
+  const int it = col / K, ky = col - it * K;
+  const cplx<R>* y = p.rec + (size_t)p.items[it] * VEC;
+  cplx<R> x0[E], x1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    x0[j] = slot >= 0 ? y[(size_t)ky * M + slot] : mk<R>(0, 0);
+    x1[j] = slot >= 0 ? y[(size_t)(K + ky) * M + slot] : mk<R>(0, 0);
+  }
+  col_inverse8<R, N>(x0, x1, p.G, it, ky, lane, s_tw);
+}
+
+// Physical fields of each item: Phys[it][x][8][pos] (fu1, fv1 include b0).
+template <typename R>
+struct RowPhysParams {
+  const cplx<R>* G;   // [nitems][8][K][N]
+  R* phys;            // [nitems][N][8][N]
+  const cplx<R>* tw;
+  R b0x, b0y;
+  int nitems;
+};
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_phys(RowPhysParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  const int tiles = N / XT;
+  const int it = blockIdx.x / tiles, x0 = (blockIdx.x - it * tiles) * XT;
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)it * 8 * K * N, 8 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  R* ph = p.phys + (((size_t)it * N + x) * 8) * N;
+#pragma unroll
+  for (int pr = 0; pr < 4; ++pr) {
+    cplx<R> z[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j)
+      z[j] = packed_pair<R, N, XT>(s_G + (2 * pr) * K * (XT + 1), s_G + (2 * pr + 1) * K * (XT + 1), lane + 32 * j, w);
+    fft_dif<R, N, true>(z, s_tw, lane);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = lane + 32 * j;
+      R a = z[j].x, bb = z[j].y;
+      if (pr == 3) { a += p.b0x; bb += p.b0y; }   // fu1, fv1 carry the mean field (mhd_jax.py:145-149)
+      ph[(2 * pr) * N + e] = a;
+      ph[(2 * pr + 1) * N + e] = bb;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tangent row pass: linearised products around the primal physical fields.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct RowTanParams {
+  const cplx<R>* G;     // tangent [B][8][K][N]
+  cplx<R>* H;           // tangent [B][2][K][N]
+  const R* phys;        // primal physical fields of this stage: [N][8][N]
+  const cplx<R>* tw;
+  int B;
+};
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_tan(RowTanParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_H = s_G + 8 * K * (XT + 1);
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 8 * K, x0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = x0 + w;
+  const R* ph = p.phys + ((size_t)x * 8) * N;
+  // tangent physical fields, pair by pair; primal values from the record
+  cplx<R> W[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) W[j] = mk<R>(0, 0);
+#pragma unroll
+  for (int pr = 0; pr < 4; ++pr) {
+    cplx<R> z[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j)
+      z[j] = packed_pair<R, N, XT>(s_G + (2 * pr) * K * (XT + 1), s_G + (2 * pr + 1) * K * (XT + 1), lane + 32 * j, w);
+    fft_dif<R, N, true>(z, s_tw, lane);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = lane + 32 * j;
+      const R da = z[j].x, db = z[j].y;
+      // pr 0: (dfx0, dfy0)  1: (dfu0, dfv0)  2: (dfx1, dfy1)  3: (dfu1, dfv1)
+      // dP1 = -d(adv0) + d(adv1),  adv_c = fu_c fx_c + fv_c fy_c   (mhd_jax.py:152,159)
+      // dP2 = d(fu0 fv1 - fv0 fu1)                                   (mhd_jax.py:163)
+      if (pr == 0) {
+        W[j].x -= ph[2 * N + e] * da + ph[3 * N + e] * db;
+      } else if (pr == 1) {
+        W[j].x -= da * ph[0 * N + e] + db * ph[1 * N + e];
+        W[j].y += da * ph[7 * N + e] - db * ph[6 * N + e];
+      } else if (pr == 2) {
+        W[j].x += ph[6 * N + e] * da + ph[7 * N + e] * db;
+      } else {
+        W[j].x += da * ph[4 * N + e] + db * ph[5 * N + e];
+        W[j].y += ph[2 * N + e] * db - ph[3 * N + e] * da;
+      }
+    }
+  }
+  fft_dit<R, N, false>(W, s_tw, lane);
+  split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * 2 * K * N, s_H, 2 * K, x0);
+}
+
+// ---------------------------------------------------------------------------
+// Tangent column pass: forward transform of the linearised products and the
+// tangent of the stepper algebra.
+// ---------------------------------------------------------------------------
+enum TanStage : int {
+  TS_START = 0,                  // inverse transforms of the tangent state (dF / dX0)
+  T4_S1 = 1, T4_S2, T4_S3, T4_S4,   // Lawson-RK4 stages
+  T43_INIT = 10, T43_A, T43_B, T43_C, T43_D, T43_E,   // Lawson-RK4(3) stages
+  T43_START = 16,                // inverse transforms of dX0 (before T43_INIT)
+};
+// Tangent slots (Lawson-RK4 uses the first three).
+enum TanSlot { D_F = 0, D_A1, D_K2, D_NS4 = 3 };
+
+template <typename R>
+struct ColTanParams {
+  const cplx<R>* H;     // [B][2][K][N]
+  cplx<R>* G;           // [B][8][K][N]
+  cplx<R>* D;           // tangent slots [B][nslot][2][K][M]
+  int nslot;
+  const cplx<R>* rec;   // primal record of this step/attempt
+  const double* dT;     // [B]
+  double t, h;          // Lawson-RK4: t unused; Lawson-RK4(3): t = T, h = attempt step
+  double dscale;        // Lawson-RK4: dh = dT * dscale; Lawson-RK4(3): dt = dT * dscale
+  const cplx<R>* tw;
+  R nu, eta;
+  int B, stage, produce;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
+  __shared__ cplx<R> s_tw[N / 2];
+  load_twiddles<R, N>(s_tw, p.tw);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (col >= p.B * K) return;
+  const int b = col / K, ky = col - b * K;
+  cplx<R>* D = p.D + (size_t)b * p.nslot * VEC;
+  const cplx<R>* Q = p.rec;
+  const bool rk43 = p.stage >= T43_INIT;
+  const bool has_rhs = !(p.stage == TS_START || p.stage == T43_A || p.stage == T43_START);
+  const R h = (R)p.h, t = (R)p.t;
+  const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
+  cplx<R> r0[E], r1[E];
+  if (has_rhs) col_load_fwd<R, N>(p.H, b, ky, lane, s_tw, r0, r1);
+  cplx<R> x0[E], x1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    if (slot < 0) continue;
+    const int kx = slot_to_kx(slot, KMAX, M);
+    const bool in_mask = !(kx == 0 && ky == 0);
+    cplx<R> dv[2];
+    dv[0] = mk<R>(0, 0); dv[1] = mk<R>(0, 0);
+    if (has_rhs) {
+      dv[0] = in_mask ? r0[j] : mk<R>(0, 0);               // tangent has no forcing
+      dv[1] = cscale(r1[j], ksq_masked<R>(kx, ky));
+    }
+#pragma unroll
+    for (int ch = 0; ch < 2; ++ch) {
+      const size_t o = ((size_t)ch * K + ky) * M + slot;
+      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
+      cplx<R> xin = mk<R>(0, 0);
+      if (!rk43) {
+        // Lawson-RK4: e = exp(h/2 L) mask, de = e L dh/2; dk = dh v + h dv with v = k/h
+        const R e = in_mask ? exp(h / R(2) * L) : R(0);
+        const R de = e * L * (dpar / R(2));
+        auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv[ch], h)); };
+        switch (p.stage) {
+          case TS_START: xin = D[D_F * VEC + o]; break;
+          case T4_S1: {
+            const cplx<R> dk1 = dk_of(Q_K1);
+            const cplx<R> df1 = cadd(cscale(Q[Q_F * VEC + o], de), cscale(D[D_F * VEC + o], e));
+            const cplx<R> da1 = cadd(cscale(Q[Q_K1 * VEC + o], de), cscale(dk1, e));
+            D[D_F * VEC + o] = df1; D[D_A1 * VEC + o] = da1;
+            xin = cadd(df1, cscale(da1, R(0.5)));
+          } break;
+          case T4_S2: {
+            const cplx<R> dk2 = dk_of(Q_K2);
+            D[D_K2 * VEC + o] = dk2;
+            xin = cadd(D[D_F * VEC + o], cscale(dk2, R(0.5)));
+          } break;
+          case T4_S3: {
+            const cplx<R> dk3 = dk_of(Q_K3);
+            const cplx<R> f1 = cscale(Q[Q_F * VEC + o], e), a1 = cscale(Q[Q_K1 * VEC + o], e);
+            const cplx<R> df2 = cadd(cscale(f1, de), cscale(D[D_F * VEC + o], e));
+            const cplx<R> db1 = cadd(cscale(a1, de), cscale(D[D_A1 * VEC + o], e));
+            const cplx<R> db2 = cadd(cscale(Q[Q_K2 * VEC + o], de), cscale(D[D_K2 * VEC + o], e));
+            const cplx<R> db3 = cadd(cscale(Q[Q_K3 * VEC + o], de), cscale(dk3, e));
+            xin = cadd(df2, db3);
+            D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_r(db1, R(6))), cdiv_r(db2, R(3))), cdiv_r(db3, R(3)));
+          } break;
+          default: {   // T4_S4
+            const cplx<R> dk4 = dk_of(Q_K4);
+            xin = cadd(D[D_F * VEC + o], cdiv_r(dk4, R(6)));
+            D[D_F * VEC + o] = xin;
+          } break;
+        }
+      } else {
+        // Lawson-RK4(3): e = exp(t L h/2), de = e L h/2 dt; dk = dt v + t dv with v = k/t
+        const R e = exp((t * L) * h / R(2));
+        const R de = e * (L * h / R(2)) * dpar;
+        auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / t), cscale(dv[ch], t)); };
+        switch (p.stage) {
+          case T43_START: xin = D[S_X0 * VEC + o]; break;
+          case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
+          case T43_A: {
+            const cplx<R> dxe = cadd(cscale(Q[RR_X0 * VEC + o], de), cscale(D[S_X0 * VEC + o], e));
+            const cplx<R> dk1e = cadd(cscale(Q[RR_K1 * VEC + o], de), cscale(D[S_K1 * VEC + o], e));
+            D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
+            xin = cadd(dxe, cscale(cscale(dk1e, h), R(0.5)));
+          } break;
+          case T43_B: {
+            const cplx<R> dk2 = dk_of(RR_K2);
+            D[S_K2 * VEC + o] = dk2;
+            xin = cadd(D[S_XE * VEC + o], cscale(cscale(dk2, h), R(0.5)));
+          } break;
+          case T43_C: {
+            const cplx<R> dk3 = dk_of(RR_K3);
+            const cplx<R> xe = cscale(Q[RR_X0 * VEC + o], e), k1e = cscale(Q[RR_K1 * VEC + o], e);
+            const cplx<R> dx2 = cadd(cscale(xe, de), cscale(D[S_XE * VEC + o], e));
+            const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(D[S_K1E * VEC + o], e));
+            const cplx<R> dk2e = cadd(cscale(Q[RR_K2 * VEC + o], de), cscale(D[S_K2 * VEC + o], e));
+            const cplx<R> dk3e = cadd(cscale(Q[RR_K3 * VEC + o], de), cscale(dk3, e));
+            D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
+            xin = cadd(dx2, cscale(dk3e, h));
+          } break;
+          case T43_D: {
+            const cplx<R> dk4 = dk_of(RR_K4);
+            const cplx<R> acc = cadd(cadd(cadd(cdiv_r(D[S_K1 * VEC + o], R(6)), cdiv_r(D[S_K2 * VEC + o], R(3))),
+                                          cdiv_r(D[S_K3 * VEC + o], R(3))), cdiv_r(dk4, R(6)));
+            xin = cadd(D[S_X2 * VEC + o], cscale(acc, h));
+            D[S_XF * VEC + o] = xin;
+          } break;
+          default: {   // T43_E: accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
+            D[S_K1 * VEC + o] = dk_of(RR_K5);
+            D[S_X0 * VEC + o] = D[S_XF * VEC + o];
+          } break;
+        }
+      }
+      if (ch == 0) x0[j] = xin; else x1[j] = xin;
+    }
+  }
+  if (!p.produce || p.stage == T43_INIT || p.stage == T43_E) return;
+  col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
+}
+
+// Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);
+// its tangent is d(e (e k1)) with e' = e L h/2 dt.
+template <typename R>
+__global__ void k_tan_reject(cplx<R>* D, int nslot, const cplx<R>* rec, const double* dT, double dscale, double t,
+                             double h, R nu, R eta, int n, int B) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const long total = (long)B * VEC;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / VEC);
+    const size_t o = i - (size_t)b * VEC;
+    const int slot = o % g.M; const int ky = (o / g.M) % g.K; const int ch = (int)(o / ((size_t)g.K * g.M));
+    const int kx = slot_to_kx(slot, g.kmax, g.M);
+    const R L = diss_L<R>(kx, ky, ch == 0 ? nu : eta);
+    const R e = exp(((R)t * L) * (R)h / R(2));
+    const R de = e * (L * (R)h / R(2)) * (R)(dT[b] * dscale);
+    cplx<R>* Db = D + (size_t)b * nslot * VEC;
+    const cplx<R> k1 = rec[RR_K1 * VEC + o];
+    const cplx<R> k1e = cscale(k1, e);
+    const cplx<R> dk1e = cadd(cscale(k1, de), cscale(Db[S_K1 * VEC + o], e));
+    Db[S_K1 * VEC + o] = cadd(cscale(k1e, de), cscale(dk1e, e));
+  }
+}
+
+// W[b] = dPhi[b] + i kx dsx[b] Phi (the tangent of shift_x before the symmetry
+// action, symmetry.py:4-5; kx masked).
+template <typename R>
+__global__ void k_tan_shift(const cplx<R>* dphi, long dstride, const cplx<R>* phi, const double* dsx, cplx<R>* W,
+                            int n, int B) {
+  const Geom g = make_geom(n);
+  const size_t VEC = (size_t)2 * g.K * g.M;
+  const long total = (long)B * VEC;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / VEC);
+    const size_t o = i - (size_t)b * VEC;
+    const int slot = o % g.M; const int ky = (o / g.M) % g.K;
+    const int kx = slot_to_kx(slot, g.kmax, g.M);
+    const R kxm = (kx == 0 && ky == 0) ? R(0) : (R)kx;
+    W[i] = cadd(dphi[(size_t)b * dstride + o], cimul(cscale(phi[o], (R)dsx[b]), kxm));
+  }
+}
+
+// Tangents of the phase conditions: dpt = mean(vt * du0), dpx = mean(vx * du0)
+// over 2 n^2 entries (loss_functions.py:124-125); one block per tangent.
+template <typename R>
+__global__ void k_phase_dot(const R* vt, const R* vx, const R* du, double* dpt, double* dpx, int n) {
+  const int b = blockIdx.x;
+  const long cnt = 2L * n * n;
+  const R* d = du + (size_t)b * cnt;
+  double st = 0.0, sx = 0.0;
+  for (long i = threadIdx.x; i < cnt; i += blockDim.x) { st += (double)vt[i] * d[i]; sx += (double)vx[i] * d[i]; }
+  __shared__ double s1[32], s2[32];
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) { st += __shfl_xor_sync(0xffffffffu, st, o); sx += __shfl_xor_sync(0xffffffffu, sx, o); }
+  if ((threadIdx.x & 31) == 0) { s1[threadIdx.x >> 5] = st; s2[threadIdx.x >> 5] = sx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, c = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += s1[w]; c += s2[w]; }
+    dpt[b] = a / (double)cnt; dpx[b] = c / (double)cnt;
+  }
+}
+
+}  // namespace ecs

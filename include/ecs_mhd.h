@@ -71,6 +71,15 @@ typedef struct {
 /* Library version string. */
 const char* ecs_version(void);
 
+/* Number of kernels this context has launched so far (instrumentation). */
+long long ecs_launch_count(const ecs_ctx* ctx);
+
+/* Times `iters` launches of a tangent-pass kernel (0: row pass k_row_tan,
+ * 1: column pass k_col_tan) on the workspace left by the last ecs_jvp call of
+ * `batch` tangents; returns ms per launch and the kernel's algorithmic bytes
+ * per launch (instrumentation for roofline reporting; no reference counterpart). */
+int ecs_bench_kernel(ecs_ctx* ctx, int which, int batch, int iters, float* ms, double* bytes, void* stream);
+
 /* Context with grid tables and workspace for grids n in {64,128,256}
  * (replaces mhd_jax.construct_domain, jax_scripts/lib/mhd_jax.py:20-94, and
  * dictionaryIO.recompute_grid_information, jax_scripts/lib/dictionaryIO.py:64-78).
@@ -105,6 +114,28 @@ int ecs_objective(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, co
 /* loss_RPO (jax_scripts/lib/loss_functions.py:99-111): mean(irfft2(f - f0)^2) per batch element. */
 int ecs_loss(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
              const double* sx, double* loss, ecs_info* info, int batch, void* stream);
+
+/* Linearise objective_RPO at one primal point (batch 1): runs the forward map
+ * with a trajectory record kept in the context for later ecs_jvp/ecs_vjp calls
+ * (replaces the primal half of jax.jvp / jax.vjp of objective_RPO,
+ * jax_scripts/lib/utils.py:108, jax_scripts/newton.py:168).  out_fields
+ * (optional) receives the objective's fields output. */
+int ecs_linearize(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
+                  const double* sx, void* out_fields, ecs_info* info, void* stream);
+
+/* Jacobian-vector products of objective_RPO at the current linearisation for
+ * `batch` tangents {dfields [batch][2][n][n], dT [batch], dsx [batch]}
+ * (jac(primal, tangent), jax_scripts/lib/utils.py:108; the Newton-GMRES matvec). */
+int ecs_jvp(ecs_ctx* ctx, const void* dfields, const double* dT, const double* dsx, void* out_dfields,
+            double* out_dT, double* out_dsx, int batch, void* stream);
+
+/* Vector-Jacobian products of objective_RPO at the current linearisation for
+ * `batch` cotangents {c_fields, c_T, c_sx}: gradients with respect to
+ * {fields, T, sx} (jax.vjp(obj, input_dict), jax_scripts/newton.py:168-169;
+ * with c_fields = out/n^2, c_T = c_sx = 0 it is the gradient of loss_RPO,
+ * jax.value_and_grad at jax_scripts/adjoint_descent.py:91). */
+int ecs_vjp(ecs_ctx* ctx, const void* c_fields, const double* c_T, const double* c_sx, void* g_fields,
+            double* g_T, double* g_sx, int batch, void* stream);
 
 #ifdef __cplusplus
 }

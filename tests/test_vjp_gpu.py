@@ -1,0 +1,105 @@
+"""VJP / adjoint gradient of the CUDA path: against torch.func.vjp of the oracle's
+torch twin (1e-12 relative), the dot-product test <u, J v> = <J^T u, v> between the
+CUDA JVP and VJP (1e-12), and central finite differences of the loss (1e-6, the FD
+truncation level)."""
+import numpy as np
+import pytest
+import torch
+from torch.func import vjp as tvjp
+
+import oracle as O
+import ecs_mhd_2d_b200 as E
+from ecs_mhd_2d_b200.synthetic import initial_condition
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+TOL_43 = 1e-10   # adaptive step-size controller sensitivity, see test_parity_gpu.TOL_43
+
+CASES = [
+    ("Lawson_RK4", dict(num_checkpoints=2, ministeps=8, shift_reflect_ny=0, rot=False)),
+    ("Lawson_RK4", dict(num_checkpoints=1, ministeps=12, shift_reflect_ny=3, rot=True)),
+    ("Lawson_RK43", dict(shift_reflect_ny=2, rot=False, adaptive_dict={"atol": 1e-5, "checkpoints": 4, "max_steps_per_checkpoint": 16})),
+    ("Lawson_RK43", dict(shift_reflect_ny=1, rot=True, adaptive_dict={"atol": 1e-7, "checkpoints": 4, "max_steps_per_checkpoint": 32})),
+]
+
+
+def oracle_vjp(u0, T, sx, cot, pd_t, mode):
+    f = lambda d: O.objective_RPO(d, pd_t, mode, xp=O.TORCH)
+    prim = {"fields": torch.from_numpy(u0), "T": torch.tensor(T, dtype=torch.float64),
+            "sx": torch.tensor(sx, dtype=torch.float64)}
+    _, fn = tvjp(f, prim)
+    c = {"fields": torch.from_numpy(cot[0]), "T": torch.tensor(cot[1], dtype=torch.float64),
+         "sx": torch.tensor(cot[2], dtype=torch.float64)}
+    return {k: v.detach().numpy() for k, v in fn(c)[0].items()}
+
+
+@pytest.mark.parametrize("mode,kw", CASES)
+def test_vjp_matches_oracle(cuda, mode, kw):
+    n, T, sx = 64, 0.1, 0.35
+    u0 = initial_condition(3, n)
+    rng = np.random.default_rng(5)
+    cf = np.stack([rng.standard_normal((2, n, n)) for _ in range(2)])
+    cT = np.array([0.7, -0.2]); csx = np.array([0.0, 1.3])
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    pdt = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", xp=O.TORCH, **kw)
+    obj = E.Objective(pd, mode)
+    prim = {"fields": torch.as_tensor(u0, device="cuda"), "T": T, "sx": sx}
+    out, jacT = E.vjp(obj, prim)
+    got = jacT({"fields": torch.as_tensor(cf, device="cuda"), "T": torch.tensor(cT), "sx": torch.tensor(csx)})[0]
+    for b in range(2):
+        want = oracle_vjp(u0, T, sx, (cf[b], cT[b], csx[b]), pdt, mode)
+        tol = TOL_43 if mode == "Lawson_RK43" else TOL
+        assert rel_l2(got["fields"][b].cpu().numpy(), want["fields"]) < tol, b
+        for k in ("T", "sx"):
+            assert abs(float(got[k][b]) - float(want[k])) <= tol * max(abs(float(want[k])), 1.0), (k, b)
+
+
+@pytest.mark.parametrize("mode,kw", CASES)
+def test_dot_product_adjointness(cuda, mode, kw):
+    """(u, J v) == (J^T u, v), the reference's own check (timestepping.py:496-504)."""
+    n = 64
+    u0 = initial_condition(6, n)
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    obj = E.Objective(pd, mode)
+    prim = {"fields": torch.as_tensor(u0, device="cuda"), "T": 0.12, "sx": -0.4}
+    rng = np.random.default_rng(8)
+    v = {"fields": torch.as_tensor(rng.standard_normal((2, n, n)), device="cuda"), "T": 0.3, "sx": -0.7}
+    u = {"fields": torch.as_tensor(rng.standard_normal((2, n, n)), device="cuda"), "T": 1.1, "sx": 0.4}
+    Jv = obj.jvp(prim, v)
+    _, jacT = E.vjp(obj, prim)
+    JTu = jacT(u)[0]
+    lhs = float(torch.sum(u["fields"] * Jv["fields"])) + 1.1 * float(Jv["T"]) + 0.4 * float(Jv["sx"])
+    rhs = float(torch.sum(JTu["fields"] * v["fields"])) + 0.3 * float(JTu["T"]) - 0.7 * float(JTu["sx"])
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
+
+
+def test_loss_gradient_finite_differences(cuda):
+    n = 64
+    u0 = initial_condition(1, n)
+    kw = dict(num_checkpoints=2, ministeps=16, shift_reflect_ny=1, rot=False)
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    inp = {"fields": torch.as_tensor(u0, device="cuda"), "T": 0.3, "sx": 0.2}
+    (loss, _), g = E.loss_and_grad(inp, pd, "Lawson_RK4")
+    rng = np.random.default_rng(2)
+    d = torch.as_tensor(rng.standard_normal((2, n, n)), device="cuda")
+    dT, dsx, eps = 0.5, -0.3, 1e-6
+    lp, _ = E.loss_RPO({"fields": inp["fields"] + eps * d, "T": 0.3 + eps * dT, "sx": 0.2 + eps * dsx}, pd, "Lawson_RK4")
+    lm, _ = E.loss_RPO({"fields": inp["fields"] - eps * d, "T": 0.3 - eps * dT, "sx": 0.2 - eps * dsx}, pd, "Lawson_RK4")
+    fd = (float(lp) - float(lm)) / (2 * eps)
+    an = float(torch.sum(g["fields"] * d)) + dT * float(g["T"]) + dsx * float(g["sx"])
+    assert abs(fd - an) <= 1e-6 * abs(an)
+
+
+def test_autograd_function(cuda):
+    n = 64
+    u0 = torch.as_tensor(initial_condition(2, n), device="cuda").requires_grad_(True)
+    T = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    sx = torch.tensor(0.1, dtype=torch.float64, device="cuda", requires_grad=True)
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", num_checkpoints=1, ministeps=16,
+                           shift_reflect_ny=0, rot=False)
+    loss = E.loss_rpo_autograd(u0, T, sx, pd, "Lawson_RK4")
+    loss.backward()
+    (l2, _), g = E.loss_and_grad({"fields": u0.detach(), "T": 0.2, "sx": 0.1}, pd, "Lawson_RK4")
+    assert torch.allclose(u0.grad, g["fields"], rtol=0, atol=1e-14 * float(g["fields"].abs().max()))
+    assert abs(float(T.grad) - float(g["T"])) <= 1e-12 * abs(float(g["T"]))
