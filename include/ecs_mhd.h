@@ -137,6 +137,17 @@ int ecs_jvp(ecs_ctx* ctx, const void* dfields, const double* dT, const double* d
 int ecs_vjp(ecs_ctx* ctx, const void* c_fields, const double* c_T, const double* c_sx, void* g_fields,
             double* g_T, double* g_sx, int batch, void* stream);
 
+/* One Arnoldi step's modified Gram-Schmidt in FP64 (jax_scripts/lib/linalg.py:65-86):
+ * for j = 0..k: h_j = <w, Q[:,j]>, w -= h_j Q[:,j]; then Hcol[k+1] = |w| and
+ * Q[:,k+1] = w / |w|.  Q is column-major with leading dimension ld >= len;
+ * Hcol points at column k of H (k+2 entries written).  k = -1 only normalises
+ * w into Q[:,0] (linalg.py:58) and writes |w| to Hcol[0].  len <= 131200. */
+int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, double* Hcol, long len, void* stream);
+
+/* y = argmin |H y - b| for the (m+1) x m upper Hessenberg H (column-major,
+ * leading dimension ldh >= m+1), m <= 128 (jnp.linalg.lstsq at linalg.py:93). */
+int ecs_hessenberg_lstsq(const double* H, int ldh, int m, const double* b, double* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
