@@ -19,7 +19,7 @@ ECS_MODE_LAWSON_RK4, ECS_MODE_LAWSON_RK43 = 1, 2
 
 STATUS = {
     0: "ECS_OK", 1: "ECS_ERR_INVALID", 2: "ECS_ERR_CUDA", 3: "ECS_ERR_BAD_MODE",
-    4: "ECS_ERR_NOT_COMPLETED", 5: "ECS_ERR_OOM", 6: "ECS_ERR_UNSUPPORTED",
+    4: "ECS_ERR_NOT_COMPLETED", 5: "ECS_ERR_OOM", 6: "ECS_ERR_UNSUPPORTED", 7: "ECS_ERR_TOO_LARGE",
 }
 
 
@@ -75,6 +75,7 @@ SIGNATURES = {
     "ecs_vjp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
     "ecs_arnoldi_mgs": (_I, [_VP, ctypes.c_long, _I, _VP, _VP, ctypes.c_long, _VP]),
     "ecs_hessenberg_lstsq": (_I, [_VP, _I, _I, _VP, _VP, _VP]),
+    "ecs_state_vel_noalloc": (_I, [_I, _D, _D, _D, _D, _VP, _VP, _VP, _I, _I, _VP]),
 }
 
 _lib = None

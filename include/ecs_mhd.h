@@ -36,7 +36,8 @@ enum {
   ECS_ERR_BAD_MODE = 3,      /* unknown integration mode (loss_functions.py:86-88) */
   ECS_ERR_NOT_COMPLETED = 4, /* adaptive integration hit its step cap (timestepping.py:313,327) */
   ECS_ERR_OOM = 5,           /* device allocation failed */
-  ECS_ERR_UNSUPPORTED = 6    /* grid size / dtype not built */
+  ECS_ERR_UNSUPPORTED = 6,   /* grid size / dtype not built */
+  ECS_ERR_TOO_LARGE = 7      /* beyond the fixed scratch of ecs_state_vel_noalloc */
 };
 
 /* Integration modes of mismatch_RPO (jax_scripts/lib/loss_functions.py:48-88). */
@@ -147,6 +148,22 @@ int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, double* Hcol, lo
 /* y = argmin |H y - b| for the (m+1) x m upper Hessenberg H (column-major,
  * leading dimension ldh >= m+1), m <= 128 (jnp.linalg.lstsq at linalg.py:93). */
 int ecs_hessenberg_lstsq(const double* H, int ldh, int m, const double* b, double* y, void* stream);
+
+/* state_vel without any device allocation.  No counterpart in the reference.
+ * For callers that cannot allocate device memory: a process whose GPU memory is
+ * owned by another allocator (JAX/XLA preallocates most of the device and hands
+ * buffers to custom calls, so a cudaMalloc from a library can fail there) or a
+ * caller that forbids allocation after start-up.  Same computation and layout
+ * as ecs_state_vel (FP64 complex f_hat / dfdt_hat [batch][2][n][n/2+1]); the
+ * physics is passed directly, with `forcing` a DEVICE real [n][n] array on the
+ * grid of construct_domain.  All scratch comes from one fixed ~5 MB device
+ * array in the library, held on every GPU that loads it until exit.
+ * Limits: n in {64, 128}, batch <= 4, else ECS_ERR_TOO_LARGE.  Calls share the
+ * array, so calls that overlap on the GPU race; each call re-initialises what
+ * must start at zero.  The first call on a device does a one-time synchronous
+ * set-up, so make it before any stream capture. */
+int ecs_state_vel_noalloc(int n, double nu, double eta, double b0x, double b0y, const double* forcing,
+                          const void* f_hat, void* dfdt_hat, int batch, int include_dissipation, void* stream);
 
 #ifdef __cplusplus
 }
