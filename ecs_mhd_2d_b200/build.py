@@ -1,17 +1,24 @@
-"""Build libecsmhd.so in-tree for sm_100a with nvcc (no JIT cache)."""
+"""Build libecsmhd.so in-tree for sm_100a with nvcc (no JIT cache).
+
+Every translation unit of csrc/ is compiled in parallel (one per (dtype, n)
+instantiation plus the C-ABI, GMRES and allocation-free units) and linked into
+ecs_mhd_2d_b200/libecsmhd.so; objects go to ecs_mhd_2d_b200/_build/.
+"""
 
 from __future__ import annotations
 
+import concurrent.futures as cf
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libecsmhd.so")
-SOURCES = ["api.cu", "gmres.cu", "noalloc.cu"]
-NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+SOURCES = ["api.cu", "gmres.cu", "noalloc.cu"] + [f"inst_{t}_{n}.cu" for t in ("f64", "f32") for n in (64, 128, 256)]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
 
 def _stale():
@@ -29,7 +36,19 @@ def build(force=False, verbose=False):
     if not force and not _stale():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", OUT + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
+    os.makedirs(OBJ, exist_ok=True)
+
+    def compile_one(src):
+        obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        cmd = [nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [nvcc, *ARCH, "-shared", "-o", OUT + ".tmp", *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

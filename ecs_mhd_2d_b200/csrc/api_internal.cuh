@@ -56,6 +56,20 @@ struct ecs_ctx {
   void* Greg = nullptr; void* Phys = nullptr; size_t reg_items = 0;   // regenerated primal fields
   long* items = nullptr; size_t items_cap = 0;
   double* hacc = nullptr; size_t hacc_bytes = 0;   // adjoint dL/dh accumulators [B][K]
+  // CUDA graph of a chunk of adaptive attempts (replayed on the caller's stream)
+  cudaStream_t cap_stream = nullptr;
+  struct Graph43 {
+    cudaGraphExec_t exec = nullptr;
+    int B = 0, cap = 0;
+    double atol = 0;
+    void* rec = nullptr; double* rec_h = nullptr; int* rec_acc = nullptr;
+    long long nodes = 0;
+  } g43;
+  struct Graph4 {
+    cudaGraphExec_t exec = nullptr;
+    int B = 0;
+    long long nodes = 0;
+  } g4;
   std::string err;
 };
 

@@ -1,0 +1,924 @@
+// Templated host orchestration of the kernels for one (dtype, n): launch
+// helpers, the Impl<R, N> operations and the context initialisation.
+// Included by one instantiation unit per (dtype, n) (inst_*.cu).
+#pragma once
+
+#include "../../include/ecs_mhd.h"
+#include "kernels.cuh"
+#include "kernels_rk43.cuh"
+#include "kernels_tan.cuh"
+#include "kernels_adj.cuh"
+#include "api_internal.cuh"
+#include "impl_table.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+namespace ecs {
+
+constexpr int XT = 8;
+constexpr int COLWARPS = 4;
+
+template <typename R, int N> size_t smem_row_rhs() { return (N / 2 + 10 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N> size_t smem_row_8f() { return (N / 2 + 8 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N> size_t smem_row_2f() { return (N / 2 + 2 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+
+template <typename R, int N>
+int configure_kernels(ecs_ctx* c) {
+  int st = ECS_OK;
+  st |= (int)cudaFuncSetAttribute(k_row_rhs<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_to_box<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_from_box<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_phys<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_8f<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
+  if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
+  return ECS_OK;
+}
+
+template <typename R, int N>
+void launch_row_to_box(ecs_ctx* c, const R* fields, cplx<R>* H, int B, cudaStream_t s) {
+  RowFwdParams<R> p; p.fields = fields; p.H = H; p.tw = (const cplx<R>*)c->tw; p.B = B;
+  ++c->launches; k_row_to_box<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_to_box(ecs_ctx* c, const cplx<R>* H, cplx<R>* V, int B, int nf, cudaStream_t s, long vstride = 0) {
+  ColBoxParams<R> p; p.H = H; p.V = V; p.tw = (const cplx<R>*)c->tw; p.B = B; p.nf = nf;
+  p.vstride = vstride > 0 ? vstride : (long)nf * Geomc<N>::K * Geomc<N>::M;
+  const int cols = B * nf * Geomc<N>::K;
+  ++c->launches; k_col_to_box<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_from_box(ecs_ctx* c, const cplx<R>* V, cplx<R>* G2, int B, const double* sx, int ny, int rot,
+                         int use_sym, int mult_ikx, cudaStream_t s, int sx_shared = 0) {
+  ColFromBoxParams<R> p; p.V = V; p.G = G2; p.tw = (const cplx<R>*)c->tw; p.sx = sx; p.sx_shared = sx_shared;
+  p.sy = (ny * 2 * M_PI) / 8;   // symmetry.py:11 s = (n*2*pi)/8
+  p.odd = (ny % 2 + 2) % 2 == 1; p.rot = rot; p.use_sym = use_sym; p.mult_ikx = mult_ikx; p.B = B;
+  const int cols = B * 2 * Geomc<N>::K;
+  ++c->launches; k_col_from_box<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
+}
+
+template <typename R, int N>
+void launch_row_from_box(ecs_ctx* c, const cplx<R>* G2, R* out, const R* base, double* rowsq, int B, int mode,
+                         cudaStream_t s) {
+  RowFromBoxParams<R> p; p.G = G2; p.out = out; p.base = base; p.rowsq = rowsq; p.tw = (const cplx<R>*)c->tw;
+  p.B = B; p.mode = mode;
+  ++c->launches; k_row_from_box<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStream_t s, cplx<R>* rec = nullptr,
+                    long rec_bstride = 0) {
+  ColParams<R> p;
+  p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.F = (cplx<R>*)c->F; p.A1 = (cplx<R>*)c->A1;
+  p.K2 = (cplx<R>*)c->K2; p.OUT = (cplx<R>*)c->OUT; p.Etab = (const R*)c->Etab; p.ctl = c->ctl;
+  p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.nu = (R)c->nu; p.eta = (R)c->eta;
+  p.B = B; p.stage = stage; p.produce = produce; p.diss = diss; p.rec = rec; p.rec_bstride = rec_bstride;
+  const int cols = B * Geomc<N>::K;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ++c->launches;
+  switch (stage) {
+    case COL_START: k_col_rk4<R, N, COL_START><<<g, bl, 0, s>>>(p); break;
+    case COL_RK4_S1: k_col_rk4<R, N, COL_RK4_S1><<<g, bl, 0, s>>>(p); break;
+    case COL_RK4_S2: k_col_rk4<R, N, COL_RK4_S2><<<g, bl, 0, s>>>(p); break;
+    case COL_RK4_S3: k_col_rk4<R, N, COL_RK4_S3><<<g, bl, 0, s>>>(p); break;
+    case COL_RK4_S4: k_col_rk4<R, N, COL_RK4_S4><<<g, bl, 0, s>>>(p); break;
+    default: k_col_rk4<R, N, COL_PLAIN><<<g, bl, 0, s>>>(p); break;
+  }
+}
+
+template <typename R, int N>
+void launch_row_rhs(ecs_ctx* c, int B, R* phys, cudaStream_t s, const StepCtl* ctl = nullptr) {
+  RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+  p.phys_bstride = 0; p.rec_index = 0; p.phys_stage = 0; p.ctl = ctl;
+  p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
+  ++c->launches; k_row_rhs<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_rk43(ecs_ctx* c, int B, int stage, cudaStream_t s, cplx<R>* rec = nullptr, int cap = 0) {
+  Col43Params<R> p;
+  p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.S = (cplx<R>*)c->S43; p.ctl = c->ctl;
+  p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.rec = rec; p.cap = cap;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
+  const int cols = B * Geomc<N>::K;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ++c->launches;
+  switch (stage) {
+    case R43_START: k_col_rk43<R, N, R43_START><<<g, bl, 0, s>>>(p); break;
+    case R43_INIT: k_col_rk43<R, N, R43_INIT><<<g, bl, 0, s>>>(p); break;
+    case R43_A: k_col_rk43<R, N, R43_A><<<g, bl, 0, s>>>(p); break;
+    case R43_B: k_col_rk43<R, N, R43_B><<<g, bl, 0, s>>>(p); break;
+    case R43_C: k_col_rk43<R, N, R43_C><<<g, bl, 0, s>>>(p); break;
+    case R43_D: k_col_rk43<R, N, R43_D><<<g, bl, 0, s>>>(p); break;
+    default: k_col_rk43<R, N, R43_E><<<g, bl, 0, s>>>(p); break;
+  }
+}
+
+template <typename R, int N>
+void launch_row_err(ecs_ctx* c, int B, double atol, cudaStream_t s, double* rec_h = nullptr, int* rec_acc = nullptr,
+                    int cap = 0) {
+  RowErrParams<R> p; p.G = (const cplx<R>*)c->G; p.ctl = c->ctl; p.tw = (const cplx<R>*)c->tw; p.atol = atol;
+  p.rec_h = rec_h; p.rec_acc = rec_acc; p.cap = cap; p.B = B;
+  ++c->launches; k_row_err<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s) {
+  ColRegenParams<R> p; p.rec = rec; p.items = items; p.G = (cplx<R>*)c->Greg; p.tw = (const cplx<R>*)c->tw;
+  p.nitems = nitems;
+  const int cols = nitems * Geomc<N>::K;
+  ++c->launches; k_col_regen<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
+  RowPhysParams<R> q; q.G = (const cplx<R>*)c->Greg; q.phys = (R*)c->Phys; q.tw = (const cplx<R>*)c->tw;
+  q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.nitems = nitems;
+  ++c->launches; k_row_phys<R, N, XT><<<nitems * (N / XT), XT * 32, smem_row_8f<R, N>(), s>>>(q);
+}
+
+template <typename R, int N>
+void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
+  RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+  p.B = B;
+  ++c->launches; k_row_tan<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* rec, const double* dT, double t,
+                    double h, double dscale, int nslot, cudaStream_t s) {
+  ColTanParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
+  p.rec = rec; p.dT = dT; p.t = t; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage; p.produce = produce;
+  const int cols = B * Geomc<N>::K;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ++c->launches;
+  switch (stage) {
+    case TS_START: k_col_tan<R, N, TS_START><<<g, bl, 0, s>>>(p); break;
+    case T4_S1: k_col_tan<R, N, T4_S1><<<g, bl, 0, s>>>(p); break;
+    case T4_S2: k_col_tan<R, N, T4_S2><<<g, bl, 0, s>>>(p); break;
+    case T4_S3: k_col_tan<R, N, T4_S3><<<g, bl, 0, s>>>(p); break;
+    case T4_S4: k_col_tan<R, N, T4_S4><<<g, bl, 0, s>>>(p); break;
+    case T43_START: k_col_tan<R, N, T43_START><<<g, bl, 0, s>>>(p); break;
+    case T43_INIT: k_col_tan<R, N, T43_INIT><<<g, bl, 0, s>>>(p); break;
+    case T43_A: k_col_tan<R, N, T43_A><<<g, bl, 0, s>>>(p); break;
+    case T43_B: k_col_tan<R, N, T43_B><<<g, bl, 0, s>>>(p); break;
+    case T43_C: k_col_tan<R, N, T43_C><<<g, bl, 0, s>>>(p); break;
+    case T43_D: k_col_tan<R, N, T43_D><<<g, bl, 0, s>>>(p); break;
+    default: k_col_tan<R, N, T43_E><<<g, bl, 0, s>>>(p); break;
+  }
+}
+
+template <typename R, int N>
+void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
+  RowAdjParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+  p.B = B;
+  ++c->launches; k_row_adj<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+}
+
+template <typename R, int N>
+void launch_col_adj(ecs_ctx* c, int B, int stage, const cplx<R>* rec, const cplx<R>* rec_prev, double t, double h,
+                    int nslot, cudaStream_t s) {
+  ColAdjParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.J = (cplx<R>*)c->D; p.nslot = nslot;
+  p.rec = rec; p.rec_prev = rec_prev; p.hacc = c->hacc; p.t = t; p.h = h; p.tw = (const cplx<R>*)c->tw;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
+  const int cols = B * Geomc<N>::K;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ++c->launches;
+  switch (stage) {
+    case AJ_PRE: k_col_adj<R, N, AJ_PRE><<<g, bl, 0, s>>>(p); break;
+    case AJ_S4: k_col_adj<R, N, AJ_S4><<<g, bl, 0, s>>>(p); break;
+    case AJ_S3: k_col_adj<R, N, AJ_S3><<<g, bl, 0, s>>>(p); break;
+    case AJ_S2: k_col_adj<R, N, AJ_S2><<<g, bl, 0, s>>>(p); break;
+    case AJ_S1: k_col_adj<R, N, AJ_S1><<<g, bl, 0, s>>>(p); break;
+    case AJ43_INIT: k_col_adj<R, N, AJ43_INIT><<<g, bl, 0, s>>>(p); break;
+    case AJ43_PRE: k_col_adj<R, N, AJ43_PRE><<<g, bl, 0, s>>>(p); break;
+    case AJ43_S5: k_col_adj<R, N, AJ43_S5><<<g, bl, 0, s>>>(p); break;
+    case AJ43_S4: k_col_adj<R, N, AJ43_S4><<<g, bl, 0, s>>>(p); break;
+    case AJ43_S3: k_col_adj<R, N, AJ43_S3><<<g, bl, 0, s>>>(p); break;
+    case AJ43_S2: k_col_adj<R, N, AJ43_S2><<<g, bl, 0, s>>>(p); break;
+    default: k_col_adj<R, N, AJ43_IPRE><<<g, bl, 0, s>>>(p); break;
+  }
+}
+
+inline int grid1d(long total, int threads = 256) {
+  long g = (total + threads - 1) / threads;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+}  // namespace ecs
+
+// ---------------------------------------------------------------------------
+// per-(dtype, N) implementation
+// ---------------------------------------------------------------------------
+namespace ecs {
+
+template <typename R, int N>
+struct Impl {
+  static constexpr int K = Geomc<N>::K, M = Geomc<N>::M;
+
+  static int to_box(ecs_ctx* c, const R* fields, cplx<R>* box, int B, cudaStream_t s) {
+    launch_row_to_box<R, N>(c, fields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, box, B, 2, s);
+    return cuda_err(c, cudaGetLastError(), "to_box");
+  }
+
+  static int from_box(ecs_ctx* c, const cplx<R>* box, R* fields, int B, cudaStream_t s) {
+    launch_col_from_box<R, N>(c, box, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, fields, nullptr, nullptr, B, 0, s);
+    return cuda_err(c, cudaGetLastError(), "from_box");
+  }
+
+  static int dealias(ecs_ctx* c, const R* fields, R* out, int B, cudaStream_t s) {
+    int st = to_box(c, fields, (cplx<R>*)c->V, B, s);
+    if (st) return st;
+    // mask[0,0] = False: drop the mean mode, then irfft2
+    for (int b = 0; b < B; ++b)
+      for (int ch = 0; ch < 2; ++ch) {
+        cudaError_t e = cudaMemsetAsync((cplx<R>*)c->V + ((size_t)(b * 2 + ch) * K) * M, 0, sizeof(cplx<R>), s);
+        if (e != cudaSuccess) return cuda_err(c, e, "dealias memset");
+      }
+    return from_box(c, (const cplx<R>*)c->V, out, B, s);
+  }
+
+  static int state_vel(ecs_ctx* c, const cplx<R>* fhat, cplx<R>* dfdt, int B, int diss, cudaStream_t s) {
+    const long nbox = (long)B * 2 * K * M;
+    ++c->launches; k_gather_box<R><<<grid1d(nbox), 256, 0, s>>>(fhat, (cplx<R>*)c->F, N, B);
+    launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
+    launch_row_rhs<R, N>(c, B, nullptr, s);
+    launch_col_rk4<R, N>(c, B, COL_PLAIN, 0, diss, s);
+    const long nfull = (long)B * 2 * N * (N / 2 + 1);
+    ++c->launches; k_scatter_box<R><<<grid1d(nfull), 256, 0, s>>>((const cplx<R>*)c->OUT, dfdt, N, B);
+    return cuda_err(c, cudaGetLastError(), "state_vel");
+  }
+
+  // Lawson-RK4 over `steps` steps of the box state in c->F (ctl/Etab prepared).
+  // Chunks of GS steps are captured once into a CUDA graph and replayed.
+  static int integrate_rk4(ecs_ctx* c, int B, long steps, cudaStream_t s) {
+    if (steps <= 0) return ECS_OK;
+    constexpr int GS = 16;
+    auto one_step = [&](cudaStream_t st_, bool last) {
+      for (int st = 1; st <= 4; ++st) {
+        launch_row_rhs<R, N>(c, B, nullptr, st_);
+        launch_col_rk4<R, N>(c, B, st, (st == 4 && last) ? 0 : 1, 0, st_);
+      }
+    };
+    auto& gk = c->g4;
+    if (steps > GS && !(gk.exec && gk.B == B)) {
+      if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
+      const long long l0 = c->launches;
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int a = 0; a < GS; ++a) one_step(c->cap_stream, false);
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&gk.exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) { gk.exec = nullptr; return cuda_err(c, e, "rk4 graph capture"); }
+      gk.nodes = c->launches - l0;
+      c->launches = l0;
+      gk.B = B;
+    }
+    launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
+    long it = 0;
+    while (steps - it > GS) {   // the final step (no inverse transforms) is launched directly
+      cudaError_t e = cudaGraphLaunch(gk.exec, s);
+      if (e != cudaSuccess) return cuda_err(c, e, "rk4 graph launch");
+      c->launches += gk.nodes;
+      it += GS;
+    }
+    for (; it < steps; ++it) one_step(s, it == steps - 1);
+    return cuda_err(c, cudaGetLastError(), "integrate_rk4");
+  }
+
+  static int rk4_setup(ecs_ctx* c, const double* T, int nc, int ms, int B, cudaStream_t s) {
+    const long tot = (long)B * 2 * K * M;
+    ++c->launches; k_rk4_setup<R><<<grid1d(tot), 256, 0, s>>>(T, nc, ms, c->ctl, (R*)c->Etab, N, c->nu, c->eta, B);
+    return cuda_err(c, cudaGetLastError(), "rk4_setup");
+  }
+
+  static int lawson_rk4(ecs_ctx* c, cplx<R>* fhat, double t, int steps, int B, cudaStream_t s) {
+    ++c->launches; k_fill<<<1, 256, 0, s>>>(c->Tbuf, t, B);
+    int st = rk4_setup(c, c->Tbuf, 1, steps, B, s);
+    if (st) return st;
+    const long nbox = (long)B * 2 * K * M;
+    ++c->launches; k_gather_box<R><<<grid1d(nbox), 256, 0, s>>>(fhat, (cplx<R>*)c->F, N, B);
+    st = integrate_rk4(c, B, steps, s);
+    if (st) return st;
+    const long nfull = (long)B * 2 * N * (N / 2 + 1);
+    ++c->launches; k_scatter_box<R><<<grid1d(nfull), 256, 0, s>>>((const cplx<R>*)c->F, fhat, N, B);
+    return cuda_err(c, cudaGetLastError(), "lawson_rk4");
+  }
+
+  // Adaptive Lawson-RK4(3) of the box states in S43[b][S_X0] (timestepping.py:151-335).
+  // Returns after all candidates completed or the attempt cap was reached.
+  static int rk43_solve(ecs_ctx* c, const ecs_shoot_cfg* cfg, const double* T, int B, cudaStream_t s,
+                        cplx<R>* rec = nullptr, double* rec_h = nullptr, int* rec_acc = nullptr, int cap = 0) {
+    const long amax = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
+    if (amax <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
+    ++c->launches; k_rk43_setup<<<(B + 127) / 128, 128, 0, s>>>(T, cfg->h0, c->ctl, B);
+    launch_col_rk43<R, N>(c, B, R43_START, s);
+    launch_row_rhs<R, N>(c, B, nullptr, s, c->ctl);
+    launch_col_rk43<R, N>(c, B, R43_INIT, s);
+    // one attempt = 5 column + 4 row + 1 error launches; a chunk of GA attempts is
+    // captured once into a CUDA graph (all per-attempt data is read from the
+    // device control block, so the same graph replays every chunk)
+    auto attempt = [&](cudaStream_t st_) {
+      launch_col_rk43<R, N>(c, B, R43_A, st_, rec, cap);
+      for (int st = R43_B; st <= R43_E; ++st) {
+        launch_row_rhs<R, N>(c, B, nullptr, st_, c->ctl);
+        launch_col_rk43<R, N>(c, B, st, st_, rec, cap);
+      }
+      launch_row_err<R, N>(c, B, cfg->atol, st_, rec_h, rec_acc, cap);
+    };
+    constexpr int GA = 16;
+    auto& gk = c->g43;
+    const bool same = gk.exec && gk.B == B && gk.atol == cfg->atol && gk.rec == (void*)rec && gk.rec_h == rec_h &&
+                      gk.rec_acc == rec_acc && gk.cap == cap;
+    if (!same && amax >= GA) {
+      if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
+      const long long l0 = c->launches;
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int a = 0; a < GA; ++a) attempt(c->cap_stream);
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&gk.exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) { gk.exec = nullptr; return cuda_err(c, e, "rk43 graph capture"); }
+      gk.nodes = c->launches - l0;
+      c->launches = l0;
+      gk.B = B; gk.atol = cfg->atol; gk.rec = rec; gk.rec_h = rec_h; gk.rec_acc = rec_acc; gk.cap = cap;
+    }
+    long a = 0;
+    while (a < amax) {
+      if (gk.exec && amax - a >= GA) {
+        cudaError_t e = cudaGraphLaunch(gk.exec, s);
+        if (e != cudaSuccess) return cuda_err(c, e, "rk43 graph launch");
+        c->launches += gk.nodes;
+        a += GA;
+      } else {
+        attempt(s);
+        a += 1;
+        if (a % GA != 0 && a != amax) continue;
+      }
+      ++c->launches; k_count_done<<<1, 32, 0, s>>>(c->ctl, c->dcount, B);
+      cudaError_t e = cudaMemcpyAsync(c->hcount, c->dcount, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return cuda_err(c, e, "rk43 completion check");
+      if (*c->hcount == B) break;
+    }
+    const long nbox = (long)B * 2 * K * M;
+    ++c->launches; k_rk43_resolve<R><<<grid1d(nbox), 256, 0, s>>>((cplx<R>*)c->S43, c->ctl, (cplx<R>*)c->F, N, B);
+    return cuda_err(c, cudaGetLastError(), "rk43_solve");
+  }
+
+  // Forward shooting map + symmetries + residual (objective_RPO / loss_RPO).
+  static int shoot(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                   R* out_fields, double* loss, ecs_info* info, int B, cudaStream_t s) {
+    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
+    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43)
+      return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");   // loss_functions.py:86-88
+    int st;
+    const long VEC = 2L * K * M;
+    if (!rk43) {
+      if (cfg->num_checkpoints <= 0 || cfg->ministeps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+      st = to_box(c, fields, (cplx<R>*)c->F, B, s);
+      if (st) return st;
+      st = rk4_setup(c, T, cfg->num_checkpoints, cfg->ministeps, B, s);
+      if (st) return st;
+      st = integrate_rk4(c, B, (long)cfg->num_checkpoints * cfg->ministeps, s);
+      if (st) return st;
+    } else {
+      launch_row_to_box<R, N>(c, fields, (cplx<R>*)c->H, B, s);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->S43 + S_X0 * VEC, B, 2, s, S_NSLOT * VEC);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->V, B, 2, s);
+      st = rk43_solve(c, cfg, T, B, s);
+      if (st) return st;
+    }
+    R* out = out_fields ? out_fields : (R*)c->fields_tmp;
+    if (rk43) {   // modes outside the box are carried unchanged by the unmasked integrating factor
+      launch_col_from_box<R, N>(c, (const cplx<R>*)c->V, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+      launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)c->fields_tmp2, fields, nullptr, B, 1, s);
+    }
+    launch_col_from_box<R, N>(c, (const cplx<R>*)c->F, (cplx<R>*)c->G, B, sx, cfg->shift_reflect_ny, cfg->rot, 1, 0, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, out, fields, nullptr, B, 1, s);
+    if (rk43) {
+      const int odd = (cfg->shift_reflect_ny % 2 + 2) % 2 == 1;
+      ++c->launches; k_sub_sym_phys<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>(out, (const R*)c->fields_tmp2, odd, cfg->rot, N, B);
+    }
+    if (loss) {
+      ++c->launches; k_rowsq<R><<<B * N, 32, 0, s>>>(out, c->rowsq, N);
+      ++c->launches; k_reduce_rows<<<(B + 127) / 128, 128, 0, s>>>(c->rowsq, loss, N, B, 1.0 / (2.0 * N * N));
+    }
+    st = cuda_err(c, cudaGetLastError(), "shoot");
+    if (st) return st;
+    if (info) {
+      if (rk43) {
+        std::vector<StepCtl> h(B);
+        cudaError_t e = cudaMemcpyAsync(h.data(), c->ctl, sizeof(StepCtl) * B, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_err(c, e, "info readback");
+        for (int b = 0; b < B; ++b) {
+          info[b].completed = h[b].done; info[b].s = h[b].s; info[b].accepted = h[b].accepted;
+          info[b].rejected = h[b].rejected; info[b].fevals = h[b].fevals;
+        }
+      } else {
+        const int steps = cfg->num_checkpoints * cfg->ministeps;
+        for (int b = 0; b < B; ++b) {
+          info[b].completed = 1; info[b].s = 1.0; info[b].accepted = steps; info[b].rejected = 0;
+          info[b].fevals = 4 * steps;
+        }
+      }
+    }
+    return ECS_OK;
+  }
+
+  // ---------------------------------------------------------------------
+  // Linearisation: primal solve of one candidate with its trajectory record,
+  // plus the stop-gradient phase fields vt, vx (loss_functions.py:113-130).
+  // ---------------------------------------------------------------------
+  static int linearize(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                       R* out_fields, ecs_info* info, cudaStream_t s) {
+    auto& L = c->lin;
+    L.valid = 0;
+    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
+    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43) return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>), fb = 2UL * N * N * sizeof(R);
+    int st = ECS_OK;
+    size_t dummy = 0;
+    if (!L.phi) {
+      L.phi = dev_alloc(c, vb, &st); L.f0box = dev_alloc(c, vb, &st);
+      L.vt = dev_alloc(c, fb, &st); L.vx = dev_alloc(c, fb, &st);
+      L.dsx = (double*)dev_alloc(c, 64, &st); L.dT = (double*)dev_alloc(c, 64, &st);
+      if (st) return st;
+    }
+    (void)dummy;
+    double hT = 0, hsx = 0;
+    cudaError_t e = cudaMemcpyAsync(&hT, T, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hsx, sx, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.dsx, sx, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(L.dT, T, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(c, e, "linearize scalars");
+    L.T = hT; L.sx = hsx; L.cfg = *cfg; L.mode = cfg->mode;
+    // f0 box and the phase fields
+    st = to_box(c, fields, (cplx<R>*)L.f0box, 1, s);
+    if (st) return st;
+    cudaMemcpyAsync(c->F, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+    launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, s);
+    launch_row_rhs<R, N>(c, 1, nullptr, s);
+    launch_col_rk4<R, N>(c, 1, COL_PLAIN, 0, 1, s);
+    st = from_box(c, (const cplx<R>*)c->OUT, (R*)L.vt, 1, s);
+    if (st) return st;
+    launch_col_from_box<R, N>(c, (const cplx<R>*)L.f0box, (cplx<R>*)c->G, 1, nullptr, 0, 0, 0, 1, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)L.vx, nullptr, nullptr, 1, 0, s);
+    if (!rk43) {
+      const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
+      if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+      st = grow(c, &L.rec, &L.rec_bytes, (size_t)steps * Q_NREC * vb);
+      if (st) return st;
+      cudaMemcpyAsync(c->F, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+      st = rk4_setup(c, T, cfg->num_checkpoints, cfg->ministeps, 1, s);
+      if (st) return st;
+      launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, s);
+      for (long it = 0; it < steps; ++it) {
+        cplx<R>* rs = (cplx<R>*)L.rec + (size_t)it * Q_NREC * VEC;
+        for (int k = 1; k <= 4; ++k) {
+          launch_row_rhs<R, N>(c, 1, nullptr, s);
+          launch_col_rk4<R, N>(c, 1, k, (k == 4 && it == steps - 1) ? 0 : 1, 0, s, rs, 0);
+        }
+      }
+      L.nrec = steps;
+      L.h = (double)(R)((hT / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
+      cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
+      if (info) { info->completed = 1; info->s = 1.0; info->accepted = (int)steps; info->rejected = 0; info->fevals = (int)(4 * steps); }
+    } else {
+      const long cap = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
+      if (cap <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
+      st = grow(c, &L.rec, &L.rec_bytes, (size_t)cap * RR_NREC * vb);
+      if (st) return st;
+      if ((size_t)cap > L.cap) {
+        if (L.rec_h) { cudaFree(L.rec_h); cudaFree(L.rec_acc); }
+        if (cudaMalloc(&L.rec_h, cap * sizeof(double)) != cudaSuccess || cudaMalloc(&L.rec_acc, cap * sizeof(int)) != cudaSuccess)
+          return set_err(c, ECS_ERR_OOM, "record allocation");
+        L.cap = cap;
+      }
+      cudaMemcpyAsync((cplx<R>*)c->S43 + S_X0 * VEC, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+      st = rk43_solve(c, cfg, T, 1, s, (cplx<R>*)L.rec, L.rec_h, L.rec_acc, (int)cap);
+      if (st) return st;
+      cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
+      StepCtl hc;
+      e = cudaMemcpyAsync(&hc, c->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return cuda_err(c, e, "linearize readback");
+      L.nrec = hc.attempts;
+      L.acc.assign(L.nrec, 0); L.hs.assign(L.nrec, 0.0);
+      if (L.nrec > 0) {
+        e = cudaMemcpy(L.acc.data(), L.rec_acc, L.nrec * sizeof(int), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(L.hs.data(), L.rec_h, L.nrec * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_err(c, e, "linearize record readback");
+      }
+      if (info) { info->completed = hc.done; info->s = hc.s; info->accepted = hc.accepted; info->rejected = hc.rejected; info->fevals = hc.fevals; }
+    }
+    if (out_fields) {
+      st = residual(c, cfg, fields, (const cplx<R>*)L.phi, (const cplx<R>*)L.f0box, L.dsx, 1, out_fields, s, 1);
+      if (st) return st;
+    }
+    L.valid = 1;
+    return cuda_err(c, cudaGetLastError(), "linearize");
+  }
+
+  // out = base - irfft2(sym(Phi)) [- P_sym(base - irfft2(box(base))) in Lawson-RK4(3) mode]
+  static int residual(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* base, const cplx<R>* phi, const cplx<R>* basebox,
+                      const double* sx, int B, R* out, cudaStream_t s, int sx_shared) {
+    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
+    if (rk43) {
+      launch_col_from_box<R, N>(c, basebox, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+      launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)c->fields_tmp2, base, nullptr, B, 1, s);
+    }
+    launch_col_from_box<R, N>(c, phi, (cplx<R>*)c->G, B, sx, cfg->shift_reflect_ny, cfg->rot, 1, 0, s, sx_shared);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, out, base, nullptr, B, 1, s);
+    if (rk43) {
+      const int odd = (cfg->shift_reflect_ny % 2 + 2) % 2 == 1;
+      ++c->launches; k_sub_sym_phys<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>(out, (const R*)c->fields_tmp2, odd, cfg->rot, N, B);
+    }
+    return cuda_err(c, cudaGetLastError(), "residual");
+  }
+
+  // Regeneration plan for the primal physical fields (offsets in box vectors).
+  static int upload_items(ecs_ctx* c, const std::vector<long>& items) {
+    if (items.size() > c->items_cap) {
+      if (c->items) cudaFree(c->items);
+      if (cudaMalloc(&c->items, items.size() * sizeof(long)) != cudaSuccess) { c->items = nullptr; c->items_cap = 0; return set_err(c, ECS_ERR_OOM, "items"); }
+      c->items_cap = items.size();
+    }
+    return cuda_err(c, cudaMemcpy(c->items, items.data(), items.size() * sizeof(long), cudaMemcpyHostToDevice), "items upload");
+  }
+
+  static size_t chunk_items() {
+    const size_t per = (size_t)8 * K * N * sizeof(cplx<R>) + (size_t)N * 8 * N * sizeof(R);
+    size_t c = ((size_t)384 << 20) / per;
+    return c < 8 ? 8 : (c > 512 ? 512 : c);
+  }
+
+  static int ensure_regen(ecs_ctx* c) {
+    const size_t ci = chunk_items();
+    if (c->reg_items >= ci && c->Greg) return ECS_OK;
+    size_t have1 = c->Greg ? 1 : 0, have2 = have1;
+    (void)have2;
+    if (c->Greg) { cudaFree(c->Greg); cudaFree(c->Phys); c->Greg = c->Phys = nullptr; }
+    size_t h1 = 0, h2 = 0;
+    int st = grow(c, &c->Greg, &h1, ci * 8 * K * N * sizeof(cplx<R>));
+    if (!st) st = grow(c, &c->Phys, &h2, ci * N * 8 * N * sizeof(R));
+    if (st) return st;
+    (void)have1;
+    c->reg_items = ci;
+    return ECS_OK;
+  }
+
+  // ---------------------------------------------------------------------
+  // JVP of objective_RPO at the current linearisation for B tangents.
+  // ---------------------------------------------------------------------
+  static int jvp(ecs_ctx* c, const R* dfields, const double* dT, const double* dsx, R* out, double* odT, double* odsx,
+                 int B, cudaStream_t s) {
+    auto& L = c->lin;
+    if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
+    int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = ensure_regen(c);
+    if (st) return st;
+    // tangent initial state: box(dfields) into slot X0 (RK4(3)) or F (RK4)
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)(rk43 ? (int)S_X0 : (int)D_F) * VEC, B, 2, s,
+                            (long)nslot * VEC);
+    // regeneration plan
+    std::vector<long> items;
+    std::vector<long> item_of;   // first item index per step / attempt (-1 if none)
+    if (!rk43) {
+      for (long a = 0; a < L.nrec; ++a) {
+        item_of.push_back((long)items.size());
+        const long base = a * Q_NREC;
+        items.push_back(base + Q_F); items.push_back(base + Q_X2); items.push_back(base + Q_X3); items.push_back(base + Q_X4);
+      }
+    } else {
+      items.push_back(RR_X0);   // x0 of attempt 0 (initial k1)
+      for (long a = 0; a < L.nrec; ++a) {
+        if (!L.acc[a]) { item_of.push_back(-1); continue; }
+        item_of.push_back((long)items.size());
+        const long base = a * RR_NREC;
+        items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
+      }
+    }
+    st = upload_items(c, items);
+    if (st) return st;
+    const long ci = (long)chunk_items();
+    long chunk_lo = -1;
+    auto phys_of = [&](long item) -> const R* {
+      if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+        chunk_lo = item;
+        const long cnt = std::min<long>(ci, (long)items.size() - item);
+        launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + item, (int)cnt, s);
+      }
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * 8 * N;
+    };
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    if (!rk43) {
+      const double dscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
+      launch_col_tan<R, N>(c, B, TS_START, 1, rec, dT, 0.0, L.h, dscale, nslot, s);
+      for (long a = 0; a < L.nrec; ++a) {
+        const cplx<R>* ra = rec + (size_t)a * Q_NREC * VEC;
+        for (int k = 1; k <= 4; ++k) {
+          launch_row_tan<R, N>(c, B, phys_of(item_of[a] + (k - 1)), s);
+          launch_col_tan<R, N>(c, B, k, (k == 4 && a == L.nrec - 1) ? 0 : 1, ra, dT, 0.0, L.h, dscale, nslot, s);
+        }
+      }
+    } else {
+      const double t = L.T;
+      launch_col_tan<R, N>(c, B, T43_START, 1, rec, dT, t, 0.0, 1.0, nslot, s);
+      launch_row_tan<R, N>(c, B, phys_of(0), s);
+      launch_col_tan<R, N>(c, B, T43_INIT, 0, rec, dT, t, 0.0, 1.0, nslot, s);
+      for (long a = 0; a < L.nrec; ++a) {
+        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
+        const double h = L.hs[a];
+        if (!L.acc[a]) {
+          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, t, h, (R)c->nu,
+                                                                (R)c->eta, N, B);
+          continue;
+        }
+        launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
+        for (int k = 0; k < 4; ++k) {
+          launch_row_tan<R, N>(c, B, phys_of(item_of[a] + k), s);
+          launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
+        }
+      }
+    }
+    // output: d fields = dfields - irfft2(sym(dPhi + i kx dsx Phi)) [- rest term]
+    ++c->launches; k_tan_shift<R><<<grid1d((long)B * VEC), 256, 0, s>>>((const cplx<R>*)c->D + (size_t)(rk43 ? (int)S_X0 : (int)D_F) * VEC,
+                                                         (long)nslot * VEC, (const cplx<R>*)L.phi, dsx,
+                                                         (cplx<R>*)c->V, N, B);
+    if (rk43) {   // box(dfields) for the rest term
+      launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->OUT, B, 2, s);
+    }
+    st = residual(c, &L.cfg, dfields, (const cplx<R>*)c->V, (const cplx<R>*)c->OUT, L.dsx, B, out, s, 1);
+    if (st) return st;
+    ++c->launches; k_phase_dot<R><<<B, 256, 0, s>>>((const R*)L.vt, (const R*)L.vx, dfields, odT, odsx, N);
+    return cuda_err(c, cudaGetLastError(), "jvp");
+  }
+
+  // ---------------------------------------------------------------------
+  // VJP of objective_RPO at the current linearisation for B cotangents.
+  // ---------------------------------------------------------------------
+  static int vjp(ecs_ctx* c, const R* cfields, const double* cT, const double* csx, R* gfields, double* gT,
+                 double* gsx, int B, cudaStream_t s) {
+    auto& L = c->lin;
+    if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const int nslot = rk43 ? (int)JJ_NS43 : (int)J_NS4;
+    int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = ensure_regen(c);
+    if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * sizeof(double));
+    if (st) return st;
+    cudaMemsetAsync(c->D, 0, (size_t)B * nslot * vb, s);
+    cudaMemsetAsync(c->hacc, 0, (size_t)B * K * sizeof(double), s);
+    // head: Ybar = -(c/n^2) rfft2(c_fields) on the box; Phibar = sym^T(Ybar); sxbar
+    launch_row_to_box<R, N>(c, cfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->V, B, 2, s);
+    ++c->launches; k_box_scale_c<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->V, (long)VEC, N, B, R(-1) / (R(N) * R(N)));
+    const int odd = (L.cfg.shift_reflect_ny % 2 + 2) % 2 == 1;
+    const double sy = (L.cfg.shift_reflect_ny * 2 * M_PI) / 8;
+    ++c->launches; k_adj_head<R><<<B, 256, 0, s>>>((const cplx<R>*)c->V, (const cplx<R>*)L.phi, L.dsx, 1, sy, odd, L.cfg.rot,
+                                     (cplx<R>*)c->D + (size_t)(rk43 ? (int)JJ_X0 : (int)J_OB) * VEC, (long)nslot * VEC,
+                                     gsx, N);
+    // regeneration plan (reverse order of use)
+    std::vector<long> items;
+    std::vector<long> item_of;
+    if (!rk43) {
+      for (long a = 0; a < L.nrec; ++a) {
+        item_of.push_back((long)items.size());
+        const long base = a * Q_NREC;
+        items.push_back(base + Q_F); items.push_back(base + Q_X2); items.push_back(base + Q_X3); items.push_back(base + Q_X4);
+      }
+    } else {
+      items.push_back(RR_X0);
+      for (long a = 0; a < L.nrec; ++a) {
+        if (!L.acc[a]) { item_of.push_back(-1); continue; }
+        item_of.push_back((long)items.size());
+        const long base = a * RR_NREC;
+        items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
+      }
+    }
+    st = upload_items(c, items);
+    if (st) return st;
+    const long ci = (long)chunk_items();
+    long chunk_lo = -1;
+    auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
+      if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+        chunk_lo = std::max<long>(0, item - ci + 1);
+        const long cnt = std::min<long>(ci, (long)items.size() - chunk_lo);
+        launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + chunk_lo, (int)cnt, s);
+      }
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * 8 * N;
+    };
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    double tscale;
+    if (!rk43) {
+      tscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
+      const double h = L.h;
+      launch_col_adj<R, N>(c, B, AJ_PRE, rec + (size_t)(L.nrec - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
+      for (long a = L.nrec - 1; a >= 0; --a) {
+        const cplx<R>* ra = rec + (size_t)a * Q_NREC * VEC;
+        const cplx<R>* rp = a > 0 ? rec + (size_t)(a - 1) * Q_NREC * VEC : nullptr;
+        for (int k = 4; k >= 1; --k) {
+          launch_row_adj<R, N>(c, B, phys_of(item_of[a] + (k - 1)), s);
+          launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
+        }
+      }
+    } else {
+      tscale = 1.0;
+      const double t = L.T;
+      for (long a = L.nrec - 1; a >= 0; --a) {
+        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
+        const double h = L.hs[a];
+        if (!L.acc[a]) {
+          const int cols = B * K;
+          ++c->launches; k_adj_reject<R><<<(cols + 3) / 4, 128, 0, s>>>((cplx<R>*)c->D, nslot, ra, c->hacc, t, h, (R)c->nu, (R)c->eta, N, B);
+          continue;
+        }
+        launch_col_adj<R, N>(c, B, AJ43_PRE, ra, nullptr, t, h, nslot, s);
+        for (int k = 3; k >= 0; --k) {
+          launch_row_adj<R, N>(c, B, phys_of(item_of[a] + k), s);
+          launch_col_adj<R, N>(c, B, AJ43_S2 + k, ra, nullptr, t, h, nslot, s);
+        }
+      }
+      launch_col_adj<R, N>(c, B, AJ43_IPRE, rec, nullptr, t, 0.0, nslot, s);
+      launch_row_adj<R, N>(c, B, phys_of(0), s);
+      launch_col_adj<R, N>(c, B, AJ43_INIT, rec, nullptr, t, 0.0, nslot, s);
+    }
+    // tail: gfields = c_fields + to_box^T(fbar0) [- (I - proj) P_sym c_fields] + phase terms
+    ++c->launches; k_box_to_fields_adj<R><<<grid1d((long)B * VEC), 256, 0, s>>>(
+        (const cplx<R>*)c->D + (size_t)(rk43 ? (int)JJ_X0 : (int)J_OB) * VEC, (long)nslot * VEC, (cplx<R>*)c->V, N, B);
+    launch_col_from_box<R, N>(c, (const cplx<R>*)c->V, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, gfields, cfields, nullptr, B, 2, s);
+    if (rk43) {
+      // tmp = P_sym c  (k_sub_sym_phys computes out -= P_sym(rest); start from zero)
+      cudaMemsetAsync(c->fields_tmp, 0, (size_t)B * 2 * N * N * sizeof(R), s);
+      ++c->launches; k_sub_sym_phys<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>((R*)c->fields_tmp, cfields, odd, L.cfg.rot, N, B);
+      // fields_tmp = -P c ; (I - proj)(-P c) = fields_tmp - from_box(to_box(fields_tmp)); g += that
+      launch_row_to_box<R, N>(c, (const R*)c->fields_tmp, (cplx<R>*)c->H, B, s);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->OUT, B, 2, s);
+      launch_col_from_box<R, N>(c, (const cplx<R>*)c->OUT, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+      launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)c->fields_tmp2, (const R*)c->fields_tmp, nullptr, B, 1, s);
+      ++c->launches; k_axpy<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>(gfields, (const R*)c->fields_tmp2, R(1), (long)B * 2 * N * N);
+    }
+    ++c->launches; k_adj_phase<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>(gfields, (const R*)L.vt, (const R*)L.vx, cT, csx, N, B);
+    ++c->launches; k_reduce_hacc<<<(B + 127) / 128, 128, 0, s>>>(c->hacc, K, tscale, gT, B);
+    return cuda_err(c, cudaGetLastError(), "vjp");
+  }
+
+  // Time `iters` launches of one hot kernel on the current workspace (after a
+  // jvp call) with CUDA events on stream s; returns ms per launch and the
+  // kernel's algorithmic bytes per launch.
+  static int bench_kernel(ecs_ctx* c, int which, int B, int iters, float* ms, double* bytes, cudaStream_t s) {
+    auto& L = c->lin;
+    if (!L.valid || !c->Phys || !c->D) return set_err(c, ECS_ERR_INVALID, "bench_kernel needs a prior ecs_jvp call");
+    const size_t VEC = 2UL * K * M, cb = sizeof(cplx<R>), rb = sizeof(R);
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
+    cudaMemsetAsync(c->Tbuf, 0, sizeof(double) * B, s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    auto launch = [&]() {
+      if (which == 0) launch_row_tan<R, N>(c, B, (const R*)c->Phys, s);
+      else if (rk43) launch_col_tan<R, N>(c, B, T43_B, 1, (const cplx<R>*)L.rec, c->Tbuf, L.T, L.h, 1.0, nslot, s);
+      else launch_col_tan<R, N>(c, B, T4_S2, 1, (const cplx<R>*)L.rec, c->Tbuf, 0.0, L.h, 1.0, nslot, s);
+    };
+    launch();
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < iters; ++i) launch();
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0; cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_err(c, e, "bench_kernel");
+    *ms = t / iters;
+    if (which == 0) *bytes = (double)B * (8 + 2) * K * N * cb + (double)N * 8 * N * rb;
+    else *bytes = (double)B * (2 * K * N * cb + 8 * K * N * cb + 2 * VEC * cb) + (double)VEC * cb;
+    return ECS_OK;
+  }
+};
+
+}  // namespace ecs
+
+namespace ecs {
+template <typename R, int N>
+int ctx_init(ecs_ctx* c, const ecs_params* prm) {
+  int st = configure_kernels<R, N>(c);
+  if (st) return st;
+  const int B = c->max_batch;
+  const size_t cb = sizeof(cplx<R>), rb = sizeof(R);
+  const size_t nbox = (size_t)B * 2 * Geomc<N>::K * Geomc<N>::M;
+  c->F = dev_alloc(c, nbox * cb, &st);
+  c->A1 = dev_alloc(c, nbox * cb, &st);
+  c->K2 = dev_alloc(c, nbox * cb, &st);
+  c->OUT = dev_alloc(c, nbox * cb, &st);
+  c->V = dev_alloc(c, nbox * cb, &st);
+  c->Etab = dev_alloc(c, nbox * rb, &st);
+  c->G = dev_alloc(c, (size_t)B * 8 * Geomc<N>::K * N * cb, &st);
+  c->H = dev_alloc(c, (size_t)B * 8 * Geomc<N>::K * N * cb, &st);
+  c->fields_tmp = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
+  c->fields_tmp2 = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
+  c->S43 = dev_alloc(c, nbox * S_NSLOT * cb, &st);
+  c->dcount = (int*)dev_alloc(c, sizeof(int), &st);
+  c->ctl = (StepCtl*)dev_alloc(c, (size_t)B * sizeof(StepCtl), &st);
+  c->rowsq = (double*)dev_alloc(c, (size_t)B * N * sizeof(double), &st);
+  c->Tbuf = (double*)dev_alloc(c, (size_t)B * sizeof(double), &st);
+  c->tw = dev_alloc(c, (N / 2) * cb, &st);
+  c->fhat = dev_alloc(c, (size_t)Geomc<N>::K * Geomc<N>::M * cb, &st);
+  if (st) return st;
+  if (cudaMallocHost((void**)&c->hcount, sizeof(int)) != cudaSuccess) return set_err(c, ECS_ERR_OOM, "pinned alloc");
+  if (cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return set_err(c, ECS_ERR_CUDA, "capture stream");
+  // twiddles exp(-2 pi i k/N), k < N/2, from long double
+  std::vector<cplx<R>> tw(N / 2);
+  const long double twopi = 6.283185307179586476925286766559005768L;
+  for (int k = 0; k < N / 2; ++k) {
+    long double a = twopi * (long double)k / (long double)N;
+    tw[k] = mk<R>((R)cosl(a), (R)(-sinl(a)));
+  }
+  cudaError_t e = cudaMemcpy(c->tw, tw.data(), tw.size() * cb, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_err(c, e, "twiddle upload");
+  // forcing on the grid x_i = i/n * 2 * pi (mhd_jax.py:47), channel omega only
+  std::vector<R> fr((size_t)2 * N * N, R(0));
+  const double pi_lit = 3.14159265358979323846;
+  for (int i = 0; i < N; ++i)
+    for (int jy = 0; jy < N; ++jy) {
+      double v;
+      if (prm->forcing) v = prm->forcing[(size_t)i * N + jy];
+      else {
+        const double y = (double)jy / N * 2 * pi_lit;
+        v = prm->kolmogorov_amp * cos(prm->kolmogorov_k * y);
+      }
+      fr[(size_t)i * N + jy] = (R)v;
+    }
+  e = cudaMemcpy(c->fields_tmp, fr.data(), fr.size() * rb, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_err(c, e, "forcing upload");
+  st = Impl<R, N>::to_box(c, (const R*)c->fields_tmp, (cplx<R>*)c->V, 1, 0);
+  if (st) return st;
+  // channel-omega box with mask[0,0] = False
+  e = cudaMemcpy(c->fhat, c->V, (size_t)Geomc<N>::K * Geomc<N>::M * cb, cudaMemcpyDeviceToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->fhat, 0, cb);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  return cuda_err(c, e, "forcing spectrum");
+}
+}  // namespace ecs
+
+namespace ecs {
+
+// Function table of one (dtype, n): the C entry points dispatch through it.
+template <typename R, int N>
+ImplTable make_table() {
+  using I = Impl<R, N>;
+  ImplTable t;
+  t.init = [](ecs_ctx* c, const ecs_params* p) { return ctx_init<R, N>(c, p); };
+  t.to_box = [](ecs_ctx* c, const void* f, void* b, int B, cudaStream_t s) {
+    return I::to_box(c, (const R*)f, (cplx<R>*)b, B, s); };
+  t.from_box = [](ecs_ctx* c, const void* b, void* f, int B, cudaStream_t s) {
+    return I::from_box(c, (const cplx<R>*)b, (R*)f, B, s); };
+  t.dealias = [](ecs_ctx* c, const void* f, void* o, int B, cudaStream_t s) {
+    return I::dealias(c, (const R*)f, (R*)o, B, s); };
+  t.state_vel = [](ecs_ctx* c, const void* f, void* o, int B, int d, cudaStream_t s) {
+    return I::state_vel(c, (const cplx<R>*)f, (cplx<R>*)o, B, d, s); };
+  t.lawson_rk4 = [](ecs_ctx* c, void* f, double t_, int st, int B, cudaStream_t s) {
+    return I::lawson_rk4(c, (cplx<R>*)f, t_, st, B, s); };
+  t.shoot = [](ecs_ctx* c, const ecs_shoot_cfg* cfg, const void* f, const double* T, const double* sx, void* o,
+               double* loss, ecs_info* info, int B, cudaStream_t s) {
+    return I::shoot(c, cfg, (const R*)f, T, sx, (R*)o, loss, info, B, s); };
+  t.linearize = [](ecs_ctx* c, const ecs_shoot_cfg* cfg, const void* f, const double* T, const double* sx, void* o,
+                   ecs_info* info, cudaStream_t s) {
+    return I::linearize(c, cfg, (const R*)f, T, sx, (R*)o, info, s); };
+  t.jvp = [](ecs_ctx* c, const void* df, const double* dT, const double* dsx, void* o, double* oT, double* osx, int B,
+             cudaStream_t s) { return I::jvp(c, (const R*)df, dT, dsx, (R*)o, oT, osx, B, s); };
+  t.vjp = [](ecs_ctx* c, const void* cf, const double* cT, const double* csx, void* g, double* gT, double* gsx, int B,
+             cudaStream_t s) { return I::vjp(c, (const R*)cf, cT, csx, (R*)g, gT, gsx, B, s); };
+  t.bench_kernel = [](ecs_ctx* c, int which, int B, int iters, float* ms, double* bytes, cudaStream_t s) {
+    return I::bench_kernel(c, which, B, iters, ms, bytes, s); };
+  return t;
+}
+
+}  // namespace ecs

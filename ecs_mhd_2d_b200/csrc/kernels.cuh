@@ -92,10 +92,11 @@ __device__ __forceinline__ void col_inverse8(const cplx<R> (&x0)[N / 32], const 
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
   const R inv_n2 = R(1) / (R(N) * R(N));
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
+  // one copy of the transform code: the (c, m) loop is not unrolled
+#pragma unroll 1
+  for (int cm = 0; cm < 8; ++cm) {
+    const int c = cm >> 2, m = cm & 3;
+    {
       cplx<R> w[E];
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -171,7 +172,7 @@ struct ColParams {
   long rec_bstride;      // elements between batch elements in rec
 };
 
-template <typename R, int N>
+template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   const int b = col / K, ky = col - b * K;
 
   cplx<R> r0[E], r1[E];
-  if (p.stage != COL_START) {
+  if (STAGE != COL_START) {
     const cplx<R>* h0 = p.H + ((size_t)(b * 2 + 0) * K + ky) * N;
     const cplx<R>* h1 = p.H + ((size_t)(b * 2 + 1) * K + ky) * N;
 #pragma unroll
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
     cplx<R> v0 = mk<R>(0, 0), v1 = mk<R>(0, 0);
-    if (p.stage != COL_START) {
+    if (STAGE != COL_START) {
       if (in_mask) v0 = cadd(r0[j], p.fhat[ky * M + slot]);   // mask * rfft2(-adv0+adv1+forcing)
       v1 = cscale(r1[j], ksq_masked<R>(kx, ky));                // k^2 mask * rfft2(u x B)
     }
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
     auto put = [&](int q, cplx<R> a0, cplx<R> a1) {
       if (rb) { rb[q * VEC + o0] = a0; rb[q * VEC + o1] = a1; }
     };
-    switch (p.stage) {
+    switch (STAGE) {
       case COL_START: {
         x0[j] = p.F[i0]; x1[j] = p.F[i1];
       } break;

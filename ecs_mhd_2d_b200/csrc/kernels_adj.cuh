@@ -114,7 +114,7 @@ struct ColAdjParams {
 
 __device__ __forceinline__ double rdot2(double ax, double ay, double bx, double by) { return ax * bx + ay * by; }
 
-template <typename R, int N>
+template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   cplx<R>* J = p.J + (size_t)b * p.nslot * VEC;
   const cplx<R>* Q = p.rec;
   const R h = (R)p.h, t = (R)p.t;
-  const bool rk43 = p.stage >= AJ43_INIT;
-  const bool has_rhs = !(p.stage == AJ_PRE || p.stage == AJ43_PRE || p.stage == AJ43_IPRE);
+  const bool rk43 = STAGE >= AJ43_INIT;
+  const bool has_rhs = !(STAGE == AJ_PRE || STAGE == AJ43_PRE || STAGE == AJ43_IPRE);
   const R cky = ky == 0 ? R(1) : R(2);
   const R inv_n2 = R(1) / (R(N) * R(N));
 
@@ -139,10 +139,10 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
 #pragma unroll
   for (int j = 0; j < E; ++j) { xb0[j] = mk<R>(0, 0); xb1[j] = mk<R>(0, 0); }
   if (has_rhs) {
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
+#pragma unroll 1
+    for (int cm = 0; cm < 8; ++cm) {
+      const int c = cm >> 2, m = cm & 3;
+      {
         const cplx<R>* hin = p.H + ((size_t)(b * 8 + 4 * c + m) * K + ky) * N;
         cplx<R> v[E];
 #pragma unroll
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
         const R e = in_mask ? exp(h / R(2) * L) : R(0);
         const R dedh = e * L / R(2);
         auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
-        switch (p.stage) {
+        switch (STAGE) {
           case AJ_PRE: {
             const cplx<R> ob = J[J_OB * VEC + o];
             J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_r(ob, R(6));
@@ -233,11 +233,11 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
         const R e = exp((t * L) * h / R(2));
         const R dedt = e * (L * h / R(2));
         auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
-        switch (p.stage) {
+        switch (STAGE) {
           case AJ43_PRE:      // from (xbar_f, k5bar) in (X0, K1) slots: RHS5 input = k5bar
           case AJ43_IPRE: {   // initial k1 = t v(x0): input = k1bar
             kb = J[JJ_K1 * VEC + o];
-            hpart += ip(kb, Q[(p.stage == AJ43_PRE ? RR_K5 : RR_K1) * VEC + o]) / (double)t;
+            hpart += ip(kb, Q[(STAGE == AJ43_PRE ? RR_K5 : RR_K1) * VEC + o]) / (double)t;
           } break;
           case AJ43_S5: {     // xbar_f += Xbar5; distribute to x2, k1'', k2', k3', k4
             const cplx<R> xfb = cadd(J[JJ_X0 * VEC + o], Xb);
@@ -293,9 +293,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) hpart += __shfl_xor_sync(0xffffffffu, hpart, o);
   if (lane == 0) p.hacc[(size_t)b * K + ky] += hpart;
-  const bool produce = (p.stage == AJ_PRE || p.stage == AJ_S4 || p.stage == AJ_S3 || p.stage == AJ_S2 ||
-                        (p.stage == AJ_S1 && p.rec_prev) || p.stage == AJ43_PRE || p.stage == AJ43_S5 ||
-                        p.stage == AJ43_S4 || p.stage == AJ43_S3 || p.stage == AJ43_IPRE);
+  const bool produce = (STAGE == AJ_PRE || STAGE == AJ_S4 || STAGE == AJ_S3 || STAGE == AJ_S2 ||
+                        (STAGE == AJ_S1 && p.rec_prev) || STAGE == AJ43_PRE || STAGE == AJ43_S5 ||
+                        STAGE == AJ43_S4 || STAGE == AJ43_S3 || STAGE == AJ43_IPRE);
   if (!produce) return;
   // unscaled inverse: Re sum lam e^{ik.x} after the row pass doubles ky > 0
   const R n2 = R(N) * R(N);

@@ -42,7 +42,7 @@ struct Col43Params {
   int B, stage;
 };
 
-template <typename R, int N>
+template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * RR_NREC * VEC
                        : nullptr;
 
-  const bool has_rhs = p.stage != R43_A && p.stage != R43_START;
+  const bool has_rhs = STAGE != R43_A && STAGE != R43_START;
   cplx<R> r0[E], r1[E];
   if (has_rhs) col_load_fwd<R, N>(p.H, b, ky, lane, s_tw, r0, r1);
   cplx<R> x0[E], x1[E];
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
       const cplx<R> kv = cscale(v[ch], t);                 // mod_vel_fn = t * vel_fn (:243)
       cplx<R> xin = mk<R>(0, 0);
-      switch (p.stage) {
+      switch (STAGE) {
         case R43_START: {
           xin = S[S_X0 * VEC + o];
         } break;
@@ -135,8 +135,8 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       if (ch == 0) x0[j] = xin; else x1[j] = xin;
     }
   }
-  if (p.stage == R43_INIT) return;
-  if (p.stage == R43_E) col_inverse2<R, N>(x0, x1, p.G, 8, b, ky, lane, s_tw);
+  if (STAGE == R43_INIT) return;
+  if (STAGE == R43_E) col_inverse2<R, N>(x0, x1, p.G, 8, b, ky, lane, s_tw);
   else col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
 }
 

@@ -187,7 +187,7 @@ struct ColTanParams {
   int B, stage, produce;
 };
 
-template <typename R, int N>
+template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
@@ -201,8 +201,8 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   const int b = col / K, ky = col - b * K;
   cplx<R>* D = p.D + (size_t)b * p.nslot * VEC;
   const cplx<R>* Q = p.rec;
-  const bool rk43 = p.stage >= T43_INIT;
-  const bool has_rhs = !(p.stage == TS_START || p.stage == T43_A || p.stage == T43_START);
+  const bool rk43 = STAGE >= T43_INIT;
+  const bool has_rhs = !(STAGE == TS_START || STAGE == T43_A || STAGE == T43_START);
   const R h = (R)p.h, t = (R)p.t;
   const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
   cplx<R> r0[E], r1[E];
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
         const R e = in_mask ? exp(h / R(2) * L) : R(0);
         const R de = e * L * (dpar / R(2));
         auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv[ch], h)); };
-        switch (p.stage) {
+        switch (STAGE) {
           case TS_START: xin = D[D_F * VEC + o]; break;
           case T4_S1: {
             const cplx<R> dk1 = dk_of(Q_K1);
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
         const R e = exp((t * L) * h / R(2));
         const R de = e * (L * h / R(2)) * dpar;
         auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / t), cscale(dv[ch], t)); };
-        switch (p.stage) {
+        switch (STAGE) {
           case T43_START: xin = D[S_X0 * VEC + o]; break;
           case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
           case T43_A: {
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
       if (ch == 0) x0[j] = xin; else x1[j] = xin;
     }
   }
-  if (!p.produce || p.stage == T43_INIT || p.stage == T43_E) return;
+  if (!p.produce || STAGE == T43_INIT || STAGE == T43_E) return;
   col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
 }
 

@@ -129,13 +129,13 @@ int na_state_vel(unsigned char* base, double nu, double eta, double b0x, double 
   cp.fhat = fbox; cp.tw = tw; cp.nu = nu; cp.eta = eta; cp.B = B; cp.stage = COL_START; cp.produce = 1;
   cp.diss = 0; cp.rec = nullptr; cp.rec_bstride = 0;
   const int cols = B * K;
-  k_col_rk4<double, N><<<(cols + 3) / 4, 128, 0, s>>>(cp);
+  k_col_rk4<double, N, COL_START><<<(cols + 3) / 4, 128, 0, s>>>(cp);
   RowParams<double> rp;
   rp.G = G; rp.H = H; rp.phys = nullptr; rp.phys_bstride = 0; rp.rec_index = 0; rp.phys_stage = 0; rp.ctl = nullptr;
   rp.tw = tw; rp.b0x = b0x; rp.b0y = b0y; rp.B = B;
   k_row_rhs<double, N, NA_XT><<<B * (N / NA_XT), NA_XT * 32, na_smem_rhs<N>(), s>>>(rp);
   cp.stage = COL_PLAIN; cp.produce = 0; cp.diss = diss;
-  k_col_rk4<double, N><<<(cols + 3) / 4, 128, 0, s>>>(cp);
+  k_col_rk4<double, N, COL_PLAIN><<<(cols + 3) / 4, 128, 0, s>>>(cp);
   const long nfull = (long)B * 2 * N * (N / 2 + 1);
   k_scatter_box<double><<<(int)((nfull + 255) / 256), 256, 0, s>>>(OUT, dfdt, N, B);
   return cudaGetLastError() == cudaSuccess ? ECS_OK : ECS_ERR_CUDA;
