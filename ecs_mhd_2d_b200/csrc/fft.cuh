@@ -28,6 +28,49 @@ __device__ __forceinline__ cplx<R> twid(const cplx<R>* __restrict__ tw, int idx)
   return w;
 }
 
+// Multiply by -i (forward) or +i (inverse): the span-2 twiddle W_4^1.
+template <typename R, bool INV>
+__device__ __forceinline__ cplx<R> mul_mi(cplx<R> a) {
+  return INV ? mk<R>(-a.y, a.x) : mk<R>(a.y, -a.x);
+}
+
+// One DIF shuffle stage of span S: lower lane v + p, upper lane (p - v) W_{2S}^{lane mod S}.
+template <typename R, int N, bool INV, int S>
+__device__ __forceinline__ void dif_shfl(cplx<R> (&v)[N / 32], const cplx<R>* __restrict__ tw, int lane) {
+  constexpr int E = N / 32;
+  const bool upper = (lane & S) != 0;
+  const R sg = upper ? R(-1) : R(1);
+  cplx<R> w = mk<R>(1, 0);
+  if (S > 2) w = upper ? twid<R, INV>(tw, (lane & (S - 1)) * (N / (2 * S))) : mk<R>(1, 0);
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const cplx<R> p = shfl_xor_c<R>(v[j], S);
+    cplx<R> t = mk<R>(p.x + sg * v[j].x, p.y + sg * v[j].y);
+    if (S == 2) { if (upper && (lane & 1)) t = mul_mi<R, INV>(t); }
+    else if (S > 2) t = cmul(t, w);
+    v[j] = t;
+  }
+}
+
+// One DIT shuffle stage of span S: lower lane v + p W, upper lane p - v W (W = W_{2S}^{lane mod S}).
+template <typename R, int N, bool INV, int S>
+__device__ __forceinline__ void dit_shfl(cplx<R> (&v)[N / 32], const cplx<R>* __restrict__ tw, int lane) {
+  constexpr int E = N / 32;
+  const bool upper = (lane & S) != 0;
+  const R sg = upper ? R(-1) : R(1);
+  cplx<R> w = mk<R>(1, 0);
+  if (S > 2) w = twid<R, INV>(tw, (lane & (S - 1)) * (N / (2 * S)));
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const cplx<R> p = shfl_xor_c<R>(v[j], S);
+    cplx<R> q = upper ? v[j] : p;          // the operand that carries the twiddle
+    const cplx<R> r = upper ? p : v[j];
+    if (S == 2) { if (lane & 1) q = mul_mi<R, INV>(q); }
+    else if (S > 2) q = cmul(q, w);
+    v[j] = mk<R>(r.x + sg * q.x, r.y + sg * q.y);
+  }
+}
+
 template <typename R, int N, bool INV>
 __device__ __forceinline__ void fft_dif(cplx<R> (&v)[N / 32], const cplx<R>* __restrict__ tw, int lane) {
   constexpr int E = N / 32;
@@ -49,32 +92,22 @@ __device__ __forceinline__ void fft_dif(cplx<R> (&v)[N / 32], const cplx<R>* __r
     }
   }
   // shuffle stages: span 16 ... 1
-#pragma unroll
-  for (int s = 16; s >= 1; s >>= 1) {
-    const cplx<R> w = twid<R, INV>(tw, (lane & (s - 1)) * (N / (2 * s)));
-    const bool upper = (lane & s) != 0;
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      cplx<R> p = shfl_xor_c<R>(v[j], s);
-      v[j] = upper ? cmul(csub(p, v[j]), w) : cadd(v[j], p);
-    }
-  }
+  dif_shfl<R, N, INV, 16>(v, tw, lane);
+  dif_shfl<R, N, INV, 8>(v, tw, lane);
+  dif_shfl<R, N, INV, 4>(v, tw, lane);
+  dif_shfl<R, N, INV, 2>(v, tw, lane);
+  dif_shfl<R, N, INV, 1>(v, tw, lane);
 }
 
 template <typename R, int N, bool INV>
 __device__ __forceinline__ void fft_dit(cplx<R> (&v)[N / 32], const cplx<R>* __restrict__ tw, int lane) {
   constexpr int E = N / 32;
   constexpr int LE = Log2E<N>::v;
-#pragma unroll
-  for (int s = 1; s <= 16; s <<= 1) {
-    const cplx<R> w = twid<R, INV>(tw, (lane & (s - 1)) * (N / (2 * s)));
-    const bool upper = (lane & s) != 0;
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      cplx<R> p = shfl_xor_c<R>(v[j], s);
-      v[j] = upper ? csub(p, cmul(v[j], w)) : cadd(v[j], cmul(p, w));
-    }
-  }
+  dit_shfl<R, N, INV, 1>(v, tw, lane);
+  dit_shfl<R, N, INV, 2>(v, tw, lane);
+  dit_shfl<R, N, INV, 4>(v, tw, lane);
+  dit_shfl<R, N, INV, 8>(v, tw, lane);
+  dit_shfl<R, N, INV, 16>(v, tw, lane);
 #pragma unroll
   for (int m = 0; m < LE; ++m) {
     const int half = 1 << m;

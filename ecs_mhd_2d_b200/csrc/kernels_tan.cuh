@@ -107,7 +107,7 @@ struct RowTanParams {
 };
 
 template <typename R, int N, int XT>
-__global__ void __launch_bounds__(XT * 32) k_row_tan(RowTanParams<R> p) {
+__global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -122,12 +122,26 @@ __global__ void __launch_bounds__(XT * 32) k_row_tan(RowTanParams<R> p) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
   const R* ph = p.phys + ((size_t)x * 8) * N;
-  // tangent physical fields, pair by pair; primal values from the record
+  // tangent physical fields, pair by pair; the primal values each pair needs
+  // are loaded before its transform so that the loads overlap the shuffles
   cplx<R> W[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) W[j] = mk<R>(0, 0);
+  // pair pr uses primal fields (f0, f1, f2, f3):
+  //   pr 0 (dfx0, dfy0): fu0 fv0        pr 1 (dfu0, dfv0): fx0 fy0 fv1 fu1
+  //   pr 2 (dfx1, dfy1): fu1 fv1        pr 3 (dfu1, dfv1): fx1 fy1 fu0 fv0
 #pragma unroll
   for (int pr = 0; pr < 4; ++pr) {
+    const int f0 = pr == 0 ? 2 : pr == 1 ? 0 : pr == 2 ? 6 : 4;
+    const int f1 = f0 + 1;
+    const int f2 = pr == 1 ? 7 : 2, f3 = pr == 1 ? 6 : 3;
+    R a0[E], a1[E], a2[E], a3[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int e = lane + 32 * j;
+      a0[j] = ph[f0 * N + e]; a1[j] = ph[f1 * N + e];
+      if (pr == 1 || pr == 3) { a2[j] = ph[f2 * N + e]; a3[j] = ph[f3 * N + e]; }
+    }
     cplx<R> z[E];
 #pragma unroll
     for (int j = 0; j < E; ++j)
@@ -135,21 +149,19 @@ __global__ void __launch_bounds__(XT * 32) k_row_tan(RowTanParams<R> p) {
     fft_dif<R, N, true>(z, s_tw, lane);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int e = lane + 32 * j;
       const R da = z[j].x, db = z[j].y;
-      // pr 0: (dfx0, dfy0)  1: (dfu0, dfv0)  2: (dfx1, dfy1)  3: (dfu1, dfv1)
       // dP1 = -d(adv0) + d(adv1),  adv_c = fu_c fx_c + fv_c fy_c   (mhd_jax.py:152,159)
       // dP2 = d(fu0 fv1 - fv0 fu1)                                   (mhd_jax.py:163)
       if (pr == 0) {
-        W[j].x -= ph[2 * N + e] * da + ph[3 * N + e] * db;
+        W[j].x -= a0[j] * da + a1[j] * db;
       } else if (pr == 1) {
-        W[j].x -= da * ph[0 * N + e] + db * ph[1 * N + e];
-        W[j].y += da * ph[7 * N + e] - db * ph[6 * N + e];
+        W[j].x -= da * a0[j] + db * a1[j];
+        W[j].y += da * a2[j] - db * a3[j];
       } else if (pr == 2) {
-        W[j].x += ph[6 * N + e] * da + ph[7 * N + e] * db;
+        W[j].x += a0[j] * da + a1[j] * db;
       } else {
-        W[j].x += da * ph[4 * N + e] + db * ph[5 * N + e];
-        W[j].y += ph[2 * N + e] * db - ph[3 * N + e] * da;
+        W[j].x += da * a0[j] + db * a1[j];
+        W[j].y += a2[j] * db - a3[j] * da;
       }
     }
   }

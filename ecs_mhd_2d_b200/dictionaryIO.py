@@ -1,0 +1,85 @@
+"""State + parameter files in the reference's .npz format
+(reference: jax_scripts/lib/dictionaryIO.py:11-78).
+
+A file holds the input dict ("fields", "T", "sx") and the parameter dict
+(nu, eta, b0, forcing_str, steps, ministeps, num_checkpoints, shift_reflect_ny,
+rot, ...) with two key lists, "input_keys" and "param_keys".
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .mhd import construct_domain, PI_LITERAL
+
+GRID_KEYS = ["x", "y", "kx", "ky", "mask", "to_u", "to_v", "inv_lap", "forcing"]
+
+
+def _np(v):
+    if isinstance(v, torch.Tensor):
+        return v.detach().cpu().numpy()
+    return np.array(v)
+
+
+def save_dicts(filename, input_dict, param_dict):
+    """Merge both dicts with their key lists and np.savez them (dictionaryIO.py:11-27)."""
+    combined = dict(input_dict)
+    combined.update(param_dict)
+    combined["input_keys"] = list(input_dict.keys())
+    combined["param_keys"] = list(param_dict.keys())
+    np.savez(filename, **{k: _np(v) for k, v in combined.items()})
+
+
+def load_dicts(filename, device=None):
+    """(input_dict, param_dict) from a file (dictionaryIO.py:30-48); numeric
+    arrays become torch tensors (on `device` if given)."""
+    loaded = np.load(filename, allow_pickle=True)
+
+    def conv(val):
+        if isinstance(val, np.ndarray) and np.issubdtype(val.dtype, np.number):
+            t = torch.as_tensor(val)
+            return t.to(device) if device is not None else t
+        return val.item() if getattr(val, "shape", None) == () else val
+
+    inp = {k: conv(loaded[k]) for k in loaded["input_keys"]}
+    par = {k: conv(loaded[k]) for k in loaded["param_keys"]}
+    return inp, par
+
+
+def remove_grid_information(param_dict):
+    """Drop the grid tensors before saving (dictionaryIO.py:52-60)."""
+    pd = dict(param_dict)
+    for key in GRID_KEYS:
+        pd.pop(key, None)
+    return pd
+
+
+class _NumpyAsJnp:
+    """The names a reference forcing_str uses (jnp.cos, jnp.sin, jnp.pi, ...)."""
+    cos, sin, exp, tanh, sqrt = np.cos, np.sin, np.exp, np.tanh, np.sqrt
+    pi = math.pi
+
+
+def forcing_from_string(forcing_str, n):
+    """Evaluate a reference forcing string such as 'lambda x,y : -4*jnp.cos(4*y)'
+    on the grid of construct_domain, with only numpy math in scope."""
+    grid = np.arange(n, dtype=np.float64) / n * 2 * PI_LITERAL
+    x, y = np.meshgrid(grid, grid, indexing="ij")
+    fn = eval(str(forcing_str), {"__builtins__": {}, "jnp": _NumpyAsJnp, "np": _NumpyAsJnp})
+    return np.asarray(fn(x, y), dtype=np.float64)
+
+
+def recompute_grid_information(input_dict, param_dict):
+    """Inverse of remove_grid_information (dictionaryIO.py:64-78)."""
+    f = input_dict["fields"]
+    n = f.shape[-1]
+    dt = f.dtype if isinstance(f, torch.Tensor) else torch.float64
+    param_dict.update(construct_domain(n, dt))
+    fr = forcing_from_string(param_dict["forcing_str"], n)
+    param_dict["forcing"] = torch.as_tensor(fr, dtype=dt, device=param_dict["x"].device)
+    b0 = param_dict.get("b0", [0.0, 0.1])
+    param_dict["b0"] = [float(b0[0]), float(b0[1])]
+    return param_dict

@@ -1,0 +1,102 @@
+"""Newton-GMRES and adjoint-descent iterations on top of the device path
+(reference drivers: jax_scripts/newton.py:151-215, jax_scripts/adjoint_descent.py:93-114).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from .autodiff import Objective, loss_and_grad, vjp
+from .linalg import gmres
+from .loss_functions import dealias
+from .utils import flatten, line_search_unravel, relative_error_RPO, unflatten
+
+
+def _as_device_dict(d, device="cuda"):
+    f = d["fields"] if isinstance(d["fields"], torch.Tensor) else torch.as_tensor(d["fields"])
+    return {"fields": f.to(device=device, dtype=torch.float64).contiguous(),
+            "T": float(d["T"]), "sx": float(d["sx"])}
+
+
+def newton_gmres_update(input_dict, param_dict, mode, inner=16, use_transpose=True, do_line_search=True,
+                        default_damp=0.1, jac_obj=None):
+    """One Newton-GMRES update (newton.py:151-215).  Solves J s = f (or
+    J^T J s = J^T f with use_transpose) with `inner` Krylov vectors, applies a
+    line search, and dealiases.  `jac_obj` (optional) is a second Objective
+    used for the Jacobian products, e.g. an FP32 one for mixed precision.
+    Returns (new_input_dict, stats)."""
+    obj = Objective(param_dict, mode)
+    jac = jac_obj or obj
+    x_dict = _as_device_dict(input_dict)
+    n = x_dict["fields"].shape[-1]
+    f = obj(x_dict)
+    b = flatten(f)
+
+    def cast_in(d):
+        if jac is obj:
+            return d
+        dt = jac.param_dict["x"].dtype
+        return {"fields": d["fields"].to(dt), "T": d["T"], "sx": d["sx"]}
+
+    def A(v):
+        t = unflatten(v, n)
+        out = jac.jvp(cast_in(x_dict), cast_in({"fields": t["fields"], "T": t["T"], "sx": t["sx"]}))
+        return flatten({"fields": out["fields"].to(torch.float64), "T": out["T"], "sx": out["sx"]})
+
+    precond = []
+    if use_transpose:
+        _, jacT = vjp(jac, cast_in(x_dict))
+
+        def A_T(v):
+            t = unflatten(v, n)
+            g = jacT({"fields": t["fields"].to(jac.param_dict["x"].dtype).contiguous(), "T": t["T"], "sx": t["sx"]})[0]
+            return flatten({"fields": g["fields"].to(torch.float64), "T": g["T"], "sx": g["sx"]})
+
+        precond = [A_T]
+    step, gmres_res = gmres(A, b, inner, 1, precond)
+    x = flatten(x_dict)
+    unravel = lambda v: unflatten(v, n)
+    if do_line_search:
+        x, damp = line_search_unravel(x, step, obj, unravel, b, max_iters=20)
+    else:
+        damp = default_damp
+        x = x - damp * step
+    new = unravel(x)
+    rel_err = relative_error_RPO(x_dict, f)
+    new = {"fields": dealias(new["fields"].contiguous(), param_dict), "T": float(new["T"]), "sx": float(new["sx"])}
+    stats = {"rel_err": float(rel_err), "|f|": float(torch.linalg.norm(b)), "gmres_rel_res": float(gmres_res),
+             "damp": damp, "T": new["T"], "sx": new["sx"]}
+    return new, stats
+
+
+def init_adam(params):
+    """Zero moments (jax_scripts/lib/adam.py:7-20)."""
+    return ({k: 0 * torch.as_tensor(v) for k, v in params.items()},
+            {k: 0 * torch.as_tensor(v) for k, v in params.items()})
+
+
+def adam_update(params, grads, m, v, t, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+    """One ADAM step on dicts (jax_scripts/lib/adam.py:23-61)."""
+    m = {k: beta1 * m[k] + (1 - beta1) * grads[k] for k in params}
+    v = {k: beta2 * v[k] + (1 - beta2) * grads[k] ** 2 for k in params}
+    m_hat = {k: m[k] / (1 - beta1 ** t) for k in params}
+    v_hat = {k: v[k] / (1 - beta2 ** t) for k in params}
+    params = {k: params[k] - lr * m_hat[k] / (torch.sqrt(v_hat[k]) + eps) for k in params}
+    return params, m, v
+
+
+def adjoint_descent_step(input_dict, param_dict, mode, m, v, t, lr=1e-2):
+    """One adjoint-descent iteration (adjoint_descent.py:93-114): gradient of
+    loss_RPO by the adjoint kernels, ADAM update, dealias.  Returns
+    (new_input_dict, m, v, loss, info)."""
+    x = _as_device_dict(input_dict)
+    (loss, info), g = loss_and_grad(x, param_dict, mode)
+    params = {"fields": x["fields"], "T": torch.tensor(x["T"], dtype=torch.float64, device="cuda"),
+              "sx": torch.tensor(x["sx"], dtype=torch.float64, device="cuda")}
+    grads = {"fields": g["fields"], "T": g["T"].reshape(()), "sx": g["sx"].reshape(())}
+    if t == 1 and not m:
+        m, v = init_adam(params)
+    params, m, v = adam_update(params, grads, m, v, t, lr=lr, beta1=0.9, beta2=0.999, eps=1e-6)
+    new = {"fields": dealias(params["fields"].contiguous(), param_dict), "T": float(params["T"]),
+           "sx": float(params["sx"])}
+    return new, m, v, float(loss), info
