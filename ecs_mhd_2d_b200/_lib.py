@@ -40,7 +40,7 @@ class EcsShootCfg(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("num_checkpoints", ctypes.c_int), ("ministeps", ctypes.c_int),
                 ("shift_reflect_ny", ctypes.c_int), ("rot", ctypes.c_int), ("atol", ctypes.c_double),
                 ("h0", ctypes.c_double), ("max_steps_per_checkpoint", ctypes.c_int),
-                ("checkpoints", ctypes.c_int)]
+                ("checkpoints", ctypes.c_int), ("ckpt_every", ctypes.c_int)]
 
 
 class EcsInfo(ctypes.Structure):

@@ -104,6 +104,7 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->g4.exec) cudaGraphExecDestroy(ctx->g4.exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->lin.rec) cudaFree(ctx->lin.rec);
+  if (ctx->lin.ckpt) cudaFree(ctx->lin.ckpt);
   if (ctx->lin.rec_h) cudaFree(ctx->lin.rec_h);
   if (ctx->lin.rec_acc) cudaFree(ctx->lin.rec_acc);
   if (ctx->D) cudaFree(ctx->D);

@@ -50,6 +50,8 @@ struct ecs_ctx {
     double* dsx = nullptr;          // primal sx on the device
     double* dT = nullptr;           // primal T on the device
     double* rec_h = nullptr; int* rec_acc = nullptr; size_t cap = 0;
+    long seg = 0;                   // Lawson-RK4 checkpoint interval (0: full record)
+    void* ckpt = nullptr; size_t ckpt_bytes = 0;   // segment start states
   } lin;
   // tangent / adjoint workspace (grown on demand)
   void* D = nullptr; size_t D_bytes = 0;          // tangent or adjoint slots

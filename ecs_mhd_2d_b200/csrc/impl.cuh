@@ -445,6 +445,32 @@ struct Impl {
     return ECS_OK;
   }
 
+  // Record `steps` Lawson-RK4 steps of the box state in c->F (batch 1) into rec
+  // (Q_NREC vectors per step); ctl/Etab must hold the step size of the call.
+  static void record_rk4_segment(ecs_ctx* c, cplx<R>* rec, long steps, cudaStream_t s) {
+    const size_t VEC = 2UL * K * M;
+    launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, s);
+    for (long it = 0; it < steps; ++it) {
+      cplx<R>* rs = rec + (size_t)it * Q_NREC * VEC;
+      for (int k = 1; k <= 4; ++k) {
+        launch_row_rhs<R, N>(c, 1, nullptr, s);
+        launch_col_rk4<R, N>(c, 1, k, (k == 4 && it == steps - 1) ? 0 : 1, 0, s, rs, 0);
+      }
+    }
+  }
+
+  // Lawson-RK4 segment [a0, a0+cnt) of the current linearisation: its record
+  // (recomputed from the checkpoint when the linearisation is segmented).
+  static const cplx<R>* rk4_segment_record(ecs_ctx* c, long a0, long cnt, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    if (!L.seg) return (const cplx<R>*)L.rec + (size_t)a0 * Q_NREC * VEC;
+    rk4_setup(c, L.dT, L.cfg.num_checkpoints, L.cfg.ministeps, 1, s);
+    cudaMemcpyAsync(c->F, (cplx<R>*)L.ckpt + (size_t)(a0 / L.seg) * VEC, vb, cudaMemcpyDeviceToDevice, s);
+    record_rk4_segment(c, (cplx<R>*)L.rec, cnt, s);
+    return (const cplx<R>*)L.rec;
+  }
+
   // ---------------------------------------------------------------------
   // Linearisation: primal solve of one candidate with its trajectory record,
   // plus the stop-gradient phase fields vt, vx (loss_functions.py:113-130).
@@ -487,19 +513,25 @@ struct Impl {
     if (!rk43) {
       const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
       if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
-      st = grow(c, &L.rec, &L.rec_bytes, (size_t)steps * Q_NREC * vb);
+      const long kseg = (cfg->ckpt_every > 0 && cfg->ckpt_every < steps) ? cfg->ckpt_every : 0;
+      st = grow(c, &L.rec, &L.rec_bytes, (size_t)(kseg ? kseg : steps) * Q_NREC * vb);
       if (st) return st;
       cudaMemcpyAsync(c->F, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
       st = rk4_setup(c, T, cfg->num_checkpoints, cfg->ministeps, 1, s);
       if (st) return st;
-      launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, s);
-      for (long it = 0; it < steps; ++it) {
-        cplx<R>* rs = (cplx<R>*)L.rec + (size_t)it * Q_NREC * VEC;
-        for (int k = 1; k <= 4; ++k) {
-          launch_row_rhs<R, N>(c, 1, nullptr, s);
-          launch_col_rk4<R, N>(c, 1, k, (k == 4 && it == steps - 1) ? 0 : 1, 0, s, rs, 0);
+      if (kseg) {   // keep only the segment start states; segments are recomputed by jvp / vjp
+        const long nseg = (steps + kseg - 1) / kseg;
+        st = grow(c, &L.ckpt, &L.ckpt_bytes, (size_t)nseg * vb);
+        if (st) return st;
+        for (long g = 0; g < nseg; ++g) {
+          cudaMemcpyAsync((cplx<R>*)L.ckpt + (size_t)g * VEC, c->F, vb, cudaMemcpyDeviceToDevice, s);
+          st = integrate_rk4(c, 1, std::min(kseg, steps - g * kseg), s);
+          if (st) return st;
         }
+      } else {
+        record_rk4_segment(c, (cplx<R>*)L.rec, steps, s);
       }
+      L.seg = kseg;
       L.nrec = steps;
       L.h = (double)(R)((hT / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
       cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
@@ -638,12 +670,32 @@ struct Impl {
     const cplx<R>* rec = (const cplx<R>*)L.rec;
     if (!rk43) {
       const double dscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
-      launch_col_tan<R, N>(c, B, TS_START, 1, rec, dT, 0.0, L.h, dscale, nslot, s);
-      for (long a = 0; a < L.nrec; ++a) {
-        const cplx<R>* ra = rec + (size_t)a * Q_NREC * VEC;
-        for (int k = 1; k <= 4; ++k) {
-          launch_row_tan<R, N>(c, B, phys_of(item_of[a] + (k - 1)), s);
-          launch_col_tan<R, N>(c, B, k, (k == 4 && a == L.nrec - 1) ? 0 : 1, ra, dT, 0.0, L.h, dscale, nslot, s);
+      const long kseg = L.seg ? L.seg : L.nrec;
+      for (long a0 = 0; a0 < L.nrec; a0 += kseg) {
+        const long cnt = std::min(kseg, L.nrec - a0);
+        const cplx<R>* rseg = rk4_segment_record(c, a0, cnt, s);
+        std::vector<long> sitems;
+        for (long it = 0; it < cnt; ++it) {
+          const long base = it * Q_NREC;
+          sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
+        }
+        st = upload_items(c, sitems);
+        if (st) return st;
+        long slo = -1;
+        auto sphys = [&](long item) -> const R* {
+          if (slo < 0 || item < slo || item >= slo + ci) {
+            slo = item;
+            launch_regen<R, N>(c, rseg, c->items + item, (int)std::min<long>(ci, (long)sitems.size() - item), s);
+          }
+          return (const R*)c->Phys + (size_t)(item - slo) * N * 8 * N;
+        };
+        launch_col_tan<R, N>(c, B, TS_START, 1, rseg, dT, 0.0, L.h, dscale, nslot, s);
+        for (long it = 0; it < cnt; ++it) {
+          const cplx<R>* ra = rseg + (size_t)it * Q_NREC * VEC;
+          for (int k = 1; k <= 4; ++k) {
+            launch_row_tan<R, N>(c, B, sphys(4 * it + (k - 1)), s);
+            launch_col_tan<R, N>(c, B, k, (k == 4 && it == cnt - 1) ? 0 : 1, ra, dT, 0.0, L.h, dscale, nslot, s);
+          }
         }
       }
     } else {
@@ -740,13 +792,35 @@ struct Impl {
     if (!rk43) {
       tscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
       const double h = L.h;
-      launch_col_adj<R, N>(c, B, AJ_PRE, rec + (size_t)(L.nrec - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
-      for (long a = L.nrec - 1; a >= 0; --a) {
-        const cplx<R>* ra = rec + (size_t)a * Q_NREC * VEC;
-        const cplx<R>* rp = a > 0 ? rec + (size_t)(a - 1) * Q_NREC * VEC : nullptr;
-        for (int k = 4; k >= 1; --k) {
-          launch_row_adj<R, N>(c, B, phys_of(item_of[a] + (k - 1)), s);
-          launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
+      const long kseg = L.seg ? L.seg : L.nrec;
+      const long nseg = (L.nrec + kseg - 1) / kseg;
+      for (long g = nseg - 1; g >= 0; --g) {
+        const long a0 = g * kseg, cnt = std::min(kseg, L.nrec - a0);
+        const cplx<R>* rseg = rk4_segment_record(c, a0, cnt, s);
+        std::vector<long> sitems;
+        for (long it = 0; it < cnt; ++it) {
+          const long base = it * Q_NREC;
+          sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
+        }
+        st = upload_items(c, sitems);
+        if (st) return st;
+        long slo = -1;
+        auto sphys = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
+          if (slo < 0 || item < slo || item >= slo + ci) {
+            slo = std::max<long>(0, item - ci + 1);
+            launch_regen<R, N>(c, rseg, c->items + slo, (int)std::min<long>(ci, (long)sitems.size() - slo), s);
+          }
+          return (const R*)c->Phys + (size_t)(item - slo) * N * 8 * N;
+        };
+        // seed the segment's last step from obar (J_OB)
+        launch_col_adj<R, N>(c, B, AJ_PRE, rseg + (size_t)(cnt - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
+        for (long it = cnt - 1; it >= 0; --it) {
+          const cplx<R>* ra = rseg + (size_t)it * Q_NREC * VEC;
+          const cplx<R>* rp = it > 0 ? rseg + (size_t)(it - 1) * Q_NREC * VEC : nullptr;
+          for (int k = 4; k >= 1; --k) {
+            launch_row_adj<R, N>(c, B, sphys(4 * it + (k - 1)), s);
+            launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
+          }
         }
       }
     } else {

@@ -100,3 +100,31 @@ def adjoint_descent_step(input_dict, param_dict, mode, m, v, t, lr=1e-2):
     new = {"fields": dealias(params["fields"].contiguous(), param_dict), "T": float(params["T"]),
            "sx": float(params["sx"])}
     return new, m, v, float(loss), info
+
+
+def mixed_precision_objectives(param_dict, mode):
+    """(FP64 objective for residuals, FP32 objective for Jacobian products) over
+    the same physics: time stepping and JVP/VJP in FP32, the Newton residual,
+    Arnoldi and Hessenberg solve in FP64."""
+    from .mhd import make_param_dict
+    n = param_dict["x"].shape[-1]
+    keep = {k: v for k, v in param_dict.items() if k not in ("x", "y", "kx", "ky", "mask", "to_u", "to_v",
+                                                             "inv_lap", "forcing", "nu", "eta", "b0")}
+    f64 = param_dict["forcing"].detach().to("cpu", torch.float64).numpy()
+    pd32 = make_param_dict(n, param_dict["nu"], param_dict["eta"], b0=param_dict["b0"], forcing=f64,
+                           data_type=torch.float32, **keep)
+    return Objective(param_dict, mode), Objective(pd32, mode)
+
+
+def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_transpose=True):
+    """Inexact Newton with FP32 Jacobian products and FP64 residuals; the last
+    residual is an FP64 refinement check.  Returns (state, history)."""
+    _, obj32 = mixed_precision_objectives(param_dict, mode)
+    x = input_dict
+    hist = []
+    for _ in range(iters):
+        x, st = newton_gmres_update(x, param_dict, mode, inner=inner, use_transpose=use_transpose, jac_obj=obj32)
+        hist.append(st)
+    f = Objective(param_dict, mode)(_as_device_dict(x))
+    hist.append({"final_rel_err": float(relative_error_RPO(_as_device_dict(x), f))})
+    return x, hist

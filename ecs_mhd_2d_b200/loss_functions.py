@@ -31,6 +31,7 @@ def shoot_cfg(param_dict, mode):
     c.h0 = float(ad.get("h0", 1e-2))
     c.max_steps_per_checkpoint = int(ad.get("max_steps_per_checkpoint", 1024))
     c.checkpoints = int(ad.get("checkpoints", 1))
+    c.ckpt_every = int(param_dict.get("ckpt_every", 0))
     return c
 
 

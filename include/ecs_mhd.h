@@ -61,6 +61,9 @@ typedef struct {
   double h0;               /* Lawson_RK43: initial step (loss_functions.py:77 uses 1e-2) */
   int max_steps_per_checkpoint; /* Lawson_RK43: adaptive_dict["max_steps_per_checkpoint"] */
   int checkpoints;         /* Lawson_RK43: adaptive_dict["checkpoints"] */
+  int ckpt_every;          /* Lawson_RK4 linearisation: keep only every k-th state and recompute
+                              segments of k steps in ecs_jvp / ecs_vjp (0 = record every step);
+                              k = ministeps mirrors jax.checkpoint at loss_functions.py:63 */
 } ecs_shoot_cfg;
 
 typedef struct {

@@ -42,3 +42,11 @@ def test_adjoint_descent_lowers_loss(cuda):
         x, m, v, loss, info = drivers.adjoint_descent_step(x, pd, "Lawson_RK4", m, v, t, lr=1e-3)
         losses.append(loss)
     assert losses[-1] < losses[0]
+
+
+def test_mixed_precision_newton_reaches_fp64_accuracy(cuda):
+    """FP32 Jacobian, FP64 residual: the Newton iteration still converges to the
+    FP64 closure level of the reference solution."""
+    x, pd = perturbed_rpo6(1e-4)
+    new, hist = drivers.mixed_precision_newton(x, pd, "Lawson_RK4", iters=2, inner=12)
+    assert hist[-1]["final_rel_err"] < 1e-8, hist

@@ -71,3 +71,18 @@ def test_jvp_linearity_and_batch_consistency(cuda):
     assert float(torch.linalg.norm(jab["fields"] - lin) / torch.linalg.norm(lin)) < 1e-13
     both = obj.jvp(prim, {"fields": torch.stack([a, b]), "T": torch.tensor([0.2, 0.0], dtype=torch.float64), "sx": torch.tensor([0.0, 0.3], dtype=torch.float64)})
     assert torch.equal(both["fields"][0], ja["fields"]) and torch.equal(both["fields"][1], jb["fields"])
+
+
+def test_fp32_jvp_against_fp64_oracle(cuda):
+    """FP32 stepping and tangent kernels stay within FP32 rounding of the FP64 oracle."""
+    n, T, sx = 64, 0.08, 0.2
+    kw = dict(num_checkpoints=1, ministeps=16, shift_reflect_ny=1, rot=False)
+    u0 = initial_condition(3, n)
+    du = initial_condition(21, n) * 0.1
+    pd32 = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", data_type=torch.float32, **kw)
+    pdt = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", xp=O.TORCH, **kw)
+    obj = E.Objective(pd32, "Lawson_RK4")
+    prim = {"fields": torch.as_tensor(u0, dtype=torch.float32, device="cuda"), "T": T, "sx": sx}
+    got = obj.jvp(prim, {"fields": torch.as_tensor(du, dtype=torch.float32, device="cuda"), "T": 0.3, "sx": -0.4})
+    want = oracle_jvp(u0, T, sx, du, 0.3, -0.4, pdt, "Lawson_RK4")
+    assert rel_l2(got["fields"].double().cpu().numpy(), want["fields"]) < 5e-5

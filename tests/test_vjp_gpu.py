@@ -103,3 +103,27 @@ def test_autograd_function(cuda):
     (l2, _), g = E.loss_and_grad({"fields": u0.detach(), "T": 0.2, "sx": 0.1}, pd, "Lawson_RK4")
     assert torch.allclose(u0.grad, g["fields"], rtol=0, atol=1e-14 * float(g["fields"].abs().max()))
     assert abs(float(T.grad) - float(g["T"])) <= 1e-12 * abs(float(g["T"]))
+
+
+def test_checkpointed_linearisation_matches_full_record(cuda):
+    """Keeping every 5th state and recomputing segments (jax.checkpoint per
+    segment, loss_functions.py:63) gives the same JVP and VJP as the full record."""
+    n = 64
+    u0 = initial_condition(4, n)
+    rng = np.random.default_rng(3)
+    base = dict(num_checkpoints=2, ministeps=8, shift_reflect_ny=1, rot=True)
+    prim = {"fields": torch.as_tensor(u0, device="cuda"), "T": 0.1, "sx": 0.3}
+    v = {"fields": torch.as_tensor(rng.standard_normal((2, n, n)), device="cuda"), "T": 0.2, "sx": -0.1}
+    u = {"fields": torch.as_tensor(rng.standard_normal((2, n, n)), device="cuda"), "T": 0.5, "sx": 0.7}
+    outs = []
+    for ck in (0, 5):
+        pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", ckpt_every=ck, **base)
+        obj = E.Objective(pd, "Lawson_RK4")
+        jv = obj.jvp(prim, v)
+        _, jacT = E.vjp(obj, prim)
+        outs.append((jv, jacT(u)[0]))
+    (j0, g0), (j1, g1) = outs
+    assert rel_l2(j1["fields"].cpu().numpy(), j0["fields"].cpu().numpy()) < 1e-14
+    assert rel_l2(g1["fields"].cpu().numpy(), g0["fields"].cpu().numpy()) < 1e-14
+    assert abs(float(g1["T"]) - float(g0["T"])) <= 1e-13 * abs(float(g0["T"]))
+    assert abs(float(g1["sx"]) - float(g0["sx"])) <= 1e-13 * max(abs(float(g0["sx"])), 1.0)
