@@ -108,6 +108,68 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def _timed(torch, flush, fn):
+    fn()
+    flush.zero_()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def secondary_workloads(E, torch, dev, flush):
+    """One timed repetition (after a warm-up) of the other measurement configs:
+    config 0 (n=64 FP64 Lawson-RK4, dt=0.005, 1024 steps, seeds 0..7),
+    config 2 (n=128 FP64 adjoint gradient, 1088 steps, T=4.26, checkpoints every 32),
+    config 3 (n=256 FP32 stepping and JVP, 2048 steps, T=4.6; FP64 residual check)."""
+    from ecs_mhd_2d_b200.synthetic import initial_condition, unit_tangents
+    out = {}
+    # config 0
+    n0 = 64
+    pd0 = E.make_param_dict(n0, 1 / 40, 1 / 40, forcing="kolmogorov+")
+    f0 = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(s, n0) for s in range(8)])), device=dev)
+    t, fT = _timed(torch, flush, lambda: E.lawson_rk4(f0, 1024 * 0.005, 1024, pd0))
+    out["config0_rk4_n64_f64"] = {"state_steps_per_s": 8 * 1024 / t, "seconds": t, "batch": 8, "steps": 1024,
+                                  "finite": bool(torch.isfinite(fT).all())}
+    # config 2
+    n2 = 128
+    pd2 = E.make_param_dict(n2, 1 / 40, 1 / 40, forcing="kolmogorov+", num_checkpoints=34, ministeps=32,
+                            shift_reflect_ny=0, rot=False, ckpt_every=32)
+    x2 = {"fields": torch.as_tensor(initial_condition(2, n2, amp=IC_AMP), device=dev), "T": 4.26, "sx": 0.1}
+    t, (lg, g) = _timed(torch, flush, lambda: E.loss_and_grad(x2, pd2, "Lawson_RK4", normalized=True))
+    out["config2_gradient_n128_f64"] = {"gradients_per_s": 1.0 / t, "seconds": t, "steps": 1088,
+                                        "ckpt_every": 32, "loss": float(lg[0])}
+    # config 3
+    n3 = 256
+    pd3_64 = E.make_param_dict(n3, 1 / 50, 1 / 50, forcing="kolmogorov+", num_checkpoints=64, ministeps=32,
+                               shift_reflect_ny=0, rot=False)
+    pd3_32 = E.make_param_dict(n3, 1 / 50, 1 / 50, forcing="kolmogorov+", num_checkpoints=64, ministeps=32,
+                               shift_reflect_ny=0, rot=False, data_type=torch.float32)
+    u3 = initial_condition(3, n3, amp=IC_AMP)
+    x64 = {"fields": torch.as_tensor(u3, device=dev), "T": 4.6, "sx": 0.12}
+    x32 = {"fields": torch.as_tensor(u3, dtype=torch.float32, device=dev), "T": 4.6, "sx": 0.12}
+    t32, o32 = _timed(torch, flush, lambda: E.objective_RPO(x32, pd3_32, "Lawson_RK4"))
+    t64, o64 = _timed(torch, flush, lambda: E.objective_RPO(x64, pd3_64, "Lawson_RK4"))
+    err = float(torch.linalg.norm(o32["fields"].double() - o64["fields"]) / torch.linalg.norm(o64["fields"]))
+    obj32 = E.Objective(pd3_32, "Lawson_RK4")
+    Bt = 16
+    tv = unit_tangents(5, n3, Bt)
+    tan = {"fields": torch.as_tensor(tv[:, 1:-1].reshape(Bt, 2, n3, n3), dtype=torch.float32, device=dev),
+           "T": torch.as_tensor(tv[:, 0]), "sx": torch.as_tensor(tv[:, -1])}
+
+    def mv():
+        obj32.linearize(x32, force=True, batch=Bt)
+        return obj32.jvp(x32, tan)
+    tj, _ = _timed(torch, flush, mv)
+    out["config3_mixed_n256"] = {"fp32_objective_steps_per_s": 2048 / t32, "fp64_objective_steps_per_s": 2048 / t64,
+                                 "fp32_vs_fp64_objective_rel_err": err, "fp32_matvecs_per_s": Bt / tj,
+                                 "matvec_batch": Bt, "steps": 2048}
+    return out
+
+
 def cpu_baseline(target_s=12.0, attempts_full=None):
     """The oracle (torch-CPU restatement, torch.func.jvp) on the host cores for a
     bounded sample: the first k attempts of the same adaptive JVP, scaled to one
@@ -157,6 +219,53 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, rank, local, world):
+    """Serving workload: a seeded Poisson stream of mixed requests {forward
+    shooting, GMRES matvec, adjoint gradient} x n in {64,128,256} x horizons
+    256-2048 steps x Re in {40,50}; n=256 runs FP32 stepping, the rest FP64.
+    Each rank serves its own stream (replicas); value = all requests / max time."""
+    import torch
+    import torch.distributed as dist
+    from ecs_mhd_2d_b200 import build as _build, serving
+    _build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    warm = serving.poisson_requests(9, rate=1000.0, seed=1000 + rank, horizons=(64,))
+    serving.Server(slots=8, chunk_steps=32).run(warm)
+    reqs = serving.poisson_requests(args.requests, rate=args.rate, seed=rank)
+    srv = serving.Server(hbm_budget=96 << 30, slots=16, chunk_steps=32, workers_per_group=4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t)
+    lat = np.array([r.latency for r in res])
+    by = {}
+    for k in ("forward", "matvec", "gradient"):
+        lk = np.array([r.latency for r in res if r.kind == k])
+        if lk.size:
+            by[k] = {"count": int(lk.size), "p50_s": float(np.percentile(lk, 50)), "p99_s": float(np.percentile(lk, 99))}
+    if rank == 0:
+        line = {"metric": "serving throughput (mixed shooting requests)", "value": world * len(res) / wall,
+                "unit": "requests/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+                "data": "synthetic Poisson stream (seeded)",
+                "config": {"workload": "serving_poisson_mixed", "requests": len(res), "arrival_rate_per_s": args.rate,
+                           "n": [64, 128, 256], "horizons": [256, 512, 1024, 2048], "Re": [40, 50],
+                           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                           "by_kind": by, "slots_per_pool": 16, "workers_per_group": 4}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -164,6 +273,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the config 0/2/3 side measurements")
+    ap.add_argument("--workload", default="matvec", choices=["matvec", "serving"],
+                    help="matvec: the headline 128^2 matvec batch; serving: 512 mixed Poisson requests")
+    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--T", type=float, default=None, help="profiling only: shorter horizon (small ncu case)")
     ap.add_argument("--cap", type=int, nargs=2, default=None, help="profiling only: checkpoints max_steps")
     args = ap.parse_args()
@@ -179,6 +293,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "serving":
+        run_serving(args, rank, local, world)
         return
 
     import torch
@@ -319,6 +436,7 @@ def main():
         torch.cuda.synchronize()
         return B * S / (e0.elapsed_time(e1) / 1e3)
     rk4_b64, rk4_b1 = rk4_rate(64), rk4_rate(1)
+    secondary = secondary_workloads(E, torch, dev, flush) if not args.no_secondary else {}
 
     if rank == 0:
         clocks = clk.summary()
@@ -330,7 +448,8 @@ def main():
                 cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
         extra = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
                  "tangent_rk_steps_per_s": value * info.get("accepted", 0),
-                 "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1}}
+                 "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1},
+                 "secondary": secondary}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial condition and tangents)",

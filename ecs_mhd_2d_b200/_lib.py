@@ -76,6 +76,11 @@ SIGNATURES = {
     "ecs_arnoldi_mgs": (_I, [_VP, ctypes.c_long, _I, _VP, _VP, ctypes.c_long, _VP]),
     "ecs_hessenberg_lstsq": (_I, [_VP, _I, _I, _VP, _VP, _VP]),
     "ecs_state_vel_noalloc": (_I, [_I, _D, _D, _D, _D, _VP, _VP, _VP, _I, _I, _VP]),
+    "ecs_pool_reset": (_I, [_VP, _VP]),
+    "ecs_pool_admit": (_I, [_VP, _I, ctypes.POINTER(EcsShootCfg), _VP, _D, _D, _VP]),
+    "ecs_pool_advance": (_I, [_VP, _I, _VP]),
+    "ecs_pool_poll": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), _VP]),
+    "ecs_pool_retire": (_I, [_VP, _I, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -21,11 +21,14 @@ class Objective:
     """objective_RPO(input_dict, param_dict, mode) as a callable with cached
     linearisations for jvp / vjp."""
 
-    def __init__(self, param_dict, mode):
+    def __init__(self, param_dict, mode, ctx=None):
+        """`ctx` pins a private context (e.g. one per serving worker thread);
+        by default contexts come from the shared per-physics cache."""
         self.param_dict, self.mode = param_dict, mode
         self.cfg = shoot_cfg(param_dict, mode)
         self._key = None
         self._ctx = None
+        self._own_ctx = ctx
         self.last_info = None
         self.last_value = None
 
@@ -43,7 +46,11 @@ class Objective:
         if fields.shape[0] != 1:
             raise ValueError("linearize takes one primal point")
         n = fields.shape[-1]
-        ctx = _ctx.get_context(self.param_dict, n, fields.dtype, batch)
+        if self._own_ctx is not None:
+            ctx = self._own_ctx
+            ctx.ensure_batch(batch)
+        else:
+            ctx = _ctx.get_context(self.param_dict, n, fields.dtype, batch)
         key = (id(ctx), ctx.handle.value if ctx.handle else None) + self._primal_key(input_dict["fields"]
                                                                                     if isinstance(input_dict["fields"], torch.Tensor)
                                                                                     else fields, T[0], sx[0])
@@ -119,11 +126,11 @@ def vjp(obj, primal_dict):
     return out, jacT
 
 
-def loss_and_grad(input_dict, param_dict, mode, normalized=False, obj=None):
+def loss_and_grad(input_dict, param_dict, mode, normalized=False, obj=None, ctx=None):
     """((loss, info), grad) of loss_RPO = mean(irfft2(f - f0)^2) (jax_scripts/lib/loss_functions.py:99-111)
     as jax.value_and_grad(..., has_aux=True) gives it (jax_scripts/adjoint_descent.py:90-96).
     normalized=True uses |shift(u(T)) - u(0)|^2 / |u(0)|^2 instead."""
-    obj = obj or Objective(param_dict, mode)
+    obj = obj or Objective(param_dict, mode, ctx=ctx)
     obj._key = None   # the loss is evaluated at a new point each call
     ctx = obj.linearize(input_dict)
     out = obj.last_value["fields"]

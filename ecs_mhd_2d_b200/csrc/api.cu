@@ -102,6 +102,7 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->hcount) cudaFreeHost(ctx->hcount);
   if (ctx->g43.exec) cudaGraphExecDestroy(ctx->g43.exec);
   if (ctx->g4.exec) cudaGraphExecDestroy(ctx->g4.exec);
+  if (ctx->gpool.exec) cudaGraphExecDestroy(ctx->gpool.exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->lin.rec) cudaFree(ctx->lin.rec);
   if (ctx->lin.ckpt) cudaFree(ctx->lin.ckpt);
@@ -195,4 +196,43 @@ int ecs_bench_kernel(ecs_ctx* ctx, int which, int batch, int iters, float* ms, d
   ECS_CHECK_CTX(ctx, batch);
   if (!ms || !bytes || iters < 1 || which < 0 || which > 1) return set_err(ctx, ECS_ERR_INVALID, "bad arguments");
   return table_of(ctx)->bench_kernel(ctx, which, batch, iters, ms, bytes, as_stream(stream));
+}
+
+int ecs_pool_reset(ecs_ctx* ctx, void* stream) {
+  if (!ctx) return ECS_ERR_INVALID;
+  return table_of(ctx)->pool_reset(ctx, as_stream(stream));
+}
+
+int ecs_pool_admit(ecs_ctx* ctx, int slot, const ecs_shoot_cfg* cfg, const void* fields, double T, double sx,
+                   void* stream) {
+  if (!ctx || !cfg || !fields) return ECS_ERR_INVALID;
+  if (slot < 0 || slot >= ctx->max_batch) return set_err(ctx, ECS_ERR_INVALID, "slot out of range");
+  return table_of(ctx)->pool_admit(ctx, slot, cfg, fields, T, sx, as_stream(stream));
+}
+
+int ecs_pool_advance(ecs_ctx* ctx, int nsteps, void* stream) {
+  if (!ctx || nsteps < 1) return ECS_ERR_INVALID;
+  return table_of(ctx)->pool_advance(ctx, nsteps, as_stream(stream));
+}
+
+int ecs_pool_poll(ecs_ctx* ctx, int* done, int* steps_done, void* stream) {
+  if (!ctx || !done) return ECS_ERR_INVALID;
+  std::vector<ecs::StepCtl> h(ctx->max_batch);
+  cudaError_t e = cudaMemcpyAsync(h.data(), ctx->ctl, sizeof(ecs::StepCtl) * ctx->max_batch, cudaMemcpyDeviceToHost,
+                                  as_stream(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+  if (e != cudaSuccess) return set_err(ctx, ECS_ERR_CUDA, cudaGetErrorString(e));
+  for (int b = 0; b < ctx->max_batch; ++b) {
+    const bool active = b < (int)ctx->pool.size() && ctx->pool[b].active;
+    done[b] = active ? h[b].done : 0;
+    if (steps_done) steps_done[b] = active ? h[b].steps_done : 0;
+  }
+  return ECS_OK;
+}
+
+int ecs_pool_retire(ecs_ctx* ctx, int slot, void* out_fields, double* loss, void* stream) {
+  if (!ctx) return ECS_ERR_INVALID;
+  if (slot < 0 || slot >= (int)ctx->pool.size() || !ctx->pool[slot].active)
+    return set_err(ctx, ECS_ERR_INVALID, "slot not active");
+  return table_of(ctx)->pool_retire(ctx, slot, out_fields, loss, as_stream(stream));
 }

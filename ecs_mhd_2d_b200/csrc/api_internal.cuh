@@ -67,6 +67,12 @@ struct ecs_ctx {
     void* rec = nullptr; double* rec_h = nullptr; int* rec_acc = nullptr;
     long long nodes = 0;
   } g43;
+  // slot pool (continuous batching of forward shootings)
+  struct PoolSlot { int active = 0, ny = 0, rot = 0; long steps = 0; };
+  std::vector<PoolSlot> pool;
+  void* pool_fields = nullptr;   // [B][2][N][N] the admitted fields (residual base)
+  double* pool_sx = nullptr;     // [B]
+  struct GraphPool { cudaGraphExec_t exec = nullptr; long long nodes = 0; } gpool;
   struct Graph4 {
     cudaGraphExec_t exec = nullptr;
     int B = 0;

@@ -84,6 +84,8 @@ struct StepCtl {
   int attempts;         // attempts recorded
   unsigned long long err_bits;  // atomicMax scratch for |err| (non-negative doubles)
   unsigned int err_blocks;      // blocks that have reported their error partial
+  int steps_total;              // slot pool: fixed steps of the request
+  int steps_done;               // slot pool: steps taken
   int pad;
 };
 

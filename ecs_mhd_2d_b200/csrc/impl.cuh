@@ -26,9 +26,12 @@ namespace ecs {
 constexpr int XT = 8;
 constexpr int COLWARPS = 4;
 
-template <typename R, int N> size_t smem_row_rhs() { return (N / 2 + 10 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (N / 2 + 10 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
+// Small batches use 2-row tiles: 4x more CTAs for the same rows.
+constexpr int XTS = 2;
+template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
 template <typename R, int N> size_t smem_row_8f() { return (N / 2 + 8 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
-template <typename R, int N> size_t smem_row_2f() { return (N / 2 + 2 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N, int X = XT> size_t smem_row_2f() { return (N / 2 + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
 template <typename R, int N>
 int configure_kernels(ecs_ctx* c) {
@@ -40,6 +43,10 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_phys<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_8f<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_rhs<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
+  st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N, XTS>());
+  st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
+  st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
   return ECS_OK;
 }
@@ -78,13 +85,14 @@ void launch_row_from_box(ecs_ctx* c, const cplx<R>* G2, R* out, const R* base, d
 
 template <typename R, int N>
 void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStream_t s, cplx<R>* rec = nullptr,
-                    long rec_bstride = 0) {
+                    long rec_bstride = 0, int use_done = 0) {
   ColParams<R> p;
   p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.F = (cplx<R>*)c->F; p.A1 = (cplx<R>*)c->A1;
   p.K2 = (cplx<R>*)c->K2; p.OUT = (cplx<R>*)c->OUT; p.Etab = (const R*)c->Etab; p.ctl = c->ctl;
   p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.nu = (R)c->nu; p.eta = (R)c->eta;
   p.B = B; p.stage = stage; p.produce = produce; p.diss = diss; p.rec = rec; p.rec_bstride = rec_bstride;
-  const int cols = B * Geomc<N>::K;
+  p.use_done = use_done;
+  const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
   ++c->launches;
   switch (stage) {
@@ -102,7 +110,9 @@ void launch_row_rhs(ecs_ctx* c, int B, R* phys, cudaStream_t s, const StepCtl* c
   RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.phys_bstride = 0; p.rec_index = 0; p.phys_stage = 0; p.ctl = ctl;
   p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
-  ++c->launches; k_row_rhs<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  ++c->launches;
+  if (small_rows<N>(B)) k_row_rhs<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
+  else k_row_rhs<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
 }
 
 template <typename R, int N>
@@ -111,7 +121,7 @@ void launch_col_rk43(ecs_ctx* c, int B, int stage, cudaStream_t s, cplx<R>* rec 
   p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.S = (cplx<R>*)c->S43; p.ctl = c->ctl;
   p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.rec = rec; p.cap = cap;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
-  const int cols = B * Geomc<N>::K;
+  const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
   ++c->launches;
   switch (stage) {
@@ -130,7 +140,9 @@ void launch_row_err(ecs_ctx* c, int B, double atol, cudaStream_t s, double* rec_
                     int cap = 0) {
   RowErrParams<R> p; p.G = (const cplx<R>*)c->G; p.ctl = c->ctl; p.tw = (const cplx<R>*)c->tw; p.atol = atol;
   p.rec_h = rec_h; p.rec_acc = rec_acc; p.cap = cap; p.B = B;
-  ++c->launches; k_row_err<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
+  ++c->launches;
+  if (small_rows<N>(B)) k_row_err<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_2f<R, N, XTS>(), s>>>(p);
+  else k_row_err<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
 }
 
 template <typename R, int N>
@@ -148,7 +160,9 @@ template <typename R, int N>
 void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
   RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B;
-  ++c->launches; k_row_tan<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  ++c->launches;
+  if (small_rows<N>(B)) k_row_tan<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
+  else k_row_tan<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
 }
 
 template <typename R, int N>
@@ -157,7 +171,7 @@ void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* re
   ColTanParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
   p.rec = rec; p.dT = dT; p.t = t; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage; p.produce = produce;
-  const int cols = B * Geomc<N>::K;
+  const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
   ++c->launches;
   switch (stage) {
@@ -180,7 +194,9 @@ template <typename R, int N>
 void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
   RowAdjParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B;
-  ++c->launches; k_row_adj<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  ++c->launches;
+  if (small_rows<N>(B)) k_row_adj<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
+  else k_row_adj<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
 }
 
 template <typename R, int N>
@@ -189,7 +205,7 @@ void launch_col_adj(ecs_ctx* c, int B, int stage, const cplx<R>* rec, const cplx
   ColAdjParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.J = (cplx<R>*)c->D; p.nslot = nslot;
   p.rec = rec; p.rec_prev = rec_prev; p.hacc = c->hacc; p.t = t; p.h = h; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
-  const int cols = B * Geomc<N>::K;
+  const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
   ++c->launches;
   switch (stage) {
@@ -744,10 +760,10 @@ struct Impl {
     const int nslot = rk43 ? (int)JJ_NS43 : (int)J_NS4;
     int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
     if (!st) st = ensure_regen(c);
-    if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * sizeof(double));
+    if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * 2 * sizeof(double));
     if (st) return st;
     cudaMemsetAsync(c->D, 0, (size_t)B * nslot * vb, s);
-    cudaMemsetAsync(c->hacc, 0, (size_t)B * K * sizeof(double), s);
+    cudaMemsetAsync(c->hacc, 0, (size_t)B * K * 2 * sizeof(double), s);
     // head: Ybar = -(c/n^2) rfft2(c_fields) on the box; Phibar = sym^T(Ybar); sxbar
     launch_row_to_box<R, N>(c, cfields, (cplx<R>*)c->H, B, s);
     launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->V, B, 2, s);
@@ -865,6 +881,95 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "vjp");
   }
 
+
+  // ---------------------------------------------------------------------
+  // Slot pool: continuous batching of fixed-step forward shootings.  Every
+  // slot has its own step size and step budget; finished or empty slots are
+  // skipped; requests are admitted between advance calls (step boundaries).
+  // ---------------------------------------------------------------------
+  static int pool_reset(ecs_ctx* c, cudaStream_t s) {
+    ++c->launches; k_pool_init<<<(c->max_batch + 127) / 128, 128, 0, s>>>(c->ctl, 0, c->max_batch, 0);
+    c->pool.assign(c->max_batch, ecs_ctx::PoolSlot());
+    return cuda_err(c, cudaGetLastError(), "pool_reset");
+  }
+
+  static int pool_admit(ecs_ctx* c, int slot, const ecs_shoot_cfg* cfg, const R* fields, double T, double sx,
+                        cudaStream_t s) {
+    if ((int)c->pool.size() != c->max_batch) { int st = pool_reset(c, s); if (st) return st; }
+    if (cfg->mode != ECS_MODE_LAWSON_RK4) return set_err(c, ECS_ERR_BAD_MODE, "the slot pool runs Lawson_RK4");
+    const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
+    if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+    const size_t VEC = 2UL * K * M, fe = 2UL * N * N;
+    R* pf = (R*)c->pool_fields + (size_t)slot * fe;
+    cudaError_t e = cudaMemcpyAsync(pf, fields, fe * sizeof(R), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_err(c, e, "pool admit copy");
+    launch_row_to_box<R, N>(c, pf, (cplx<R>*)c->H, 1, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->F + (size_t)slot * VEC, 1, 2, s);
+    ++c->launches; k_fill<<<1, 32, 0, s>>>(c->Tbuf + slot, T, 1);
+    ++c->launches; k_fill<<<1, 32, 0, s>>>(c->pool_sx + slot, sx, 1);
+    ++c->launches;
+    k_rk4_setup<R><<<grid1d((long)VEC), 256, 0, s>>>(c->Tbuf + slot, cfg->num_checkpoints, cfg->ministeps,
+                                                     c->ctl + slot, (R*)c->Etab + (size_t)slot * VEC, N, c->nu,
+                                                     c->eta, 1);
+    ++c->launches; k_pool_init<<<1, 32, 0, s>>>(c->ctl, slot, 1, (int)steps);
+    auto& ps = c->pool[slot];
+    ps.active = 1; ps.ny = cfg->shift_reflect_ny; ps.rot = cfg->rot; ps.steps = steps;
+    return cuda_err(c, cudaGetLastError(), "pool_admit");
+  }
+
+  static int pool_advance(ecs_ctx* c, int nsteps, cudaStream_t s) {
+    const int B = c->max_batch;
+    auto one_step = [&](cudaStream_t st_) {
+      for (int st = 1; st <= 4; ++st) {
+        launch_row_rhs<R, N>(c, B, nullptr, st_, c->ctl);
+        launch_col_rk4<R, N>(c, B, st, 1, 0, st_, nullptr, 0, 1);
+      }
+      ++c->launches; k_pool_count<<<(B + 127) / 128, 128, 0, st_>>>(c->ctl, B);
+    };
+    constexpr int GS = 8;
+    auto& gk = c->gpool;
+    if (!gk.exec) {
+      const long long l0 = c->launches;
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int a = 0; a < GS; ++a) one_step(c->cap_stream);
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&gk.exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) { gk.exec = nullptr; return cuda_err(c, e, "pool graph capture"); }
+      gk.nodes = c->launches - l0;
+      c->launches = l0;
+    }
+    launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s, nullptr, 0, 1);
+    int it = 0;
+    for (; it + GS <= nsteps; it += GS) {
+      cudaError_t e = cudaGraphLaunch(gk.exec, s);
+      if (e != cudaSuccess) return cuda_err(c, e, "pool graph launch");
+      c->launches += gk.nodes;
+    }
+    for (; it < nsteps; ++it) one_step(s);
+    return cuda_err(c, cudaGetLastError(), "pool_advance");
+  }
+
+  static int pool_retire(ecs_ctx* c, int slot, R* out_fields, double* loss, cudaStream_t s) {
+    const size_t VEC = 2UL * K * M, fe = 2UL * N * N;
+    auto& ps = c->pool[slot];
+    const R* pf = (const R*)c->pool_fields + (size_t)slot * fe;
+    launch_col_from_box<R, N>(c, (const cplx<R>*)c->F + (size_t)slot * VEC, (cplx<R>*)c->G, 1, c->pool_sx + slot,
+                              ps.ny, ps.rot, 1, 0, s, 1);
+    R* out = out_fields ? out_fields : (R*)c->fields_tmp;
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, out, pf, nullptr, 1, 1, s);
+    if (loss) {
+      ++c->launches; k_rowsq<R><<<N, 32, 0, s>>>(out, c->rowsq, N);
+      ++c->launches; k_reduce_rows<<<1, 128, 0, s>>>(c->rowsq, loss, N, 1, 1.0 / (2.0 * N * N));
+    }
+    ps.active = 0;
+    ++c->launches; k_pool_init<<<1, 32, 0, s>>>(c->ctl, slot, 1, 0);
+    return cuda_err(c, cudaGetLastError(), "pool_retire");
+  }
+
   // Time `iters` launches of one hot kernel on the current workspace (after a
   // jvp call) with CUDA events on stream s; returns ms per launch and the
   // kernel's algorithmic bytes per launch.
@@ -919,6 +1024,8 @@ int ctx_init(ecs_ctx* c, const ecs_params* prm) {
   c->fields_tmp2 = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
   c->S43 = dev_alloc(c, nbox * S_NSLOT * cb, &st);
   c->dcount = (int*)dev_alloc(c, sizeof(int), &st);
+  c->pool_fields = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
+  c->pool_sx = (double*)dev_alloc(c, (size_t)B * sizeof(double), &st);
   c->ctl = (StepCtl*)dev_alloc(c, (size_t)B * sizeof(StepCtl), &st);
   c->rowsq = (double*)dev_alloc(c, (size_t)B * N * sizeof(double), &st);
   c->Tbuf = (double*)dev_alloc(c, (size_t)B * sizeof(double), &st);
@@ -992,6 +1099,12 @@ ImplTable make_table() {
              cudaStream_t s) { return I::vjp(c, (const R*)cf, cT, csx, (R*)g, gT, gsx, B, s); };
   t.bench_kernel = [](ecs_ctx* c, int which, int B, int iters, float* ms, double* bytes, cudaStream_t s) {
     return I::bench_kernel(c, which, B, iters, ms, bytes, s); };
+  t.pool_reset = [](ecs_ctx* c, cudaStream_t s) { return I::pool_reset(c, s); };
+  t.pool_admit = [](ecs_ctx* c, int slot, const ecs_shoot_cfg* cfg, const void* f, double T, double sx,
+                    cudaStream_t s) { return I::pool_admit(c, slot, cfg, (const R*)f, T, sx, s); };
+  t.pool_advance = [](ecs_ctx* c, int nsteps, cudaStream_t s) { return I::pool_advance(c, nsteps, s); };
+  t.pool_retire = [](ecs_ctx* c, int slot, void* o, double* loss, cudaStream_t s) {
+    return I::pool_retire(c, slot, (R*)o, loss, s); };
   return t;
 }
 

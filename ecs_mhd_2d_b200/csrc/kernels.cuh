@@ -134,6 +134,63 @@ __device__ __forceinline__ void col_inverse2(const cplx<R> (&x0)[N / 32], const 
 }
 
 // ---------------------------------------------------------------------------
+// per-channel column helpers (one warp per (batch, ky, channel))
+// ---------------------------------------------------------------------------
+
+// Load column H[b][f][ky][:] (nf fields per batch element) and transform it
+// along x (forward, natural -> bit-reversed order).
+template <typename R, int N>
+__device__ __forceinline__ void col_load_fwd1(const cplx<R>* __restrict__ H, int nf, int b, int f, int ky, int lane,
+                                              const cplx<R>* s_tw, cplx<R> (&r)[N / 32]) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const cplx<R>* h = H + ((size_t)(b * nf + f) * K + ky) * N;
+#pragma unroll
+  for (int j = 0; j < E; ++j) r[j] = h[lane + 32 * j];
+  fft_dif<R, N, false>(r, s_tw, lane);
+}
+
+// Stage input of channel c (bit-reversed slot order) -> its 4 multiplied
+// inverse transforms along x (fields 4c..4c+3 of state_vel, mhd_jax.py:136-141),
+// scaled by 1/n^2.  One copy of the transform code: the m loop is not unrolled.
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse4(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int b, int c,
+                                             int ky, int lane, const cplx<R>* s_tw) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const R inv_n2 = R(1) / (R(N) * R(N));
+#pragma unroll 1
+  for (int m = 0; m < 4; ++m) {
+    cplx<R> w[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      w[j] = cscale(cimul(x[j], spectral_mu<R>(m, kx, ky)), inv_n2);
+    }
+    fft_dit<R, N, true>(w, s_tw, lane);
+    cplx<R>* gout = G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
+#pragma unroll
+    for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+  }
+}
+
+// One plain inverse transform along x of a box column, scaled, to field f of
+// G[b] (nf fields per batch element).
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse1(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int nf, int b,
+                                             int f, int ky, int lane, const cplx<R>* s_tw, R scale) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  cplx<R> w[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) w[j] = cscale(x[j], scale);
+  fft_dit<R, N, true>(w, s_tw, lane);
+  cplx<R>* gout = G + ((size_t)(b * nf + f) * K + ky) * N;
+#pragma unroll
+  for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+}
+
+// ---------------------------------------------------------------------------
 // Column pass of the forward RHS fused with the Lawson-RK4 stage algebra
 // (reference: timestepping.lawson_rk4, jax_scripts/lib/timestepping.py:69-80).
 // ---------------------------------------------------------------------------
@@ -170,127 +227,87 @@ struct ColParams {
   int diss;              // COL_PLAIN: add L f (f = F)
   cplx<R>* rec;          // optional record of this step: [Q_NREC][2][K][M] per batch element
   long rec_bstride;      // elements between batch elements in rec
+  int use_done;          // skip batch elements whose ctl.done is set (slot pool)
 };
 
 template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
   __shared__ cplx<R> s_tw[N / 2];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (col >= p.B * K) return;
-  const int b = col / K, ky = col - b * K;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  const int c = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
 
-  cplx<R> r0[E], r1[E];
-  if (STAGE != COL_START) {
-    const cplx<R>* h0 = p.H + ((size_t)(b * 2 + 0) * K + ky) * N;
-    const cplx<R>* h1 = p.H + ((size_t)(b * 2 + 1) * K + ky) * N;
-#pragma unroll
-    for (int j = 0; j < E; ++j) { r0[j] = h0[lane + 32 * j]; r1[j] = h1[lane + 32 * j]; }
-    fft_dif<R, N, false>(r0, s_tw, lane);
-    fft_dif<R, N, false>(r1, s_tw, lane);
-  }
+  cplx<R> r[E];
+  if (STAGE != COL_START) col_load_fwd1<R, N>(p.H, 2, b, c, ky, lane, s_tw, r);
+  if (p.use_done && p.ctl[b].done) return;
   const R h = (R)p.ctl[b].h;
-  cplx<R> x0[E], x1[E];
-  const size_t base0 = ((size_t)(b * 2 + 0) * K + ky) * M;
-  const size_t base1 = ((size_t)(b * 2 + 1) * K + ky) * M;
+  const size_t base = ((size_t)(b * 2 + c) * K + ky) * M;
+  cplx<R>* rb = p.rec ? p.rec + (size_t)b * p.rec_bstride : nullptr;
+  cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int pos = bitrev<N>(lane + 32 * j);
-    const int slot = pos_to_slot(pos, N, KMAX, M);
-    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    x[j] = mk<R>(0, 0);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
-    cplx<R> v0 = mk<R>(0, 0), v1 = mk<R>(0, 0);
+    cplx<R> v = mk<R>(0, 0);
     if (STAGE != COL_START) {
-      if (in_mask) v0 = cadd(r0[j], p.fhat[ky * M + slot]);   // mask * rfft2(-adv0+adv1+forcing)
-      v1 = cscale(r1[j], ksq_masked<R>(kx, ky));                // k^2 mask * rfft2(u x B)
+      if (c == 0) { if (in_mask) v = cadd(r[j], p.fhat[ky * M + slot]); }   // mask * rfft2(-adv0+adv1+forcing)
+      else v = cscale(r[j], ksq_masked<R>(kx, ky));                           // k^2 mask * rfft2(u x B)
     }
-    const size_t i0 = base0 + slot, i1 = base1 + slot;
-    cplx<R>* rb = p.rec ? p.rec + (size_t)b * p.rec_bstride : nullptr;
-    const size_t VEC = (size_t)2 * K * M;
-    const size_t o0 = (size_t)ky * M + slot, o1 = (size_t)(K + ky) * M + slot;
-    auto put = [&](int q, cplx<R> a0, cplx<R> a1) {
-      if (rb) { rb[q * VEC + o0] = a0; rb[q * VEC + o1] = a1; }
-    };
+    const size_t i = base + slot;
+    const size_t o = ((size_t)c * K + ky) * M + slot;
+    auto put = [&](int q, cplx<R> a) { if (rb) rb[q * VEC + o] = a; };
     switch (STAGE) {
-      case COL_START: {
-        x0[j] = p.F[i0]; x1[j] = p.F[i1];
+      case COL_START: x[j] = p.F[i]; break;
+      case COL_RK4_S1: {   // k1 = h v(f); f = e f; k1 = e k1; X2 = f + k1/2   (timestepping.py:74-76)
+        const R e = p.Etab[i];
+        cplx<R> k1 = cscale(v, h);
+        put(Q_F, p.F[i]); put(Q_K1, k1);
+        const cplx<R> f = cscale(p.F[i], e);
+        k1 = cscale(k1, e);
+        p.F[i] = f; p.A1[i] = k1;
+        x[j] = cadd(f, cscale(k1, R(0.5)));
+        put(Q_X2, x[j]);
       } break;
-      case COL_RK4_S1: {   // k1 = h v(f); f = e f; k1 = e k1; X2 = f + k1/2
-        const R e0 = p.Etab[i0], e1 = p.Etab[i1];
-        cplx<R> k10 = cscale(v0, h), k11 = cscale(v1, h);
-        put(Q_F, p.F[i0], p.F[i1]);
-        put(Q_K1, k10, k11);
-        cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
-        k10 = cscale(k10, e0); k11 = cscale(k11, e1);
-        p.F[i0] = f0; p.F[i1] = f1; p.A1[i0] = k10; p.A1[i1] = k11;
-        x0[j] = cadd(f0, cscale(k10, R(0.5))); x1[j] = cadd(f1, cscale(k11, R(0.5)));
-        put(Q_X2, x0[j], x1[j]);
+      case COL_RK4_S2: {   // k2 = h v(X2); X3 = f + k2/2   (:76-77)
+        const cplx<R> k2 = cscale(v, h);
+        p.K2[i] = k2;
+        x[j] = cadd(p.F[i], cscale(k2, R(0.5)));
+        put(Q_K2, k2); put(Q_X3, x[j]);
       } break;
-      case COL_RK4_S2: {   // k2 = h v(X2); X3 = f + k2/2
-        cplx<R> k20 = cscale(v0, h), k21 = cscale(v1, h);
-        p.K2[i0] = k20; p.K2[i1] = k21;
-        x0[j] = cadd(p.F[i0], cscale(k20, R(0.5))); x1[j] = cadd(p.F[i1], cscale(k21, R(0.5)));
-        put(Q_K2, k20, k21);
-        put(Q_X3, x0[j], x1[j]);
+      case COL_RK4_S3: {   // k3; f,k1,k2,k3 *= e; X4 = f + k3; acc = f + k1/6 + k2/3 + k3/3   (:77-80)
+        const R e = p.Etab[i];
+        cplx<R> k3 = cscale(v, h);
+        put(Q_K3, k3);
+        const cplx<R> f = cscale(p.F[i], e), a = cscale(p.A1[i], e), q2 = cscale(p.K2[i], e);
+        k3 = cscale(k3, e);
+        x[j] = cadd(f, k3);
+        put(Q_X4, x[j]);
+        p.F[i] = cadd(cadd(cadd(f, cdiv_r(a, R(6))), cdiv_r(q2, R(3))), cdiv_r(k3, R(3)));
       } break;
-      case COL_RK4_S3: {   // k3; f,k1,k2,k3 *= e; X4 = f + k3; acc = f + k1/6 + k2/3 + k3/3
-        const R e0 = p.Etab[i0], e1 = p.Etab[i1];
-        cplx<R> k30 = cscale(v0, h), k31 = cscale(v1, h);
-        put(Q_K3, k30, k31);
-        cplx<R> f0 = cscale(p.F[i0], e0), f1 = cscale(p.F[i1], e1);
-        cplx<R> a0 = cscale(p.A1[i0], e0), a1 = cscale(p.A1[i1], e1);
-        cplx<R> c0 = cscale(p.K2[i0], e0), c1 = cscale(p.K2[i1], e1);
-        k30 = cscale(k30, e0); k31 = cscale(k31, e1);
-        x0[j] = cadd(f0, k30); x1[j] = cadd(f1, k31);
-        put(Q_X4, x0[j], x1[j]);
-        cplx<R> s0 = cadd(cadd(cadd(f0, cdiv_r(a0, R(6))), cdiv_r(c0, R(3))), cdiv_r(k30, R(3)));
-        cplx<R> s1 = cadd(cadd(cadd(f1, cdiv_r(a1, R(6))), cdiv_r(c1, R(3))), cdiv_r(k31, R(3)));
-        p.F[i0] = s0; p.F[i1] = s1;
+      case COL_RK4_S4: {   // k4; f = acc + k4/6   (:79-80)
+        const cplx<R> k4 = cscale(v, h);
+        put(Q_K4, k4);
+        const cplx<R> f = cadd(p.F[i], cdiv_r(k4, R(6)));
+        p.F[i] = f;
+        x[j] = f;
       } break;
-      case COL_RK4_S4: {   // k4; f = acc + k4/6
-        cplx<R> k40 = cscale(v0, h), k41 = cscale(v1, h);
-        put(Q_K4, k40, k41);
-        cplx<R> f0 = cadd(p.F[i0], cdiv_r(k40, R(6))), f1 = cadd(p.F[i1], cdiv_r(k41, R(6)));
-        p.F[i0] = f0; p.F[i1] = f1;
-        x0[j] = f0; x1[j] = f1;
-      } break;
-      default: {           // COL_PLAIN: state_vel output
-        if (p.diss) {
-          v0 = cadd(v0, cscale(p.F[i0], diss_L<R>(kx, ky, p.nu)));
-          v1 = cadd(v1, cscale(p.F[i1], diss_L<R>(kx, ky, p.eta)));
-        }
-        p.OUT[i0] = v0; p.OUT[i1] = v1;
+      default: {           // COL_PLAIN: state_vel output (mhd_jax.py:171-173)
+        if (p.diss) v = cadd(v, cscale(p.F[i], diss_L<R>(kx, ky, c == 0 ? p.nu : p.eta)));
+        p.OUT[i] = v;
       } break;
     }
   }
   if (!p.produce) return;
-  // stage input -> 8 multiplied inverse transforms along x (irfft2 over kx, scaled 1/n^2)
-  const R inv_n2 = R(1) / (R(N) * R(N));
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      cplx<R> w[E];
-#pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int pos = bitrev<N>(lane + 32 * j);
-        const int kx = pos_to_k(pos, N);
-        const cplx<R> xv = c == 0 ? x0[j] : x1[j];
-        const R mu = spectral_mu<R>(m, kx, ky);
-        w[j] = cscale(cimul(xv, mu), inv_n2);
-      }
-      fft_dit<R, N, true>(w, s_tw, lane);
-      cplx<R>* gout = p.G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
-#pragma unroll
-      for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
-    }
-  }
+  col_inverse4<R, N>(x, p.G, b, c, ky, lane, s_tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -725,6 +742,26 @@ __global__ void k_rowsq(const R* f, double* rowsq, int n) {
 template <typename R>
 __global__ void k_axpy(R* y, const R* x, R a, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+
+// Slot pool: initialise one slot's control (steps_total = 0 marks it inactive).
+static __global__ void k_pool_init(StepCtl* ctl, int first, int count, int steps_total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  StepCtl& c = ctl[first + i];
+  c.steps_total = steps_total; c.steps_done = 0; c.done = steps_total > 0 ? 0 : 1;
+  c.attempts = 0; c.accepted = 0; c.rejected = 0; c.pending_accept = 0;
+}
+
+// Slot pool: count one finished step per active slot; a slot whose budget is
+// spent is marked done and skipped by every later launch.
+static __global__ void k_pool_count(StepCtl* ctl, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  StepCtl& c = ctl[b];
+  if (c.done || c.steps_total <= 0) return;
+  c.steps_done += 1;
+  if (c.steps_done >= c.steps_total) c.done = 1;
 }
 
 // Deterministic per-batch reduction of row partials: out[b] = scale * sum_x rowsq[b][x].

@@ -105,7 +105,7 @@ struct ColAdjParams {
   int nslot;
   const cplx<R>* rec;   // primal record of this step / attempt
   const cplx<R>* rec_prev;   // Lawson-RK4 AJ_S1: record of the previous step (null at the first step)
-  double* hacc;         // [B][K] accumulators of dL/dh (RK4) or dL/dt (RK4(3))
+  double* hacc;         // [B][K][2] accumulators of dL/dh (RK4) or dL/dt (RK4(3))
   double t, h;
   const cplx<R>* tw;
   R nu, eta;
@@ -123,185 +123,167 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (col >= p.B * K) return;
-  const int b = col / K, ky = col - b * K;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
   cplx<R>* J = p.J + (size_t)b * p.nslot * VEC;
   const cplx<R>* Q = p.rec;
   const R h = (R)p.h, t = (R)p.t;
-  const bool rk43 = STAGE >= AJ43_INIT;
-  const bool has_rhs = !(STAGE == AJ_PRE || STAGE == AJ43_PRE || STAGE == AJ43_IPRE);
+  constexpr bool rk43 = STAGE >= AJ43_INIT;
+  constexpr bool has_rhs = !(STAGE == AJ_PRE || STAGE == AJ43_PRE || STAGE == AJ43_IPRE);
   const R cky = ky == 0 ? R(1) : R(2);
   const R inv_n2 = R(1) / (R(N) * R(N));
+  const R coeff = ch == 0 ? p.nu : p.eta;
 
-  // Xbar_c = (c/n^2) sum_m (-i mu_m) rfft2(fbar_mc)
-  cplx<R> xb0[E], xb1[E];
+  // Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_{m,c})
+  cplx<R> xb[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) { xb0[j] = mk<R>(0, 0); xb1[j] = mk<R>(0, 0); }
+  for (int j = 0; j < E; ++j) xb[j] = mk<R>(0, 0);
   if (has_rhs) {
 #pragma unroll 1
-    for (int cm = 0; cm < 8; ++cm) {
-      const int c = cm >> 2, m = cm & 3;
-      {
-        const cplx<R>* hin = p.H + ((size_t)(b * 8 + 4 * c + m) * K + ky) * N;
-        cplx<R> v[E];
+    for (int m = 0; m < 4; ++m) {
+      cplx<R> v[E];
+      col_load_fwd1<R, N>(p.H, 8, b, 4 * ch + m, ky, lane, s_tw, v);
 #pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = hin[lane + 32 * j];
-        fft_dif<R, N, false>(v, s_tw, lane);
-#pragma unroll
-        for (int j = 0; j < E; ++j) {
-          const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
-          const cplx<R> tmul = cimul(v[j], -spectral_mu<R>(m, kx, ky));
-          if (c == 0) xb0[j] = cadd(xb0[j], tmul); else xb1[j] = cadd(xb1[j], tmul);
-        }
+      for (int j = 0; j < E; ++j) {
+        const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+        xb[j] = cadd(xb[j], cimul(v[j], -spectral_mu<R>(m, kx, ky)));
       }
     }
 #pragma unroll
-    for (int j = 0; j < E; ++j) { xb0[j] = cscale(xb0[j], cky * inv_n2); xb1[j] = cscale(xb1[j], cky * inv_n2); }
+    for (int j = 0; j < E; ++j) xb[j] = cscale(xb[j], cky * inv_n2);
   }
 
   double hpart = 0.0;
-  cplx<R> lam0[E], lam1[E];   // next adjoint-RHS input (mask lam_w / c, k^2 mask lam_j / c), unscaled inverse
+  bool feed = true;
+  cplx<R> lam[E];   // next adjoint-RHS input (mask lam_w or k^2 mask lam_j) / c_ky
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    lam0[j] = mk<R>(0, 0); lam1[j] = mk<R>(0, 0);
+    lam[j] = mk<R>(0, 0);
     const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
-#pragma unroll
-    for (int ch = 0; ch < 2; ++ch) {
-      const size_t o = ((size_t)ch * K + ky) * M + slot;
-      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
-      const cplx<R> Xb = ch == 0 ? xb0[j] : xb1[j];
-      cplx<R> kb = mk<R>(0, 0);   // cotangent k-bar fed to the next adjoint RHS (before the h or t factor)
-      bool feed = true;
-      if (!rk43) {
-        const R e = in_mask ? exp(h / R(2) * L) : R(0);
-        const R dedh = e * L / R(2);
-        auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
-        switch (STAGE) {
-          case AJ_PRE: {
-            const cplx<R> ob = J[J_OB * VEC + o];
-            J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_r(ob, R(6));
-            J[J_K2 * VEC + o] = cdiv_r(ob, R(3)); J[J_B3 * VEC + o] = cdiv_r(ob, R(3));
-            kb = cdiv_r(ob, R(6));                                   // k4bar
-            hpart += ip(kb, Q[Q_K4 * VEC + o]) / (double)h;
-          } break;
-          case AJ_S4: {
-            const cplx<R> f2b = cadd(J[J_F2 * VEC + o], Xb), b3b = cadd(J[J_B3 * VEC + o], Xb);
-            const cplx<R> b2b = J[J_K2 * VEC + o], b1b = J[J_A1 * VEC + o];
-            const cplx<R> f = Q[Q_F * VEC + o], k1 = Q[Q_K1 * VEC + o];
-            const double eb = ip(b3b, Q[Q_K3 * VEC + o]) + ip(b2b, Q[Q_K2 * VEC + o]) + ip(b1b, cscale(k1, e)) +
-                              ip(f2b, cscale(f, e));
-            hpart += eb * (double)dedh;
-            kb = cscale(b3b, e);                                     // k3bar
-            hpart += ip(kb, Q[Q_K3 * VEC + o]) / (double)h;
-            J[J_F2 * VEC + o] = cscale(f2b, e);                      // f1bar
-            J[J_A1 * VEC + o] = cscale(b1b, e);                      // a1bar
-            J[J_K2 * VEC + o] = cscale(b2b, e);                      // k2bar
-          } break;
-          case AJ_S3: {
-            J[J_F2 * VEC + o] = cadd(J[J_F2 * VEC + o], Xb);
-            kb = cadd(J[J_K2 * VEC + o], cscale(Xb, R(0.5)));        // k2bar final
-            hpart += ip(kb, Q[Q_K2 * VEC + o]) / (double)h;
-          } break;
-          case AJ_S2: {
-            const cplx<R> f1b = cadd(J[J_F2 * VEC + o], Xb);
-            const cplx<R> a1b = cadd(J[J_A1 * VEC + o], cscale(Xb, R(0.5)));
-            const double eb = ip(a1b, Q[Q_K1 * VEC + o]) + ip(f1b, Q[Q_F * VEC + o]);
-            hpart += eb * (double)dedh;
-            kb = cscale(a1b, e);                                     // k1bar
-            hpart += ip(kb, Q[Q_K1 * VEC + o]) / (double)h;
-            J[J_OB * VEC + o] = cscale(f1b, e);                      // fbar (without the RHS1 term)
-          } break;
-          default: {   // AJ_S1: fbar += X1bar; then seed the previous step (if any)
-            const cplx<R> fb = cadd(J[J_OB * VEC + o], Xb);
-            J[J_OB * VEC + o] = fb;
-            if (p.rec_prev) {
-              J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_r(fb, R(6));
-              J[J_K2 * VEC + o] = cdiv_r(fb, R(3)); J[J_B3 * VEC + o] = cdiv_r(fb, R(3));
-              kb = cdiv_r(fb, R(6));
-              hpart += ip(kb, p.rec_prev[Q_K4 * VEC + o]) / (double)h;
-            } else {
-              feed = false;
-            }
-          } break;
-        }
-        kb = cscale(kb, h);
-      } else {
-        const R e = exp((t * L) * h / R(2));
-        const R dedt = e * (L * h / R(2));
-        auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
-        switch (STAGE) {
-          case AJ43_PRE:      // from (xbar_f, k5bar) in (X0, K1) slots: RHS5 input = k5bar
-          case AJ43_IPRE: {   // initial k1 = t v(x0): input = k1bar
-            kb = J[JJ_K1 * VEC + o];
-            hpart += ip(kb, Q[(STAGE == AJ43_PRE ? RR_K5 : RR_K1) * VEC + o]) / (double)t;
-          } break;
-          case AJ43_S5: {     // xbar_f += Xbar5; distribute to x2, k1'', k2', k3', k4
-            const cplx<R> xfb = cadd(J[JJ_X0 * VEC + o], Xb);
-            J[JJ_X2 * VEC + o] = xfb;
-            J[JJ_K1PP * VEC + o] = cdiv_r(cscale(xfb, h), R(6));
-            J[JJ_K2P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
-            J[JJ_K3P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
-            kb = cdiv_r(cscale(xfb, h), R(6));                       // k4bar
-            hpart += ip(kb, Q[RR_K4 * VEC + o]) / (double)t;
-          } break;
-          case AJ43_S4: {     // Y4 = x2 + h k3'
-            const cplx<R> x2b = cadd(J[JJ_X2 * VEC + o], Xb);
-            const cplx<R> k3pb = cadd(J[JJ_K3P * VEC + o], cscale(Xb, h));
-            const cplx<R> k2pb = J[JJ_K2P * VEC + o], k1ppb = J[JJ_K1PP * VEC + o];
-            const cplx<R> x0 = Q[RR_X0 * VEC + o], k1 = Q[RR_K1 * VEC + o];
-            const double eb = ip(k3pb, Q[RR_K3 * VEC + o]) + ip(k2pb, Q[RR_K2 * VEC + o]) +
-                              ip(k1ppb, cscale(k1, e)) + ip(x2b, cscale(x0, e));
-            hpart += eb * (double)dedt;
-            kb = cscale(k3pb, e);                                    // k3bar
-            hpart += ip(kb, Q[RR_K3 * VEC + o]) / (double)t;
-            J[JJ_K2 * VEC + o] = cscale(k2pb, e);                    // k2bar (partial)
-            J[JJ_K1P * VEC + o] = cscale(k1ppb, e);                  // k1'bar (partial)
-            J[JJ_XB * VEC + o] = cscale(x2b, e);                     // xbar (partial)
-          } break;
-          case AJ43_S3: {     // Y3 = x + h k2/2
-            J[JJ_XB * VEC + o] = cadd(J[JJ_XB * VEC + o], Xb);
-            kb = cadd(J[JJ_K2 * VEC + o], cscale(cscale(Xb, h), R(0.5)));   // k2bar final
-            hpart += ip(kb, Q[RR_K2 * VEC + o]) / (double)t;
-          } break;
-          default: {          // AJ43_S2: Y2 = x + h k1'/2; then x0bar, k1bar of this attempt
-            const cplx<R> xbb = cadd(J[JJ_XB * VEC + o], Xb);
-            const cplx<R> k1pb = cadd(J[JJ_K1P * VEC + o], cscale(cscale(Xb, h), R(0.5)));
-            const double eb = ip(k1pb, Q[RR_K1 * VEC + o]) + ip(xbb, Q[RR_X0 * VEC + o]);
-            hpart += eb * (double)dedt;
-            J[JJ_X0 * VEC + o] = cscale(xbb, e);
-            J[JJ_K1 * VEC + o] = cscale(k1pb, e);
+    const size_t o = ((size_t)ch * K + ky) * M + slot;
+    const R L = diss_L<R>(kx, ky, coeff);
+    const cplx<R> Xb = xb[j];
+    cplx<R> kb = mk<R>(0, 0);   // cotangent fed to the next adjoint RHS (before the h or t factor)
+    auto ip = [&](cplx<R> a, cplx<R> bb) { return rdot2(a.x, a.y, bb.x, bb.y); };
+    if (!rk43) {
+      const R e = in_mask ? exp(h / R(2) * L) : R(0);
+      const R dedh = e * L / R(2);
+      switch (STAGE) {
+        case AJ_PRE: {
+          const cplx<R> ob = J[J_OB * VEC + o];
+          J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_r(ob, R(6));
+          J[J_K2 * VEC + o] = cdiv_r(ob, R(3)); J[J_B3 * VEC + o] = cdiv_r(ob, R(3));
+          kb = cdiv_r(ob, R(6));                                   // k4bar
+          hpart += ip(kb, Q[Q_K4 * VEC + o]) / (double)h;
+        } break;
+        case AJ_S4: {
+          const cplx<R> f2b = cadd(J[J_F2 * VEC + o], Xb), b3b = cadd(J[J_B3 * VEC + o], Xb);
+          const cplx<R> b2b = J[J_K2 * VEC + o], b1b = J[J_A1 * VEC + o];
+          const cplx<R> f = Q[Q_F * VEC + o], k1 = Q[Q_K1 * VEC + o];
+          const double eb = ip(b3b, Q[Q_K3 * VEC + o]) + ip(b2b, Q[Q_K2 * VEC + o]) + ip(b1b, cscale(k1, e)) +
+                            ip(f2b, cscale(f, e));
+          hpart += eb * (double)dedh;
+          kb = cscale(b3b, e);                                     // k3bar
+          hpart += ip(kb, Q[Q_K3 * VEC + o]) / (double)h;
+          J[J_F2 * VEC + o] = cscale(f2b, e);                      // f1bar
+          J[J_A1 * VEC + o] = cscale(b1b, e);                      // a1bar
+          J[J_K2 * VEC + o] = cscale(b2b, e);                      // k2bar
+        } break;
+        case AJ_S3: {
+          J[J_F2 * VEC + o] = cadd(J[J_F2 * VEC + o], Xb);
+          kb = cadd(J[J_K2 * VEC + o], cscale(Xb, R(0.5)));        // k2bar final
+          hpart += ip(kb, Q[Q_K2 * VEC + o]) / (double)h;
+        } break;
+        case AJ_S2: {
+          const cplx<R> f1b = cadd(J[J_F2 * VEC + o], Xb);
+          const cplx<R> a1b = cadd(J[J_A1 * VEC + o], cscale(Xb, R(0.5)));
+          const double eb = ip(a1b, Q[Q_K1 * VEC + o]) + ip(f1b, Q[Q_F * VEC + o]);
+          hpart += eb * (double)dedh;
+          kb = cscale(a1b, e);                                     // k1bar
+          hpart += ip(kb, Q[Q_K1 * VEC + o]) / (double)h;
+          J[J_OB * VEC + o] = cscale(f1b, e);                      // fbar (without the RHS1 term)
+        } break;
+        default: {   // AJ_S1: fbar += X1bar; then seed the previous step (if any)
+          const cplx<R> fb = cadd(J[J_OB * VEC + o], Xb);
+          J[J_OB * VEC + o] = fb;
+          if (p.rec_prev) {
+            J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_r(fb, R(6));
+            J[J_K2 * VEC + o] = cdiv_r(fb, R(3)); J[J_B3 * VEC + o] = cdiv_r(fb, R(3));
+            kb = cdiv_r(fb, R(6));
+            hpart += ip(kb, p.rec_prev[Q_K4 * VEC + o]) / (double)h;
+          } else {
             feed = false;
-          } break;
-          case AJ43_INIT: {   // initial k1 = t v(x0): x0bar += Xbar
-            J[JJ_X0 * VEC + o] = cadd(J[JJ_X0 * VEC + o], Xb);
-            feed = false;
-          } break;
-        }
-        kb = cscale(kb, t);
+          }
+        } break;
       }
-      if (feed) {
-        // lambda = kb (the cotangent of v); next inverse input (mask lam_w, k^2 mask lam_j) / c
-        const cplx<R> lin = ch == 0 ? (in_mask ? kb : mk<R>(0, 0)) : cscale(kb, ksq_masked<R>(kx, ky));
-        if (ch == 0) lam0[j] = cdiv_r(lin, cky); else lam1[j] = cdiv_r(lin, cky);
+      kb = cscale(kb, h);
+    } else {
+      const R e = exp((t * L) * h / R(2));
+      const R dedt = e * (L * h / R(2));
+      switch (STAGE) {
+        case AJ43_PRE:      // from (xbar_f, k5bar) in (X0, K1) slots: RHS5 input = k5bar
+        case AJ43_IPRE: {   // initial k1 = t v(x0): input = k1bar
+          kb = J[JJ_K1 * VEC + o];
+          hpart += ip(kb, Q[(STAGE == AJ43_PRE ? RR_K5 : RR_K1) * VEC + o]) / (double)t;
+        } break;
+        case AJ43_S5: {     // xbar_f += Xbar5; distribute to x2, k1'', k2', k3', k4
+          const cplx<R> xfb = cadd(J[JJ_X0 * VEC + o], Xb);
+          J[JJ_X2 * VEC + o] = xfb;
+          J[JJ_K1PP * VEC + o] = cdiv_r(cscale(xfb, h), R(6));
+          J[JJ_K2P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
+          J[JJ_K3P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
+          kb = cdiv_r(cscale(xfb, h), R(6));                       // k4bar
+          hpart += ip(kb, Q[RR_K4 * VEC + o]) / (double)t;
+        } break;
+        case AJ43_S4: {     // Y4 = x2 + h k3'
+          const cplx<R> x2b = cadd(J[JJ_X2 * VEC + o], Xb);
+          const cplx<R> k3pb = cadd(J[JJ_K3P * VEC + o], cscale(Xb, h));
+          const cplx<R> k2pb = J[JJ_K2P * VEC + o], k1ppb = J[JJ_K1PP * VEC + o];
+          const cplx<R> x0 = Q[RR_X0 * VEC + o], k1 = Q[RR_K1 * VEC + o];
+          const double eb = ip(k3pb, Q[RR_K3 * VEC + o]) + ip(k2pb, Q[RR_K2 * VEC + o]) +
+                            ip(k1ppb, cscale(k1, e)) + ip(x2b, cscale(x0, e));
+          hpart += eb * (double)dedt;
+          kb = cscale(k3pb, e);                                    // k3bar
+          hpart += ip(kb, Q[RR_K3 * VEC + o]) / (double)t;
+          J[JJ_K2 * VEC + o] = cscale(k2pb, e);                    // k2bar (partial)
+          J[JJ_K1P * VEC + o] = cscale(k1ppb, e);                  // k1'bar (partial)
+          J[JJ_XB * VEC + o] = cscale(x2b, e);                     // xbar (partial)
+        } break;
+        case AJ43_S3: {     // Y3 = x + h k2/2
+          J[JJ_XB * VEC + o] = cadd(J[JJ_XB * VEC + o], Xb);
+          kb = cadd(J[JJ_K2 * VEC + o], cscale(cscale(Xb, h), R(0.5)));   // k2bar final
+          hpart += ip(kb, Q[RR_K2 * VEC + o]) / (double)t;
+        } break;
+        case AJ43_S2: {     // Y2 = x + h k1'/2; then x0bar, k1bar of this attempt
+          const cplx<R> xbb = cadd(J[JJ_XB * VEC + o], Xb);
+          const cplx<R> k1pb = cadd(J[JJ_K1P * VEC + o], cscale(cscale(Xb, h), R(0.5)));
+          const double eb = ip(k1pb, Q[RR_K1 * VEC + o]) + ip(xbb, Q[RR_X0 * VEC + o]);
+          hpart += eb * (double)dedt;
+          J[JJ_X0 * VEC + o] = cscale(xbb, e);
+          J[JJ_K1 * VEC + o] = cscale(k1pb, e);
+          feed = false;
+        } break;
+        default: {          // AJ43_INIT: initial k1 = t v(x0): x0bar += Xbar
+          J[JJ_X0 * VEC + o] = cadd(J[JJ_X0 * VEC + o], Xb);
+          feed = false;
+        } break;
       }
+      kb = cscale(kb, t);
     }
+    // lambda = kb; next inverse input (mask lam_w, k^2 mask lam_j) / c_ky
+    const cplx<R> lin = ch == 0 ? (in_mask ? kb : mk<R>(0, 0)) : cscale(kb, ksq_masked<R>(kx, ky));
+    lam[j] = cdiv_r(lin, cky);
   }
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) hpart += __shfl_xor_sync(0xffffffffu, hpart, o);
-  if (lane == 0) p.hacc[(size_t)b * K + ky] += hpart;
-  const bool produce = (STAGE == AJ_PRE || STAGE == AJ_S4 || STAGE == AJ_S3 || STAGE == AJ_S2 ||
-                        (STAGE == AJ_S1 && p.rec_prev) || STAGE == AJ43_PRE || STAGE == AJ43_S5 ||
-                        STAGE == AJ43_S4 || STAGE == AJ43_S3 || STAGE == AJ43_IPRE);
-  if (!produce) return;
-  // unscaled inverse: Re sum lam e^{ik.x} after the row pass doubles ky > 0
-  const R n2 = R(N) * R(N);
-#pragma unroll
-  for (int j = 0; j < E; ++j) { lam0[j] = cscale(lam0[j], n2); lam1[j] = cscale(lam1[j], n2); }
-  col_inverse2<R, N>(lam0, lam1, p.G, 8, b, ky, lane, s_tw);
+  if (lane == 0) p.hacc[((size_t)b * K + ky) * 2 + ch] += hpart;
+  if (!feed) return;
+  // unscaled inverse: Re sum lam e^{ik.x} once the row pass doubles ky > 0
+  col_inverse1<R, N>(lam, p.G, 8, b, ch, ky, lane, s_tw, R(1));
 }
 
 // Rejected Lawson-RK4(3) attempt in reverse: k1_next = e (e k1).
@@ -332,7 +314,7 @@ __global__ void k_adj_reject(cplx<R>* J, int nslot, const cplx<R>* rec, double* 
     }
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-  if (lane == 0) hacc[(size_t)b * g.K + ky] += part;
+  if (lane == 0) hacc[((size_t)b * g.K + ky) * 2] += part;
 }
 
 // Head of the adjoint: from Ybar = cotangent of sym(Phi) (box, already
@@ -420,12 +402,12 @@ __global__ void k_adj_phase(R* gfields, const R* vt, const R* vx, const double* 
   }
 }
 
-// Deterministic reduction of the [B][K] accumulators: out[b] = scale * sum_ky hacc.
+// Deterministic reduction of the [B][K][2] accumulators: out[b] = scale * sum hacc[b].
 static __global__ void k_reduce_hacc(const double* hacc, int K, double scale, double* out, int B) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   double s = 0.0;
-  for (int k = 0; k < K; ++k) s += hacc[(size_t)b * K + k];
+  for (int k = 0; k < 2 * K; ++k) s += hacc[(size_t)b * 2 * K + k];
   out[b] = s * scale;
 }
 

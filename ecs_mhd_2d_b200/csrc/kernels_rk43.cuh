@@ -51,9 +51,9 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (col >= p.B * K) return;
-  const int b = col / K, ky = col - b * K;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
   const StepCtl& c = p.ctl[b];
   if (c.done) return;
   const R t = (R)c.t, h = (R)c.h;
@@ -61,83 +61,78 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   cplx<R>* S = p.S + (size_t)b * S_NSLOT * VEC;
   cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * RR_NREC * VEC
                        : nullptr;
-
   const bool has_rhs = STAGE != R43_A && STAGE != R43_START;
-  cplx<R> r0[E], r1[E];
-  if (has_rhs) col_load_fwd<R, N>(p.H, b, ky, lane, s_tw, r0, r1);
-  cplx<R> x0[E], x1[E];
+  cplx<R> r[E];
+  if (has_rhs) col_load_fwd1<R, N>(p.H, 2, b, ch, ky, lane, s_tw, r);
+  const R coeff = ch == 0 ? p.nu : p.eta;
+  cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    x[j] = mk<R>(0, 0);
     const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
-    cplx<R> v[2];
-    v[0] = mk<R>(0, 0); v[1] = mk<R>(0, 0);
-    if (has_rhs) rhs_vals<R>(r0[j], r1[j], kx, ky, p.fhat[ky * M + slot], v[0], v[1]);
-#pragma unroll
-    for (int ch = 0; ch < 2; ++ch) {
-      const size_t o = ((size_t)ch * K + ky) * M + slot;
-      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
-      const cplx<R> kv = cscale(v[ch], t);                 // mod_vel_fn = t * vel_fn (:243)
-      cplx<R> xin = mk<R>(0, 0);
-      switch (STAGE) {
-        case R43_START: {
-          xin = S[S_X0 * VEC + o];
-        } break;
-        case R43_INIT: {
-          S[S_K1 * VEC + o] = kv;
-        } break;
-        case R43_A: {                                      // :266-270
-          cplx<R> xs = pend ? S[S_XF * VEC + o] : S[S_X0 * VEC + o];
-          cplx<R> ks = pend ? S[S_K5 * VEC + o] : S[S_K1 * VEC + o];
-          if (pend) { S[S_X0 * VEC + o] = xs; S[S_K1 * VEC + o] = ks; }
-          if (rec) { rec[RR_X0 * VEC + o] = xs; rec[RR_K1 * VEC + o] = ks; }
-          const R e = exp((t * L) * h / R(2));             // e = exp(mod_L * h/2), not masked (:263)
-          const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
-          S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
-          xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
-          if (rec) rec[RR_Y2 * VEC + o] = xin;
-        } break;
-        case R43_B: {                                      // :270-271
-          S[S_K2 * VEC + o] = kv;
-          if (rec) rec[RR_K2 * VEC + o] = kv;
-          xin = cadd(S[S_XE * VEC + o], cscale(cscale(kv, h), R(0.5)));
-          if (rec) rec[RR_Y3 * VEC + o] = xin;
-        } break;
-        case R43_C: {                                      // :271-280
-          if (rec) rec[RR_K3 * VEC + o] = kv;
-          const R e = exp((t * L) * h / R(2));
-          const cplx<R> x2 = cscale(S[S_XE * VEC + o], e);
-          const cplx<R> k1ee = cscale(S[S_K1E * VEC + o], e);
-          const cplx<R> k2e = cscale(S[S_K2 * VEC + o], e);
-          const cplx<R> k3e = cscale(kv, e);
-          S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
-          S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
-          xin = cadd(x2, cscale(k3e, h));
-          if (rec) rec[RR_Y4 * VEC + o] = xin;
-        } break;
-        case R43_D: {                                      // :280-281
-          S[S_K4 * VEC + o] = kv;
-          if (rec) rec[RR_K4 * VEC + o] = kv;
-          cplx<R> acc = cadd(cadd(cadd(cdiv_r(S[S_K1 * VEC + o], R(6)), cdiv_r(S[S_K2 * VEC + o], R(3))),
-                                  cdiv_r(S[S_K3 * VEC + o], R(3))), cdiv_r(kv, R(6)));
-          xin = cadd(S[S_X2 * VEC + o], cscale(acc, h));
-          S[S_XF * VEC + o] = xin;
-          if (rec) rec[RR_XF * VEC + o] = xin;
-        } break;
-        default: {                                         // R43_E: :282, :288
-          S[S_K5 * VEC + o] = kv;
-          if (rec) rec[RR_K5 * VEC + o] = kv;
-          xin = cdiv_r(cscale(csub(kv, S[S_K4 * VEC + o]), h), R(6));
-        } break;
-      }
-      if (ch == 0) x0[j] = xin; else x1[j] = xin;
+    cplx<R> v = mk<R>(0, 0);
+    if (has_rhs) {
+      if (ch == 0) { if (!(kx == 0 && ky == 0)) v = cadd(r[j], p.fhat[ky * M + slot]); }
+      else v = cscale(r[j], ksq_masked<R>(kx, ky));
     }
+    const size_t o = ((size_t)ch * K + ky) * M + slot;
+    const R L = diss_L<R>(kx, ky, coeff);
+    const cplx<R> kv = cscale(v, t);                 // mod_vel_fn = t * vel_fn (timestepping.py:243)
+    cplx<R> xin = mk<R>(0, 0);
+    switch (STAGE) {
+      case R43_START: xin = S[S_X0 * VEC + o]; break;
+      case R43_INIT: S[S_K1 * VEC + o] = kv; break;
+      case R43_A: {                                  // :266-270
+        const cplx<R> xs = pend ? S[S_XF * VEC + o] : S[S_X0 * VEC + o];
+        const cplx<R> ks = pend ? S[S_K5 * VEC + o] : S[S_K1 * VEC + o];
+        if (pend) { S[S_X0 * VEC + o] = xs; S[S_K1 * VEC + o] = ks; }
+        if (rec) { rec[RR_X0 * VEC + o] = xs; rec[RR_K1 * VEC + o] = ks; }
+        const R e = exp((t * L) * h / R(2));         // e = exp(mod_L * h/2), not masked (:263)
+        const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
+        S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
+        xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
+        if (rec) rec[RR_Y2 * VEC + o] = xin;
+      } break;
+      case R43_B: {                                  // :270-271
+        S[S_K2 * VEC + o] = kv;
+        if (rec) rec[RR_K2 * VEC + o] = kv;
+        xin = cadd(S[S_XE * VEC + o], cscale(cscale(kv, h), R(0.5)));
+        if (rec) rec[RR_Y3 * VEC + o] = xin;
+      } break;
+      case R43_C: {                                  // :271-280
+        if (rec) rec[RR_K3 * VEC + o] = kv;
+        const R e = exp((t * L) * h / R(2));
+        const cplx<R> x2 = cscale(S[S_XE * VEC + o], e);
+        const cplx<R> k1ee = cscale(S[S_K1E * VEC + o], e);
+        const cplx<R> k2e = cscale(S[S_K2 * VEC + o], e);
+        const cplx<R> k3e = cscale(kv, e);
+        S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
+        S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
+        xin = cadd(x2, cscale(k3e, h));
+        if (rec) rec[RR_Y4 * VEC + o] = xin;
+      } break;
+      case R43_D: {                                  // :280-281
+        S[S_K4 * VEC + o] = kv;
+        if (rec) rec[RR_K4 * VEC + o] = kv;
+        const cplx<R> acc = cadd(cadd(cadd(cdiv_r(S[S_K1 * VEC + o], R(6)), cdiv_r(S[S_K2 * VEC + o], R(3))),
+                                      cdiv_r(S[S_K3 * VEC + o], R(3))), cdiv_r(kv, R(6)));
+        xin = cadd(S[S_X2 * VEC + o], cscale(acc, h));
+        S[S_XF * VEC + o] = xin;
+        if (rec) rec[RR_XF * VEC + o] = xin;
+      } break;
+      default: {                                     // R43_E: :282, :288
+        S[S_K5 * VEC + o] = kv;
+        if (rec) rec[RR_K5 * VEC + o] = kv;
+        xin = cdiv_r(cscale(csub(kv, S[S_K4 * VEC + o]), h), R(6));
+      } break;
+    }
+    x[j] = xin;
   }
   if (STAGE == R43_INIT) return;
-  if (STAGE == R43_E) col_inverse2<R, N>(x0, x1, p.G, 8, b, ky, lane, s_tw);
-  else col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
+  if (STAGE == R43_E) col_inverse1<R, N>(x, p.G, 8, b, ch, ky, lane, s_tw, R(1) / (R(N) * R(N)));
+  else col_inverse4<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
 // Error norm max|irfft2(d)| of the two channels (timestepping.py:288-291) with

@@ -208,118 +208,115 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (col >= p.B * K) return;
-  const int b = col / K, ky = col - b * K;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
   cplx<R>* D = p.D + (size_t)b * p.nslot * VEC;
   const cplx<R>* Q = p.rec;
-  const bool rk43 = STAGE >= T43_INIT;
-  const bool has_rhs = !(STAGE == TS_START || STAGE == T43_A || STAGE == T43_START);
+  constexpr bool rk43 = STAGE >= T43_INIT;
+  constexpr bool has_rhs = !(STAGE == TS_START || STAGE == T43_A || STAGE == T43_START);
   const R h = (R)p.h, t = (R)p.t;
   const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
-  cplx<R> r0[E], r1[E];
-  if (has_rhs) col_load_fwd<R, N>(p.H, b, ky, lane, s_tw, r0, r1);
-  cplx<R> x0[E], x1[E];
+  cplx<R> r[E];
+  if (has_rhs) col_load_fwd1<R, N>(p.H, 2, b, ch, ky, lane, s_tw, r);
+  const R coeff = ch == 0 ? p.nu : p.eta;
+  cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    x0[j] = mk<R>(0, 0); x1[j] = mk<R>(0, 0);
+    x[j] = mk<R>(0, 0);
     const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
-    cplx<R> dv[2];
-    dv[0] = mk<R>(0, 0); dv[1] = mk<R>(0, 0);
+    cplx<R> dv = mk<R>(0, 0);
     if (has_rhs) {
-      dv[0] = in_mask ? r0[j] : mk<R>(0, 0);               // tangent has no forcing
-      dv[1] = cscale(r1[j], ksq_masked<R>(kx, ky));
+      if (ch == 0) { if (in_mask) dv = r[j]; }           // the tangent has no forcing
+      else dv = cscale(r[j], ksq_masked<R>(kx, ky));
     }
-#pragma unroll
-    for (int ch = 0; ch < 2; ++ch) {
-      const size_t o = ((size_t)ch * K + ky) * M + slot;
-      const R L = diss_L<R>(kx, ky, ch == 0 ? p.nu : p.eta);
-      cplx<R> xin = mk<R>(0, 0);
-      if (!rk43) {
-        // Lawson-RK4: e = exp(h/2 L) mask, de = e L dh/2; dk = dh v + h dv with v = k/h
-        const R e = in_mask ? exp(h / R(2) * L) : R(0);
-        const R de = e * L * (dpar / R(2));
-        auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv[ch], h)); };
-        switch (STAGE) {
-          case TS_START: xin = D[D_F * VEC + o]; break;
-          case T4_S1: {
-            const cplx<R> dk1 = dk_of(Q_K1);
-            const cplx<R> df1 = cadd(cscale(Q[Q_F * VEC + o], de), cscale(D[D_F * VEC + o], e));
-            const cplx<R> da1 = cadd(cscale(Q[Q_K1 * VEC + o], de), cscale(dk1, e));
-            D[D_F * VEC + o] = df1; D[D_A1 * VEC + o] = da1;
-            xin = cadd(df1, cscale(da1, R(0.5)));
-          } break;
-          case T4_S2: {
-            const cplx<R> dk2 = dk_of(Q_K2);
-            D[D_K2 * VEC + o] = dk2;
-            xin = cadd(D[D_F * VEC + o], cscale(dk2, R(0.5)));
-          } break;
-          case T4_S3: {
-            const cplx<R> dk3 = dk_of(Q_K3);
-            const cplx<R> f1 = cscale(Q[Q_F * VEC + o], e), a1 = cscale(Q[Q_K1 * VEC + o], e);
-            const cplx<R> df2 = cadd(cscale(f1, de), cscale(D[D_F * VEC + o], e));
-            const cplx<R> db1 = cadd(cscale(a1, de), cscale(D[D_A1 * VEC + o], e));
-            const cplx<R> db2 = cadd(cscale(Q[Q_K2 * VEC + o], de), cscale(D[D_K2 * VEC + o], e));
-            const cplx<R> db3 = cadd(cscale(Q[Q_K3 * VEC + o], de), cscale(dk3, e));
-            xin = cadd(df2, db3);
-            D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_r(db1, R(6))), cdiv_r(db2, R(3))), cdiv_r(db3, R(3)));
-          } break;
-          default: {   // T4_S4
-            const cplx<R> dk4 = dk_of(Q_K4);
-            xin = cadd(D[D_F * VEC + o], cdiv_r(dk4, R(6)));
-            D[D_F * VEC + o] = xin;
-          } break;
-        }
-      } else {
-        // Lawson-RK4(3): e = exp(t L h/2), de = e L h/2 dt; dk = dt v + t dv with v = k/t
-        const R e = exp((t * L) * h / R(2));
-        const R de = e * (L * h / R(2)) * dpar;
-        auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / t), cscale(dv[ch], t)); };
-        switch (STAGE) {
-          case T43_START: xin = D[S_X0 * VEC + o]; break;
-          case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
-          case T43_A: {
-            const cplx<R> dxe = cadd(cscale(Q[RR_X0 * VEC + o], de), cscale(D[S_X0 * VEC + o], e));
-            const cplx<R> dk1e = cadd(cscale(Q[RR_K1 * VEC + o], de), cscale(D[S_K1 * VEC + o], e));
-            D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
-            xin = cadd(dxe, cscale(cscale(dk1e, h), R(0.5)));
-          } break;
-          case T43_B: {
-            const cplx<R> dk2 = dk_of(RR_K2);
-            D[S_K2 * VEC + o] = dk2;
-            xin = cadd(D[S_XE * VEC + o], cscale(cscale(dk2, h), R(0.5)));
-          } break;
-          case T43_C: {
-            const cplx<R> dk3 = dk_of(RR_K3);
-            const cplx<R> xe = cscale(Q[RR_X0 * VEC + o], e), k1e = cscale(Q[RR_K1 * VEC + o], e);
-            const cplx<R> dx2 = cadd(cscale(xe, de), cscale(D[S_XE * VEC + o], e));
-            const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(D[S_K1E * VEC + o], e));
-            const cplx<R> dk2e = cadd(cscale(Q[RR_K2 * VEC + o], de), cscale(D[S_K2 * VEC + o], e));
-            const cplx<R> dk3e = cadd(cscale(Q[RR_K3 * VEC + o], de), cscale(dk3, e));
-            D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
-            xin = cadd(dx2, cscale(dk3e, h));
-          } break;
-          case T43_D: {
-            const cplx<R> dk4 = dk_of(RR_K4);
-            const cplx<R> acc = cadd(cadd(cadd(cdiv_r(D[S_K1 * VEC + o], R(6)), cdiv_r(D[S_K2 * VEC + o], R(3))),
-                                          cdiv_r(D[S_K3 * VEC + o], R(3))), cdiv_r(dk4, R(6)));
-            xin = cadd(D[S_X2 * VEC + o], cscale(acc, h));
-            D[S_XF * VEC + o] = xin;
-          } break;
-          default: {   // T43_E: accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
-            D[S_K1 * VEC + o] = dk_of(RR_K5);
-            D[S_X0 * VEC + o] = D[S_XF * VEC + o];
-          } break;
-        }
+    const size_t o = ((size_t)ch * K + ky) * M + slot;
+    const R L = diss_L<R>(kx, ky, coeff);
+    cplx<R> xin = mk<R>(0, 0);
+    if (!rk43) {
+      // Lawson-RK4: e = exp(h/2 L) mask, de = e L dh/2; dk = dh v + h dv with v = k/h
+      const R e = in_mask ? exp(h / R(2) * L) : R(0);
+      const R de = e * L * (dpar / R(2));
+      auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv, h)); };
+      switch (STAGE) {
+        case TS_START: xin = D[D_F * VEC + o]; break;
+        case T4_S1: {
+          const cplx<R> dk1 = dk_of(Q_K1);
+          const cplx<R> df1 = cadd(cscale(Q[Q_F * VEC + o], de), cscale(D[D_F * VEC + o], e));
+          const cplx<R> da1 = cadd(cscale(Q[Q_K1 * VEC + o], de), cscale(dk1, e));
+          D[D_F * VEC + o] = df1; D[D_A1 * VEC + o] = da1;
+          xin = cadd(df1, cscale(da1, R(0.5)));
+        } break;
+        case T4_S2: {
+          const cplx<R> dk2 = dk_of(Q_K2);
+          D[D_K2 * VEC + o] = dk2;
+          xin = cadd(D[D_F * VEC + o], cscale(dk2, R(0.5)));
+        } break;
+        case T4_S3: {
+          const cplx<R> dk3 = dk_of(Q_K3);
+          const cplx<R> f1 = cscale(Q[Q_F * VEC + o], e), a1 = cscale(Q[Q_K1 * VEC + o], e);
+          const cplx<R> df2 = cadd(cscale(f1, de), cscale(D[D_F * VEC + o], e));
+          const cplx<R> db1 = cadd(cscale(a1, de), cscale(D[D_A1 * VEC + o], e));
+          const cplx<R> db2 = cadd(cscale(Q[Q_K2 * VEC + o], de), cscale(D[D_K2 * VEC + o], e));
+          const cplx<R> db3 = cadd(cscale(Q[Q_K3 * VEC + o], de), cscale(dk3, e));
+          xin = cadd(df2, db3);
+          D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_r(db1, R(6))), cdiv_r(db2, R(3))), cdiv_r(db3, R(3)));
+        } break;
+        default: {   // T4_S4
+          const cplx<R> dk4 = dk_of(Q_K4);
+          xin = cadd(D[D_F * VEC + o], cdiv_r(dk4, R(6)));
+          D[D_F * VEC + o] = xin;
+        } break;
       }
-      if (ch == 0) x0[j] = xin; else x1[j] = xin;
+    } else {
+      // Lawson-RK4(3): e = exp(t L h/2), de = e L h/2 dt; dk = dt v + t dv with v = k/t
+      const R e = exp((t * L) * h / R(2));
+      const R de = e * (L * h / R(2)) * dpar;
+      auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / t), cscale(dv, t)); };
+      switch (STAGE) {
+        case T43_START: xin = D[S_X0 * VEC + o]; break;
+        case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
+        case T43_A: {
+          const cplx<R> dxe = cadd(cscale(Q[RR_X0 * VEC + o], de), cscale(D[S_X0 * VEC + o], e));
+          const cplx<R> dk1e = cadd(cscale(Q[RR_K1 * VEC + o], de), cscale(D[S_K1 * VEC + o], e));
+          D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
+          xin = cadd(dxe, cscale(cscale(dk1e, h), R(0.5)));
+        } break;
+        case T43_B: {
+          const cplx<R> dk2 = dk_of(RR_K2);
+          D[S_K2 * VEC + o] = dk2;
+          xin = cadd(D[S_XE * VEC + o], cscale(cscale(dk2, h), R(0.5)));
+        } break;
+        case T43_C: {
+          const cplx<R> dk3 = dk_of(RR_K3);
+          const cplx<R> xe = cscale(Q[RR_X0 * VEC + o], e), k1e = cscale(Q[RR_K1 * VEC + o], e);
+          const cplx<R> dx2 = cadd(cscale(xe, de), cscale(D[S_XE * VEC + o], e));
+          const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(D[S_K1E * VEC + o], e));
+          const cplx<R> dk2e = cadd(cscale(Q[RR_K2 * VEC + o], de), cscale(D[S_K2 * VEC + o], e));
+          const cplx<R> dk3e = cadd(cscale(Q[RR_K3 * VEC + o], de), cscale(dk3, e));
+          D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
+          xin = cadd(dx2, cscale(dk3e, h));
+        } break;
+        case T43_D: {
+          const cplx<R> dk4 = dk_of(RR_K4);
+          const cplx<R> acc = cadd(cadd(cadd(cdiv_r(D[S_K1 * VEC + o], R(6)), cdiv_r(D[S_K2 * VEC + o], R(3))),
+                                        cdiv_r(D[S_K3 * VEC + o], R(3))), cdiv_r(dk4, R(6)));
+          xin = cadd(D[S_X2 * VEC + o], cscale(acc, h));
+          D[S_XF * VEC + o] = xin;
+        } break;
+        default: {   // T43_E: accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
+          D[S_K1 * VEC + o] = dk_of(RR_K5);
+          D[S_X0 * VEC + o] = D[S_XF * VEC + o];
+        } break;
+      }
     }
+    x[j] = xin;
   }
   if (!p.produce || STAGE == T43_INIT || STAGE == T43_E) return;
-  col_inverse8<R, N>(x0, x1, p.G, b, ky, lane, s_tw);
+  col_inverse4<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
 // Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);

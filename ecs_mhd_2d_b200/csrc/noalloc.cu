@@ -128,7 +128,7 @@ int na_state_vel(unsigned char* base, double nu, double eta, double b0x, double 
   cp.H = H; cp.G = G; cp.F = F; cp.A1 = nullptr; cp.K2 = nullptr; cp.OUT = OUT; cp.Etab = nullptr; cp.ctl = ctl;
   cp.fhat = fbox; cp.tw = tw; cp.nu = nu; cp.eta = eta; cp.B = B; cp.stage = COL_START; cp.produce = 1;
   cp.diss = 0; cp.rec = nullptr; cp.rec_bstride = 0;
-  const int cols = B * K;
+  const int cols = B * K * 2;   // one warp per (batch, ky, channel)
   k_col_rk4<double, N, COL_START><<<(cols + 3) / 4, 128, 0, s>>>(cp);
   RowParams<double> rp;
   rp.G = G; rp.H = H; rp.phys = nullptr; rp.phys_bstride = 0; rp.rec_index = 0; rp.phys_stage = 0; rp.ctl = nullptr;

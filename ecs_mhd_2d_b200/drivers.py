@@ -116,14 +116,24 @@ def mixed_precision_objectives(param_dict, mode):
     return Objective(param_dict, mode), Objective(pd32, mode)
 
 
-def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_transpose=True):
-    """Inexact Newton with FP32 Jacobian products and FP64 residuals; the last
-    residual is an FP64 refinement check.  Returns (state, history)."""
+def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_transpose=False, refine=1):
+    """Inexact Newton with FP32 Jacobian products (stepping, JVP, VJP in FP32) and
+    FP64 residuals, Arnoldi and least squares, followed by `refine` FP64
+    refinement sweeps (Newton steps with FP64 Jacobian products).  The FP32
+    phase solves J s = f directly by default: the Gauss-Newton form
+    J^T J s = J^T f squares the condition number of the shooting Jacobian, which
+    FP32 products cannot resolve.  Returns (state, history); history[-1] holds
+    the final FP64 relative residual."""
     _, obj32 = mixed_precision_objectives(param_dict, mode)
     x = input_dict
     hist = []
     for _ in range(iters):
         x, st = newton_gmres_update(x, param_dict, mode, inner=inner, use_transpose=use_transpose, jac_obj=obj32)
+        st["jacobian"] = "fp32"
+        hist.append(st)
+    for _ in range(refine):
+        x, st = newton_gmres_update(x, param_dict, mode, inner=inner, use_transpose=True)
+        st["jacobian"] = "fp64"
         hist.append(st)
     f = Objective(param_dict, mode)(_as_device_dict(x))
     hist.append({"final_rel_err": float(relative_error_RPO(_as_device_dict(x), f))})

@@ -152,6 +152,24 @@ int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, double* Hcol, lo
  * leading dimension ldh >= m+1), m <= 128 (jnp.linalg.lstsq at linalg.py:93). */
 int ecs_hessenberg_lstsq(const double* H, int ldh, int m, const double* b, double* y, void* stream);
 
+/* Slot pool: continuous batching of Lawson_RK4 forward shootings
+ * (objective_RPO / loss_RPO, loss_functions.py:99-148) over the context's
+ * max_batch slots.  Each slot carries its own T, sx, symmetry and step count;
+ * finished or empty slots are skipped by every launch, and new requests are
+ * admitted between ecs_pool_advance calls while the others keep running.
+ *   ecs_pool_reset   mark every slot empty
+ *   ecs_pool_admit   load fields [2][n][n] (device) into an empty slot
+ *   ecs_pool_advance advance all active slots by up to nsteps steps
+ *   ecs_pool_poll    HOST arrays done[max_batch], steps_done[max_batch] (synchronises)
+ *   ecs_pool_retire  residual irfft2(f0 - g.Phi_T(f0)) [2][n][n] and/or loss of a
+ *                    finished slot (device pointers; either may be NULL); frees it */
+int ecs_pool_reset(ecs_ctx* ctx, void* stream);
+int ecs_pool_admit(ecs_ctx* ctx, int slot, const ecs_shoot_cfg* cfg, const void* fields, double T, double sx,
+                   void* stream);
+int ecs_pool_advance(ecs_ctx* ctx, int nsteps, void* stream);
+int ecs_pool_poll(ecs_ctx* ctx, int* done, int* steps_done, void* stream);
+int ecs_pool_retire(ecs_ctx* ctx, int slot, void* out_fields, double* loss, void* stream);
+
 /* state_vel without any device allocation.  No counterpart in the reference.
  * For callers that cannot allocate device memory: a process whose GPU memory is
  * owned by another allocator (JAX/XLA preallocates most of the device and hands
