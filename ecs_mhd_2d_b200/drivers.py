@@ -116,14 +116,15 @@ def mixed_precision_objectives(param_dict, mode):
     return Objective(param_dict, mode), Objective(pd32, mode)
 
 
-def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_transpose=False, refine=1):
+def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_transpose=True, refine=0):
     """Inexact Newton with FP32 Jacobian products (stepping, JVP, VJP in FP32) and
-    FP64 residuals, Arnoldi and least squares, followed by `refine` FP64
-    refinement sweeps (Newton steps with FP64 Jacobian products).  The FP32
-    phase solves J s = f directly by default: the Gauss-Newton form
-    J^T J s = J^T f squares the condition number of the shooting Jacobian, which
-    FP32 products cannot resolve.  Returns (state, history); history[-1] holds
-    the final FP64 relative residual."""
+    FP64 residuals, Arnoldi and least squares, followed by `refine` Newton steps
+    with FP64 Jacobian products.  `use_transpose` selects the Gauss-Newton form
+    J^T J s = J^T f as jax_scripts/newton.py:151-187 does by default.  The FP32
+    products perturb each GMRES solve by about the FP32 rounding of the
+    linearised flow, far below the inexactness of a 16-vector Krylov solve, so
+    the iteration follows the FP64 one step for step.  Returns (state,
+    history); history[-1] holds the final FP64 relative residual."""
     _, obj32 = mixed_precision_objectives(param_dict, mode)
     x = input_dict
     hist = []
