@@ -386,6 +386,19 @@ def main():
         te = float(t)
     e2e_value = world * BATCH * args.steps / (te / 1e3)
 
+    # phase split of one step (untimed pass, CUDA events): primal linearisation vs tangent sweep
+    def _ev_ms(fn):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+    phase_ms = {"linearize": _ev_ms(lambda: obj.linearize(prim, force=True, batch=BATCH)),
+                "jvp": _ev_ms(lambda: obj.jvp(prim, tan))}
+
     # roofline of the dominant kernel, timed live on this stream
     step()
     torch.cuda.synchronize()
@@ -449,6 +462,7 @@ def main():
         extra = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
                  "tangent_rk_steps_per_s": value * info.get("accepted", 0),
                  "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1},
+                 "phase_ms": phase_ms,
                  "secondary": secondary}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -26,12 +26,13 @@ namespace ecs {
 constexpr int XT = 8;
 constexpr int COLWARPS = 4;
 
-template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (N / 2 + 10 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
+// Row kernels with NG (or 3 adjoint) input and NH (or NHA adjoint) output tiles: 7 tiles of K x (X+1).
+template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (tw_smem(N) + 7 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 // Small batches use 2-row tiles: 4x more CTAs for the same rows.
 constexpr int XTS = 2;
 template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
-template <typename R, int N> size_t smem_row_8f() { return (N / 2 + 8 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
-template <typename R, int N, int X = XT> size_t smem_row_2f() { return (N / 2 + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
+template <typename R, int N> size_t smem_row_phys() { return (tw_smem(N) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N, int X = XT> size_t smem_row_2f() { return (tw_smem(N) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
 template <typename R, int N>
 int configure_kernels(ecs_ctx* c) {
@@ -40,7 +41,7 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_to_box<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_from_box<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N>());
-  st |= (int)cudaFuncSetAttribute(k_row_phys<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_8f<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_phys<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_phys<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_rhs<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
@@ -106,9 +107,8 @@ void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStr
 }
 
 template <typename R, int N>
-void launch_row_rhs(ecs_ctx* c, int B, R* phys, cudaStream_t s, const StepCtl* ctl = nullptr) {
-  RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
-  p.phys_bstride = 0; p.rec_index = 0; p.phys_stage = 0; p.ctl = ctl;
+void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = nullptr) {
+  RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.tw = (const cplx<R>*)c->tw; p.ctl = ctl;
   p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
   ++c->launches;
   if (small_rows<N>(B)) k_row_rhs<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
@@ -149,11 +149,11 @@ template <typename R, int N>
 void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s) {
   ColRegenParams<R> p; p.rec = rec; p.items = items; p.G = (cplx<R>*)c->Greg; p.tw = (const cplx<R>*)c->tw;
   p.nitems = nitems;
-  const int cols = nitems * Geomc<N>::K;
+  const int cols = nitems * Geomc<N>::K * 2;
   ++c->launches; k_col_regen<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
   RowPhysParams<R> q; q.G = (const cplx<R>*)c->Greg; q.phys = (R*)c->Phys; q.tw = (const cplx<R>*)c->tw;
   q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.nitems = nitems;
-  ++c->launches; k_row_phys<R, N, XT><<<nitems * (N / XT), XT * 32, smem_row_8f<R, N>(), s>>>(q);
+  ++c->launches; k_row_phys<R, N, XT><<<nitems * (N / XT), XT * 32, smem_row_phys<R, N>(), s>>>(q);
 }
 
 template <typename R, int N>
@@ -270,7 +270,7 @@ struct Impl {
     const long nbox = (long)B * 2 * K * M;
     ++c->launches; k_gather_box<R><<<grid1d(nbox), 256, 0, s>>>(fhat, (cplx<R>*)c->F, N, B);
     launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
-    launch_row_rhs<R, N>(c, B, nullptr, s);
+    launch_row_rhs<R, N>(c, B, s);
     launch_col_rk4<R, N>(c, B, COL_PLAIN, 0, diss, s);
     const long nfull = (long)B * 2 * N * (N / 2 + 1);
     ++c->launches; k_scatter_box<R><<<grid1d(nfull), 256, 0, s>>>((const cplx<R>*)c->OUT, dfdt, N, B);
@@ -284,7 +284,7 @@ struct Impl {
     constexpr int GS = 16;
     auto one_step = [&](cudaStream_t st_, bool last) {
       for (int st = 1; st <= 4; ++st) {
-        launch_row_rhs<R, N>(c, B, nullptr, st_);
+        launch_row_rhs<R, N>(c, B, st_);
         launch_col_rk4<R, N>(c, B, st, (st == 4 && last) ? 0 : 1, 0, st_);
       }
     };
@@ -344,7 +344,7 @@ struct Impl {
     if (amax <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
     ++c->launches; k_rk43_setup<<<(B + 127) / 128, 128, 0, s>>>(T, cfg->h0, c->ctl, B);
     launch_col_rk43<R, N>(c, B, R43_START, s);
-    launch_row_rhs<R, N>(c, B, nullptr, s, c->ctl);
+    launch_row_rhs<R, N>(c, B, s, c->ctl);
     launch_col_rk43<R, N>(c, B, R43_INIT, s);
     // one attempt = 5 column + 4 row + 1 error launches; a chunk of GA attempts is
     // captured once into a CUDA graph (all per-attempt data is read from the
@@ -352,7 +352,7 @@ struct Impl {
     auto attempt = [&](cudaStream_t st_) {
       launch_col_rk43<R, N>(c, B, R43_A, st_, rec, cap);
       for (int st = R43_B; st <= R43_E; ++st) {
-        launch_row_rhs<R, N>(c, B, nullptr, st_, c->ctl);
+        launch_row_rhs<R, N>(c, B, st_, c->ctl);
         launch_col_rk43<R, N>(c, B, st, st_, rec, cap);
       }
       launch_row_err<R, N>(c, B, cfg->atol, st_, rec_h, rec_acc, cap);
@@ -469,7 +469,7 @@ struct Impl {
     for (long it = 0; it < steps; ++it) {
       cplx<R>* rs = rec + (size_t)it * Q_NREC * VEC;
       for (int k = 1; k <= 4; ++k) {
-        launch_row_rhs<R, N>(c, 1, nullptr, s);
+        launch_row_rhs<R, N>(c, 1, s);
         launch_col_rk4<R, N>(c, 1, k, (k == 4 && it == steps - 1) ? 0 : 1, 0, s, rs, 0);
       }
     }
@@ -520,7 +520,7 @@ struct Impl {
     if (st) return st;
     cudaMemcpyAsync(c->F, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
     launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, s);
-    launch_row_rhs<R, N>(c, 1, nullptr, s);
+    launch_row_rhs<R, N>(c, 1, s);
     launch_col_rk4<R, N>(c, 1, COL_PLAIN, 0, 1, s);
     st = from_box(c, (const cplx<R>*)c->OUT, (R*)L.vt, 1, s);
     if (st) return st;
@@ -616,7 +616,7 @@ struct Impl {
   }
 
   static size_t chunk_items() {
-    const size_t per = (size_t)8 * K * N * sizeof(cplx<R>) + (size_t)N * 8 * N * sizeof(R);
+    const size_t per = (size_t)NG * K * N * sizeof(cplx<R>) + (size_t)N * NPH * N * sizeof(R);
     size_t c = ((size_t)384 << 20) / per;
     return c < 8 ? 8 : (c > 512 ? 512 : c);
   }
@@ -628,8 +628,8 @@ struct Impl {
     (void)have2;
     if (c->Greg) { cudaFree(c->Greg); cudaFree(c->Phys); c->Greg = c->Phys = nullptr; }
     size_t h1 = 0, h2 = 0;
-    int st = grow(c, &c->Greg, &h1, ci * 8 * K * N * sizeof(cplx<R>));
-    if (!st) st = grow(c, &c->Phys, &h2, ci * N * 8 * N * sizeof(R));
+    int st = grow(c, &c->Greg, &h1, ci * NG * K * N * sizeof(cplx<R>));
+    if (!st) st = grow(c, &c->Phys, &h2, ci * N * NPH * N * sizeof(R));
     if (st) return st;
     (void)have1;
     c->reg_items = ci;
@@ -681,7 +681,7 @@ struct Impl {
         const long cnt = std::min<long>(ci, (long)items.size() - item);
         launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + item, (int)cnt, s);
       }
-      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * 8 * N;
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
     };
     const cplx<R>* rec = (const cplx<R>*)L.rec;
     if (!rk43) {
@@ -703,7 +703,7 @@ struct Impl {
             slo = item;
             launch_regen<R, N>(c, rseg, c->items + item, (int)std::min<long>(ci, (long)sitems.size() - item), s);
           }
-          return (const R*)c->Phys + (size_t)(item - slo) * N * 8 * N;
+          return (const R*)c->Phys + (size_t)(item - slo) * N * NPH * N;
         };
         launch_col_tan<R, N>(c, B, TS_START, 1, rseg, dT, 0.0, L.h, dscale, nslot, s);
         for (long it = 0; it < cnt; ++it) {
@@ -801,7 +801,7 @@ struct Impl {
         const long cnt = std::min<long>(ci, (long)items.size() - chunk_lo);
         launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + chunk_lo, (int)cnt, s);
       }
-      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * 8 * N;
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
     };
     const cplx<R>* rec = (const cplx<R>*)L.rec;
     double tscale;
@@ -826,7 +826,7 @@ struct Impl {
             slo = std::max<long>(0, item - ci + 1);
             launch_regen<R, N>(c, rseg, c->items + slo, (int)std::min<long>(ci, (long)sitems.size() - slo), s);
           }
-          return (const R*)c->Phys + (size_t)(item - slo) * N * 8 * N;
+          return (const R*)c->Phys + (size_t)(item - slo) * N * NPH * N;
         };
         // seed the segment's last step from obar (J_OB)
         launch_col_adj<R, N>(c, B, AJ_PRE, rseg + (size_t)(cnt - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
@@ -921,7 +921,7 @@ struct Impl {
     const int B = c->max_batch;
     auto one_step = [&](cudaStream_t st_) {
       for (int st = 1; st <= 4; ++st) {
-        launch_row_rhs<R, N>(c, B, nullptr, st_, c->ctl);
+        launch_row_rhs<R, N>(c, B, st_, c->ctl);
         launch_col_rk4<R, N>(c, B, st, 1, 0, st_, nullptr, 0, 1);
       }
       ++c->launches; k_pool_count<<<(B + 127) / 128, 128, 0, st_>>>(c->ctl, B);
@@ -996,8 +996,8 @@ struct Impl {
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     if (e != cudaSuccess) return cuda_err(c, e, "bench_kernel");
     *ms = t / iters;
-    if (which == 0) *bytes = (double)B * (8 + 2) * K * N * cb + (double)N * 8 * N * rb;
-    else *bytes = (double)B * (2 * K * N * cb + 8 * K * N * cb + 2 * VEC * cb) + (double)VEC * cb;
+    if (which == 0) *bytes = (double)B * (NG + NH) * K * N * cb + (double)N * NPH * N * rb;
+    else *bytes = (double)B * (NH * K * N * cb + NG * K * N * cb + 2 * VEC * cb) + (double)VEC * cb;
     return ECS_OK;
   }
 };
@@ -1018,8 +1018,9 @@ int ctx_init(ecs_ctx* c, const ecs_params* prm) {
   c->OUT = dev_alloc(c, nbox * cb, &st);
   c->V = dev_alloc(c, nbox * cb, &st);
   c->Etab = dev_alloc(c, nbox * rb, &st);
-  c->G = dev_alloc(c, (size_t)B * 8 * Geomc<N>::K * N * cb, &st);
-  c->H = dev_alloc(c, (size_t)B * 8 * Geomc<N>::K * N * cb, &st);
+  // G holds NG (stepping) or 2 (boundary) fields, H holds NH, NHA or 2
+  c->G = dev_alloc(c, (size_t)B * NG * Geomc<N>::K * N * cb, &st);
+  c->H = dev_alloc(c, (size_t)B * NHA * Geomc<N>::K * N * cb, &st);
   c->fields_tmp = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
   c->fields_tmp2 = dev_alloc(c, (size_t)B * 2 * N * N * rb, &st);
   c->S43 = dev_alloc(c, nbox * S_NSLOT * cb, &st);

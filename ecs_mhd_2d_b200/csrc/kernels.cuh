@@ -1,17 +1,32 @@
 // Hot-path kernels of the pseudo-spectral MHD right-hand side and the Lawson
 // steppers.  One right-hand-side evaluation (reference: state_vel,
 // jax_scripts/lib/mhd_jax.py:105-175) is split into two passes around the two
-// transposes of a 2D FFT:
+// transposes of a 2D FFT.
 //
-//   column pass (one warp per (batch, ky) column, x contiguous):
-//     [forward FFT along x of the two product fields of the previous RHS]
-//     -> spectral epilogue (dealias mask, k^2, forcing, stepper stage algebra)
-//     -> stage input -> 4 spectral multipliers per channel (i kx, i ky,
-//        i ky/k^2, -i kx/k^2) -> 8 inverse FFTs along x -> G
+// Nonlinear terms.  The reference forms
+//   dw/dt = -(u.grad w) + (B.grad j) + f,   dj/dt = k^2 rfft2(u B_y - v B_x)
+// from 8 physical fields (the x and y derivatives of w and j and the uncurled
+// velocities u, v, B_x, B_y, B with the mean field b0).  For divergence-free u
+// and B with w = dv/dx - du/dy (and j likewise from B) the advection terms
+// equal Basdevant's form
+//   u.grad w = d_xy(v^2 - u^2) + (d_xx - d_yy)(u v)
+// so that, with
+//   P1 = (u^2 - v^2) - (B_x^2 - B_y^2),  P2 = B_x B_y - u v,  P3 = u B_y - v B_x,
+//   dw/dt = mask (-kx ky P1^ + (ky^2 - kx^2) P2^ + f^),   dj/dt = k^2 mask P3^.
+// Products of two fields on the 2/3-dealiased box alias only onto modes outside
+// the box, so the retained modes of both forms are equal in exact arithmetic;
+// this form needs 4 physical fields instead of 8 and 7 column transforms
+// instead of 10.
+//
+//   column pass (one warp per (batch, ky, channel), x contiguous):
+//     [forward FFTs along x of the product rows of the previous RHS: P1, P2
+//      (channel w) or P3 (channel j)]
+//     -> spectral epilogue (multipliers, dealias mask, forcing, stepper stage algebra)
+//     -> stage input -> the two uncurling multipliers i ky/k^2, -i kx/k^2
+//        -> 2 inverse FFTs along x -> G (u, v or B_x, B_y)
 //   row pass (one warp per physical row x, CTA = XT rows staged in shared memory):
-//     8 half-spectra rows of G -> 4 complex inverse FFTs (two real fields
-//     packed per transform) -> pointwise products (advection, induction,
-//     mean field) -> 1 forward FFT (two products packed) -> split -> H
+//     4 half-spectra rows of G -> 2 complex inverse FFTs (two real fields
+//     packed per transform) -> P1, P2, P3 -> 2 forward FFTs -> split -> H
 //
 // The box layout and intermediate layouts are documented in common.cuh.
 #pragma once
@@ -20,6 +35,12 @@
 #include "fft.cuh"
 
 namespace ecs {
+
+// Field counts of the intermediate arrays (per batch element).
+constexpr int NG = 4;    // G[b][NG][K][N]: inverse column transforms of u, v, B_x, B_y (no mean field)
+constexpr int NH = 3;    // H[b][NH][K][N]: row transforms of P1, P2, P3
+constexpr int NPH = 4;   // physical record rows: u, v, B_x + b0x, B_y + b0y
+constexpr int NHA = 4;   // adjoint H[b][NHA][K][N]: row transforms of the cotangents of u, v, B_x, B_y
 
 // ---------------------------------------------------------------------------
 // spectral helpers
@@ -54,87 +75,17 @@ __device__ __forceinline__ R diss_L(int kx, int ky, R coeff) {
   return (-ksq_masked<R>(kx, ky)) * coeff;
 }
 
-// ---------------------------------------------------------------------------
-// column-pass building blocks (one warp per (batch, ky) column)
-// ---------------------------------------------------------------------------
-
-// Load the two product columns H[b][0..1][ky][:] and transform them along x
-// (forward, natural -> bit-reversed order).
-template <typename R, int N>
-__device__ __forceinline__ void col_load_fwd(const cplx<R>* __restrict__ H, int b, int ky, int lane,
-                                             const cplx<R>* s_tw, cplx<R> (&r0)[N / 32], cplx<R> (&r1)[N / 32]) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
-  const cplx<R>* h0 = H + ((size_t)(b * 2 + 0) * K + ky) * N;
-  const cplx<R>* h1 = H + ((size_t)(b * 2 + 1) * K + ky) * N;
-#pragma unroll
-  for (int j = 0; j < E; ++j) { r0[j] = h0[lane + 32 * j]; r1[j] = h1[lane + 32 * j]; }
-  fft_dif<R, N, false>(r0, s_tw, lane);
-  fft_dif<R, N, false>(r1, s_tw, lane);
-}
-
-// Nonlinear time derivative at one box mode from the transformed products:
-// v_omega = mask*(rfft2(P1) + rfft2(forcing)), v_j = k^2 mask rfft2(P2)  (mhd_jax.py:159-164).
+// Multiplier of the transformed product row f in {0: P1, 1: P2, 2: P3} in the
+// nonlinear time derivative: -kx ky, ky^2 - kx^2 (channel w), k^2 (channel j).
+// Integer arithmetic, exact; zero at (0,0), which the mask removes.
 template <typename R>
-__device__ __forceinline__ void rhs_vals(cplx<R> r0, cplx<R> r1, int kx, int ky, cplx<R> fh, cplx<R>& v0,
-                                         cplx<R>& v1) {
-  const bool in_mask = !(kx == 0 && ky == 0);
-  v0 = in_mask ? cadd(r0, fh) : mk<R>(0, 0);
-  v1 = cscale(r1, ksq_masked<R>(kx, ky));
-}
-
-// Stage input (x0, x1 in bit-reversed slot order) -> the 8 multiplied inverse
-// transforms along x of state_vel (mhd_jax.py:136-141), scaled by 1/n^2.
-template <typename R, int N>
-__device__ __forceinline__ void col_inverse8(const cplx<R> (&x0)[N / 32], const cplx<R> (&x1)[N / 32],
-                                             cplx<R>* __restrict__ G, int b, int ky, int lane,
-                                             const cplx<R>* s_tw) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
-  const R inv_n2 = R(1) / (R(N) * R(N));
-  // one copy of the transform code: the (c, m) loop is not unrolled
-#pragma unroll 1
-  for (int cm = 0; cm < 8; ++cm) {
-    const int c = cm >> 2, m = cm & 3;
-    {
-      cplx<R> w[E];
-#pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
-        const cplx<R> xv = c == 0 ? x0[j] : x1[j];
-        w[j] = cscale(cimul(xv, spectral_mu<R>(m, kx, ky)), inv_n2);
-      }
-      fft_dit<R, N, true>(w, s_tw, lane);
-      cplx<R>* gout = G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
-#pragma unroll
-      for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
-    }
-  }
-}
-
-// Plain inverse transforms along x of two box columns, scaled 1/n^2, written to
-// fields 0 and 1 of G[b] (pitch `nf` fields per batch element).
-template <typename R, int N>
-__device__ __forceinline__ void col_inverse2(const cplx<R> (&x0)[N / 32], const cplx<R> (&x1)[N / 32],
-                                             cplx<R>* __restrict__ G, int nf, int b, int ky, int lane,
-                                             const cplx<R>* s_tw) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
-  const R inv_n2 = R(1) / (R(N) * R(N));
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    cplx<R> w[E];
-#pragma unroll
-    for (int j = 0; j < E; ++j) w[j] = cscale(c == 0 ? x0[j] : x1[j], inv_n2);
-    fft_dit<R, N, true>(w, s_tw, lane);
-    cplx<R>* gout = G + ((size_t)(b * nf + c) * K + ky) * N;
-#pragma unroll
-    for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
-  }
+__device__ __forceinline__ R prod_mult(int f, int kx, int ky) {
+  const int m = f == 0 ? -kx * ky : f == 1 ? ky * ky - kx * kx : kx * kx + ky * ky;
+  return (R)m;
 }
 
 // ---------------------------------------------------------------------------
-// per-channel column helpers (one warp per (batch, ky, channel))
+// column-pass building blocks (one warp per (batch, ky, channel))
 // ---------------------------------------------------------------------------
 
 // Load column H[b][f][ky][:] (nf fields per batch element) and transform it
@@ -150,28 +101,59 @@ __device__ __forceinline__ void col_load_fwd1(const cplx<R>* __restrict__ H, int
   fft_dif<R, N, false>(r, s_tw, lane);
 }
 
-// Stage input of channel c (bit-reversed slot order) -> its 4 multiplied
-// inverse transforms along x (fields 4c..4c+3 of state_vel, mhd_jax.py:136-141),
-// scaled by 1/n^2.  One copy of the transform code: the m loop is not unrolled.
+// Nonlinear time derivative of channel ch (without forcing) at every position
+// of the column ky, bit-reversed slot order, from the product rows in H:
+//   ch 0: -kx ky rfft2(P1) + (ky^2 - kx^2) rfft2(P2)  (two transforms in lockstep),
+//   ch 1: k^2 rfft2(P3).
 template <typename R, int N>
-__device__ __forceinline__ void col_inverse4(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int b, int c,
-                                             int ky, int lane, const cplx<R>* s_tw) {
+__device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int b, int ch, int ky, int lane,
+                                             const cplx<R>* s_tw, cplx<R> (&v)[N / 32]) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
-  const R inv_n2 = R(1) / (R(N) * R(N));
-#pragma unroll 1
-  for (int m = 0; m < 4; ++m) {
-    cplx<R> w[E];
+  if (ch == 0) {
+    const cplx<R>* h0 = H + ((size_t)(b * NH + 0) * K + ky) * N;
+    const cplx<R>* h1 = H + ((size_t)(b * NH + 1) * K + ky) * N;
+    cplx<R> r[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) { v[j] = h0[lane + 32 * j]; r[j] = h1[lane + 32 * j]; }
+    fft_dif2<R, N, false>(v, r, s_tw, lane);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
-      w[j] = cscale(cimul(x[j], spectral_mu<R>(m, kx, ky)), inv_n2);
+      const R m0 = prod_mult<R>(0, kx, ky), m1 = prod_mult<R>(1, kx, ky);
+      v[j] = mk<R>(m0 * v[j].x + m1 * r[j].x, m0 * v[j].y + m1 * r[j].y);
     }
-    fft_dit<R, N, true>(w, s_tw, lane);
-    cplx<R>* gout = G + ((size_t)(b * 8 + c * 4 + m) * K + ky) * N;
+  } else {
+    col_load_fwd1<R, N>(H, NH, b, 2, ky, lane, s_tw, v);
 #pragma unroll
-    for (int j = 0; j < E; ++j) gout[lane + 32 * j] = w[j];
+    for (int j = 0; j < E; ++j) {
+      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      v[j] = cscale(v[j], prod_mult<R>(2, kx, ky));
+    }
   }
+}
+
+// Stage input x of channel c (bit-reversed slot order) -> its two uncurled
+// fields i (ky/k^2) x and i (-kx/k^2) x (mhd_jax.py:140-141) transformed along
+// x in lockstep, scaled by 1/n^2, to G fields 2c and 2c+1.
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse_uv(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int b, int c,
+                                               int ky, int lane, const cplx<R>* s_tw) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  const R inv_n2 = R(1) / (R(N) * R(N));
+  cplx<R> wu[E], wv[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+    wu[j] = cscale(cimul(x[j], spectral_mu<R>(2, kx, ky)), inv_n2);
+    wv[j] = cscale(cimul(x[j], spectral_mu<R>(3, kx, ky)), inv_n2);
+  }
+  fft_dit2<R, N, true>(wu, wv, s_tw, lane);
+  cplx<R>* gu = G + ((size_t)(b * NG + 2 * c) * K + ky) * N;
+  cplx<R>* gv = gu + (size_t)K * N;
+#pragma unroll
+  for (int j = 0; j < E; ++j) { gu[lane + 32 * j] = wu[j]; gv[lane + 32 * j] = wv[j]; }
 }
 
 // One plain inverse transform along x of a box column, scaled, to field f of
@@ -210,8 +192,8 @@ enum ColStage : int {
 
 template <typename R>
 struct ColParams {
-  const cplx<R>* H;      // [B][2][K][N]
-  cplx<R>* G;            // [B][8][K][N]
+  const cplx<R>* H;      // [B][NH][K][N]
+  cplx<R>* G;            // [B][NG][K][N]
   cplx<R>* F;            // [B][2][K][M]   state / accumulator
   cplx<R>* A1;           // [B][2][K][M]   e*k1
   cplx<R>* K2;           // [B][2][K][M]   k2
@@ -235,7 +217,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -243,9 +225,9 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   if (colid >= p.B * K * 2) return;
   const int c = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
 
-  cplx<R> r[E];
-  if (STAGE != COL_START) col_load_fwd1<R, N>(p.H, 2, b, c, ky, lane, s_tw, r);
   if (p.use_done && p.ctl[b].done) return;
+  cplx<R> r[E];
+  if (STAGE != COL_START) col_load_rhs<R, N>(p.H, b, c, ky, lane, s_tw, r);
   const R h = (R)p.ctl[b].h;
   const size_t base = ((size_t)(b * 2 + c) * K + ky) * M;
   cplx<R>* rb = p.rec ? p.rec + (size_t)b * p.rec_bstride : nullptr;
@@ -259,8 +241,8 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
     const bool in_mask = !(kx == 0 && ky == 0);
     cplx<R> v = mk<R>(0, 0);
     if (STAGE != COL_START) {
-      if (c == 0) { if (in_mask) v = cadd(r[j], p.fhat[ky * M + slot]); }   // mask * rfft2(-adv0+adv1+forcing)
-      else v = cscale(r[j], ksq_masked<R>(kx, ky));                           // k^2 mask * rfft2(u x B)
+      v = r[j];                                                        // zero at (0,0)
+      if (c == 0 && in_mask) v = cadd(v, p.fhat[ky * M + slot]);       // mask * rfft2(forcing)
     }
     const size_t i = base + slot;
     const size_t o = ((size_t)c * K + ky) * M + slot;
@@ -307,7 +289,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
     }
   }
   if (!p.produce) return;
-  col_inverse4<R, N>(x, p.G, b, c, ky, lane, s_tw);
+  col_inverse_uv<R, N>(x, p.G, b, c, ky, lane, s_tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -316,24 +298,20 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
 
 template <typename R>
 struct RowParams {
-  const cplx<R>* G;   // [B][8][K][N]
-  cplx<R>* H;         // [B][2][K][N]
-  R* phys;            // optional record of the 8 physical fields, see phys_row()
-  long phys_bstride;  // elements per batch element in phys
-  int rec_index;      // record slot (attempt); < 0: ctl[b].attempts
-  int phys_stage;     // stage slot 0..3 within the record
-  const StepCtl* ctl; // per-batch control (done flags, attempt counters) or null
+  const cplx<R>* G;   // [B][NG][K][N]
+  cplx<R>* H;         // [B][NH][K][N]
+  const StepCtl* ctl; // per-batch control (done flags) or null
   const cplx<R>* tw;
   R b0x, b0y;
   int B;
 };
 
-// Physical-field record: phys[b][rec][stage(4)][x][field(8)][pos] with pos the
-// warp-FFT position order (see fft.cuh), so that readers with the same
-// transform structure use identical indexing.
+// Physical-field record of one stage: phys[x][NPH][pos] with pos the warp-FFT
+// position order (see fft.cuh), so that readers with the same transform
+// structure use identical indexing.
 template <typename R, int N>
-__device__ __forceinline__ R* phys_row(R* base, long bstride, int b, int rec, int stage, int x) {
-  return base + (size_t)b * bstride + (((size_t)rec * 4 + stage) * N + x) * 8 * N;
+__device__ __forceinline__ const R* phys_row(const R* base, int x) {
+  return base + (size_t)x * NPH * N;
 }
 
 // Load a [nf][K][XT] tile of a [B][nf][K][N] array into shared memory with row pitch XT+1.
@@ -371,6 +349,33 @@ __device__ __forceinline__ cplx<R> packed_pair(const cplx<R>* sA, const cplx<R>*
   return mk<R>(0, 0);
 }
 
+// Full Hermitian spectrum value at position q of one real field (imaginary
+// part of the transform left zero) from its half-spectrum row sA.
+template <typename R, int N, int XT>
+__device__ __forceinline__ cplx<R> packed_one(const cplx<R>* sA, int q, int w) {
+  constexpr int K = (N - 1) / 3 + 1;
+  if (q < K) {
+    cplx<R> a = sA[q * (XT + 1) + w];
+    if (q == 0) a.y = 0;
+    return a;
+  }
+  if (q > N - K) return cconj(sA[(N - q) * (XT + 1) + w]);
+  return mk<R>(0, 0);
+}
+
+// Half spectrum (ky < K) of a natural-order forward transform W of one real
+// field, written to shared row s1.
+template <typename R, int N, int XT>
+__device__ __forceinline__ void store_one(const cplx<R> (&W)[N / 32], cplx<R>* s1, int w, int lane) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int q = lane + 32 * j;
+    if (q < K) s1[q * (XT + 1) + w] = W[j];
+  }
+}
+
 // Split a natural-order forward transform W of (P1 + i P2) into the half
 // spectra of P1 and P2 and write ky < K into shared rows s1, s2.
 template <typename R, int N, int XT>
@@ -396,57 +401,38 @@ __global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
-  cplx<R>* s_H = s_G + 8 * K * (XT + 1);
+  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_H = s_G + NG * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   if (p.ctl && p.ctl[b].done) return;   // whole block belongs to one batch element
   load_twiddles<R, N>(s_tw, p.tw);
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 8 * K, x0);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int x = x0 + w;
-  R* ph = nullptr;
-  if (p.phys) {
-    const int rec = p.rec_index >= 0 ? p.rec_index : p.ctl[b].attempts;
-    ph = phys_row<R, N>(p.phys, p.phys_bstride, b, rec, p.phys_stage, x);
-  }
 
-  // pairs: (fx0,fy0) (fu0,fv0) (fx1,fy1) (fu1,fv1)
-  cplx<R> xy0[E], uv0[E], xy1[E], uv1[E];
+  // pairs (u, v) and (B_x, B_y) without the mean field (mhd_jax.py:140-149)
+  cplx<R> uv[E], bb[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const int q = lane + 32 * j;
-    xy0[j] = packed_pair<R, N, XT>(s_G + 0 * K * (XT + 1), s_G + 1 * K * (XT + 1), q, w);
-    uv0[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), q, w);
-    xy1[j] = packed_pair<R, N, XT>(s_G + 4 * K * (XT + 1), s_G + 5 * K * (XT + 1), q, w);
-    uv1[j] = packed_pair<R, N, XT>(s_G + 6 * K * (XT + 1), s_G + 7 * K * (XT + 1), q, w);
+    uv[j] = packed_pair<R, N, XT>(s_G + 0 * K * (XT + 1), s_G + 1 * K * (XT + 1), q, w);
+    bb[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), q, w);
   }
-  fft_dif<R, N, true>(xy0, s_tw, lane);
-  fft_dif<R, N, true>(uv0, s_tw, lane);
-  fft_dif<R, N, true>(xy1, s_tw, lane);
-  fft_dif<R, N, true>(uv1, s_tw, lane);
+  fft_dif2<R, N, true>(uv, bb, s_tw, lane);
   cplx<R> W[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const R fx0 = xy0[j].x, fy0 = xy0[j].y, fu0 = uv0[j].x, fv0 = uv0[j].y;
-    const R fx1 = xy1[j].x, fy1 = xy1[j].y;
-    const R fu1 = uv1[j].x + p.b0x, fv1 = uv1[j].y + p.b0y;   // mhd_jax.py:145-149
-    const R adv0 = fu0 * fx0 + fv0 * fy0;                      // :152
-    const R adv1 = fu1 * fx1 + fv1 * fy1;
-    const R P1 = -adv0 + adv1;                                 // :159 (forcing added spectrally)
-    const R P2 = fu0 * fv1 - fv0 * fu1;                        // :163
-    W[j] = mk<R>(P1, P2);
-    if (ph) {
-      const int e = lane + 32 * j;
-      ph[0 * N + e] = fx0; ph[1 * N + e] = fy0; ph[2 * N + e] = fu0; ph[3 * N + e] = fv0;
-      ph[4 * N + e] = fx1; ph[5 * N + e] = fy1; ph[6 * N + e] = fu1; ph[7 * N + e] = fv1;
-    }
+    const R u = uv[j].x, v = uv[j].y;
+    const R bx = bb[j].x + p.b0x, by = bb[j].y + p.b0y;
+    W[j] = mk<R>((u - v) * (u + v) - (bx - by) * (bx + by), bx * by - u * v);   // (P1, P2)
+    bb[j] = mk<R>(u * by - v * bx, R(0));                                       // (P3, 0), mhd_jax.py:163
   }
-  fft_dit<R, N, false>(W, s_tw, lane);
+  fft_dit2<R, N, false>(W, bb, s_tw, lane);
   split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
+  store_one<R, N, XT>(bb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
-  store_tile<R, N, XT>(p.H + (size_t)b * 2 * K * N, s_H, 2 * K, x0);
+  store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,7 +454,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_to_box(RowFwdParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_H = s_tw + N / 2;
+  cplx<R>* s_H = s_tw + tw_smem(N);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);
@@ -503,7 +489,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(128) k_col_to_box(ColBoxParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -566,7 +552,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -622,7 +608,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_from_box(RowFromBoxParams<R> p)
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_G = s_tw + tw_smem(N);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);

@@ -7,10 +7,15 @@
 // Euclidean dot.  With these, the transposes of the box transforms are
 //   to_box^T(Y)   = n^2 irfft2(Y / c_ky)        (c_ky = 1 for ky = 0, else 2)
 //   from_box^T(w) = (c_ky / n^2) rfft2(w)
-// so one adjoint right-hand side is again a column pass and a row pass:
-//   lambda -> P1bar = Re sum mask lambda_w e^{ik.x},  P2bar = Re sum k^2 mask lambda_j e^{ik.x}
-//   -> product adjoints with the primal fields -> 8 forward transforms
-//   -> Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_mc).
+// so one adjoint right-hand side is again a column pass and a row pass
+// (Basdevant form of the products, see kernels.cuh):
+//   lambda -> P1bar = Re sum (-kx ky) lambda_w e^{ik.x},  P2bar = Re sum (ky^2 - kx^2) lambda_w e^{ik.x},
+//             P3bar = Re sum k^2 lambda_j e^{ik.x}
+//   -> product adjoints with the primal fields
+//        ubar  =  2u P1bar - v P2bar + B_y P3bar,   vbar  = -2v P1bar - u P2bar - B_x P3bar,
+//        Bxbar = -2B_x P1bar + B_y P2bar - v P3bar, Bybar =  2B_y P1bar + B_x P2bar + u P3bar
+//   -> 4 forward transforms
+//   -> Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_mc), mu_m in {ky/k^2, -kx/k^2}.
 #pragma once
 
 #include "kernels.cuh"
@@ -24,9 +29,9 @@ namespace ecs {
 // ---------------------------------------------------------------------------
 template <typename R>
 struct RowAdjParams {
-  const cplx<R>* G;     // [B][8][K][N]: fields 0,1 hold the inverse columns of (mask lam_w, k^2 mask lam_j)/c
-  cplx<R>* H;           // [B][8][K][N]: rfft2 rows of the 8 adjoint fields
-  const R* phys;        // primal physical fields of this stage [N][8][N]
+  const cplx<R>* G;     // [B][NG][K][N]: fields 0..2 hold the inverse columns of the P1, P2, P3 cotangents (/c_ky)
+  cplx<R>* H;           // [B][NHA][K][N]: rfft2 rows of the 4 adjoint fields
+  const R* phys;        // primal physical fields of this stage [N][NPH][N]
   const cplx<R>* tw;
   int B;
 };
@@ -37,48 +42,41 @@ __global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
-  cplx<R>* s_H = s_G + 2 * K * (XT + 1);
+  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_H = s_G + 3 * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
-  load_twiddles<R, N>(s_tw, p.tw);
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 2 * K, x0);
-  __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
-  const R* ph = p.phys + ((size_t)x * 8) * N;
-  cplx<R> P[E];   // (P1bar, P2bar) in position order
+  const R* ph = phys_row<R, N>(p.phys, x);
+  R pu[E], pv[E], pbx[E], pby[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) P[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), lane + 32 * j, w);
-  fft_dif<R, N, true>(P, s_tw, lane);
-  // primal fields: 0 fx0 1 fy0 2 fu0 3 fv0 4 fx1 5 fy1 6 fu1 7 fv1 (fu1, fv1 with b0)
-  // P1 = -(fu0 fx0 + fv0 fy0) + (fu1 fx1 + fv1 fy1),  P2 = fu0 fv1 - fv0 fu1   (mhd_jax.py:152-163)
-#pragma unroll
-  for (int pr = 0; pr < 4; ++pr) {
-    cplx<R> z[E];
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int e = lane + 32 * j;
-      const R p1 = P[j].x, p2 = P[j].y;
-      R a, c;
-      if (pr == 0) {          // (fx0bar, fy0bar)
-        a = -ph[2 * N + e] * p1; c = -ph[3 * N + e] * p1;
-      } else if (pr == 1) {   // (fu0bar, fv0bar)
-        a = -ph[0 * N + e] * p1 + ph[7 * N + e] * p2;
-        c = -ph[1 * N + e] * p1 - ph[6 * N + e] * p2;
-      } else if (pr == 2) {   // (fx1bar, fy1bar)
-        a = ph[6 * N + e] * p1; c = ph[7 * N + e] * p1;
-      } else {                // (fu1bar, fv1bar)
-        a = ph[4 * N + e] * p1 - ph[3 * N + e] * p2;
-        c = ph[5 * N + e] * p1 + ph[2 * N + e] * p2;
-      }
-      z[j] = mk<R>(a, c);
-    }
-    fft_dit<R, N, false>(z, s_tw, lane);
-    split_store<R, N, XT>(z, s_H + (2 * pr) * K * (XT + 1), s_H + (2 * pr + 1) * K * (XT + 1), w, lane);
+  for (int j = 0; j < E; ++j) {
+    const int e = lane + 32 * j;
+    pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
   }
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, 3 * K, x0);
   __syncthreads();
-  store_tile<R, N, XT>(p.H + (size_t)b * 8 * K * N, s_H, 8 * K, x0);
+  cplx<R> P12[E], P3[E];   // (P1bar, P2bar) and (P3bar, 0) in position order
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    P12[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), lane + 32 * j, w);
+    P3[j] = packed_one<R, N, XT>(s_G + 2 * K * (XT + 1), lane + 32 * j, w);
+  }
+  fft_dif2<R, N, true>(P12, P3, s_tw, lane);
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const R p1 = P12[j].x, p2 = P12[j].y, p3 = P3[j].x;
+    const R u = pu[j], v = pv[j], bx = pbx[j], by = pby[j];
+    P12[j] = mk<R>(R(2) * u * p1 - v * p2 + by * p3, -R(2) * v * p1 - u * p2 - bx * p3);     // (ubar, vbar)
+    P3[j] = mk<R>(-R(2) * bx * p1 + by * p2 - v * p3, R(2) * by * p1 + bx * p2 + u * p3);    // (Bxbar, Bybar)
+  }
+  fft_dit2<R, N, false>(P12, P3, s_tw, lane);
+  split_store<R, N, XT>(P12, s_H, s_H + K * (XT + 1), w, lane);
+  split_store<R, N, XT>(P3, s_H + 2 * K * (XT + 1), s_H + 3 * K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * NHA * K * N, s_H, NHA * K, x0);
 }
 
 // ---------------------------------------------------------------------------
@@ -99,8 +97,8 @@ enum AdjSlot43 { JJ_X0 = 0, JJ_K1, JJ_X2, JJ_XB, JJ_K1P, JJ_K1PP, JJ_K2, JJ_K2P,
 
 template <typename R>
 struct ColAdjParams {
-  const cplx<R>* H;     // [B][8][K][N]
-  cplx<R>* G;           // [B][8][K][N] (fields 0,1 written)
+  const cplx<R>* H;     // [B][NHA][K][N]
+  cplx<R>* G;           // [B][NG][K][N] (fields 0..2 written)
   cplx<R>* J;           // adjoint slots [B][nslot][2][K][M]
   int nslot;
   const cplx<R>* rec;   // primal record of this step / attempt
@@ -119,7 +117,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -135,20 +133,21 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   const R inv_n2 = R(1) / (R(N) * R(N));
   const R coeff = ch == 0 ? p.nu : p.eta;
 
-  // Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_{m,c})
+  // Xbar_c = (c_ky/n^2) sum_m (-i mu_m) rfft2(fbar_{m,c}), m over the two uncurled fields of channel c
   cplx<R> xb[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) xb[j] = mk<R>(0, 0);
   if (has_rhs) {
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      cplx<R> v[E];
-      col_load_fwd1<R, N>(p.H, 8, b, 4 * ch + m, ky, lane, s_tw, v);
+    const cplx<R>* h0 = p.H + ((size_t)(b * NHA + 2 * ch) * K + ky) * N;
+    const cplx<R>* h1 = h0 + (size_t)K * N;
+    cplx<R> v1[E];
 #pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
-        xb[j] = cadd(xb[j], cimul(v[j], -spectral_mu<R>(m, kx, ky)));
-      }
+    for (int j = 0; j < E; ++j) { xb[j] = h0[lane + 32 * j]; v1[j] = h1[lane + 32 * j]; }
+    fft_dif2<R, N, false>(xb, v1, s_tw, lane);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      xb[j] = cadd(cimul(xb[j], -spectral_mu<R>(2, kx, ky)), cimul(v1[j], -spectral_mu<R>(3, kx, ky)));
     }
 #pragma unroll
     for (int j = 0; j < E; ++j) xb[j] = cscale(xb[j], cky * inv_n2);
@@ -156,7 +155,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
 
   double hpart = 0.0;
   bool feed = true;
-  cplx<R> lam[E];   // next adjoint-RHS input (mask lam_w or k^2 mask lam_j) / c_ky
+  cplx<R> lam[E];   // next adjoint-RHS input lambda / c_ky (multipliers applied per product below)
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     lam[j] = mk<R>(0, 0);
@@ -274,16 +273,36 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
       }
       kb = cscale(kb, t);
     }
-    // lambda = kb; next inverse input (mask lam_w, k^2 mask lam_j) / c_ky
-    const cplx<R> lin = ch == 0 ? (in_mask ? kb : mk<R>(0, 0)) : cscale(kb, ksq_masked<R>(kx, ky));
-    lam[j] = cdiv_r(lin, cky);
+    // lambda = kb; the product multipliers vanish at (0,0), which the mask removes
+    lam[j] = cdiv_r(kb, cky);
   }
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) hpart += __shfl_xor_sync(0xffffffffu, hpart, o);
   if (lane == 0) p.hacc[((size_t)b * K + ky) * 2 + ch] += hpart;
   if (!feed) return;
-  // unscaled inverse: Re sum lam e^{ik.x} once the row pass doubles ky > 0
-  col_inverse1<R, N>(lam, p.G, 8, b, ch, ky, lane, s_tw, R(1));
+  // unscaled inverses Re sum mult_f lam e^{ik.x} (the row pass doubles ky > 0):
+  // P1bar, P2bar from channel w, P3bar from channel j
+  if (ch == 0) {
+    cplx<R> z0[E], z1[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      z0[j] = cscale(lam[j], prod_mult<R>(0, kx, ky));
+      z1[j] = cscale(lam[j], prod_mult<R>(1, kx, ky));
+    }
+    fft_dit2<R, N, true>(z0, z1, s_tw, lane);
+    cplx<R>* g0 = p.G + ((size_t)(b * NG + 0) * K + ky) * N;
+    cplx<R>* g1 = g0 + (size_t)K * N;
+#pragma unroll
+    for (int j = 0; j < E; ++j) { g0[lane + 32 * j] = z0[j]; g1[lane + 32 * j] = z1[j]; }
+  } else {
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      lam[j] = cscale(lam[j], prod_mult<R>(2, kx, ky));
+    }
+    col_inverse1<R, N>(lam, p.G, NG, b, 2, ky, lane, s_tw, R(1));
+  }
 }
 
 // Rejected Lawson-RK4(3) attempt in reverse: k1_next = e (e k1).

@@ -30,8 +30,8 @@ enum Rk43Stage : int {
 
 template <typename R>
 struct Col43Params {
-  const cplx<R>* H;     // [B][2][K][N]
-  cplx<R>* G;           // [B][8][K][N]
+  const cplx<R>* H;     // [B][NH][K][N]
+  cplx<R>* G;           // [B][NG][K][N]
   cplx<R>* S;           // [B][S_NSLOT][2][K][M]
   StepCtl* ctl;         // [B]
   const cplx<R>* fhat;  // [K][M]
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
                        : nullptr;
   const bool has_rhs = STAGE != R43_A && STAGE != R43_START;
   cplx<R> r[E];
-  if (has_rhs) col_load_fwd1<R, N>(p.H, 2, b, ch, ky, lane, s_tw, r);
+  if (has_rhs) col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
   const R coeff = ch == 0 ? p.nu : p.eta;
   cplx<R> x[E];
 #pragma unroll
@@ -74,8 +74,8 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
     const int kx = slot_to_kx(slot, KMAX, M);
     cplx<R> v = mk<R>(0, 0);
     if (has_rhs) {
-      if (ch == 0) { if (!(kx == 0 && ky == 0)) v = cadd(r[j], p.fhat[ky * M + slot]); }
-      else v = cscale(r[j], ksq_masked<R>(kx, ky));
+      v = r[j];                                                        // zero at (0,0)
+      if (ch == 0 && !(kx == 0 && ky == 0)) v = cadd(v, p.fhat[ky * M + slot]);
     }
     const size_t o = ((size_t)ch * K + ky) * M + slot;
     const R L = diss_L<R>(kx, ky, coeff);
@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
     x[j] = xin;
   }
   if (STAGE == R43_INIT) return;
-  if (STAGE == R43_E) col_inverse1<R, N>(x, p.G, 8, b, ch, ky, lane, s_tw, R(1) / (R(N) * R(N)));
-  else col_inverse4<R, N>(x, p.G, b, ch, ky, lane, s_tw);
+  if (STAGE == R43_E) col_inverse1<R, N>(x, p.G, NG, b, ch, ky, lane, s_tw, R(1) / (R(N) * R(N)));
+  else col_inverse_uv<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
 // Error norm max|irfft2(d)| of the two channels (timestepping.py:288-291) with
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
 // candidate (timestepping.py:294-310).
 template <typename R>
 struct RowErrParams {
-  const cplx<R>* G;     // [B][8][K][N], fields 0,1 hold the inverse columns of d
+  const cplx<R>* G;     // [B][NG][K][N], fields 0,1 hold the inverse columns of d
   StepCtl* ctl;
   const cplx<R>* tw;
   double atol;
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_G = s_tw + tw_smem(N);
   __shared__ double s_max[XT];
   __shared__ int s_last;
   const int tiles = N / XT;
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
   StepCtl& c = p.ctl[b];
   if (c.done) return;
   load_twiddles<R, N>(s_tw, p.tw);
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 2 * K, x0);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, 2 * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   cplx<R> z[E];

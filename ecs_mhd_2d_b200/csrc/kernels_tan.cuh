@@ -3,10 +3,13 @@
 //
 // A batch of B tangents shares one primal trajectory.  The primal solve records,
 // per step (Lawson-RK4) or attempt (Lawson-RK4(3)), the compact stage inputs and
-// stage derivatives; the tangent pass regenerates the primal's 8 physical
-// fields for a chunk of stages in one batched launch pair (shared by all
-// tangents) and then advances the tangents with linearised products
-//   d(u.grad w) = du.grad w + u.grad dw, ...
+// stage derivatives; the tangent pass regenerates the primal's 4 physical
+// fields (u, v, B_x, B_y) for a chunk of stages in one batched launch pair
+// (shared by all tangents) and then advances the tangents with the linearised
+// products of the Basdevant form (see kernels.cuh)
+//   dP1 = 2 (u du - v dv) - 2 (B_x dB_x - B_y dB_y)
+//   dP2 = B_x dB_y + B_y dB_x - u dv - v du
+//   dP3 = u dB_y + B_y du - v dB_x - B_x dv
 // and the product rule through the integrating factor, e' = e L h'/2.
 #pragma once
 
@@ -23,7 +26,7 @@ template <typename R>
 struct ColRegenParams {
   const cplx<R>* rec;     // record base
   const long* items;      // [nitems] offsets (in box vectors) of the stage inputs in rec
-  cplx<R>* G;             // [nitems][8][K][N]
+  cplx<R>* G;             // [nitems][NG][K][N]
   const cplx<R>* tw;
   int nitems;
 };
@@ -33,29 +36,28 @@ __global__ void __launch_bounds__(128) k_col_regen(ColRegenParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (col >= p.nitems * K) return;
-  const int it = col / K, ky = col - it * K;
-  const cplx<R>* y = p.rec + (size_t)p.items[it] * VEC;
-  cplx<R> x0[E], x1[E];
+  if (col >= p.nitems * K * 2) return;
+  const int ch = col & 1, ik = col >> 1, it = ik / K, ky = ik - it * K;   // one warp per (item, ky, channel)
+  const cplx<R>* y = p.rec + (size_t)p.items[it] * VEC + (size_t)(ch * K + ky) * M;
+  cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
-    x0[j] = slot >= 0 ? y[(size_t)ky * M + slot] : mk<R>(0, 0);
-    x1[j] = slot >= 0 ? y[(size_t)(K + ky) * M + slot] : mk<R>(0, 0);
+    x[j] = slot >= 0 ? y[slot] : mk<R>(0, 0);
   }
-  col_inverse8<R, N>(x0, x1, p.G, it, ky, lane, s_tw);
+  col_inverse_uv<R, N>(x, p.G, it, ch, ky, lane, s_tw);
 }
 
-// Physical fields of each item: Phys[it][x][8][pos] (fu1, fv1 include b0).
+// Physical fields of each item: Phys[it][x][NPH][pos] (B_x, B_y include b0).
 template <typename R>
 struct RowPhysParams {
-  const cplx<R>* G;   // [nitems][8][K][N]
-  R* phys;            // [nitems][N][8][N]
+  const cplx<R>* G;   // [nitems][NG][K][N]
+  R* phys;            // [nitems][N][NPH][N]
   const cplx<R>* tw;
   R b0x, b0y;
   int nitems;
@@ -67,30 +69,27 @@ __global__ void __launch_bounds__(XT * 32) k_row_phys(RowPhysParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
+  cplx<R>* s_G = s_tw + tw_smem(N);
   const int tiles = N / XT;
   const int it = blockIdx.x / tiles, x0 = (blockIdx.x - it * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);
-  load_tile<R, N, XT>(s_G, p.G + (size_t)it * 8 * K * N, 8 * K, x0);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)it * NG * K * N, NG * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
-  R* ph = p.phys + (((size_t)it * N + x) * 8) * N;
+  R* ph = p.phys + (((size_t)it * N + x) * NPH) * N;
+  cplx<R> uv[E], bb[E];
 #pragma unroll
-  for (int pr = 0; pr < 4; ++pr) {
-    cplx<R> z[E];
+  for (int j = 0; j < E; ++j) {
+    uv[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), lane + 32 * j, w);
+    bb[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), lane + 32 * j, w);
+  }
+  fft_dif2<R, N, true>(uv, bb, s_tw, lane);
 #pragma unroll
-    for (int j = 0; j < E; ++j)
-      z[j] = packed_pair<R, N, XT>(s_G + (2 * pr) * K * (XT + 1), s_G + (2 * pr + 1) * K * (XT + 1), lane + 32 * j, w);
-    fft_dif<R, N, true>(z, s_tw, lane);
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int e = lane + 32 * j;
-      R a = z[j].x, bb = z[j].y;
-      if (pr == 3) { a += p.b0x; bb += p.b0y; }   // fu1, fv1 carry the mean field (mhd_jax.py:145-149)
-      ph[(2 * pr) * N + e] = a;
-      ph[(2 * pr + 1) * N + e] = bb;
-    }
+  for (int j = 0; j < E; ++j) {
+    const int e = lane + 32 * j;
+    ph[e] = uv[j].x; ph[N + e] = uv[j].y;
+    ph[2 * N + e] = bb[j].x + p.b0x; ph[3 * N + e] = bb[j].y + p.b0y;   // B carries the mean field (mhd_jax.py:145-149)
   }
 }
 
@@ -99,9 +98,9 @@ __global__ void __launch_bounds__(XT * 32) k_row_phys(RowPhysParams<R> p) {
 // ---------------------------------------------------------------------------
 template <typename R>
 struct RowTanParams {
-  const cplx<R>* G;     // tangent [B][8][K][N]
-  cplx<R>* H;           // tangent [B][2][K][N]
-  const R* phys;        // primal physical fields of this stage: [N][8][N]
+  const cplx<R>* G;     // tangent [B][NG][K][N]
+  cplx<R>* H;           // tangent [B][NH][K][N]
+  const R* phys;        // primal physical fields of this stage: [N][NPH][N]
   const cplx<R>* tw;
   int B;
 };
@@ -112,63 +111,45 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + N / 2;
-  cplx<R>* s_H = s_G + 8 * K * (XT + 1);
+  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_H = s_G + NG * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
-  load_twiddles<R, N>(s_tw, p.tw);
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * 8 * K * N, 8 * K, x0);
-  __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
-  const R* ph = p.phys + ((size_t)x * 8) * N;
-  // tangent physical fields, pair by pair; the primal values each pair needs
-  // are loaded before its transform so that the loads overlap the shuffles
-  cplx<R> W[E];
+  // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
+  // the tile load and the inverse transforms
+  const R* ph = phys_row<R, N>(p.phys, x);
+  R pu[E], pv[E], pbx[E], pby[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) W[j] = mk<R>(0, 0);
-  // pair pr uses primal fields (f0, f1, f2, f3):
-  //   pr 0 (dfx0, dfy0): fu0 fv0        pr 1 (dfu0, dfv0): fx0 fy0 fv1 fu1
-  //   pr 2 (dfx1, dfy1): fu1 fv1        pr 3 (dfu1, dfv1): fx1 fy1 fu0 fv0
-#pragma unroll
-  for (int pr = 0; pr < 4; ++pr) {
-    const int f0 = pr == 0 ? 2 : pr == 1 ? 0 : pr == 2 ? 6 : 4;
-    const int f1 = f0 + 1;
-    const int f2 = pr == 1 ? 7 : 2, f3 = pr == 1 ? 6 : 3;
-    R a0[E], a1[E], a2[E], a3[E];
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int e = lane + 32 * j;
-      a0[j] = ph[f0 * N + e]; a1[j] = ph[f1 * N + e];
-      if (pr == 1 || pr == 3) { a2[j] = ph[f2 * N + e]; a3[j] = ph[f3 * N + e]; }
-    }
-    cplx<R> z[E];
-#pragma unroll
-    for (int j = 0; j < E; ++j)
-      z[j] = packed_pair<R, N, XT>(s_G + (2 * pr) * K * (XT + 1), s_G + (2 * pr + 1) * K * (XT + 1), lane + 32 * j, w);
-    fft_dif<R, N, true>(z, s_tw, lane);
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const R da = z[j].x, db = z[j].y;
-      // dP1 = -d(adv0) + d(adv1),  adv_c = fu_c fx_c + fv_c fy_c   (mhd_jax.py:152,159)
-      // dP2 = d(fu0 fv1 - fv0 fu1)                                   (mhd_jax.py:163)
-      if (pr == 0) {
-        W[j].x -= a0[j] * da + a1[j] * db;
-      } else if (pr == 1) {
-        W[j].x -= da * a0[j] + db * a1[j];
-        W[j].y += da * a2[j] - db * a3[j];
-      } else if (pr == 2) {
-        W[j].x += a0[j] * da + a1[j] * db;
-      } else {
-        W[j].x += da * a0[j] + db * a1[j];
-        W[j].y += a2[j] * db - a3[j] * da;
-      }
-    }
+  for (int j = 0; j < E; ++j) {
+    const int e = lane + 32 * j;
+    pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
   }
-  fft_dit<R, N, false>(W, s_tw, lane);
-  split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
+  load_twiddles<R, N>(s_tw, p.tw);
+  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
-  store_tile<R, N, XT>(p.H + (size_t)b * 2 * K * N, s_H, 2 * K, x0);
+  cplx<R> duv[E], dbb[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int q = lane + 32 * j;
+    duv[j] = packed_pair<R, N, XT>(s_G + 0 * K * (XT + 1), s_G + 1 * K * (XT + 1), q, w);
+    dbb[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), q, w);
+  }
+  fft_dif2<R, N, true>(duv, dbb, s_tw, lane);
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const R du = duv[j].x, dv = duv[j].y, dbx = dbb[j].x, dby = dbb[j].y;
+    const R u = pu[j], v = pv[j], bx = pbx[j], by = pby[j];
+    duv[j] = mk<R>(R(2) * ((u * du - v * dv) - (bx * dbx - by * dby)),     // dP1
+                   (bx * dby + by * dbx) - (u * dv + v * du));              // dP2
+    dbb[j] = mk<R>((u * dby + by * du) - (v * dbx + bx * dv), R(0));        // dP3
+  }
+  fft_dit2<R, N, false>(duv, dbb, s_tw, lane);
+  split_store<R, N, XT>(duv, s_H, s_H + K * (XT + 1), w, lane);
+  store_one<R, N, XT>(dbb, s_H + 2 * K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }
 
 // ---------------------------------------------------------------------------
@@ -186,8 +167,8 @@ enum TanSlot { D_F = 0, D_A1, D_K2, D_NS4 = 3 };
 
 template <typename R>
 struct ColTanParams {
-  const cplx<R>* H;     // [B][2][K][N]
-  cplx<R>* G;           // [B][8][K][N]
+  const cplx<R>* H;     // [B][NH][K][N]
+  cplx<R>* G;           // [B][NG][K][N]
   cplx<R>* D;           // tangent slots [B][nslot][2][K][M]
   int nslot;
   const cplx<R>* rec;   // primal record of this step/attempt
@@ -204,7 +185,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[N / 2];
+  __shared__ cplx<R> s_tw[tw_smem(N)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -218,7 +199,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   const R h = (R)p.h, t = (R)p.t;
   const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
   cplx<R> r[E];
-  if (has_rhs) col_load_fwd1<R, N>(p.H, 2, b, ch, ky, lane, s_tw, r);
+  if (has_rhs) col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
   const R coeff = ch == 0 ? p.nu : p.eta;
   cplx<R> x[E];
 #pragma unroll
@@ -229,10 +210,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
     cplx<R> dv = mk<R>(0, 0);
-    if (has_rhs) {
-      if (ch == 0) { if (in_mask) dv = r[j]; }           // the tangent has no forcing
-      else dv = cscale(r[j], ksq_masked<R>(kx, ky));
-    }
+    if (has_rhs) dv = r[j];                              // the tangent has no forcing
     const size_t o = ((size_t)ch * K + ky) * M + slot;
     const R L = diss_L<R>(kx, ky, coeff);
     cplx<R> xin = mk<R>(0, 0);
@@ -316,7 +294,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
     x[j] = xin;
   }
   if (!p.produce || STAGE == T43_INIT || STAGE == T43_E) return;
-  col_inverse4<R, N>(x, p.G, b, ch, ky, lane, s_tw);
+  col_inverse_uv<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
 // Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);

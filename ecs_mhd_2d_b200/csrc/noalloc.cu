@@ -9,7 +9,7 @@
 // the same fused state_vel kernels as ecs_state_vel but takes every byte of its
 // scratch from one file-scope device array of fixed size.
 //
-// Limits: FP64, n in {64, 128}, batch <= 4; the array is ~5 MB and stays
+// Limits: FP64, n in {64, 128}, batch <= 4; the array is ~3.8 MB and stays
 // resident on every GPU that loads the library until the process exits.
 // Calls share the array: two calls that overlap on the GPU (different streams,
 // or different host threads on one device) race and corrupt each other.
@@ -45,9 +45,9 @@ constexpr size_t OFF_FIELDS = al(OFF_CTL + NA_MAX_BATCH * sizeof(StepCtl));     
 constexpr size_t OFF_FBOX = al(OFF_FIELDS + 2 * NA_MAX_N * NA_MAX_N * sizeof(double));   // forcing box [2][K][M]
 constexpr size_t OFF_F = al(OFF_FBOX + 2 * NA_K * NA_M * CB);                    // input box [B][2][K][M]
 constexpr size_t OFF_OUT = al(OFF_F + NA_MAX_BATCH * 2 * NA_K * NA_M * CB);      // output box
-constexpr size_t OFF_G = al(OFF_OUT + NA_MAX_BATCH * 2 * NA_K * NA_M * CB);      // [B][8][K][n]
-constexpr size_t OFF_H = al(OFF_G + NA_MAX_BATCH * 8 * NA_K * NA_MAX_N * CB);    // [B][2][K][n]
-constexpr size_t NA_BYTES = al(OFF_H + NA_MAX_BATCH * 2 * NA_K * NA_MAX_N * CB);
+constexpr size_t OFF_G = al(OFF_OUT + NA_MAX_BATCH * 2 * NA_K * NA_M * CB);      // [B][NG][K][n]
+constexpr size_t OFF_H = al(OFF_G + NA_MAX_BATCH * NG * NA_K * NA_MAX_N * CB);   // [B][NH][K][n]
+constexpr size_t NA_BYTES = al(OFF_H + NA_MAX_BATCH * NH * NA_K * NA_MAX_N * CB);
 
 std::mutex g_mutex;
 unsigned char* g_base[128] = {};   // device address of the scratch array, per device ordinal
@@ -71,8 +71,8 @@ int na_setup_twiddles(unsigned char* base, size_t off) {
                                                                                                 : ECS_ERR_CUDA;
 }
 
-template <int N> size_t na_smem_rhs() { return (N / 2 + 10 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
-template <int N> size_t na_smem_2f() { return (N / 2 + 2 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
+template <int N> size_t na_smem_rhs() { return (tw_smem(N) + (NG + NH) * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
+template <int N> size_t na_smem_2f() { return (tw_smem(N) + 2 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
 
 // One-time set-up on the current device (synchronous).
 int na_setup(unsigned char** out) {
@@ -131,7 +131,7 @@ int na_state_vel(unsigned char* base, double nu, double eta, double b0x, double 
   const int cols = B * K * 2;   // one warp per (batch, ky, channel)
   k_col_rk4<double, N, COL_START><<<(cols + 3) / 4, 128, 0, s>>>(cp);
   RowParams<double> rp;
-  rp.G = G; rp.H = H; rp.phys = nullptr; rp.phys_bstride = 0; rp.rec_index = 0; rp.phys_stage = 0; rp.ctl = nullptr;
+  rp.G = G; rp.H = H; rp.ctl = nullptr;
   rp.tw = tw; rp.b0x = b0x; rp.b0y = b0y; rp.B = B;
   k_row_rhs<double, N, NA_XT><<<B * (N / NA_XT), NA_XT * 32, na_smem_rhs<N>(), s>>>(rp);
   cp.stage = COL_PLAIN; cp.produce = 0; cp.diss = diss;

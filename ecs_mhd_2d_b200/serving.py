@@ -82,7 +82,8 @@ def context_bytes(n, dtype, batch):
     rb = 8 if dtype == torch.float64 else 4
     cb = 2 * rb
     box = batch * 2 * K * M
-    return (5 * box * cb + box * rb + 2 * batch * 8 * K * n * cb + 3 * batch * 2 * n * n * rb
+    # F, A1, K2, OUT, V; Etab; G [B][4][K][n] and H [B][4][K][n]; three real field buffers; RK4(3) slots
+    return (5 * box * cb + box * rb + 2 * batch * 4 * K * n * cb + 3 * batch * 2 * n * n * rb
             + 10 * box * cb + (64 << 20))
 
 

@@ -177,7 +177,7 @@ int ecs_pool_retire(ecs_ctx* ctx, int slot, void* out_fields, double* loss, void
  * caller that forbids allocation after start-up.  Same computation and layout
  * as ecs_state_vel (FP64 complex f_hat / dfdt_hat [batch][2][n][n/2+1]); the
  * physics is passed directly, with `forcing` a DEVICE real [n][n] array on the
- * grid of construct_domain.  All scratch comes from one fixed ~5 MB device
+ * grid of construct_domain.  All scratch comes from one fixed ~3.8 MB device
  * array in the library, held on every GPU that loads it until exit.
  * Limits: n in {64, 128}, batch <= 4, else ECS_ERR_TOO_LARGE.  Calls share the
  * array, so calls that overlap on the GPU race; each call re-initialises what
