@@ -6,7 +6,9 @@ Lawson_RK43 mode at a seeded base point (n=128, Re=Rm=50, Kolmogorov forcing
 batch of 64 seeded unit-norm tangents [T, fields, sx] through the hand-written
 tangent kernels: 64 JVP matvecs (jax_scripts/newton.py:165; jax.jvp at
 jax_scripts/lib/utils.py:108).  The primal adaptive solve with its trajectory
-record is inside every timed step.
+record is inside every timed step; it runs through ecs_linearize_jvp, which
+overlaps the batch-1 primal with the tangent sweep as jax.jvp computes both.
+`config.phase_ms` reports the two halves run separately.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -316,9 +318,8 @@ def main():
            "T": torch.as_tensor(tvh[:, 0]), "sx": torch.as_tensor(tvh[:, -1])}
     obj = E.Objective(pd, "Lawson_RK43")
 
-    def step():
-        obj.linearize(prim, force=True, batch=BATCH)
-        return obj.jvp(prim, tan)
+    def step():   # primal solve with record overlapped with the 64-tangent sweep (jax.jvp semantics)
+        return obj.linearize_jvp(prim, tan)[1]
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(args.warmup):
@@ -372,8 +373,7 @@ def main():
         p = {"fields": u0_pin.to(dev, non_blocking=True), "T": T0, "sx": SX0}
         tg = {"fields": tf_pin.to(dev, non_blocking=True), "T": tT_pin.to(dev, non_blocking=True),
               "sx": tsx_pin.to(dev, non_blocking=True)}
-        obj.linearize(p, force=True, batch=BATCH)
-        o = obj.jvp(p, tg)
+        o = obj.linearize_jvp(p, tg)[1]
         out_pin.copy_(o["fields"], non_blocking=True)
         oT_pin.copy_(o["T"], non_blocking=True)
         e1.record()

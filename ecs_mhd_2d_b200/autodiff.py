@@ -68,6 +68,40 @@ class Objective:
                           "rejected": info.rejected, "fevals": info.fevals}
         return ctx
 
+    def linearize_jvp(self, primal_dict, tangent_dict):
+        """Objective value and tangents in one call (jax.jvp(obj, (x,), (v,)),
+        jax_scripts/lib/utils.py:108): the primal solve is re-run with its
+        record and overlapped with the tangent sweep (ecs_linearize_jvp); the
+        linearisation is kept for later jvp / vjp calls.  Returns (value, jvp)."""
+        fields, T, sx, _ = prep_inputs(primal_dict)
+        if fields.shape[0] != 1:
+            raise ValueError("linearize_jvp takes one primal point")
+        dfields, dT, dsx, batched = prep_inputs(tangent_dict)
+        B, n = dfields.shape[0], fields.shape[-1]
+        if self._own_ctx is not None:
+            ctx = self._own_ctx
+            ctx.ensure_batch(B)
+        else:
+            ctx = _ctx.get_context(self.param_dict, n, fields.dtype, B)
+        out = torch.empty_like(fields)
+        info = _lib.EcsInfo()
+        dout = torch.empty_like(dfields)
+        oT = torch.empty(B, dtype=torch.float64, device=dfields.device)
+        osx = torch.empty(B, dtype=torch.float64, device=dfields.device)
+        ctx.call("ecs_linearize_jvp", self.cfg, _ctx.ptr(fields), _ctx.ptr(T), _ctx.ptr(sx), _ctx.ptr(out), info,
+                 _ctx.ptr(dfields), _ctx.ptr(dT), _ctx.ptr(dsx), _ctx.ptr(dout), _ctx.ptr(oT), _ctx.ptr(osx), B,
+                 _ctx.stream_ptr())
+        key = (id(ctx), ctx.handle.value if ctx.handle else None) + self._primal_key(
+            primal_dict["fields"] if isinstance(primal_dict["fields"], torch.Tensor) else fields, T[0], sx[0])
+        self._key, self._ctx = key, ctx
+        self._fields_ref = (fields, T, sx)
+        zero = torch.zeros((), dtype=torch.float64, device=out.device)
+        self.last_value = {"fields": out[0], "T": zero, "sx": zero.clone()}
+        self.last_info = {"completed": bool(info.completed), "s": info.s, "accepted": info.accepted,
+                          "rejected": info.rejected, "fevals": info.fevals}
+        tan = {"fields": dout, "T": oT, "sx": osx} if batched else {"fields": dout[0], "T": oT[0], "sx": osx[0]}
+        return self.last_value, tan
+
     def jvp(self, primal_dict, tangent_dict):
         """Tangent of objective_RPO at primal_dict; tangent_dict may carry a leading batch dim."""
         dfields, dT, dsx, batched = prep_inputs(tangent_dict)

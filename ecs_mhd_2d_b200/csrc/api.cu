@@ -6,6 +6,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -83,6 +84,7 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   ecs_ctx* c = new ecs_ctx();
   c->n = n; c->dtype = dtype; c->max_batch = max_batch; c->g = make_geom(n);
   c->nu = params->nu; c->eta = params->eta; c->b0x = params->b0x; c->b0y = params->b0y;
+  if (const char* v = getenv("ECS_PDL")) c->pdl = atoi(v) != 0 ? 1 : 0;
   int st;
   const ecs::ImplTable* t = ecs::impl_table(dtype, n);
   st = t ? t->init(c, params) : ECS_ERR_UNSUPPORTED;
@@ -104,6 +106,14 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->g4.exec) cudaGraphExecDestroy(ctx->g4.exec);
   if (ctx->gpool.exec) cudaGraphExecDestroy(ctx->gpool.exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->pstream) cudaStreamDestroy(ctx->pstream);
+  for (cudaEvent_t e : ctx->pev) if (e) cudaEventDestroy(e);
+  if (ctx->Gp) cudaFree(ctx->Gp);
+  if (ctx->Hp) cudaFree(ctx->Hp);
+  if (ctx->hctl) cudaFreeHost(ctx->hctl);
+  if (ctx->hchunk_acc) cudaFreeHost(ctx->hchunk_acc);
+  if (ctx->hchunk_h) cudaFreeHost(ctx->hchunk_h);
+  if (ctx->hitems) cudaFreeHost(ctx->hitems);
   if (ctx->lin.rec) cudaFree(ctx->lin.rec);
   if (ctx->lin.ckpt) cudaFree(ctx->lin.ckpt);
   if (ctx->lin.rec_h) cudaFree(ctx->lin.rec_h);
@@ -180,6 +190,16 @@ int ecs_jvp(ecs_ctx* ctx, const void* dfields, const double* dT, const double* d
   if (!dfields || !dT || !dsx || !out_dfields || !out_dT || !out_dsx) return set_err(ctx, ECS_ERR_INVALID, "null pointer");
   return table_of(ctx)->jvp(ctx, dfields, dT, dsx, out_dfields, out_dT, out_dsx, batch,
                                      as_stream(stream));
+}
+
+int ecs_linearize_jvp(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T, const double* sx,
+                      void* out_fields, ecs_info* info, const void* dfields, const double* dT, const double* dsx,
+                      void* out_dfields, double* out_dT, double* out_dsx, int batch, void* stream) {
+  ECS_CHECK_CTX(ctx, batch);
+  if (!cfg || !fields || !T || !sx || !dfields || !dT || !dsx || !out_dfields || !out_dT || !out_dsx)
+    return set_err(ctx, ECS_ERR_INVALID, "null pointer");
+  return table_of(ctx)->linearize_jvp(ctx, cfg, fields, T, sx, out_fields, info, dfields, dT, dsx, out_dfields, out_dT,
+                                      out_dsx, batch, as_stream(stream));
 }
 
 int ecs_vjp(ecs_ctx* ctx, const void* c_fields, const double* c_T, const double* c_sx, void* g_fields, double* g_T,

@@ -34,6 +34,7 @@ struct ecs_ctx {
   double* Tbuf = nullptr;
   std::vector<void*> allocs;
   long long launches = 0;           // kernels launched through this context
+  int pdl = 1;                      // stepping kernels use programmatic dependent launch (ECS_PDL=0 disables)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;
@@ -65,8 +66,20 @@ struct ecs_ctx {
     int B = 0, cap = 0;
     double atol = 0;
     void* rec = nullptr; double* rec_h = nullptr; int* rec_acc = nullptr;
+    void* G = nullptr; void* H = nullptr;   // scratch the captured kernels use
     long long nodes = 0;
   } g43;
+  // pipelined linearisation + JVP (ecs_linearize_jvp): the batch-1 primal runs on
+  // a high-priority stream with its own scratch while the tangents run on the
+  // caller's stream; per chunk of attempts the primal's control block and
+  // accept flags come back through double-buffered pinned memory
+  cudaStream_t pstream = nullptr;
+  cudaEvent_t pev[2] = {nullptr, nullptr};
+  void* Gp = nullptr; void* Hp = nullptr;   // [NG][K][N], [NHA][K][N] primal scratch (batch 1)
+  ecs::StepCtl* hctl = nullptr;             // pinned [2]
+  int* hchunk_acc = nullptr;                // pinned [2][16]
+  double* hchunk_h = nullptr;               // pinned [2][16]
+  long* hitems = nullptr; size_t hitems_cap = 0;   // pinned staging of regeneration items
   // slot pool (continuous batching of forward shootings)
   struct PoolSlot { int active = 0, ny = 0, rot = 0; long steps = 0; };
   std::vector<PoolSlot> pool;

@@ -51,6 +51,18 @@ template <typename R> __device__ __forceinline__ cplx<R> shfl_c(cplx<R> v, int s
   return v;
 }
 
+// Programmatic dependent launch.  A stepping kernel is launched with
+// programmatic stream serialization, so it may start while its predecessor in
+// the stream is still running.  It calls pdl_trigger() first (its successor may
+// be scheduled once every CTA of this grid has started) and pdl_wait() before
+// its first access to global memory other than the constant twiddle table:
+// the wait returns when the predecessor grid has completed and its writes are
+// visible.  Every such kernel waits before any early return, so completion of
+// a grid implies completion of all grids before it.  Both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Box geometry for a grid side n.
 struct Geom {
   int n, kmax, K, M;

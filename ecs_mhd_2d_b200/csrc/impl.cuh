@@ -34,6 +34,24 @@ template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; 
 template <typename R, int N> size_t smem_row_phys() { return (tw_smem(N) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N, int X = XT> size_t smem_row_2f() { return (tw_smem(N) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
+// Launch a stepping kernel of batch B; with c->pdl set and B >= 8, with
+// programmatic stream serialization (the kernel waits on its predecessor
+// itself, see pdl_wait).  Measured at n=128 FP64: the batch-64 tangent kernels
+// gain 5-7%, while single-state chains lose (their launches are already
+// overlapped inside CUDA graphs), hence the batch threshold.
+template <typename... P, typename... A>
+inline void launch_step(ecs_ctx* c, int B, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                        A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at; cfg.numAttrs = (c->pdl && B >= 8) ? 1 : 0;
+  ++c->launches;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <typename R, int N>
 int configure_kernels(ecs_ctx* c) {
   int st = ECS_OK;
@@ -95,14 +113,13 @@ void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStr
   p.use_done = use_done;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
-  ++c->launches;
   switch (stage) {
-    case COL_START: k_col_rk4<R, N, COL_START><<<g, bl, 0, s>>>(p); break;
-    case COL_RK4_S1: k_col_rk4<R, N, COL_RK4_S1><<<g, bl, 0, s>>>(p); break;
-    case COL_RK4_S2: k_col_rk4<R, N, COL_RK4_S2><<<g, bl, 0, s>>>(p); break;
-    case COL_RK4_S3: k_col_rk4<R, N, COL_RK4_S3><<<g, bl, 0, s>>>(p); break;
-    case COL_RK4_S4: k_col_rk4<R, N, COL_RK4_S4><<<g, bl, 0, s>>>(p); break;
-    default: k_col_rk4<R, N, COL_PLAIN><<<g, bl, 0, s>>>(p); break;
+    case COL_START: launch_step(c, B, k_col_rk4<R, N, COL_START>, g, bl, 0, s, p); break;
+    case COL_RK4_S1: launch_step(c, B, k_col_rk4<R, N, COL_RK4_S1>, g, bl, 0, s, p); break;
+    case COL_RK4_S2: launch_step(c, B, k_col_rk4<R, N, COL_RK4_S2>, g, bl, 0, s, p); break;
+    case COL_RK4_S3: launch_step(c, B, k_col_rk4<R, N, COL_RK4_S3>, g, bl, 0, s, p); break;
+    case COL_RK4_S4: launch_step(c, B, k_col_rk4<R, N, COL_RK4_S4>, g, bl, 0, s, p); break;
+    default: launch_step(c, B, k_col_rk4<R, N, COL_PLAIN>, g, bl, 0, s, p); break;
   }
 }
 
@@ -110,9 +127,8 @@ template <typename R, int N>
 void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = nullptr) {
   RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.tw = (const cplx<R>*)c->tw; p.ctl = ctl;
   p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
-  ++c->launches;
-  if (small_rows<N>(B)) k_row_rhs<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
-  else k_row_rhs<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  if (small_rows<N>(B)) launch_step(c, B, k_row_rhs<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
+  else launch_step(c, B, k_row_rhs<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
 }
 
 template <typename R, int N>
@@ -123,15 +139,14 @@ void launch_col_rk43(ecs_ctx* c, int B, int stage, cudaStream_t s, cplx<R>* rec 
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
-  ++c->launches;
   switch (stage) {
-    case R43_START: k_col_rk43<R, N, R43_START><<<g, bl, 0, s>>>(p); break;
-    case R43_INIT: k_col_rk43<R, N, R43_INIT><<<g, bl, 0, s>>>(p); break;
-    case R43_A: k_col_rk43<R, N, R43_A><<<g, bl, 0, s>>>(p); break;
-    case R43_B: k_col_rk43<R, N, R43_B><<<g, bl, 0, s>>>(p); break;
-    case R43_C: k_col_rk43<R, N, R43_C><<<g, bl, 0, s>>>(p); break;
-    case R43_D: k_col_rk43<R, N, R43_D><<<g, bl, 0, s>>>(p); break;
-    default: k_col_rk43<R, N, R43_E><<<g, bl, 0, s>>>(p); break;
+    case R43_START: launch_step(c, B, k_col_rk43<R, N, R43_START>, g, bl, 0, s, p); break;
+    case R43_INIT: launch_step(c, B, k_col_rk43<R, N, R43_INIT>, g, bl, 0, s, p); break;
+    case R43_A: launch_step(c, B, k_col_rk43<R, N, R43_A>, g, bl, 0, s, p); break;
+    case R43_B: launch_step(c, B, k_col_rk43<R, N, R43_B>, g, bl, 0, s, p); break;
+    case R43_C: launch_step(c, B, k_col_rk43<R, N, R43_C>, g, bl, 0, s, p); break;
+    case R43_D: launch_step(c, B, k_col_rk43<R, N, R43_D>, g, bl, 0, s, p); break;
+    default: launch_step(c, B, k_col_rk43<R, N, R43_E>, g, bl, 0, s, p); break;
   }
 }
 
@@ -140,9 +155,8 @@ void launch_row_err(ecs_ctx* c, int B, double atol, cudaStream_t s, double* rec_
                     int cap = 0) {
   RowErrParams<R> p; p.G = (const cplx<R>*)c->G; p.ctl = c->ctl; p.tw = (const cplx<R>*)c->tw; p.atol = atol;
   p.rec_h = rec_h; p.rec_acc = rec_acc; p.cap = cap; p.B = B;
-  ++c->launches;
-  if (small_rows<N>(B)) k_row_err<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_2f<R, N, XTS>(), s>>>(p);
-  else k_row_err<R, N, XT><<<B * (N / XT), XT * 32, smem_row_2f<R, N>(), s>>>(p);
+  if (small_rows<N>(B)) launch_step(c, B, k_row_err<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_2f<R, N, XTS>(), s, p);
+  else launch_step(c, B, k_row_err<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_2f<R, N>(), s, p);
 }
 
 template <typename R, int N>
@@ -160,9 +174,8 @@ template <typename R, int N>
 void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
   RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B;
-  ++c->launches;
-  if (small_rows<N>(B)) k_row_tan<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
-  else k_row_tan<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
+  else launch_step(c, B, k_row_tan<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
 }
 
 template <typename R, int N>
@@ -173,20 +186,19 @@ void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* re
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage; p.produce = produce;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
-  ++c->launches;
   switch (stage) {
-    case TS_START: k_col_tan<R, N, TS_START><<<g, bl, 0, s>>>(p); break;
-    case T4_S1: k_col_tan<R, N, T4_S1><<<g, bl, 0, s>>>(p); break;
-    case T4_S2: k_col_tan<R, N, T4_S2><<<g, bl, 0, s>>>(p); break;
-    case T4_S3: k_col_tan<R, N, T4_S3><<<g, bl, 0, s>>>(p); break;
-    case T4_S4: k_col_tan<R, N, T4_S4><<<g, bl, 0, s>>>(p); break;
-    case T43_START: k_col_tan<R, N, T43_START><<<g, bl, 0, s>>>(p); break;
-    case T43_INIT: k_col_tan<R, N, T43_INIT><<<g, bl, 0, s>>>(p); break;
-    case T43_A: k_col_tan<R, N, T43_A><<<g, bl, 0, s>>>(p); break;
-    case T43_B: k_col_tan<R, N, T43_B><<<g, bl, 0, s>>>(p); break;
-    case T43_C: k_col_tan<R, N, T43_C><<<g, bl, 0, s>>>(p); break;
-    case T43_D: k_col_tan<R, N, T43_D><<<g, bl, 0, s>>>(p); break;
-    default: k_col_tan<R, N, T43_E><<<g, bl, 0, s>>>(p); break;
+    case TS_START: launch_step(c, B, k_col_tan<R, N, TS_START>, g, bl, 0, s, p); break;
+    case T4_S1: launch_step(c, B, k_col_tan<R, N, T4_S1>, g, bl, 0, s, p); break;
+    case T4_S2: launch_step(c, B, k_col_tan<R, N, T4_S2>, g, bl, 0, s, p); break;
+    case T4_S3: launch_step(c, B, k_col_tan<R, N, T4_S3>, g, bl, 0, s, p); break;
+    case T4_S4: launch_step(c, B, k_col_tan<R, N, T4_S4>, g, bl, 0, s, p); break;
+    case T43_START: launch_step(c, B, k_col_tan<R, N, T43_START>, g, bl, 0, s, p); break;
+    case T43_INIT: launch_step(c, B, k_col_tan<R, N, T43_INIT>, g, bl, 0, s, p); break;
+    case T43_A: launch_step(c, B, k_col_tan<R, N, T43_A>, g, bl, 0, s, p); break;
+    case T43_B: launch_step(c, B, k_col_tan<R, N, T43_B>, g, bl, 0, s, p); break;
+    case T43_C: launch_step(c, B, k_col_tan<R, N, T43_C>, g, bl, 0, s, p); break;
+    case T43_D: launch_step(c, B, k_col_tan<R, N, T43_D>, g, bl, 0, s, p); break;
+    default: launch_step(c, B, k_col_tan<R, N, T43_E>, g, bl, 0, s, p); break;
   }
 }
 
@@ -194,9 +206,8 @@ template <typename R, int N>
 void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
   RowAdjParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B;
-  ++c->launches;
-  if (small_rows<N>(B)) k_row_adj<R, N, XTS><<<B * (N / XTS), XTS * 32, smem_row_rhs<R, N, XTS>(), s>>>(p);
-  else k_row_adj<R, N, XT><<<B * (N / XT), XT * 32, smem_row_rhs<R, N>(), s>>>(p);
+  if (small_rows<N>(B)) launch_step(c, B, k_row_adj<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
+  else launch_step(c, B, k_row_adj<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
 }
 
 template <typename R, int N>
@@ -207,20 +218,19 @@ void launch_col_adj(ecs_ctx* c, int B, int stage, const cplx<R>* rec, const cplx
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
   const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
-  ++c->launches;
   switch (stage) {
-    case AJ_PRE: k_col_adj<R, N, AJ_PRE><<<g, bl, 0, s>>>(p); break;
-    case AJ_S4: k_col_adj<R, N, AJ_S4><<<g, bl, 0, s>>>(p); break;
-    case AJ_S3: k_col_adj<R, N, AJ_S3><<<g, bl, 0, s>>>(p); break;
-    case AJ_S2: k_col_adj<R, N, AJ_S2><<<g, bl, 0, s>>>(p); break;
-    case AJ_S1: k_col_adj<R, N, AJ_S1><<<g, bl, 0, s>>>(p); break;
-    case AJ43_INIT: k_col_adj<R, N, AJ43_INIT><<<g, bl, 0, s>>>(p); break;
-    case AJ43_PRE: k_col_adj<R, N, AJ43_PRE><<<g, bl, 0, s>>>(p); break;
-    case AJ43_S5: k_col_adj<R, N, AJ43_S5><<<g, bl, 0, s>>>(p); break;
-    case AJ43_S4: k_col_adj<R, N, AJ43_S4><<<g, bl, 0, s>>>(p); break;
-    case AJ43_S3: k_col_adj<R, N, AJ43_S3><<<g, bl, 0, s>>>(p); break;
-    case AJ43_S2: k_col_adj<R, N, AJ43_S2><<<g, bl, 0, s>>>(p); break;
-    default: k_col_adj<R, N, AJ43_IPRE><<<g, bl, 0, s>>>(p); break;
+    case AJ_PRE: launch_step(c, B, k_col_adj<R, N, AJ_PRE>, g, bl, 0, s, p); break;
+    case AJ_S4: launch_step(c, B, k_col_adj<R, N, AJ_S4>, g, bl, 0, s, p); break;
+    case AJ_S3: launch_step(c, B, k_col_adj<R, N, AJ_S3>, g, bl, 0, s, p); break;
+    case AJ_S2: launch_step(c, B, k_col_adj<R, N, AJ_S2>, g, bl, 0, s, p); break;
+    case AJ_S1: launch_step(c, B, k_col_adj<R, N, AJ_S1>, g, bl, 0, s, p); break;
+    case AJ43_INIT: launch_step(c, B, k_col_adj<R, N, AJ43_INIT>, g, bl, 0, s, p); break;
+    case AJ43_PRE: launch_step(c, B, k_col_adj<R, N, AJ43_PRE>, g, bl, 0, s, p); break;
+    case AJ43_S5: launch_step(c, B, k_col_adj<R, N, AJ43_S5>, g, bl, 0, s, p); break;
+    case AJ43_S4: launch_step(c, B, k_col_adj<R, N, AJ43_S4>, g, bl, 0, s, p); break;
+    case AJ43_S3: launch_step(c, B, k_col_adj<R, N, AJ43_S3>, g, bl, 0, s, p); break;
+    case AJ43_S2: launch_step(c, B, k_col_adj<R, N, AJ43_S2>, g, bl, 0, s, p); break;
+    default: launch_step(c, B, k_col_adj<R, N, AJ43_IPRE>, g, bl, 0, s, p); break;
   }
 }
 
@@ -339,7 +349,8 @@ struct Impl {
   // Adaptive Lawson-RK4(3) of the box states in S43[b][S_X0] (timestepping.py:151-335).
   // Returns after all candidates completed or the attempt cap was reached.
   static int rk43_solve(ecs_ctx* c, const ecs_shoot_cfg* cfg, const double* T, int B, cudaStream_t s,
-                        cplx<R>* rec = nullptr, double* rec_h = nullptr, int* rec_acc = nullptr, int cap = 0) {
+                        cplx<R>* rec = nullptr, double* rec_h = nullptr, int* rec_acc = nullptr, int cap = 0,
+                        bool launch = true) {
     const long amax = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
     if (amax <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
     ++c->launches; k_rk43_setup<<<(B + 127) / 128, 128, 0, s>>>(T, cfg->h0, c->ctl, B);
@@ -360,7 +371,7 @@ struct Impl {
     constexpr int GA = 16;
     auto& gk = c->g43;
     const bool same = gk.exec && gk.B == B && gk.atol == cfg->atol && gk.rec == (void*)rec && gk.rec_h == rec_h &&
-                      gk.rec_acc == rec_acc && gk.cap == cap;
+                      gk.rec_acc == rec_acc && gk.cap == cap && gk.G == c->G && gk.H == c->H;
     if (!same && amax >= GA) {
       if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
       const long long l0 = c->launches;
@@ -376,7 +387,9 @@ struct Impl {
       gk.nodes = c->launches - l0;
       c->launches = l0;
       gk.B = B; gk.atol = cfg->atol; gk.rec = rec; gk.rec_h = rec_h; gk.rec_acc = rec_acc; gk.cap = cap;
+      gk.G = c->G; gk.H = c->H;
     }
+    if (!launch) return ECS_OK;   // set-up and graph only (the pipelined linearisation drives the chunks)
     long a = 0;
     while (a < amax) {
       if (gk.exec && amax - a >= GA) {
@@ -491,13 +504,13 @@ struct Impl {
   // Linearisation: primal solve of one candidate with its trajectory record,
   // plus the stop-gradient phase fields vt, vx (loss_functions.py:113-130).
   // ---------------------------------------------------------------------
-  static int linearize(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
-                       R* out_fields, ecs_info* info, cudaStream_t s) {
+  // Linearisation prologue: scalars, box(f0), the phase fields vt and vx.
+  static int lin_prologue(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                          cudaStream_t s) {
     auto& L = c->lin;
     L.valid = 0;
-    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
-    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43) return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>), fb = 2UL * N * N * sizeof(R);
+    (void)VEC;
     int st = ECS_OK;
     size_t dummy = 0;
     if (!L.phi) {
@@ -526,6 +539,36 @@ struct Impl {
     if (st) return st;
     launch_col_from_box<R, N>(c, (const cplx<R>*)L.f0box, (cplx<R>*)c->G, 1, nullptr, 0, 0, 0, 1, s);
     launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)L.vx, nullptr, nullptr, 1, 0, s);
+    return cuda_err(c, cudaGetLastError(), "linearize prologue");
+  }
+
+  // Lawson-RK4(3) record buffers for `cap` attempts and the start state.
+  static int lin43_alloc(ecs_ctx* c, const ecs_shoot_cfg* cfg, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const long cap = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
+    if (cap <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
+    int st = grow(c, &L.rec, &L.rec_bytes, (size_t)cap * RR_NREC * vb);
+    if (st) return st;
+    if ((size_t)cap > L.cap) {
+      if (L.rec_h) { cudaFree(L.rec_h); cudaFree(L.rec_acc); }
+      if (cudaMalloc(&L.rec_h, cap * sizeof(double)) != cudaSuccess || cudaMalloc(&L.rec_acc, cap * sizeof(int)) != cudaSuccess)
+        return set_err(c, ECS_ERR_OOM, "record allocation");
+      L.cap = cap;
+    }
+    cudaMemcpyAsync((cplx<R>*)c->S43 + S_X0 * VEC, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+    return cuda_err(c, cudaGetLastError(), "record allocation");
+  }
+
+  static int linearize(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                       R* out_fields, ecs_info* info, cudaStream_t s) {
+    auto& L = c->lin;
+    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
+    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43) return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    int st = lin_prologue(c, cfg, fields, T, sx, s);
+    if (st) return st;
+    cudaError_t e = cudaSuccess;
     if (!rk43) {
       const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
       if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
@@ -549,21 +592,13 @@ struct Impl {
       }
       L.seg = kseg;
       L.nrec = steps;
-      L.h = (double)(R)((hT / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
+      L.h = (double)(R)((L.T / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
       cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
       if (info) { info->completed = 1; info->s = 1.0; info->accepted = (int)steps; info->rejected = 0; info->fevals = (int)(4 * steps); }
     } else {
       const long cap = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
-      if (cap <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
-      st = grow(c, &L.rec, &L.rec_bytes, (size_t)cap * RR_NREC * vb);
+      st = lin43_alloc(c, cfg, s);
       if (st) return st;
-      if ((size_t)cap > L.cap) {
-        if (L.rec_h) { cudaFree(L.rec_h); cudaFree(L.rec_acc); }
-        if (cudaMalloc(&L.rec_h, cap * sizeof(double)) != cudaSuccess || cudaMalloc(&L.rec_acc, cap * sizeof(int)) != cudaSuccess)
-          return set_err(c, ECS_ERR_OOM, "record allocation");
-        L.cap = cap;
-      }
-      cudaMemcpyAsync((cplx<R>*)c->S43 + S_X0 * VEC, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
       st = rk43_solve(c, cfg, T, 1, s, (cplx<R>*)L.rec, L.rec_h, L.rec_acc, (int)cap);
       if (st) return st;
       cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
@@ -734,7 +769,17 @@ struct Impl {
         }
       }
     }
-    // output: d fields = dfields - irfft2(sym(dPhi + i kx dsx Phi)) [- rest term]
+    return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
+  }
+
+  // JVP output from the final tangent state:
+  // d fields = dfields - irfft2(sym(dPhi + i kx dsx Phi)) [- rest term]; phase-condition tangents.
+  static int jvp_finish(ecs_ctx* c, const R* dfields, const double* dsx, R* out, double* odT, double* odsx, int B,
+                        cudaStream_t s) {
+    auto& L = c->lin;
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const size_t VEC = 2UL * K * M;
+    const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
     ++c->launches; k_tan_shift<R><<<grid1d((long)B * VEC), 256, 0, s>>>((const cplx<R>*)c->D + (size_t)(rk43 ? (int)S_X0 : (int)D_F) * VEC,
                                                          (long)nslot * VEC, (const cplx<R>*)L.phi, dsx,
                                                          (cplx<R>*)c->V, N, B);
@@ -742,10 +787,185 @@ struct Impl {
       launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
       launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->OUT, B, 2, s);
     }
-    st = residual(c, &L.cfg, dfields, (const cplx<R>*)c->V, (const cplx<R>*)c->OUT, L.dsx, B, out, s, 1);
+    int st = residual(c, &L.cfg, dfields, (const cplx<R>*)c->V, (const cplx<R>*)c->OUT, L.dsx, B, out, s, 1);
     if (st) return st;
     ++c->launches; k_phase_dot<R><<<B, 256, 0, s>>>((const R*)L.vt, (const R*)L.vx, dfields, odT, odsx, N);
     return cuda_err(c, cudaGetLastError(), "jvp");
+  }
+
+  // Streams, events and buffers of the pipelined linearisation (allocations
+  // synchronise the device, so they all happen before the pipelined phase).
+  static int ensure_pipeline(ecs_ctx* c, long amax) {
+    constexpr int GA = 16;
+    if (!c->pstream) {
+      int lo = 0, hi = 0;
+      cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+      if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->pstream, cudaStreamNonBlocking, hi);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[0], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[1], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaMalloc(&c->Gp, (size_t)NG * K * N * sizeof(cplx<R>));
+      if (e == cudaSuccess) e = cudaMalloc(&c->Hp, (size_t)NHA * K * N * sizeof(cplx<R>));
+      if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->hctl, 2 * sizeof(StepCtl), cudaHostAllocDefault);
+      if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->hchunk_acc, 2 * GA * sizeof(int), cudaHostAllocDefault);
+      if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->hchunk_h, 2 * GA * sizeof(double), cudaHostAllocDefault);
+      if (e != cudaSuccess) return cuda_err(c, e, "pipeline set-up");
+    }
+    const size_t need = (size_t)(4 * amax + 1);
+    if (c->hitems_cap < need) {
+      if (c->hitems) cudaFreeHost(c->hitems);
+      c->hitems = nullptr; c->hitems_cap = 0;
+      if (cudaHostAlloc((void**)&c->hitems, need * sizeof(long), cudaHostAllocDefault) != cudaSuccess)
+        return set_err(c, ECS_ERR_OOM, "item staging");
+      c->hitems_cap = need;
+    }
+    if (c->items_cap < need) {
+      if (c->items) cudaFree(c->items);
+      c->items = nullptr; c->items_cap = 0;
+      if (cudaMalloc(&c->items, need * sizeof(long)) != cudaSuccess) return set_err(c, ECS_ERR_OOM, "items");
+      c->items_cap = need;
+    }
+    return ECS_OK;
+  }
+
+  // ---------------------------------------------------------------------
+  // Linearisation and JVP in one call, pipelined (Lawson-RK4(3)), as jax.jvp
+  // returns (objective, J v) together.  The batch-1 primal solve runs on a
+  // high-priority context stream with its own scratch, in chunks of GA
+  // attempts (the captured attempt graph); after each chunk the host reads back
+  // the control block and accept flags and queues the tangent sweep over those
+  // attempts on the caller's stream behind the chunk's event.  The primal
+  // occupies a few SMs, the tangent batch the rest, so the primal is hidden
+  // behind the tangents.  Every kernel sees the same inputs as in
+  // ecs_linearize followed by ecs_jvp, so the results are the same.  Fixed-step
+  // mode, or an attempt cap that is not a multiple of GA, runs the two in sequence.
+  // ---------------------------------------------------------------------
+  static int linearize_jvp(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                           R* out_fields, ecs_info* info, const R* dfields, const double* dT, const double* dsx,
+                           R* out, double* odT, double* odsx, int B, cudaStream_t s) {
+    constexpr int GA = 16;
+    const long amax = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
+    if (cfg->mode != ECS_MODE_LAWSON_RK43 || amax < GA || amax % GA != 0) {
+      const int st = linearize(c, cfg, fields, T, sx, out_fields, info, s);
+      return st ? st : jvp(c, dfields, dT, dsx, out, odT, odsx, B, s);
+    }
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const int nslot = (int)S_NSLOT;
+    int st = ensure_pipeline(c, amax);
+    if (!st) st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = ensure_regen(c);
+    if (!st) st = lin_prologue(c, cfg, fields, T, sx, s);
+    if (!st) st = lin43_alloc(c, cfg, s);
+    if (st) return st;
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    // tangent initial state: box(dfields) into slot X0
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)S_X0 * VEC, B, 2, s, (long)nslot * VEC);
+    // primal set-up and attempt graph on the primal stream, after everything queued so far
+    cudaStream_t ps = c->pstream;
+    cudaError_t e = cudaEventRecord(c->pev[0], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ps, c->pev[0], 0);
+    if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
+    void* const Gs = c->G; void* const Hs = c->H;
+    c->G = c->Gp; c->H = c->Hp;
+    st = rk43_solve(c, cfg, T, 1, ps, (cplx<R>*)L.rec, L.rec_h, L.rec_acc, (int)amax, false);
+    c->G = Gs; c->H = Hs;
+    if (st) return st;
+    const auto& gk = c->g43;
+    auto launch_chunk = [&](long chunk, int bi) -> cudaError_t {
+      cudaError_t e2 = cudaGraphLaunch(gk.exec, ps);
+      c->launches += gk.nodes;
+      if (e2 == cudaSuccess) e2 = cudaMemcpyAsync(c->hctl + bi, c->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, ps);
+      if (e2 == cudaSuccess)
+        e2 = cudaMemcpyAsync(c->hchunk_acc + bi * GA, L.rec_acc + chunk * GA, GA * sizeof(int), cudaMemcpyDeviceToHost, ps);
+      if (e2 == cudaSuccess)
+        e2 = cudaMemcpyAsync(c->hchunk_h + bi * GA, L.rec_h + chunk * GA, GA * sizeof(double), cudaMemcpyDeviceToHost, ps);
+      if (e2 == cudaSuccess) e2 = cudaEventRecord(c->pev[bi], ps);
+      return e2;
+    };
+    // tangent sweep over attempts [a_lo, a_hi) whose record is complete
+    L.acc.clear(); L.hs.clear();
+    const long ci = (long)chunk_items();
+    long nitems = 0, win_lo = -1, win_cnt = 0;
+    auto phys_of = [&](long item) -> const R* {
+      if (win_lo < 0 || item < win_lo || item >= win_lo + win_cnt) {
+        win_lo = item; win_cnt = std::min(ci, nitems - item);
+        launch_regen<R, N>(c, rec, c->items + item, (int)win_cnt, s);
+      }
+      return (const R*)c->Phys + (size_t)(item - win_lo) * N * NPH * N;
+    };
+    const double t = L.T;
+    std::vector<long> item_of;
+    auto tangent_chunk = [&](long a_lo, long a_hi, const int* acc, const double* hh) -> int {
+      const long i0 = nitems;
+      long* stage = c->hitems + i0;
+      long cnt = 0;
+      if (a_lo == 0) stage[cnt++] = RR_X0;   // x0 of attempt 0 (initial k1)
+      item_of.assign(a_hi - a_lo, -1);
+      for (long a = a_lo; a < a_hi; ++a) {
+        L.acc.push_back(acc[a - a_lo]); L.hs.push_back(hh[a - a_lo]);
+        if (!acc[a - a_lo]) continue;
+        item_of[a - a_lo] = i0 + cnt;
+        const long base = a * RR_NREC;
+        stage[cnt++] = base + RR_Y2; stage[cnt++] = base + RR_Y3; stage[cnt++] = base + RR_Y4; stage[cnt++] = base + RR_XF;
+      }
+      if (cnt > 0) {
+        const cudaError_t e2 = cudaMemcpyAsync(c->items + i0, stage, cnt * sizeof(long), cudaMemcpyHostToDevice, s);
+        if (e2 != cudaSuccess) return cuda_err(c, e2, "item upload");
+      }
+      nitems += cnt;
+      if (a_lo == 0) {
+        launch_col_tan<R, N>(c, B, T43_START, 1, rec, dT, t, 0.0, 1.0, nslot, s);
+        launch_row_tan<R, N>(c, B, phys_of(0), s);
+        launch_col_tan<R, N>(c, B, T43_INIT, 0, rec, dT, t, 0.0, 1.0, nslot, s);
+      }
+      for (long a = a_lo; a < a_hi; ++a) {
+        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
+        const double h = hh[a - a_lo];
+        if (!acc[a - a_lo]) {
+          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, t, h,
+                                                                                (R)c->nu, (R)c->eta, N, B);
+          continue;
+        }
+        launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
+        for (int k = 0; k < 4; ++k) {
+          launch_row_tan<R, N>(c, B, phys_of(item_of[a - a_lo] + k), s);
+          launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
+        }
+      }
+      return cuda_err(c, cudaGetLastError(), "pipelined tangent");
+    };
+    // chunk i+1 of the primal is queued before the tangents of chunk i
+    long launched = 1, a_done = 0;
+    int bi = 0;
+    e = launch_chunk(0, 0);
+    StepCtl hc{};
+    while (true) {
+      if (e == cudaSuccess) e = cudaEventSynchronize(c->pev[bi]);
+      if (e != cudaSuccess) return cuda_err(c, e, "pipelined linearisation");
+      hc = c->hctl[bi];
+      const long a_now = hc.attempts;
+      const bool more = !hc.done && launched * GA < amax;
+      if (more) { e = launch_chunk(launched, bi ^ 1); ++launched; }
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->pev[bi], 0);
+      if (e != cudaSuccess) return cuda_err(c, e, "pipelined linearisation");
+      st = tangent_chunk(a_done, a_now, c->hchunk_acc + bi * GA, c->hchunk_h + bi * GA);
+      if (st) return st;
+      a_done = a_now;
+      if (!more) break;
+      bi ^= 1;
+    }
+    // primal epilogue on the caller's stream (it waited for every chunk)
+    ++c->launches; k_rk43_resolve<R><<<grid1d((long)VEC), 256, 0, s>>>((cplx<R>*)c->S43, c->ctl, (cplx<R>*)c->F, N, 1);
+    cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
+    L.nrec = a_done;
+    if (info) { info->completed = hc.done; info->s = hc.s; info->accepted = hc.accepted; info->rejected = hc.rejected; info->fevals = hc.fevals; }
+    if (out_fields) {
+      st = residual(c, cfg, fields, (const cplx<R>*)L.phi, (const cplx<R>*)L.f0box, L.dsx, 1, out_fields, s, 1);
+      if (st) return st;
+    }
+    L.valid = 1;
+    return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
   }
 
   // ---------------------------------------------------------------------
@@ -1096,6 +1316,10 @@ ImplTable make_table() {
     return I::linearize(c, cfg, (const R*)f, T, sx, (R*)o, info, s); };
   t.jvp = [](ecs_ctx* c, const void* df, const double* dT, const double* dsx, void* o, double* oT, double* osx, int B,
              cudaStream_t s) { return I::jvp(c, (const R*)df, dT, dsx, (R*)o, oT, osx, B, s); };
+  t.linearize_jvp = [](ecs_ctx* c, const ecs_shoot_cfg* cfg, const void* f, const double* T, const double* sx, void* o,
+                       ecs_info* info, const void* df, const double* dT, const double* dsx, void* od, double* oT,
+                       double* osx, int B, cudaStream_t s) {
+    return I::linearize_jvp(c, cfg, (const R*)f, T, sx, (R*)o, info, (const R*)df, dT, dsx, (R*)od, oT, osx, B, s); };
   t.vjp = [](ecs_ctx* c, const void* cf, const double* cT, const double* csx, void* g, double* gT, double* gsx, int B,
              cudaStream_t s) { return I::vjp(c, (const R*)cf, cT, csx, (R*)g, gT, gsx, B, s); };
   t.bench_kernel = [](ecs_ctx* c, int which, int B, int iters, float* ms, double* bytes, cudaStream_t s) {

@@ -48,6 +48,9 @@ __global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   const R* ph = phys_row<R, N>(p.phys, x);
   R pu[E], pv[E], pbx[E], pby[E];
 #pragma unroll
@@ -55,7 +58,6 @@ __global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
     const int e = lane + 32 * j;
     pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
   }
-  load_twiddles<R, N>(s_tw, p.tw);
   load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, 3 * K, x0);
   __syncthreads();
   cplx<R> P12[E], P3[E];   // (P1bar, P2bar) and (P3bar, 0) in position order
@@ -118,7 +120,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
   __shared__ cplx<R> s_tw[tw_smem(N)];
+  pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);

@@ -48,7 +48,9 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
   __shared__ cplx<R> s_tw[tw_smem(N)];
+  pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -178,9 +180,11 @@ __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
   __shared__ int s_last;
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   StepCtl& c = p.ctl[b];
   if (c.done) return;
-  load_twiddles<R, N>(s_tw, p.tw);
   load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, 2 * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

@@ -117,6 +117,9 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
   // the tile load and the inverse transforms
   const R* ph = phys_row<R, N>(p.phys, x);
@@ -126,7 +129,6 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
     const int e = lane + 32 * j;
     pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
   }
-  load_twiddles<R, N>(s_tw, p.tw);
   load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   cplx<R> duv[E], dbb[E];
@@ -186,7 +188,9 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
   __shared__ cplx<R> s_tw[tw_smem(N)];
+  pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);

@@ -133,6 +133,19 @@ int ecs_linearize(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, co
 int ecs_jvp(ecs_ctx* ctx, const void* dfields, const double* dT, const double* dsx, void* out_dfields,
             double* out_dT, double* out_dsx, int batch, void* stream);
 
+/* ecs_linearize and ecs_jvp in one call, as jax.jvp(obj, (x,), (v,)) returns
+ * the objective and the Jacobian-vector products together
+ * (jax_scripts/lib/utils.py:108).  In Lawson-RK4(3) mode the batch-1 primal
+ * solve runs on a context-owned high-priority stream and the tangent sweep over
+ * each completed chunk of attempts is queued on `stream` behind it, so the two
+ * overlap; results equal ecs_linearize followed by ecs_jvp, and the
+ * linearisation stays in the context for later ecs_jvp / ecs_vjp calls.
+ * Requires stream to be the only stream using ctx during the call. */
+int ecs_linearize_jvp(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
+                      const double* sx, void* out_fields, ecs_info* info, const void* dfields,
+                      const double* dT, const double* dsx, void* out_dfields, double* out_dT,
+                      double* out_dsx, int batch, void* stream);
+
 /* Vector-Jacobian products of objective_RPO at the current linearisation for
  * `batch` cotangents {c_fields, c_T, c_sx}: gradients with respect to
  * {fields, T, sx} (jax.vjp(obj, input_dict), jax_scripts/newton.py:168-169;
