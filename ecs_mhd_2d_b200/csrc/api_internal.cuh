@@ -35,6 +35,7 @@ struct ecs_ctx {
   std::vector<void*> allocs;
   long long launches = 0;           // kernels launched through this context
   int pdl = 1;                      // stepping kernels use programmatic dependent launch (ECS_PDL=0 disables)
+  int tgroups = 2;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1: one stream)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;
@@ -76,6 +77,8 @@ struct ecs_ctx {
   cudaStream_t pstream = nullptr;
   cudaEvent_t pev[2] = {nullptr, nullptr};
   void* Gp = nullptr; void* Hp = nullptr;   // [NG][K][N], [NHA][K][N] primal scratch (batch 1)
+  cudaStream_t tstream = nullptr;           // second tangent group
+  cudaEvent_t tfork = nullptr, tjoin[2] = {nullptr, nullptr};
   ecs::StepCtl* hctl = nullptr;             // pinned [2]
   int* hchunk_acc = nullptr;                // pinned [2][16]
   double* hchunk_h = nullptr;               // pinned [2][16]

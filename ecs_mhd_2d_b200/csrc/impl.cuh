@@ -160,12 +160,12 @@ void launch_row_err(ecs_ctx* c, int B, double atol, cudaStream_t s, double* rec_
 }
 
 template <typename R, int N>
-void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s) {
+void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s, R* phys = nullptr) {
   ColRegenParams<R> p; p.rec = rec; p.items = items; p.G = (cplx<R>*)c->Greg; p.tw = (const cplx<R>*)c->tw;
   p.nitems = nitems;
   const int cols = nitems * Geomc<N>::K * 2;
   ++c->launches; k_col_regen<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
-  RowPhysParams<R> q; q.G = (const cplx<R>*)c->Greg; q.phys = (R*)c->Phys; q.tw = (const cplx<R>*)c->tw;
+  RowPhysParams<R> q; q.G = (const cplx<R>*)c->Greg; q.phys = phys ? phys : (R*)c->Phys; q.tw = (const cplx<R>*)c->tw;
   q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.nitems = nitems;
   ++c->launches; k_row_phys<R, N, XT><<<nitems * (N / XT), XT * 32, smem_row_phys<R, N>(), s>>>(q);
 }
@@ -803,6 +803,10 @@ struct Impl {
       if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->pstream, cudaStreamNonBlocking, hi);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[0], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[1], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->tstream, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tfork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[0], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[1], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaMalloc(&c->Gp, (size_t)NG * K * N * sizeof(cplx<R>));
       if (e == cudaSuccess) e = cudaMalloc(&c->Hp, (size_t)NHA * K * N * sizeof(cplx<R>));
       if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->hctl, 2 * sizeof(StepCtl), cudaHostAllocDefault);
@@ -883,19 +887,52 @@ struct Impl {
       if (e2 == cudaSuccess) e2 = cudaEventRecord(c->pev[bi], ps);
       return e2;
     };
-    // tangent sweep over attempts [a_lo, a_hi) whose record is complete
+    // Tangent sweep over attempts [a_lo, a_hi) whose record is complete.  The
+    // batch is split into two groups swept on two streams (group 0 on the
+    // caller's stream), so that one group's row kernels and the other's column
+    // kernels share the SMs and fill each other's tails.  The attempts' primal
+    // fields are regenerated per chunk on the caller's stream, into alternating
+    // halves of the regeneration buffer when two chunks fit.
     L.acc.clear(); L.hs.clear();
     const long ci = (long)chunk_items();
-    long nitems = 0, win_lo = -1, win_cnt = 0;
-    auto phys_of = [&](long item) -> const R* {
-      if (win_lo < 0 || item < win_lo || item >= win_lo + win_cnt) {
-        win_lo = item; win_cnt = std::min(ci, nitems - item);
-        launch_regen<R, N>(c, rec, c->items + item, (int)win_cnt, s);
-      }
-      return (const R*)c->Phys + (size_t)(item - win_lo) * N * NPH * N;
-    };
+    const int ngrp = (B >= 32 && c->tgroups > 1) ? 2 : 1;
+    const int bsplit[3] = {0, ngrp == 2 ? B / 2 : B, B};
+    const bool dbl = ci >= 2 * (4 * GA + 1);
+    bool joined[2] = {true, true};
+    long nitems = 0;
+    int half = 0;
     const double t = L.T;
     std::vector<long> item_of;
+    auto sweep = [&](int g, long a_lo, long a_hi, const int* acc, const double* hh, const R* phys0, long item_lo) {
+      const int b0 = bsplit[g], Bg = bsplit[g + 1] - b0;
+      cudaStream_t st = g == 0 ? s : c->tstream;
+      void* const G0 = c->G; void* const H0 = c->H; void* const D0 = c->D;
+      c->G = (cplx<R>*)G0 + (size_t)b0 * NG * K * N;
+      c->H = (cplx<R>*)H0 + (size_t)b0 * NH * K * N;
+      c->D = (cplx<R>*)D0 + (size_t)b0 * nslot * VEC;
+      const double* dTg = dT + b0;
+      auto phys = [&](long item) { return phys0 + (size_t)(item - item_lo) * N * NPH * N; };
+      if (a_lo == 0) {
+        launch_col_tan<R, N>(c, Bg, T43_START, 1, rec, dTg, t, 0.0, 1.0, nslot, st);
+        launch_row_tan<R, N>(c, Bg, phys(0), st);
+        launch_col_tan<R, N>(c, Bg, T43_INIT, 0, rec, dTg, t, 0.0, 1.0, nslot, st);
+      }
+      for (long a = a_lo; a < a_hi; ++a) {
+        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
+        const double h = hh[a - a_lo];
+        if (!acc[a - a_lo]) {
+          ++c->launches; k_tan_reject<R><<<grid1d((long)Bg * VEC), 256, 0, st>>>((cplx<R>*)c->D, nslot, ra, dTg, 1.0, t, h,
+                                                                                 (R)c->nu, (R)c->eta, N, Bg);
+          continue;
+        }
+        launch_col_tan<R, N>(c, Bg, T43_A, 1, ra, dTg, t, h, 1.0, nslot, st);
+        for (int k = 0; k < 4; ++k) {
+          launch_row_tan<R, N>(c, Bg, phys(item_of[a - a_lo] + k), st);
+          launch_col_tan<R, N>(c, Bg, T43_B + k, 1, ra, dTg, t, h, 1.0, nslot, st);
+        }
+      }
+      c->G = G0; c->H = H0; c->D = D0;
+    };
     auto tangent_chunk = [&](long a_lo, long a_hi, const int* acc, const double* hh) -> int {
       const long i0 = nitems;
       long* stage = c->hitems + i0;
@@ -909,30 +946,28 @@ struct Impl {
         const long base = a * RR_NREC;
         stage[cnt++] = base + RR_Y2; stage[cnt++] = base + RR_Y3; stage[cnt++] = base + RR_Y4; stage[cnt++] = base + RR_XF;
       }
-      if (cnt > 0) {
-        const cudaError_t e2 = cudaMemcpyAsync(c->items + i0, stage, cnt * sizeof(long), cudaMemcpyHostToDevice, s);
-        if (e2 != cudaSuccess) return cuda_err(c, e2, "item upload");
-      }
       nitems += cnt;
-      if (a_lo == 0) {
-        launch_col_tan<R, N>(c, B, T43_START, 1, rec, dT, t, 0.0, 1.0, nslot, s);
-        launch_row_tan<R, N>(c, B, phys_of(0), s);
-        launch_col_tan<R, N>(c, B, T43_INIT, 0, rec, dT, t, 0.0, 1.0, nslot, s);
+      cudaError_t e2 = cudaSuccess;
+      const int hb = dbl ? half : 0;
+      R* phys0 = (R*)c->Phys + (dbl ? (size_t)hb * (ci / 2) * N * NPH * N : 0);
+      if (cnt > 0) {
+        e2 = cudaMemcpyAsync(c->items + i0, stage, cnt * sizeof(long), cudaMemcpyHostToDevice, s);
+        // the second group's last reads of this half must be done before it is overwritten
+        if (e2 == cudaSuccess && !joined[hb]) { e2 = cudaStreamWaitEvent(s, c->tjoin[hb], 0); joined[hb] = true; }
+        if (e2 != cudaSuccess) return cuda_err(c, e2, "item upload");
+        launch_regen<R, N>(c, rec, c->items + i0, (int)cnt, s, phys0);
       }
-      for (long a = a_lo; a < a_hi; ++a) {
-        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
-        const double h = hh[a - a_lo];
-        if (!acc[a - a_lo]) {
-          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, t, h,
-                                                                                (R)c->nu, (R)c->eta, N, B);
-          continue;
-        }
-        launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
-        for (int k = 0; k < 4; ++k) {
-          launch_row_tan<R, N>(c, B, phys_of(item_of[a - a_lo] + k), s);
-          launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
-        }
+      if (ngrp == 2) {
+        e2 = cudaEventRecord(c->tfork, s);
+        if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(c->tstream, c->tfork, 0);
+        if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent fork");
+        sweep(1, a_lo, a_hi, acc, hh, phys0, i0);
+        e2 = cudaEventRecord(c->tjoin[hb], c->tstream);
+        if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent join");
+        joined[hb] = false;
       }
+      sweep(0, a_lo, a_hi, acc, hh, phys0, i0);
+      if (dbl) half ^= 1;
       return cuda_err(c, cudaGetLastError(), "pipelined tangent");
     };
     // chunk i+1 of the primal is queued before the tangents of chunk i
@@ -955,7 +990,9 @@ struct Impl {
       if (!more) break;
       bi ^= 1;
     }
-    // primal epilogue on the caller's stream (it waited for every chunk)
+    // join the second tangent group; primal epilogue on the caller's stream (it waited for every chunk)
+    for (int hb = 0; hb < 2; ++hb)
+      if (!joined[hb]) { e = cudaStreamWaitEvent(s, c->tjoin[hb], 0); if (e != cudaSuccess) return cuda_err(c, e, "tangent join"); }
     ++c->launches; k_rk43_resolve<R><<<grid1d((long)VEC), 256, 0, s>>>((cplx<R>*)c->S43, c->ctl, (cplx<R>*)c->F, N, 1);
     cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
     L.nrec = a_done;

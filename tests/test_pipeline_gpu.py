@@ -59,6 +59,22 @@ def test_linearize_jvp_equals_sequential(cuda, mode, kw, T):
         assert torch.equal(again[k], want[k]), k
 
 
+def test_linearize_jvp_two_groups(cuda):
+    """Batches of 32 or more tangents are swept as two groups on two streams;
+    each tangent's result is the same as in the single sequential sweep."""
+    n, B = 64, 34
+    kw = CASES[0][1]
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    prim, tan = _inputs(n, B)
+    prim["T"] = 0.3
+    seq = E.Objective(pd, "Lawson_RK43")
+    seq.linearize(prim, force=True, batch=B)
+    want = {k: v.clone() for k, v in seq.jvp(prim, tan).items()}
+    got = E.Objective(pd, "Lawson_RK43").linearize_jvp(prim, tan)[1]
+    for k in ("fields", "T", "sx"):
+        assert torch.equal(got[k], want[k]), k
+
+
 def test_linearize_jvp_repeated_calls(cuda):
     """Back-to-back pipelined calls on one context (graph and buffers reused)
     give the same result each time."""
