@@ -85,7 +85,7 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   c->n = n; c->dtype = dtype; c->max_batch = max_batch; c->g = make_geom(n);
   c->nu = params->nu; c->eta = params->eta; c->b0x = params->b0x; c->b0y = params->b0y;
   if (const char* v = getenv("ECS_PDL")) c->pdl = atoi(v) != 0 ? 1 : 0;
-  if (const char* v = getenv("ECS_TGROUPS")) c->tgroups = atoi(v) > 1 ? 2 : 1;
+  if (const char* v = getenv("ECS_TGROUPS")) c->tgroups = std::max(1, std::min(ecs_ctx::MAXG, atoi(v)));
   int st;
   const ecs::ImplTable* t = ecs::impl_table(dtype, n);
   st = t ? t->init(c, params) : ECS_ERR_UNSUPPORTED;
@@ -109,9 +109,11 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->pstream) cudaStreamDestroy(ctx->pstream);
   for (cudaEvent_t e : ctx->pev) if (e) cudaEventDestroy(e);
-  if (ctx->tstream) cudaStreamDestroy(ctx->tstream);
+  for (int g = 0; g < ecs_ctx::MAXG; ++g) {
+    if (ctx->tstream[g]) cudaStreamDestroy(ctx->tstream[g]);
+    for (cudaEvent_t e : ctx->tjoin[g]) if (e) cudaEventDestroy(e);
+  }
   if (ctx->tfork) cudaEventDestroy(ctx->tfork);
-  for (cudaEvent_t e : ctx->tjoin) if (e) cudaEventDestroy(e);
   if (ctx->Gp) cudaFree(ctx->Gp);
   if (ctx->Hp) cudaFree(ctx->Hp);
   if (ctx->hctl) cudaFreeHost(ctx->hctl);

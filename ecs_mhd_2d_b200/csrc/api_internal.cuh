@@ -35,7 +35,7 @@ struct ecs_ctx {
   std::vector<void*> allocs;
   long long launches = 0;           // kernels launched through this context
   int pdl = 1;                      // stepping kernels use programmatic dependent launch (ECS_PDL=0 disables)
-  int tgroups = 2;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1: one stream)
+  int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;
@@ -77,8 +77,9 @@ struct ecs_ctx {
   cudaStream_t pstream = nullptr;
   cudaEvent_t pev[2] = {nullptr, nullptr};
   void* Gp = nullptr; void* Hp = nullptr;   // [NG][K][N], [NHA][K][N] primal scratch (batch 1)
-  cudaStream_t tstream = nullptr;           // second tangent group
-  cudaEvent_t tfork = nullptr, tjoin[2] = {nullptr, nullptr};
+  static constexpr int MAXG = 4;            // tangent groups of ecs_linearize_jvp
+  cudaStream_t tstream[MAXG] = {};          // streams of groups 1.. (group 0 uses the caller's stream)
+  cudaEvent_t tfork = nullptr, tjoin[MAXG][2] = {};
   ecs::StepCtl* hctl = nullptr;             // pinned [2]
   int* hchunk_acc = nullptr;                // pinned [2][16]
   double* hchunk_h = nullptr;               // pinned [2][16]

@@ -803,10 +803,12 @@ struct Impl {
       if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->pstream, cudaStreamNonBlocking, hi);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[0], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[1], cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->tstream, cudaStreamNonBlocking);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tfork, cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[0], cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[1], cudaEventDisableTiming);
+      for (int g = 1; g < ecs_ctx::MAXG && e == cudaSuccess; ++g) {
+        e = cudaStreamCreateWithFlags(&c->tstream[g], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[g][0], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[g][1], cudaEventDisableTiming);
+      }
       if (e == cudaSuccess) e = cudaMalloc(&c->Gp, (size_t)NG * K * N * sizeof(cplx<R>));
       if (e == cudaSuccess) e = cudaMalloc(&c->Hp, (size_t)NHA * K * N * sizeof(cplx<R>));
       if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->hctl, 2 * sizeof(StepCtl), cudaHostAllocDefault);
@@ -888,24 +890,27 @@ struct Impl {
       return e2;
     };
     // Tangent sweep over attempts [a_lo, a_hi) whose record is complete.  The
-    // batch is split into two groups swept on two streams (group 0 on the
-    // caller's stream), so that one group's row kernels and the other's column
-    // kernels share the SMs and fill each other's tails.  The attempts' primal
-    // fields are regenerated per chunk on the caller's stream, into alternating
-    // halves of the regeneration buffer when two chunks fit.
+    // batch is split into groups (of at least 16 tangents) swept on their own
+    // streams (group 0 on the caller's stream), so that one group's row kernels
+    // and another's column kernels share the SMs and fill each other's tails.
+    // The attempts' primal fields are regenerated per chunk on the caller's
+    // stream, into alternating halves of the regeneration buffer when two
+    // chunks fit.
     L.acc.clear(); L.hs.clear();
     const long ci = (long)chunk_items();
-    const int ngrp = (B >= 32 && c->tgroups > 1) ? 2 : 1;
-    const int bsplit[3] = {0, ngrp == 2 ? B / 2 : B, B};
+    const int ngrp = std::max(1, std::min(c->tgroups, B / 16));
+    int bsplit[ecs_ctx::MAXG + 1];
+    for (int g = 0; g <= ngrp; ++g) bsplit[g] = (int)((long)B * g / ngrp);
     const bool dbl = ci >= 2 * (4 * GA + 1);
-    bool joined[2] = {true, true};
+    bool joined[ecs_ctx::MAXG][2];
+    for (auto& j : joined) j[0] = j[1] = true;
     long nitems = 0;
     int half = 0;
     const double t = L.T;
     std::vector<long> item_of;
     auto sweep = [&](int g, long a_lo, long a_hi, const int* acc, const double* hh, const R* phys0, long item_lo) {
       const int b0 = bsplit[g], Bg = bsplit[g + 1] - b0;
-      cudaStream_t st = g == 0 ? s : c->tstream;
+      cudaStream_t st = g == 0 ? s : c->tstream[g];
       void* const G0 = c->G; void* const H0 = c->H; void* const D0 = c->D;
       c->G = (cplx<R>*)G0 + (size_t)b0 * NG * K * N;
       c->H = (cplx<R>*)H0 + (size_t)b0 * NH * K * N;
@@ -952,19 +957,23 @@ struct Impl {
       R* phys0 = (R*)c->Phys + (dbl ? (size_t)hb * (ci / 2) * N * NPH * N : 0);
       if (cnt > 0) {
         e2 = cudaMemcpyAsync(c->items + i0, stage, cnt * sizeof(long), cudaMemcpyHostToDevice, s);
-        // the second group's last reads of this half must be done before it is overwritten
-        if (e2 == cudaSuccess && !joined[hb]) { e2 = cudaStreamWaitEvent(s, c->tjoin[hb], 0); joined[hb] = true; }
+        // the other groups' last reads of this half must be done before it is overwritten
+        for (int g = 1; g < ngrp && e2 == cudaSuccess; ++g)
+          if (!joined[g][hb]) { e2 = cudaStreamWaitEvent(s, c->tjoin[g][hb], 0); joined[g][hb] = true; }
         if (e2 != cudaSuccess) return cuda_err(c, e2, "item upload");
         launch_regen<R, N>(c, rec, c->items + i0, (int)cnt, s, phys0);
       }
-      if (ngrp == 2) {
+      if (ngrp > 1) {
         e2 = cudaEventRecord(c->tfork, s);
-        if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(c->tstream, c->tfork, 0);
         if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent fork");
-        sweep(1, a_lo, a_hi, acc, hh, phys0, i0);
-        e2 = cudaEventRecord(c->tjoin[hb], c->tstream);
-        if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent join");
-        joined[hb] = false;
+        for (int g = 1; g < ngrp; ++g) {
+          e2 = cudaStreamWaitEvent(c->tstream[g], c->tfork, 0);
+          if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent fork");
+          sweep(g, a_lo, a_hi, acc, hh, phys0, i0);
+          e2 = cudaEventRecord(c->tjoin[g][hb], c->tstream[g]);
+          if (e2 != cudaSuccess) return cuda_err(c, e2, "tangent join");
+          joined[g][hb] = false;
+        }
       }
       sweep(0, a_lo, a_hi, acc, hh, phys0, i0);
       if (dbl) half ^= 1;
@@ -990,9 +999,13 @@ struct Impl {
       if (!more) break;
       bi ^= 1;
     }
-    // join the second tangent group; primal epilogue on the caller's stream (it waited for every chunk)
-    for (int hb = 0; hb < 2; ++hb)
-      if (!joined[hb]) { e = cudaStreamWaitEvent(s, c->tjoin[hb], 0); if (e != cudaSuccess) return cuda_err(c, e, "tangent join"); }
+    // join the tangent groups; primal epilogue on the caller's stream (it waited for every chunk)
+    for (int g = 1; g < ngrp; ++g)
+      for (int hb = 0; hb < 2; ++hb)
+        if (!joined[g][hb]) {
+          e = cudaStreamWaitEvent(s, c->tjoin[g][hb], 0);
+          if (e != cudaSuccess) return cuda_err(c, e, "tangent join");
+        }
     ++c->launches; k_rk43_resolve<R><<<grid1d((long)VEC), 256, 0, s>>>((cplx<R>*)c->S43, c->ctl, (cplx<R>*)c->F, N, 1);
     cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
     L.nrec = a_done;

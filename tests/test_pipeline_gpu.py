@@ -59,10 +59,12 @@ def test_linearize_jvp_equals_sequential(cuda, mode, kw, T):
         assert torch.equal(again[k], want[k]), k
 
 
-def test_linearize_jvp_two_groups(cuda):
-    """Batches of 32 or more tangents are swept as two groups on two streams;
-    each tangent's result is the same as in the single sequential sweep."""
-    n, B = 64, 34
+@pytest.mark.parametrize("B", [34, 64])
+def test_linearize_jvp_groups(cuda, B):
+    """Batches of 32 or more tangents are swept as groups on several streams
+    (three by default, one to four with ECS_TGROUPS); each tangent's result is the
+    same as in the single sequential sweep."""
+    n = 64
     kw = CASES[0][1]
     pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
     prim, tan = _inputs(n, B)
