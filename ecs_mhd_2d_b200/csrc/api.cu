@@ -26,6 +26,11 @@ int ecs_box_dims(const ecs_ctx* ctx, int* K, int* M) {
 
 namespace ecs {
 
+std::mutex& capture_mutex() {
+  static std::mutex m;
+  return m;
+}
+
 int set_err(ecs_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
@@ -75,12 +80,15 @@ static const ecs::ImplTable* table_of(const ecs_ctx* c) { return ecs::impl_table
 static cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
 
 
+static int ctx_destroy_locked(ecs_ctx* ctx);
+
 int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ecs_ctx** out) {
   if (!out || !params) return ECS_ERR_INVALID;
   *out = nullptr;
   if (!(n == 64 || n == 128 || n == 256)) return ECS_ERR_UNSUPPORTED;
   if (!(dtype == ECS_F64 || dtype == ECS_F32)) return ECS_ERR_UNSUPPORTED;
   if (max_batch < 1) return ECS_ERR_INVALID;
+  std::lock_guard<std::mutex> capture_guard(ecs::capture_mutex());   // set-up synchronises the device
   ecs_ctx* c = new ecs_ctx();
   c->n = n; c->dtype = dtype; c->max_batch = max_batch; c->g = make_geom(n);
   c->nu = params->nu; c->eta = params->eta; c->b0x = params->b0x; c->b0y = params->b0y;
@@ -91,14 +99,14 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   st = t ? t->init(c, params) : ECS_ERR_UNSUPPORTED;
   if (st != ECS_OK) {
     fprintf(stderr, "ecs_ctx_create: %s\n", c->err.c_str());
-    ecs_ctx_destroy(c);
+    ctx_destroy_locked(c);
     return st;
   }
   *out = c;
   return ECS_OK;
 }
 
-int ecs_ctx_destroy(ecs_ctx* ctx) {
+static int ctx_destroy_locked(ecs_ctx* ctx) {
   if (!ctx) return ECS_OK;
   cudaDeviceSynchronize();
   for (void* p : ctx->allocs) cudaFree(p);
@@ -122,6 +130,7 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->hitems) cudaFreeHost(ctx->hitems);
   if (ctx->lin.rec) cudaFree(ctx->lin.rec);
   if (ctx->lin.ckpt) cudaFree(ctx->lin.ckpt);
+  if (ctx->lin.rec2) cudaFree(ctx->lin.rec2);
   if (ctx->lin.rec_h) cudaFree(ctx->lin.rec_h);
   if (ctx->lin.rec_acc) cudaFree(ctx->lin.rec_acc);
   if (ctx->D) cudaFree(ctx->D);
@@ -131,6 +140,11 @@ int ecs_ctx_destroy(ecs_ctx* ctx) {
   if (ctx->hacc) cudaFree(ctx->hacc);
   delete ctx;
   return ECS_OK;
+}
+
+int ecs_ctx_destroy(ecs_ctx* ctx) {
+  std::lock_guard<std::mutex> capture_guard(ecs::capture_mutex());   // synchronises the device
+  return ctx_destroy_locked(ctx);
 }
 
 int ecs_to_box(ecs_ctx* ctx, const void* fields, void* box, int batch, void* stream) {

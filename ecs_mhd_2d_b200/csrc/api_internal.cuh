@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -54,6 +55,7 @@ struct ecs_ctx {
     double* rec_h = nullptr; int* rec_acc = nullptr; size_t cap = 0;
     long seg = 0;                   // Lawson-RK4 checkpoint interval (0: full record)
     void* ckpt = nullptr; size_t ckpt_bytes = 0;   // segment start states
+    void* rec2 = nullptr; size_t rec2_bytes = 0;   // second segment record (pipelined adjoint)
   } lin;
   // tangent / adjoint workspace (grown on demand)
   void* D = nullptr; size_t D_bytes = 0;          // tangent or adjoint slots
@@ -107,6 +109,10 @@ template <int N> struct Geomc {
 };
 
 int set_err(ecs_ctx* c, int code, const std::string& msg);
+// Held by every CUDA graph capture (begin to instantiate) and by context
+// creation and destruction, whose set-up synchronises the device: a
+// device-wide synchronisation while another thread captures is an error.
+std::mutex& capture_mutex();
 int cuda_err(ecs_ctx* c, cudaError_t e, const char* where);
 void* dev_alloc(ecs_ctx* c, size_t bytes, int* st);
 // (re)allocate a growable device buffer owned by the context (not in allocs)

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <mutex>
 
 // ---------------------------------------------------------------------------
 // launch helpers
@@ -303,6 +304,7 @@ struct Impl {
       if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
       const long long l0 = c->launches;
       cudaGraph_t graph = nullptr;
+      std::lock_guard<std::mutex> capture_guard(capture_mutex());   // no set-up of another context meanwhile
       cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
         for (int a = 0; a < GS; ++a) one_step(c->cap_stream, false);
@@ -376,6 +378,7 @@ struct Impl {
       if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
       const long long l0 = c->launches;
       cudaGraph_t graph = nullptr;
+      std::lock_guard<std::mutex> capture_guard(capture_mutex());   // no set-up of another context meanwhile
       cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
         for (int a = 0; a < GA; ++a) attempt(c->cap_stream);
@@ -490,14 +493,15 @@ struct Impl {
 
   // Lawson-RK4 segment [a0, a0+cnt) of the current linearisation: its record
   // (recomputed from the checkpoint when the linearisation is segmented).
-  static const cplx<R>* rk4_segment_record(ecs_ctx* c, long a0, long cnt, cudaStream_t s) {
+  static const cplx<R>* rk4_segment_record(ecs_ctx* c, long a0, long cnt, cudaStream_t s, void* buf = nullptr) {
     auto& L = c->lin;
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
     if (!L.seg) return (const cplx<R>*)L.rec + (size_t)a0 * Q_NREC * VEC;
+    cplx<R>* dst = (cplx<R>*)(buf ? buf : L.rec);
     rk4_setup(c, L.dT, L.cfg.num_checkpoints, L.cfg.ministeps, 1, s);
     cudaMemcpyAsync(c->F, (cplx<R>*)L.ckpt + (size_t)(a0 / L.seg) * VEC, vb, cudaMemcpyDeviceToDevice, s);
-    record_rk4_segment(c, (cplx<R>*)L.rec, cnt, s);
-    return (const cplx<R>*)L.rec;
+    record_rk4_segment(c, dst, cnt, s);
+    return dst;
   }
 
   // ---------------------------------------------------------------------
@@ -609,8 +613,9 @@ struct Impl {
       L.nrec = hc.attempts;
       L.acc.assign(L.nrec, 0); L.hs.assign(L.nrec, 0.0);
       if (L.nrec > 0) {
-        e = cudaMemcpy(L.acc.data(), L.rec_acc, L.nrec * sizeof(int), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(L.hs.data(), L.rec_h, L.nrec * sizeof(double), cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(L.acc.data(), L.rec_acc, L.nrec * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(L.hs.data(), L.rec_h, L.nrec * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_err(c, e, "linearize record readback");
       }
       if (info) { info->completed = hc.done; info->s = hc.s; info->accepted = hc.accepted; info->rejected = hc.rejected; info->fevals = hc.fevals; }
@@ -641,13 +646,15 @@ struct Impl {
   }
 
   // Regeneration plan for the primal physical fields (offsets in box vectors).
-  static int upload_items(ecs_ctx* c, const std::vector<long>& items) {
+  static int upload_items(ecs_ctx* c, const std::vector<long>& items, cudaStream_t s) {
     if (items.size() > c->items_cap) {
       if (c->items) cudaFree(c->items);
       if (cudaMalloc(&c->items, items.size() * sizeof(long)) != cudaSuccess) { c->items = nullptr; c->items_cap = 0; return set_err(c, ECS_ERR_OOM, "items"); }
       c->items_cap = items.size();
     }
-    return cuda_err(c, cudaMemcpy(c->items, items.data(), items.size() * sizeof(long), cudaMemcpyHostToDevice), "items upload");
+    // pageable source: the call returns once the vector has been staged
+    return cuda_err(c, cudaMemcpyAsync(c->items, items.data(), items.size() * sizeof(long), cudaMemcpyHostToDevice, s),
+                    "items upload");
   }
 
   static size_t chunk_items() {
@@ -706,7 +713,7 @@ struct Impl {
         items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
       }
     }
-    st = upload_items(c, items);
+    st = upload_items(c, items, s);
     if (st) return st;
     const long ci = (long)chunk_items();
     long chunk_lo = -1;
@@ -730,7 +737,7 @@ struct Impl {
           const long base = it * Q_NREC;
           sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
         }
-        st = upload_items(c, sitems);
+        st = upload_items(c, sitems, s);
         if (st) return st;
         long slo = -1;
         auto sphys = [&](long item) -> const R* {
@@ -804,8 +811,8 @@ struct Impl {
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[0], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->pev[1], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tfork, cudaEventDisableTiming);
-      for (int g = 1; g < ecs_ctx::MAXG && e == cudaSuccess; ++g) {
-        e = cudaStreamCreateWithFlags(&c->tstream[g], cudaStreamNonBlocking);
+      for (int g = 0; g < ecs_ctx::MAXG && e == cudaSuccess; ++g) {   // group 0 runs on the caller's stream
+        if (g > 0) e = cudaStreamCreateWithFlags(&c->tstream[g], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[g][0], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->tjoin[g][1], cudaEventDisableTiming);
       }
@@ -833,6 +840,96 @@ struct Impl {
     return ECS_OK;
   }
 
+  // Fixed-step Lawson-RK4 form of linearize_jvp (full record): the batch-1
+  // primal records chunks of steps on the primal stream, each followed by an
+  // event; the tangent sweep of a chunk (regeneration of its primal fields
+  // included) waits on that event on the caller's stream.  No host round trip:
+  // the host queues both streams ahead.
+  static int linearize_jvp_rk4(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T,
+                               const double* sx, R* out_fields, ecs_info* info, const R* dfields, const double* dT,
+                               const double* dsx, R* out, double* odT, double* odsx, int B, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
+    const int nslot = (int)D_NS4;
+    int st = ensure_pipeline(c, steps);
+    if (!st) st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = ensure_regen(c);
+    if (!st) st = lin_prologue(c, cfg, fields, T, sx, s);
+    if (!st) st = grow(c, &L.rec, &L.rec_bytes, (size_t)steps * Q_NREC * vb);
+    if (st) return st;
+    cudaMemcpyAsync(c->F, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+    st = rk4_setup(c, T, cfg->num_checkpoints, cfg->ministeps, 1, s);
+    if (st) return st;
+    L.seg = 0;
+    L.nrec = steps;
+    L.h = (double)(R)((L.T / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
+    L.acc.clear(); L.hs.clear();
+    const double dscale = 1.0 / ((double)cfg->num_checkpoints * (double)cfg->ministeps);
+    // tangent initial state: box(dfields) into slot F; regeneration items (4 per step) staged once
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)D_F * VEC, B, 2, s, (long)nslot * VEC);
+    for (long it = 0; it < steps; ++it) {
+      long* q = c->hitems + 4 * it;
+      const long base = it * Q_NREC;
+      q[0] = base + Q_F; q[1] = base + Q_X2; q[2] = base + Q_X3; q[3] = base + Q_X4;
+    }
+    cudaError_t e = cudaMemcpyAsync(c->items, c->hitems, 4 * steps * sizeof(long), cudaMemcpyHostToDevice, s);
+    cudaStream_t ps = c->pstream;
+    if (e == cudaSuccess) e = cudaEventRecord(c->pev[0], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ps, c->pev[0], 0);
+    if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
+    cplx<R>* rec = (cplx<R>*)L.rec;
+    const long ci = (long)chunk_items();
+    const long CS = std::max(1L, std::min(16L, ci / 4));   // steps per chunk (their items fit one regeneration)
+    const long nch = (steps + CS - 1) / CS;
+    auto primal_chunk = [&](long k) -> cudaError_t {
+      void* const Gs = c->G; void* const Hs = c->H;
+      c->G = c->Gp; c->H = c->Hp;
+      if (k == 0) launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, ps);
+      for (long it = k * CS; it < std::min(steps, (k + 1) * CS); ++it) {
+        cplx<R>* rs = rec + (size_t)it * Q_NREC * VEC;
+        for (int q = 1; q <= 4; ++q) {
+          launch_row_rhs<R, N>(c, 1, ps);
+          launch_col_rk4<R, N>(c, 1, q, (q == 4 && it == steps - 1) ? 0 : 1, 0, ps, rs, 0);
+        }
+      }
+      c->G = Gs; c->H = Hs;
+      return cudaEventRecord(c->pev[k & 1], ps);
+    };
+    auto tangent_chunk = [&](long k) -> cudaError_t {
+      cudaError_t e2 = cudaStreamWaitEvent(s, c->pev[k & 1], 0);
+      if (e2 != cudaSuccess) return e2;
+      const long a0 = k * CS, cnt = std::min(steps, (k + 1) * CS) - a0;
+      launch_regen<R, N>(c, rec, c->items + 4 * a0, (int)(4 * cnt), s);
+      if (k == 0) launch_col_tan<R, N>(c, B, TS_START, 1, rec, dT, 0.0, L.h, dscale, nslot, s);
+      for (long it = a0; it < a0 + cnt; ++it) {
+        const cplx<R>* ra = rec + (size_t)it * Q_NREC * VEC;
+        for (int q = 1; q <= 4; ++q) {
+          launch_row_tan<R, N>(c, B, (const R*)c->Phys + (size_t)(4 * (it - a0) + q - 1) * N * NPH * N, s);
+          launch_col_tan<R, N>(c, B, q, (q == 4 && it == steps - 1) ? 0 : 1, ra, dT, 0.0, L.h, dscale, nslot, s);
+        }
+      }
+      return cudaGetLastError();
+    };
+    // chunk k+1 of the primal is queued before the tangents of chunk k (each event is
+    // waited on before the chunk two ahead records it again)
+    e = primal_chunk(0);
+    for (long k = 0; k < nch && e == cudaSuccess; ++k) {
+      if (k + 1 < nch) e = primal_chunk(k + 1);
+      if (e == cudaSuccess) e = tangent_chunk(k);
+    }
+    if (e != cudaSuccess) return cuda_err(c, e, "pipelined linearisation");
+    cudaMemcpyAsync(L.phi, c->F, vb, cudaMemcpyDeviceToDevice, s);
+    if (info) { info->completed = 1; info->s = 1.0; info->accepted = (int)steps; info->rejected = 0; info->fevals = (int)(4 * steps); }
+    if (out_fields) {
+      st = residual(c, cfg, fields, (const cplx<R>*)L.phi, (const cplx<R>*)L.f0box, L.dsx, 1, out_fields, s, 1);
+      if (st) return st;
+    }
+    L.valid = 1;
+    return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
+  }
+
   // ---------------------------------------------------------------------
   // Linearisation and JVP in one call, pipelined (Lawson-RK4(3)), as jax.jvp
   // returns (objective, J v) together.  The batch-1 primal solve runs on a
@@ -850,6 +947,9 @@ struct Impl {
                            R* out, double* odT, double* odsx, int B, cudaStream_t s) {
     constexpr int GA = 16;
     const long amax = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
+    const long steps4 = (long)cfg->num_checkpoints * cfg->ministeps;
+    if (cfg->mode == ECS_MODE_LAWSON_RK4 && steps4 > 0 && !(cfg->ckpt_every > 0 && cfg->ckpt_every < steps4))
+      return linearize_jvp_rk4(c, cfg, fields, T, sx, out_fields, info, dfields, dT, dsx, out, odT, odsx, B, s);
     if (cfg->mode != ECS_MODE_LAWSON_RK43 || amax < GA || amax % GA != 0) {
       const int st = linearize(c, cfg, fields, T, sx, out_fields, info, s);
       return st ? st : jvp(c, dfields, dT, dsx, out, odT, odsx, B, s);
@@ -1061,7 +1161,7 @@ struct Impl {
         items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
       }
     }
-    st = upload_items(c, items);
+    st = upload_items(c, items, s);
     if (st) return st;
     const long ci = (long)chunk_items();
     long chunk_lo = -1;
@@ -1080,15 +1180,51 @@ struct Impl {
       const double h = L.h;
       const long kseg = L.seg ? L.seg : L.nrec;
       const long nseg = (L.nrec + kseg - 1) / kseg;
+      // Checkpointed record: segment g-1 is recomputed (batch 1, on the primal
+      // stream with its own scratch, into the other of two record buffers)
+      // while the adjoint sweeps segment g on the caller's stream.
+      const bool pipe = L.seg && nseg > 1;
+      if (pipe) {
+        st = ensure_pipeline(c, kseg);
+        if (!st) st = grow(c, &L.rec2, &L.rec2_bytes, (size_t)kseg * Q_NREC * vb);
+        if (st) return st;
+        cudaError_t e = cudaEventRecord(c->pev[0], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->pstream, c->pev[0], 0);
+        if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
+      }
+      void* bufs[2] = {L.rec, L.rec2};
+      auto recompute = [&](long g) -> cudaError_t {   // on the primal stream, into bufs[g & 1]
+        void* const Gs = c->G; void* const Hs = c->H;
+        c->G = c->Gp; c->H = c->Hp;
+        rk4_segment_record(c, g * kseg, std::min(kseg, L.nrec - g * kseg), c->pstream, bufs[g & 1]);
+        c->G = Gs; c->H = Hs;
+        return cudaEventRecord(c->pev[g & 1], c->pstream);
+      };
+      if (pipe) {
+        const cudaError_t e = recompute(nseg - 1);
+        if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
+      }
       for (long g = nseg - 1; g >= 0; --g) {
         const long a0 = g * kseg, cnt = std::min(kseg, L.nrec - a0);
-        const cplx<R>* rseg = rk4_segment_record(c, a0, cnt, s);
+        const cplx<R>* rseg;
+        if (pipe) {
+          cudaError_t e = cudaSuccess;
+          if (g > 0) {   // the buffer of segment g-1 was last read by the adjoint of segment g+1
+            if (g + 1 < nseg) e = cudaStreamWaitEvent(c->pstream, c->tjoin[0][(g + 1) & 1], 0);
+            if (e == cudaSuccess) e = recompute(g - 1);
+          }
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->pev[g & 1], 0);
+          if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
+          rseg = (const cplx<R>*)bufs[g & 1];
+        } else {
+          rseg = rk4_segment_record(c, a0, cnt, s);
+        }
         std::vector<long> sitems;
         for (long it = 0; it < cnt; ++it) {
           const long base = it * Q_NREC;
           sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
         }
-        st = upload_items(c, sitems);
+        st = upload_items(c, sitems, s);
         if (st) return st;
         long slo = -1;
         auto sphys = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
@@ -1107,6 +1243,10 @@ struct Impl {
             launch_row_adj<R, N>(c, B, sphys(4 * it + (k - 1)), s);
             launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
           }
+        }
+        if (pipe) {   // the adjoint of segment g is done with bufs[g & 1]
+          const cudaError_t e = cudaEventRecord(c->tjoin[0][g & 1], s);
+          if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
         }
       }
     } else {
@@ -1201,6 +1341,7 @@ struct Impl {
     if (!gk.exec) {
       const long long l0 = c->launches;
       cudaGraph_t graph = nullptr;
+      std::lock_guard<std::mutex> capture_guard(capture_mutex());   // no set-up of another context meanwhile
       cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
         for (int a = 0; a < GS; ++a) one_step(c->cap_stream);

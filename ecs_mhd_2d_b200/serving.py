@@ -70,10 +70,16 @@ def _nc_ms(steps):
     return steps // ms, ms
 
 
+def _ckpt(req):
+    """Matvecs keep the full record (their primal solve overlaps the tangent
+    sweep); gradients keep one state per ministeps segment."""
+    return 0 if req.kind == "matvec" else _nc_ms(req.steps)[1]
+
+
 def _param_dict(req, dtype):
     nc, ms = _nc_ms(req.steps)
     return make_param_dict(req.n, 1.0 / req.Re, 1.0 / req.Re, forcing="kolmogorov+", data_type=dtype,
-                           num_checkpoints=nc, ministeps=ms, shift_reflect_ny=0, rot=False, ckpt_every=ms)
+                           num_checkpoints=nc, ministeps=ms, shift_reflect_ny=0, rot=False, ckpt_every=_ckpt(req))
 
 
 def context_bytes(n, dtype, batch):
@@ -202,7 +208,7 @@ def run_adjoint_request(req, ctx, stream):
             tv = req.tangent
             tan = {"fields": torch.as_tensor(tv[1:-1].reshape(2, n, n), dtype=req.dtype).to("cuda").contiguous(),
                    "T": float(tv[0]), "sx": float(tv[-1])}
-            o = obj.jvp(x, tan)
+            _, o = obj.linearize_jvp(x, tan)
             out = {"fields": o["fields"].clone(), "T": float(o["T"]), "sx": float(o["sx"])}
         else:
             (loss, info), g = loss_and_grad(x, pd, "Lawson_RK4", ctx=ctx)
@@ -276,7 +282,7 @@ class Server:
             return True
         ws = self.workers.setdefault(key, [])
         idle = [w for w in ws if not w.busy]
-        need = record_bytes(r.n, r.dtype, r.steps, _nc_ms(r.steps)[1])
+        need = record_bytes(r.n, r.dtype, r.steps, _ckpt(r))
         if not idle:
             if len(ws) >= self.workers_per_group:
                 return False

@@ -12,7 +12,8 @@ from ecs_mhd_2d_b200.synthetic import initial_condition
 pytestmark = pytest.mark.gpu
 
 CASES = [
-    # (mode, param kwargs, T): attempt caps are multiples of 16 (the pipelined chunk) or not (sequential fallback)
+    # (mode, param kwargs, T): attempt caps that are multiples of 16 (the pipelined chunk) or not (sequential
+    # fallback); fixed steps with a full record (pipelined) or checkpointed (sequential fallback)
     ("Lawson_RK43", dict(shift_reflect_ny=2, rot=False,
                          adaptive_dict={"atol": 1e-6, "checkpoints": 4, "max_steps_per_checkpoint": 32}), 0.3),
     ("Lawson_RK43", dict(shift_reflect_ny=5, rot=True,
@@ -20,6 +21,8 @@ CASES = [
     ("Lawson_RK43", dict(shift_reflect_ny=1, rot=False,
                          adaptive_dict={"atol": 1e-6, "checkpoints": 3, "max_steps_per_checkpoint": 7}), 0.2),
     ("Lawson_RK4", dict(num_checkpoints=2, ministeps=8, shift_reflect_ny=0, rot=False), 0.1),
+    ("Lawson_RK4", dict(num_checkpoints=5, ministeps=15, shift_reflect_ny=3, rot=True), 0.4),   # 75 steps: 5 chunks
+    ("Lawson_RK4", dict(num_checkpoints=4, ministeps=8, shift_reflect_ny=0, rot=False, ckpt_every=8), 0.2),
 ]
 
 
