@@ -62,6 +62,23 @@ def param_dict(E):
                              adaptive_dict=ad)
 
 
+def max_over_ranks(x, world, device):
+    """The maximum of a per-rank time over all ranks: replicas are timed
+    independently and the job takes as long as its slowest rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def whole_job_rate(world, units_per_rank, t_max_s):
+    """Units processed by all ranks per second of the slowest rank (weak scaling)."""
+    return world * units_per_rank / t_max_s
+
+
 def host_inputs(seed):
     from ecs_mhd_2d_b200.synthetic import initial_condition, unit_tangents
     u0 = initial_condition(IC_SEED + seed, N, amp=IC_AMP)
@@ -237,7 +254,7 @@ def cpu_baseline(target_s=12.0, attempts_full=None):
 def run_reference(args, rank):
     if rank != 0:
         return
-    ref_attempts = 1988   # attempts of this workload's adaptive solve (accepted + rejected), see DESIGN.md
+    ref_attempts = 1988   # attempts of this workload's adaptive solve: 1983 accepted + 5 rejected (CUDA path and oracle)
     cb = cpu_baseline(attempts_full=ref_attempts)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": BATCH / cb["value"] * 1e3,
@@ -269,11 +286,7 @@ def run_serving(args, rank, local, world):
     t0 = time.perf_counter()
     res = srv.run(reqs)
     torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        wall = float(t)
+    wall = max_over_ranks(time.perf_counter() - t0, world, "cuda")
     lat = np.array([r.latency for r in res])
     by = {}
     for k in ("forward", "matvec", "gradient"):
@@ -281,7 +294,7 @@ def run_serving(args, rank, local, world):
         if lk.size:
             by[k] = {"count": int(lk.size), "p50_s": float(np.percentile(lk, 50)), "p99_s": float(np.percentile(lk, 99))}
     if rank == 0:
-        line = {"metric": "serving throughput (mixed shooting requests)", "value": world * len(res) / wall,
+        line = {"metric": "serving throughput (mixed shooting requests)", "value": whole_job_rate(world, len(res), wall),
                 "unit": "requests/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
                 "data": "synthetic Poisson stream (seeded)",
@@ -374,13 +387,9 @@ def main():
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
     launches = lib.ecs_launch_count(ctx.handle) - n_launch0
-    t_total = sum(times)
-    if world > 1:
-        t = torch.tensor([t_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t)
+    t_total = max_over_ranks(sum(times), world, dev)
     ms_per_step = t_total / args.steps
-    value = world * BATCH * args.steps / (t_total / 1e3)
+    value = whole_job_rate(world, BATCH * args.steps, t_total / 1e3)
 
     # end to end through the public API from pinned host buffers
     u0_pin = torch.as_tensor(u0h).pin_memory()
@@ -406,12 +415,8 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         e2e_times.append(e0.elapsed_time(e1))
-    te = sum(e2e_times)
-    if world > 1:
-        t = torch.tensor([te], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t)
-    e2e_value = world * BATCH * args.steps / (te / 1e3)
+    te = max_over_ranks(sum(e2e_times), world, dev)
+    e2e_value = whole_job_rate(world, BATCH * args.steps, te / 1e3)
 
     # phase split of one step (untimed pass, CUDA events): primal linearisation vs tangent sweep
     def _ev_ms(fn):
