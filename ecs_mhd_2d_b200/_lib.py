@@ -15,7 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libecsmhd.so")
 
 ECS_F64, ECS_F32 = 0, 1
-ECS_MODE_LAWSON_RK4, ECS_MODE_LAWSON_RK43 = 1, 2
+ECS_MODE_LAWSON_RK4, ECS_MODE_LAWSON_RK43, ECS_MODE_RK4, ECS_MODE_LAWSON_RK6, ECS_MODE_TDRK4 = 1, 2, 3, 4, 5
 
 STATUS = {
     0: "ECS_OK", 1: "ECS_ERR_INVALID", 2: "ECS_ERR_CUDA", 3: "ECS_ERR_BAD_MODE",

@@ -122,7 +122,7 @@ def _as_objective(obj, param_dict):
         return obj
     if isinstance(obj, str):
         return Objective(param_dict, obj)
-    raise TypeError("obj must be an Objective or a mode string ('Lawson_RK4', 'Lawson_RK43')")
+    raise TypeError("obj must be an Objective or a mode string (e.g. 'Lawson_RK4', 'TDRK4')")
 
 
 def compile_objective_and_Jacobian(input_dict, param_dict, obj):

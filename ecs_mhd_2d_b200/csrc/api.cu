@@ -113,6 +113,8 @@ static int ctx_destroy_locked(ecs_ctx* ctx) {
   if (ctx->hcount) cudaFreeHost(ctx->hcount);
   if (ctx->g43.exec) cudaGraphExecDestroy(ctx->g43.exec);
   if (ctx->g4.exec) cudaGraphExecDestroy(ctx->g4.exec);
+  for (auto& g : ctx->gfx) if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (ctx->fxphys) cudaFree(ctx->fxphys);
   if (ctx->gpool.exec) cudaGraphExecDestroy(ctx->gpool.exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->pstream) cudaStreamDestroy(ctx->pstream);
@@ -123,6 +125,7 @@ static int ctx_destroy_locked(ecs_ctx* ctx) {
   }
   if (ctx->tfork) cudaEventDestroy(ctx->tfork);
   if (ctx->Gp) cudaFree(ctx->Gp);
+  if (ctx->Gx) cudaFree(ctx->Gx);
   if (ctx->Hp) cudaFree(ctx->Hp);
   if (ctx->hctl) cudaFreeHost(ctx->hctl);
   if (ctx->hchunk_acc) cudaFreeHost(ctx->hchunk_acc);

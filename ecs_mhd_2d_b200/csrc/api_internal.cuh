@@ -79,6 +79,7 @@ struct ecs_ctx {
   cudaStream_t pstream = nullptr;
   cudaEvent_t pev[2] = {nullptr, nullptr};
   void* Gp = nullptr; void* Hp = nullptr;   // [NG][K][N], [NHA][K][N] primal scratch (batch 1)
+  void* Gx = nullptr; size_t Gx_bytes = 0;  // TDRK4 tangent/adjoint: second G array [B][NG][K][N]
   static constexpr int MAXG = 4;            // tangent groups of ecs_linearize_jvp
   cudaStream_t tstream[MAXG] = {};          // streams of groups 1.. (group 0 uses the caller's stream)
   cudaEvent_t tfork = nullptr, tjoin[MAXG][2] = {};
@@ -97,6 +98,9 @@ struct ecs_ctx {
     int B = 0;
     long long nodes = 0;
   } g4;
+  // 16-step graphs of the other fixed-step modes (RK4, Lawson-RK6, TDRK4)
+  struct GraphFx { cudaGraphExec_t exec = nullptr; int B = 0; void* phys = nullptr; long long nodes = 0; } gfx[3];
+  void* fxphys = nullptr; size_t fxphys_bytes = 0;   // TDRK4: recorded u, v, B_x, B_y per batch element
   std::string err;
 };
 

@@ -8,6 +8,7 @@
 #include "kernels_rk43.cuh"
 #include "kernels_tan.cuh"
 #include "kernels_adj.cuh"
+#include "kernels_fx.cuh"
 #include "api_internal.cuh"
 #include "impl_table.h"
 
@@ -17,6 +18,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <utility>
 #include <mutex>
 
 // ---------------------------------------------------------------------------
@@ -32,6 +34,7 @@ template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (tw_smem
 // Small batches use 2-row tiles: 4x more CTAs for the same rows.
 constexpr int XTS = 2;
 template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
+template <typename R, int N> size_t smem_row_tan2() { return (tw_smem(N) + 11 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N> size_t smem_row_phys() { return (tw_smem(N) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N, int X = XT> size_t smem_row_2f() { return (tw_smem(N) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
@@ -63,6 +66,8 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_phys<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_phys<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_tan2<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_tan2<R, N>());
+  st |= (int)cudaFuncSetAttribute(k_row_adj2<R, N, XT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N>());
   st |= (int)cudaFuncSetAttribute(k_row_rhs<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
@@ -125,8 +130,10 @@ void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStr
 }
 
 template <typename R, int N>
-void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = nullptr) {
+void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = nullptr, R* phys = nullptr,
+                    long phys_bstride = 0) {
   RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.tw = (const cplx<R>*)c->tw; p.ctl = ctl;
+  p.phys = phys; p.phys_bstride = phys_bstride;
   p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
   if (small_rows<N>(B)) launch_step(c, B, k_row_rhs<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
   else launch_step(c, B, k_row_rhs<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
@@ -161,20 +168,21 @@ void launch_row_err(ecs_ctx* c, int B, double atol, cudaStream_t s, double* rec_
 }
 
 template <typename R, int N>
-void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s, R* phys = nullptr) {
+void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems, cudaStream_t s, R* phys = nullptr,
+                  bool mean = true) {
   ColRegenParams<R> p; p.rec = rec; p.items = items; p.G = (cplx<R>*)c->Greg; p.tw = (const cplx<R>*)c->tw;
   p.nitems = nitems;
   const int cols = nitems * Geomc<N>::K * 2;
   ++c->launches; k_col_regen<R, N><<<(cols + COLWARPS - 1) / COLWARPS, COLWARPS * 32, 0, s>>>(p);
   RowPhysParams<R> q; q.G = (const cplx<R>*)c->Greg; q.phys = phys ? phys : (R*)c->Phys; q.tw = (const cplx<R>*)c->tw;
-  q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.nitems = nitems;
+  q.b0x = mean ? (R)c->b0x : R(0); q.b0y = mean ? (R)c->b0y : R(0); q.nitems = nitems;   // no mean field in derivatives
   ++c->launches; k_row_phys<R, N, XT><<<nitems * (N / XT), XT * 32, smem_row_phys<R, N>(), s>>>(q);
 }
 
 template <typename R, int N>
-void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
+void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_bstride = 0) {
   RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
-  p.B = B;
+  p.B = B; p.phys_bstride = phys_bstride;
   if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
   else launch_step(c, B, k_row_tan<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
 }
@@ -233,6 +241,51 @@ void launch_col_adj(ecs_ctx* c, int B, int stage, const cplx<R>* rec, const cplx
     case AJ43_S2: launch_step(c, B, k_col_adj<R, N, AJ43_S2>, g, bl, 0, s, p); break;
     default: launch_step(c, B, k_col_adj<R, N, AJ43_IPRE>, g, bl, 0, s, p); break;
   }
+}
+
+template <typename R, int N, int SCHEME, int... ST>
+void launch_col_fx_sw(ecs_ctx* c, int B, int stage, cudaStream_t s, const ColFxParams<R>& p,
+                      std::integer_sequence<int, ST...>) {
+  const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ((stage == ST ? launch_step(c, B, k_col_fx<R, N, SCHEME, ST>, g, bl, 0, s, p) : void()), ...);
+}
+
+template <typename R, int N>
+void launch_col_fx(ecs_ctx* c, int B, int scheme, int stage, int produce, cudaStream_t s, cplx<R>* rec = nullptr) {
+  ColFxParams<R> p;
+  p.rec = rec;
+  p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.S = (cplx<R>*)c->S43; p.Etab = (const R*)c->Etab; p.ctl = c->ctl;
+  p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B;
+  p.produce = produce;
+  if (scheme == FX_RK4) launch_col_fx_sw<R, N, FX_RK4>(c, B, stage, s, p, std::make_integer_sequence<int, 5>{});
+  else if (scheme == FX_RK6) launch_col_fx_sw<R, N, FX_RK6>(c, B, stage, s, p, std::make_integer_sequence<int, 9>{});
+  else launch_col_fx_sw<R, N, FX_TD4>(c, B, stage, s, p, std::make_integer_sequence<int, 5>{});
+}
+
+template <typename R, int N>
+void launch_row_tan2(ecs_ctx* c, int B, const cplx<R>* Ga, const cplx<R>* Gb, const R* phys_a, const R* phys_b,
+                     cudaStream_t s) {
+  RowTan2Params<R> p; p.Ga = Ga; p.Gb = Gb; p.H = (cplx<R>*)c->H; p.phys_a = phys_a; p.phys_b = phys_b;
+  p.tw = (const cplx<R>*)c->tw; p.B = B;
+  launch_step(c, B, k_row_tan2<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_tan2<R, N>(), s, p);
+}
+
+template <typename R, int N, int... ST>
+void launch_col_tdj_sw(ecs_ctx* c, int B, int stage, cudaStream_t s, const ColTdjParams<R>& p,
+                       std::integer_sequence<int, ST...>) {
+  const int cols = B * Geomc<N>::K * 2;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ((stage == ST ? launch_step(c, B, k_col_tdj<R, N, ST>, g, bl, 0, s, p) : void()), ...);
+}
+
+template <typename R, int N>
+void launch_col_tdj(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* rec, const double* dT, double h,
+                    double dscale, int nslot, cudaStream_t s) {
+  ColTdjParams<R> p; p.H = (const cplx<R>*)c->H; p.Ga = (cplx<R>*)c->G; p.Gb = (cplx<R>*)c->Gx; p.D = (cplx<R>*)c->D;
+  p.nslot = nslot; p.rec = rec; p.dT = dT; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.produce = produce;
+  launch_col_tdj_sw<R, N>(c, B, stage, s, p, std::make_integer_sequence<int, 5>{});
 }
 
 inline int grid1d(long total, int threads = 256) {
@@ -329,6 +382,66 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "integrate_rk4");
   }
 
+  // Fixed-step RK4 / Lawson-RK6 / TDRK4 over `steps` steps from slot X_F of S43
+  // (h and e from fx_setup); 16-step CUDA graphs per scheme.
+  static int integrate_fx(ecs_ctx* c, int scheme, int B, long steps, cudaStream_t s) {
+    if (steps <= 0) return ECS_OK;
+    constexpr int GS = 16;
+    R* phys = nullptr;
+    const long pstride = (long)N * NPH * N;
+    if (scheme == FX_TD4) {
+      const int st = grow(c, &c->fxphys, &c->fxphys_bytes, (size_t)B * pstride * sizeof(R));
+      if (st) return st;
+      phys = (R*)c->fxphys;
+    }
+    const int nst = scheme == FX_RK6 ? 8 : 4;
+    auto one_step = [&](cudaStream_t st_, bool last) {
+      for (int q = 1; q <= nst; ++q) {
+        const int produce = (q == nst && last) ? 0 : 1;
+        if (scheme == FX_TD4 && (q == 2 || q == 4)) launch_row_tan<R, N>(c, B, phys, st_, pstride);   // jac(., k)
+        else launch_row_rhs<R, N>(c, B, st_, nullptr, phys, pstride);
+        launch_col_fx<R, N>(c, B, scheme, q, produce, st_);
+      }
+    };
+    auto& gk = c->gfx[scheme];
+    if (steps > GS && !(gk.exec && gk.B == B && gk.phys == (void*)phys)) {
+      if (gk.exec) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
+      const long long l0 = c->launches;
+      cudaGraph_t graph = nullptr;
+      std::lock_guard<std::mutex> capture_guard(capture_mutex());   // no set-up of another context meanwhile
+      cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int a = 0; a < GS; ++a) one_step(c->cap_stream, false);
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&gk.exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) { gk.exec = nullptr; return cuda_err(c, e, "fixed-step graph capture"); }
+      gk.nodes = c->launches - l0;
+      c->launches = l0;
+      gk.B = B; gk.phys = phys;
+    }
+    launch_col_fx<R, N>(c, B, scheme, 0, 1, s);
+    long it = 0;
+    while (steps - it > GS) {
+      cudaError_t e = cudaGraphLaunch(gk.exec, s);
+      if (e != cudaSuccess) return cuda_err(c, e, "fixed-step graph launch");
+      c->launches += gk.nodes;
+      it += GS;
+    }
+    for (; it < steps; ++it) one_step(s, it == steps - 1);
+    return cuda_err(c, cudaGetLastError(), "integrate_fx");
+  }
+
+  // modes whose right-hand side (or unmasked integrating factor) leaves the modes outside the box unchanged
+  static bool carry_mode(int mode) {
+    return mode == ECS_MODE_LAWSON_RK43 || mode == ECS_MODE_RK4 || mode == ECS_MODE_TDRK4;
+  }
+
+  static int fx_scheme(int mode) {
+    return mode == ECS_MODE_RK4 ? (int)FX_RK4 : mode == ECS_MODE_LAWSON_RK6 ? (int)FX_RK6 : (int)FX_TD4;
+  }
+
   static int rk4_setup(ecs_ctx* c, const double* T, int nc, int ms, int B, cudaStream_t s) {
     const long tot = (long)B * 2 * K * M;
     ++c->launches; k_rk4_setup<R><<<grid1d(tot), 256, 0, s>>>(T, nc, ms, c->ctl, (R*)c->Etab, N, c->nu, c->eta, B);
@@ -420,11 +533,30 @@ struct Impl {
   static int shoot(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
                    R* out_fields, double* loss, ecs_info* info, int B, cudaStream_t s) {
     const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
-    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43)
+    const bool fx = cfg->mode == ECS_MODE_RK4 || cfg->mode == ECS_MODE_LAWSON_RK6 || cfg->mode == ECS_MODE_TDRK4;
+    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43 && !fx)
       return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");   // loss_functions.py:86-88
     int st;
     const long VEC = 2L * K * M;
-    if (!rk43) {
+    // modes outside the box are carried unchanged by the adaptive stepper (unmasked
+    // integrating factor) and by RK4 / TDRK4 (masked right-hand side, no factor)
+    const bool carry = carry_mode(cfg->mode);
+    if (fx) {
+      if (cfg->num_checkpoints <= 0 || cfg->ministeps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+      const int scheme = fx_scheme(cfg->mode);
+      launch_row_to_box<R, N>(c, fields, (cplx<R>*)c->H, B, s);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->S43 + X_F * VEC, B, 2, s, S_NSLOT * VEC);
+      launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->V, B, 2, s);
+      ++c->launches;
+      k_fx_setup<R><<<grid1d((long)B * VEC), 256, 0, s>>>(T, cfg->num_checkpoints, cfg->ministeps, 6, c->ctl,
+                                                           (R*)c->Etab, N, c->nu, c->eta, B);
+      st = integrate_fx(c, scheme, B, (long)cfg->num_checkpoints * cfg->ministeps, s);
+      if (st) return st;
+      const cudaError_t e = cudaMemcpy2DAsync(c->F, VEC * sizeof(cplx<R>), (const cplx<R>*)c->S43 + X_F * VEC,
+                                              S_NSLOT * VEC * sizeof(cplx<R>), VEC * sizeof(cplx<R>), B,
+                                              cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return cuda_err(c, e, "fixed-step result");
+    } else if (!rk43) {
       if (cfg->num_checkpoints <= 0 || cfg->ministeps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
       st = to_box(c, fields, (cplx<R>*)c->F, B, s);
       if (st) return st;
@@ -440,13 +572,13 @@ struct Impl {
       if (st) return st;
     }
     R* out = out_fields ? out_fields : (R*)c->fields_tmp;
-    if (rk43) {   // modes outside the box are carried unchanged by the unmasked integrating factor
+    if (carry) {   // fields - irfft2(box(fields)): the modes outside the box
       launch_col_from_box<R, N>(c, (const cplx<R>*)c->V, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
       launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)c->fields_tmp2, fields, nullptr, B, 1, s);
     }
     launch_col_from_box<R, N>(c, (const cplx<R>*)c->F, (cplx<R>*)c->G, B, sx, cfg->shift_reflect_ny, cfg->rot, 1, 0, s);
     launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, out, fields, nullptr, B, 1, s);
-    if (rk43) {
+    if (carry) {
       const int odd = (cfg->shift_reflect_ny % 2 + 2) % 2 == 1;
       ++c->launches; k_sub_sym_phys<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>(out, (const R*)c->fields_tmp2, odd, cfg->rot, N, B);
     }
@@ -564,11 +696,111 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "record allocation");
   }
 
+  // TDRK4 linearisation (batch 1): the forward solve recording per step the
+  // start state, k1, a1, f_temp, k2, a2 (TR_NREC box vectors).
+  static int linearize_td(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                          R* out_fields, ecs_info* info, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
+    if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+    int st = lin_prologue(c, cfg, fields, T, sx, s);
+    if (!st) st = grow(c, &L.rec, &L.rec_bytes, (size_t)steps * TR_NREC * vb);
+    if (!st) st = grow(c, &c->fxphys, &c->fxphys_bytes, (size_t)N * NPH * N * sizeof(R));
+    if (st) return st;
+    cudaMemcpyAsync((cplx<R>*)c->S43 + X_F * VEC, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+    ++c->launches;
+    k_fx_setup<R><<<grid1d((long)VEC), 256, 0, s>>>(T, cfg->num_checkpoints, cfg->ministeps, 6, c->ctl, (R*)c->Etab, N,
+                                                    c->nu, c->eta, 1);
+    R* phys = (R*)c->fxphys;
+    cplx<R>* rec = (cplx<R>*)L.rec;
+    launch_col_fx<R, N>(c, 1, FX_TD4, 0, 1, s);
+    for (long it = 0; it < steps; ++it) {
+      cplx<R>* rs = rec + (size_t)it * TR_NREC * VEC;
+      for (int q = 1; q <= 4; ++q) {
+        if (q == 2 || q == 4) launch_row_tan<R, N>(c, 1, phys, s, 0);
+        else launch_row_rhs<R, N>(c, 1, s, nullptr, phys, 0);
+        launch_col_fx<R, N>(c, 1, FX_TD4, q, (q == 4 && it == steps - 1) ? 0 : 1, s, rs);
+      }
+    }
+    cudaMemcpyAsync(L.phi, (cplx<R>*)c->S43 + X_F * VEC, vb, cudaMemcpyDeviceToDevice, s);
+    L.seg = 0;
+    L.nrec = steps;
+    L.h = (double)(R)((L.T / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
+    L.acc.clear(); L.hs.clear();
+    if (info) { info->completed = 1; info->s = 1.0; info->accepted = (int)steps; info->rejected = 0; info->fevals = (int)(4 * steps); }
+    if (out_fields) {
+      st = residual(c, cfg, fields, (const cplx<R>*)L.phi, (const cplx<R>*)L.f0box, L.dsx, 1, out_fields, s, 1);
+      if (st) return st;
+    }
+    L.valid = 1;
+    return cuda_err(c, cudaGetLastError(), "linearize (TDRK4)");
+  }
+
+  // TDRK4 JVP sweep for B tangents (see kernels_fx.cuh for the tangent algebra):
+  // per step the primal's f and f_temp (with the mean field) and k1, k2 (without)
+  // are regenerated in chunks of steps and shared by the batch.
+  static int jvp_td(ecs_ctx* c, const R* dfields, const double* dT, const double* dsx, R* out, double* odT,
+                    double* odsx, int B, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const int nslot = (int)DT_NSLOT;
+    int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = grow(c, &c->Gx, &c->Gx_bytes, (size_t)B * NG * K * N * sizeof(cplx<R>));
+    if (!st) st = ensure_regen(c);
+    if (st) return st;
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)DT_F * VEC, B, 2, s, (long)nslot * VEC);
+    const long steps = L.nrec;
+    const long ci = (long)chunk_items();
+    const long CS = std::max(1L, std::min(64L, ci / 4));   // steps per regeneration chunk (4 items each)
+    // items: per chunk, the states [f, f_temp] of its steps, then the derivatives [k1, k2]
+    std::vector<long> items;
+    items.reserve((size_t)(4 * steps));
+    for (long a0 = 0; a0 < steps; a0 += CS) {
+      const long cnt = std::min(CS, steps - a0);
+      for (long it = a0; it < a0 + cnt; ++it) { items.push_back(it * TR_NREC + TR_F); items.push_back(it * TR_NREC + TR_FT); }
+      for (long it = a0; it < a0 + cnt; ++it) { items.push_back(it * TR_NREC + TR_K1); items.push_back(it * TR_NREC + TR_K2); }
+    }
+    st = upload_items(c, items, s);
+    if (st) return st;
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    const double dscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
+    const size_t pst = (size_t)N * NPH * N;
+    const cplx<R>* Ga = (const cplx<R>*)c->G;
+    const cplx<R>* Gb = (const cplx<R>*)c->Gx;
+    launch_col_tdj<R, N>(c, B, 0, 1, rec, dT, L.h, dscale, nslot, s);
+    for (long a0 = 0; a0 < steps; a0 += CS) {
+      const long cnt = std::min(CS, steps - a0);
+      R* P = (R*)c->Phys;
+      launch_regen<R, N>(c, rec, c->items + 4 * a0, (int)(2 * cnt), s, P, true);
+      launch_regen<R, N>(c, rec, c->items + 4 * a0 + 2 * cnt, (int)(2 * cnt), s, P + 2 * cnt * pst, false);
+      for (long it = a0; it < a0 + cnt; ++it) {
+        const cplx<R>* ra = rec + (size_t)it * TR_NREC * VEC;
+        const R* pf = P + (size_t)(2 * (it - a0)) * pst;
+        const R* pft = pf + pst;
+        const R* pk1 = P + (size_t)(2 * cnt + 2 * (it - a0)) * pst;
+        const R* pk2 = pk1 + pst;
+        launch_row_tan<R, N>(c, B, pf, s);                        // N'(f) df
+        launch_col_tdj<R, N>(c, B, 1, 1, ra, dT, L.h, dscale, nslot, s);
+        launch_row_tan2<R, N>(c, B, Ga, Gb, pf, pk1, s);          // N'(f) dk1 + N'(k1) df
+        launch_col_tdj<R, N>(c, B, 2, 1, ra, dT, L.h, dscale, nslot, s);
+        launch_row_tan<R, N>(c, B, pft, s);                       // N'(f_temp) dft
+        launch_col_tdj<R, N>(c, B, 3, 1, ra, dT, L.h, dscale, nslot, s);
+        launch_row_tan2<R, N>(c, B, Ga, Gb, pft, pk2, s);         // N'(f_temp) dk2 + N'(k2) dft
+        launch_col_tdj<R, N>(c, B, 4, it == steps - 1 ? 0 : 1, ra, dT, L.h, dscale, nslot, s);
+      }
+    }
+    return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
+  }
+
   static int linearize(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
                        R* out_fields, ecs_info* info, cudaStream_t s) {
     auto& L = c->lin;
     const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
-    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43) return set_err(c, ECS_ERR_BAD_MODE, "unknown integration mode");
+    if (cfg->mode == ECS_MODE_TDRK4) return linearize_td(c, cfg, fields, T, sx, out_fields, info, s);
+    if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43)
+      return set_err(c, ECS_ERR_BAD_MODE, "linearisation (JVP/VJP) supports Lawson_RK4, Lawson_RK43 and TDRK4");
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
     int st = lin_prologue(c, cfg, fields, T, sx, s);
     if (st) return st;
@@ -631,7 +863,7 @@ struct Impl {
   // out = base - irfft2(sym(Phi)) [- P_sym(base - irfft2(box(base))) in Lawson-RK4(3) mode]
   static int residual(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* base, const cplx<R>* phi, const cplx<R>* basebox,
                       const double* sx, int B, R* out, cudaStream_t s, int sx_shared) {
-    const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
+    const bool rk43 = carry_mode(cfg->mode);   // modes outside the box carried unchanged
     if (rk43) {
       launch_col_from_box<R, N>(c, basebox, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
       launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)c->fields_tmp2, base, nullptr, B, 1, s);
@@ -685,6 +917,7 @@ struct Impl {
                  int B, cudaStream_t s) {
     auto& L = c->lin;
     if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
+    if (L.mode == ECS_MODE_TDRK4) return jvp_td(c, dfields, dT, dsx, out, odT, odsx, B, s);
     const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
     const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
@@ -784,13 +1017,14 @@ struct Impl {
   static int jvp_finish(ecs_ctx* c, const R* dfields, const double* dsx, R* out, double* odT, double* odsx, int B,
                         cudaStream_t s) {
     auto& L = c->lin;
-    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4;
     const size_t VEC = 2UL * K * M;
-    const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
-    ++c->launches; k_tan_shift<R><<<grid1d((long)B * VEC), 256, 0, s>>>((const cplx<R>*)c->D + (size_t)(rk43 ? (int)S_X0 : (int)D_F) * VEC,
+    const int nslot = rk43 ? (int)S_NSLOT : td ? (int)DT_NSLOT : (int)D_NS4;
+    const int fslot = rk43 ? (int)S_X0 : td ? (int)DT_F : (int)D_F;
+    ++c->launches; k_tan_shift<R><<<grid1d((long)B * VEC), 256, 0, s>>>((const cplx<R>*)c->D + (size_t)fslot * VEC,
                                                          (long)nslot * VEC, (const cplx<R>*)L.phi, dsx,
                                                          (cplx<R>*)c->V, N, B);
-    if (rk43) {   // box(dfields) for the rest term
+    if (carry_mode(L.mode)) {   // box(dfields) for the rest term
       launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
       launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->OUT, B, 2, s);
     }
@@ -1118,6 +1352,73 @@ struct Impl {
     return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
   }
 
+  // TDRK4 adjoint sweep, last step first (see kernels_fx.cuh); the primal's
+  // f, f_temp (with the mean field) and k1, k2 are regenerated per chunk of steps.
+  static int vjp_td_sweep(ecs_ctx* c, int B, int nslot, cudaStream_t s) {
+    auto& L = c->lin;
+    const size_t VEC = 2UL * K * M;
+    int st = grow(c, &c->Gx, &c->Gx_bytes, (size_t)B * NHA * K * N * sizeof(cplx<R>));
+    if (st) return st;
+    const long steps = L.nrec;
+    const long ci = (long)chunk_items();
+    const long CS = std::max(1L, std::min(64L, ci / 4));
+    std::vector<long> items;
+    items.reserve((size_t)(4 * steps));
+    for (long a0 = 0; a0 < steps; a0 += CS) {
+      const long cnt = std::min(CS, steps - a0);
+      for (long it = a0; it < a0 + cnt; ++it) { items.push_back(it * TR_NREC + TR_F); items.push_back(it * TR_NREC + TR_FT); }
+      for (long it = a0; it < a0 + cnt; ++it) { items.push_back(it * TR_NREC + TR_K1); items.push_back(it * TR_NREC + TR_K2); }
+    }
+    st = upload_items(c, items, s);
+    if (st) return st;
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    const size_t pst = (size_t)N * NPH * N;
+    const double h = L.h;
+    auto col = [&](int stage, const cplx<R>* ra) {
+      ColTdaParams<R> p; p.Ha = (const cplx<R>*)c->H; p.Hb = (const cplx<R>*)c->Gx; p.G = (cplx<R>*)c->G;
+      p.J = (cplx<R>*)c->D; p.nslot = nslot; p.rec = ra; p.hacc = c->hacc; p.h = h; p.tw = (const cplx<R>*)c->tw;
+      p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B;
+      const int cols = B * K * 2;
+      const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+      switch (stage) {
+        case TA_SEED: launch_step(c, B, k_col_tda<R, N, TA_SEED>, g, bl, 0, s, p); break;
+        case TA_B: launch_step(c, B, k_col_tda<R, N, TA_B>, g, bl, 0, s, p); break;
+        case TA_C: launch_step(c, B, k_col_tda<R, N, TA_C>, g, bl, 0, s, p); break;
+        case TA_D: launch_step(c, B, k_col_tda<R, N, TA_D>, g, bl, 0, s, p); break;
+        default: launch_step(c, B, k_col_tda<R, N, TA_E>, g, bl, 0, s, p); break;
+      }
+    };
+    auto row2 = [&](const R* pa, const R* pb) {
+      RowAdj2Params<R> p; p.G = (const cplx<R>*)c->G; p.Ha = (cplx<R>*)c->H; p.Hb = (cplx<R>*)c->Gx;
+      p.phys_a = pa; p.phys_b = pb; p.tw = (const cplx<R>*)c->tw; p.B = B;
+      launch_step(c, B, k_row_adj2<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
+    };
+    const long nch = (steps + CS - 1) / CS;
+    for (long ch = nch - 1; ch >= 0; --ch) {
+      const long a0 = ch * CS, cnt = std::min(CS, steps - a0);
+      R* P = (R*)c->Phys;
+      launch_regen<R, N>(c, rec, c->items + 4 * a0, (int)(2 * cnt), s, P, true);
+      launch_regen<R, N>(c, rec, c->items + 4 * a0 + 2 * cnt, (int)(2 * cnt), s, P + 2 * cnt * pst, false);
+      for (long it = a0 + cnt - 1; it >= a0; --it) {
+        const cplx<R>* ra = rec + (size_t)it * TR_NREC * VEC;
+        const R* pf = P + (size_t)(2 * (it - a0)) * pst;
+        const R* pft = pf + pst;
+        const R* pk1 = P + (size_t)(2 * cnt + 2 * (it - a0)) * pst;
+        const R* pk2 = pk1 + pst;
+        col(TA_SEED, ra);
+        row2(pft, pk2);                      // N'(f_temp)^T, N'(k2)^T of h a2bar
+        col(TA_B, ra);
+        launch_row_adj<R, N>(c, B, pft, s);  // N'(f_temp)^T of h k2bar
+        col(TA_C, ra);
+        row2(pf, pk1);                       // N'(f)^T, N'(k1)^T of h a1bar
+        col(TA_D, ra);
+        launch_row_adj<R, N>(c, B, pf, s);   // N'(f)^T of h k1bar
+        col(TA_E, ra);
+      }
+    }
+    return cuda_err(c, cudaGetLastError(), "vjp (TDRK4)");
+  }
+
   // ---------------------------------------------------------------------
   // VJP of objective_RPO at the current linearisation for B cotangents.
   // ---------------------------------------------------------------------
@@ -1125,9 +1426,10 @@ struct Impl {
                  double* gsx, int B, cudaStream_t s) {
     auto& L = c->lin;
     if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
-    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4;
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
-    const int nslot = rk43 ? (int)JJ_NS43 : (int)J_NS4;
+    const int nslot = rk43 ? (int)JJ_NS43 : td ? (int)JT_NSLOT : (int)J_NS4;
+    const int fslot = rk43 ? (int)JJ_X0 : td ? (int)JT_F : (int)J_OB;   // cotangent of the final / initial state
     int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
     if (!st) st = ensure_regen(c);
     if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * 2 * sizeof(double));
@@ -1141,141 +1443,147 @@ struct Impl {
     const int odd = (L.cfg.shift_reflect_ny % 2 + 2) % 2 == 1;
     const double sy = (L.cfg.shift_reflect_ny * 2 * M_PI) / 8;
     ++c->launches; k_adj_head<R><<<B, 256, 0, s>>>((const cplx<R>*)c->V, (const cplx<R>*)L.phi, L.dsx, 1, sy, odd, L.cfg.rot,
-                                     (cplx<R>*)c->D + (size_t)(rk43 ? (int)JJ_X0 : (int)J_OB) * VEC, (long)nslot * VEC,
+                                     (cplx<R>*)c->D + (size_t)fslot * VEC, (long)nslot * VEC,
                                      gsx, N);
-    // regeneration plan (reverse order of use)
-    std::vector<long> items;
-    std::vector<long> item_of;
-    if (!rk43) {
-      for (long a = 0; a < L.nrec; ++a) {
-        item_of.push_back((long)items.size());
-        const long base = a * Q_NREC;
-        items.push_back(base + Q_F); items.push_back(base + Q_X2); items.push_back(base + Q_X3); items.push_back(base + Q_X4);
-      }
-    } else {
-      items.push_back(RR_X0);
-      for (long a = 0; a < L.nrec; ++a) {
-        if (!L.acc[a]) { item_of.push_back(-1); continue; }
-        item_of.push_back((long)items.size());
-        const long base = a * RR_NREC;
-        items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
-      }
-    }
-    st = upload_items(c, items, s);
-    if (st) return st;
-    const long ci = (long)chunk_items();
-    long chunk_lo = -1;
-    auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
-      if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
-        chunk_lo = std::max<long>(0, item - ci + 1);
-        const long cnt = std::min<long>(ci, (long)items.size() - chunk_lo);
-        launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + chunk_lo, (int)cnt, s);
-      }
-      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
-    };
-    const cplx<R>* rec = (const cplx<R>*)L.rec;
-    double tscale;
-    if (!rk43) {
+    double tscale = 1.0;
+    if (td) {
+      st = vjp_td_sweep(c, B, nslot, s);
+      if (st) return st;
       tscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
-      const double h = L.h;
-      const long kseg = L.seg ? L.seg : L.nrec;
-      const long nseg = (L.nrec + kseg - 1) / kseg;
-      // Checkpointed record: segment g-1 is recomputed (batch 1, on the primal
-      // stream with its own scratch, into the other of two record buffers)
-      // while the adjoint sweeps segment g on the caller's stream.
-      const bool pipe = L.seg && nseg > 1;
-      if (pipe) {
-        st = ensure_pipeline(c, kseg);
-        if (!st) st = grow(c, &L.rec2, &L.rec2_bytes, (size_t)kseg * Q_NREC * vb);
-        if (st) return st;
-        cudaError_t e = cudaEventRecord(c->pev[0], s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->pstream, c->pev[0], 0);
-        if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
-      }
-      void* bufs[2] = {L.rec, L.rec2};
-      auto recompute = [&](long g) -> cudaError_t {   // on the primal stream, into bufs[g & 1]
-        void* const Gs = c->G; void* const Hs = c->H;
-        c->G = c->Gp; c->H = c->Hp;
-        rk4_segment_record(c, g * kseg, std::min(kseg, L.nrec - g * kseg), c->pstream, bufs[g & 1]);
-        c->G = Gs; c->H = Hs;
-        return cudaEventRecord(c->pev[g & 1], c->pstream);
-      };
-      if (pipe) {
-        const cudaError_t e = recompute(nseg - 1);
-        if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
-      }
-      for (long g = nseg - 1; g >= 0; --g) {
-        const long a0 = g * kseg, cnt = std::min(kseg, L.nrec - a0);
-        const cplx<R>* rseg;
-        if (pipe) {
-          cudaError_t e = cudaSuccess;
-          if (g > 0) {   // the buffer of segment g-1 was last read by the adjoint of segment g+1
-            if (g + 1 < nseg) e = cudaStreamWaitEvent(c->pstream, c->tjoin[0][(g + 1) & 1], 0);
-            if (e == cudaSuccess) e = recompute(g - 1);
-          }
-          if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->pev[g & 1], 0);
-          if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
-          rseg = (const cplx<R>*)bufs[g & 1];
-        } else {
-          rseg = rk4_segment_record(c, a0, cnt, s);
-        }
-        std::vector<long> sitems;
-        for (long it = 0; it < cnt; ++it) {
-          const long base = it * Q_NREC;
-          sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
-        }
-        st = upload_items(c, sitems, s);
-        if (st) return st;
-        long slo = -1;
-        auto sphys = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
-          if (slo < 0 || item < slo || item >= slo + ci) {
-            slo = std::max<long>(0, item - ci + 1);
-            launch_regen<R, N>(c, rseg, c->items + slo, (int)std::min<long>(ci, (long)sitems.size() - slo), s);
-          }
-          return (const R*)c->Phys + (size_t)(item - slo) * N * NPH * N;
-        };
-        // seed the segment's last step from obar (J_OB)
-        launch_col_adj<R, N>(c, B, AJ_PRE, rseg + (size_t)(cnt - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
-        for (long it = cnt - 1; it >= 0; --it) {
-          const cplx<R>* ra = rseg + (size_t)it * Q_NREC * VEC;
-          const cplx<R>* rp = it > 0 ? rseg + (size_t)(it - 1) * Q_NREC * VEC : nullptr;
-          for (int k = 4; k >= 1; --k) {
-            launch_row_adj<R, N>(c, B, sphys(4 * it + (k - 1)), s);
-            launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
-          }
-        }
-        if (pipe) {   // the adjoint of segment g is done with bufs[g & 1]
-          const cudaError_t e = cudaEventRecord(c->tjoin[0][g & 1], s);
-          if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
-        }
-      }
     } else {
-      tscale = 1.0;
-      const double t = L.T;
-      for (long a = L.nrec - 1; a >= 0; --a) {
-        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
-        const double h = L.hs[a];
-        if (!L.acc[a]) {
-          const int cols = B * K;
-          ++c->launches; k_adj_reject<R><<<(cols + 3) / 4, 128, 0, s>>>((cplx<R>*)c->D, nslot, ra, c->hacc, t, h, (R)c->nu, (R)c->eta, N, B);
-          continue;
+      // regeneration plan (reverse order of use)
+      std::vector<long> items;
+      std::vector<long> item_of;
+      if (!rk43) {
+        for (long a = 0; a < L.nrec; ++a) {
+          item_of.push_back((long)items.size());
+          const long base = a * Q_NREC;
+          items.push_back(base + Q_F); items.push_back(base + Q_X2); items.push_back(base + Q_X3); items.push_back(base + Q_X4);
         }
-        launch_col_adj<R, N>(c, B, AJ43_PRE, ra, nullptr, t, h, nslot, s);
-        for (int k = 3; k >= 0; --k) {
-          launch_row_adj<R, N>(c, B, phys_of(item_of[a] + k), s);
-          launch_col_adj<R, N>(c, B, AJ43_S2 + k, ra, nullptr, t, h, nslot, s);
+      } else {
+        items.push_back(RR_X0);
+        for (long a = 0; a < L.nrec; ++a) {
+          if (!L.acc[a]) { item_of.push_back(-1); continue; }
+          item_of.push_back((long)items.size());
+          const long base = a * RR_NREC;
+          items.push_back(base + RR_Y2); items.push_back(base + RR_Y3); items.push_back(base + RR_Y4); items.push_back(base + RR_XF);
         }
       }
-      launch_col_adj<R, N>(c, B, AJ43_IPRE, rec, nullptr, t, 0.0, nslot, s);
-      launch_row_adj<R, N>(c, B, phys_of(0), s);
-      launch_col_adj<R, N>(c, B, AJ43_INIT, rec, nullptr, t, 0.0, nslot, s);
+      st = upload_items(c, items, s);
+      if (st) return st;
+      const long ci = (long)chunk_items();
+      long chunk_lo = -1;
+      auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
+        if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+          chunk_lo = std::max<long>(0, item - ci + 1);
+          const long cnt = std::min<long>(ci, (long)items.size() - chunk_lo);
+          launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + chunk_lo, (int)cnt, s);
+        }
+        return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
+      };
+      const cplx<R>* rec = (const cplx<R>*)L.rec;
+      if (!rk43) {
+        tscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
+        const double h = L.h;
+        const long kseg = L.seg ? L.seg : L.nrec;
+        const long nseg = (L.nrec + kseg - 1) / kseg;
+        // Checkpointed record: segment g-1 is recomputed (batch 1, on the primal
+        // stream with its own scratch, into the other of two record buffers)
+        // while the adjoint sweeps segment g on the caller's stream.
+        const bool pipe = L.seg && nseg > 1;
+        if (pipe) {
+          st = ensure_pipeline(c, kseg);
+          if (!st) st = grow(c, &L.rec2, &L.rec2_bytes, (size_t)kseg * Q_NREC * vb);
+          if (st) return st;
+          cudaError_t e = cudaEventRecord(c->pev[0], s);
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(c->pstream, c->pev[0], 0);
+          if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
+        }
+        void* bufs[2] = {L.rec, L.rec2};
+        auto recompute = [&](long g) -> cudaError_t {   // on the primal stream, into bufs[g & 1]
+          void* const Gs = c->G; void* const Hs = c->H;
+          c->G = c->Gp; c->H = c->Hp;
+          rk4_segment_record(c, g * kseg, std::min(kseg, L.nrec - g * kseg), c->pstream, bufs[g & 1]);
+          c->G = Gs; c->H = Hs;
+          return cudaEventRecord(c->pev[g & 1], c->pstream);
+        };
+        if (pipe) {
+          const cudaError_t e = recompute(nseg - 1);
+          if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
+        }
+        for (long g = nseg - 1; g >= 0; --g) {
+          const long a0 = g * kseg, cnt = std::min(kseg, L.nrec - a0);
+          const cplx<R>* rseg;
+          if (pipe) {
+            cudaError_t e = cudaSuccess;
+            if (g > 0) {   // the buffer of segment g-1 was last read by the adjoint of segment g+1
+              if (g + 1 < nseg) e = cudaStreamWaitEvent(c->pstream, c->tjoin[0][(g + 1) & 1], 0);
+              if (e == cudaSuccess) e = recompute(g - 1);
+            }
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->pev[g & 1], 0);
+            if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
+            rseg = (const cplx<R>*)bufs[g & 1];
+          } else {
+            rseg = rk4_segment_record(c, a0, cnt, s);
+          }
+          std::vector<long> sitems;
+          for (long it = 0; it < cnt; ++it) {
+            const long base = it * Q_NREC;
+            sitems.push_back(base + Q_F); sitems.push_back(base + Q_X2); sitems.push_back(base + Q_X3); sitems.push_back(base + Q_X4);
+          }
+          st = upload_items(c, sitems, s);
+          if (st) return st;
+          long slo = -1;
+          auto sphys = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
+            if (slo < 0 || item < slo || item >= slo + ci) {
+              slo = std::max<long>(0, item - ci + 1);
+              launch_regen<R, N>(c, rseg, c->items + slo, (int)std::min<long>(ci, (long)sitems.size() - slo), s);
+            }
+            return (const R*)c->Phys + (size_t)(item - slo) * N * NPH * N;
+          };
+          // seed the segment's last step from obar (J_OB)
+          launch_col_adj<R, N>(c, B, AJ_PRE, rseg + (size_t)(cnt - 1) * Q_NREC * VEC, nullptr, 0.0, h, nslot, s);
+          for (long it = cnt - 1; it >= 0; --it) {
+            const cplx<R>* ra = rseg + (size_t)it * Q_NREC * VEC;
+            const cplx<R>* rp = it > 0 ? rseg + (size_t)(it - 1) * Q_NREC * VEC : nullptr;
+            for (int k = 4; k >= 1; --k) {
+              launch_row_adj<R, N>(c, B, sphys(4 * it + (k - 1)), s);
+              launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, h, nslot, s);
+            }
+          }
+          if (pipe) {   // the adjoint of segment g is done with bufs[g & 1]
+            const cudaError_t e = cudaEventRecord(c->tjoin[0][g & 1], s);
+            if (e != cudaSuccess) return cuda_err(c, e, "segment recomputation");
+          }
+        }
+      } else {
+        tscale = 1.0;
+        const double t = L.T;
+        for (long a = L.nrec - 1; a >= 0; --a) {
+          const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
+          const double h = L.hs[a];
+          if (!L.acc[a]) {
+            const int cols = B * K;
+            ++c->launches; k_adj_reject<R><<<(cols + 3) / 4, 128, 0, s>>>((cplx<R>*)c->D, nslot, ra, c->hacc, t, h, (R)c->nu, (R)c->eta, N, B);
+            continue;
+          }
+          launch_col_adj<R, N>(c, B, AJ43_PRE, ra, nullptr, t, h, nslot, s);
+          for (int k = 3; k >= 0; --k) {
+            launch_row_adj<R, N>(c, B, phys_of(item_of[a] + k), s);
+            launch_col_adj<R, N>(c, B, AJ43_S2 + k, ra, nullptr, t, h, nslot, s);
+          }
+        }
+        launch_col_adj<R, N>(c, B, AJ43_IPRE, rec, nullptr, t, 0.0, nslot, s);
+        launch_row_adj<R, N>(c, B, phys_of(0), s);
+        launch_col_adj<R, N>(c, B, AJ43_INIT, rec, nullptr, t, 0.0, nslot, s);
+      }
     }
     // tail: gfields = c_fields + to_box^T(fbar0) [- (I - proj) P_sym c_fields] + phase terms
     ++c->launches; k_box_to_fields_adj<R><<<grid1d((long)B * VEC), 256, 0, s>>>(
-        (const cplx<R>*)c->D + (size_t)(rk43 ? (int)JJ_X0 : (int)J_OB) * VEC, (long)nslot * VEC, (cplx<R>*)c->V, N, B);
+        (const cplx<R>*)c->D + (size_t)fslot * VEC, (long)nslot * VEC, (cplx<R>*)c->V, N, B);
     launch_col_from_box<R, N>(c, (const cplx<R>*)c->V, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
     launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, gfields, cfields, nullptr, B, 2, s);
-    if (rk43) {
+    if (carry_mode(L.mode)) {
       // tmp = P_sym c  (k_sub_sym_phys computes out -= P_sym(rest); start from zero)
       cudaMemsetAsync(c->fields_tmp, 0, (size_t)B * 2 * N * N * sizeof(R), s);
       ++c->launches; k_sub_sym_phys<R><<<grid1d((long)B * 2 * N * N), 256, 0, s>>>((R*)c->fields_tmp, cfields, odd, L.cfg.rot, N, B);

@@ -302,6 +302,8 @@ template <typename R>
 struct RowParams {
   const cplx<R>* G;   // [B][NG][K][N]
   cplx<R>* H;         // [B][NH][K][N]
+  R* phys;            // optional record of u, v, B_x, B_y: phys + b * phys_bstride is [N][NPH][N]
+  long phys_bstride;
   const StepCtl* ctl; // per-batch control (done flags) or null
   const cplx<R>* tw;
   R b0x, b0y;
@@ -425,10 +427,15 @@ __global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
   }
   fft_dif2<R, N, true>(uv, bb, s_tw, lane);
   cplx<R> W[E];
+  R* ph = p.phys ? p.phys + (size_t)b * p.phys_bstride + (size_t)(x0 + w) * NPH * N : nullptr;
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const R u = uv[j].x, v = uv[j].y;
     const R bx = bb[j].x + p.b0x, by = bb[j].y + p.b0y;
+    if (ph) {
+      const int e = lane + 32 * j;
+      ph[e] = u; ph[N + e] = v; ph[2 * N + e] = bx; ph[3 * N + e] = by;
+    }
     W[j] = mk<R>((u - v) * (u + v) - (bx - by) * (bx + by), bx * by - u * v);   // (P1, P2)
     bb[j] = mk<R>(u * by - v * bx, R(0));                                       // (P3, 0), mhd_jax.py:163
   }

@@ -100,7 +100,8 @@ template <typename R>
 struct RowTanParams {
   const cplx<R>* G;     // tangent [B][NG][K][N]
   cplx<R>* H;           // tangent [B][NH][K][N]
-  const R* phys;        // primal physical fields of this stage: [N][NPH][N]
+  const R* phys;        // primal physical fields of this stage: phys + b * phys_bstride is [N][NPH][N]
+  long phys_bstride;    // 0: one primal shared by the batch
   const cplx<R>* tw;
   int B;
 };
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   pdl_wait();
   // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
   // the tile load and the inverse transforms
-  const R* ph = phys_row<R, N>(p.phys, x);
+  const R* ph = phys_row<R, N>(p.phys + (size_t)b * p.phys_bstride, x);
   R pu[E], pv[E], pbx[E], pby[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {

@@ -131,7 +131,7 @@ int na_state_vel(unsigned char* base, double nu, double eta, double b0x, double 
   const int cols = B * K * 2;   // one warp per (batch, ky, channel)
   k_col_rk4<double, N, COL_START><<<(cols + 3) / 4, 128, 0, s>>>(cp);
   RowParams<double> rp;
-  rp.G = G; rp.H = H; rp.ctl = nullptr;
+  rp.G = G; rp.H = H; rp.ctl = nullptr; rp.phys = nullptr; rp.phys_bstride = 0;
   rp.tw = tw; rp.b0x = b0x; rp.b0y = b0y; rp.B = B;
   k_row_rhs<double, N, NA_XT><<<B * (N / NA_XT), NA_XT * 32, na_smem_rhs<N>(), s>>>(rp);
   cp.stage = COL_PLAIN; cp.produce = 0; cp.diss = diss;

@@ -12,7 +12,8 @@ import torch
 from . import _lib
 from . import context as _ctx
 
-MODES = {"Lawson_RK4": _lib.ECS_MODE_LAWSON_RK4, "Lawson_RK43": _lib.ECS_MODE_LAWSON_RK43}
+MODES = {"Lawson_RK4": _lib.ECS_MODE_LAWSON_RK4, "Lawson_RK43": _lib.ECS_MODE_LAWSON_RK43,
+         "RK4": _lib.ECS_MODE_RK4, "Lawson_RK6": _lib.ECS_MODE_LAWSON_RK6, "TDRK4": _lib.ECS_MODE_TDRK4}
 
 
 def shoot_cfg(param_dict, mode):
@@ -24,6 +25,8 @@ def shoot_cfg(param_dict, mode):
     c.mode = MODES[mode]
     c.num_checkpoints = int(param_dict.get("num_checkpoints", 1))
     c.ministeps = int(param_dict.get("ministeps", param_dict.get("steps", 1)))
+    if mode == "Lawson_RK6":   # one run of param_dict["steps"] steps over T (loss_functions.py:66-71)
+        c.num_checkpoints, c.ministeps = 1, int(param_dict["steps"])
     c.shift_reflect_ny = int(param_dict.get("shift_reflect_ny", 0))
     c.rot = int(bool(param_dict.get("rot", False)))
     ad = param_dict.get("adaptive_dict", {}) or {}

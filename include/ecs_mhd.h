@@ -40,8 +40,12 @@ enum {
   ECS_ERR_TOO_LARGE = 7      /* beyond the fixed scratch of ecs_state_vel_noalloc */
 };
 
-/* Integration modes of mismatch_RPO (jax_scripts/lib/loss_functions.py:48-88). */
-enum { ECS_MODE_LAWSON_RK4 = 1, ECS_MODE_LAWSON_RK43 = 2 };
+/* Integration modes of mismatch_RPO (jax_scripts/lib/loss_functions.py:48-88):
+ * Lawson_RK4 :57-65, Lawson_RK43 :72-77, RK4 (classic, dissipation in the
+ * right-hand side) :49-56, Lawson_RK6 (num_checkpoints = 1, ministeps =
+ * param_dict["steps"]) :66-71, TDRK4 (two-derivative RK4) :78-85. */
+enum { ECS_MODE_LAWSON_RK4 = 1, ECS_MODE_LAWSON_RK43 = 2, ECS_MODE_RK4 = 3, ECS_MODE_LAWSON_RK6 = 4,
+       ECS_MODE_TDRK4 = 5 };
 
 typedef struct {
   double nu, eta;          /* param_dict["nu"], ["eta"] */

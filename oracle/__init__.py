@@ -2,7 +2,8 @@
 
 This package restates, on the CPU and in FP64, the reference algorithm of
 mgolden30/ECS_MHD_2D for the pseudo-spectral 2D MHD right-hand side, the
-Lawson-RK4 and adaptive Lawson-RK4(3) steppers, the symmetry operations, the RPO
+steppers of every shooting mode (RK4, Lawson-RK4, Lawson-RK6, TDRK4 and the
+adaptive Lawson-RK4(3)), the symmetry operations, the RPO
 shooting objective/loss and their tangent (JVP) and adjoint (VJP).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
@@ -22,8 +23,8 @@ XLA/DUCC/cuFFT.
 
 from .mhd_oracle import (  # noqa: F401
     NUMPY, TORCH, Backend,
-    construct_domain, dissipation, state_vel,
-    rk4, lawson_rk4, lawson_rk43,
+    construct_domain, dissipation, state_vel, state_vel_jvp,
+    rk4, lawson_rk4, lawson_rk6, tdrk4, lawson_rk43,
     shift_x, shift_reflect, rot180,
     mismatch_RPO, loss_RPO, phase_conditions, objective_RPO,
     make_param_dict, ravel_dict, unravel_dict,

@@ -185,6 +185,43 @@ def state_vel(fields, param_dict, include_dissipation, xp: Backend = NUMPY):
     return dfdt
 
 
+def state_vel_jvp(fields, tangent, param_dict, include_dissipation, xp: Backend = NUMPY):
+    """Forward-mode derivative of ``state_vel`` (mhd_jax.py:105-175) at `fields`
+    along `tangent` -- what ``jax.jvp(v_fn, (f,), (k,))`` evaluates inside tdrk4
+    (timestepping.py:133).  The product rule applied to the statements of
+    state_vel: the mean field b0 and the forcing are constants, every other
+    factor is linear in the input."""
+    kx = param_dict["kx"]
+    ky = param_dict["ky"]
+    mask = param_dict["mask"]
+    to_u = param_dict["to_u"]
+    to_v = param_dict["to_v"]
+    b0 = param_dict["b0"]
+    fx = xp.irfft2(1j * kx * fields)                                 # :136
+    fy = xp.irfft2(1j * ky * fields)                                 # :137
+    fu = xp.irfft2(1j * to_u * fields)                               # :140
+    fv = xp.irfft2(1j * to_v * fields)                               # :141
+    bx = xp.reshape(xp.asarray(np.array([0.0, float(b0[0])]), fx.dtype), (2, 1, 1))  # :145
+    by = xp.reshape(xp.asarray(np.array([0.0, float(b0[1])]), fx.dtype), (2, 1, 1))  # :146
+    fu = fu + bx                                                     # :148
+    fv = fv + by
+    dx = xp.irfft2(1j * kx * tangent)
+    dy = xp.irfft2(1j * ky * tangent)
+    du = xp.irfft2(1j * to_u * tangent)
+    dv = xp.irfft2(1j * to_v * tangent)
+    dadv = fu * dx + du * fx + fv * dy + dv * fy                     # d(:152)
+    k_sq = (kx * kx + ky * ky) * mask                                # :154
+    dwdt = -dadv[..., 0, :, :] + dadv[..., 1, :, :]                  # d(:159), forcing constant
+    dwdt = mask * xp.rfft2(dwdt)                                     # :160
+    djdt = (fu[..., 0, :, :] * dv[..., 1, :, :] + du[..., 0, :, :] * fv[..., 1, :, :]
+            - fv[..., 0, :, :] * du[..., 1, :, :] - dv[..., 0, :, :] * fu[..., 1, :, :])  # d(:163)
+    djdt = k_sq * xp.rfft2(djdt)                                     # :164
+    dfdt = xp.concatenate([xp.expand_dims(dwdt, -3), xp.expand_dims(djdt, -3)], -3)
+    if include_dissipation:                                          # :171
+        dfdt = dfdt + dissipation(param_dict, xp) * tangent
+    return dfdt
+
+
 # ---------------------------------------------------------------------------
 # timestepping.py
 # ---------------------------------------------------------------------------
@@ -215,6 +252,47 @@ def lawson_rk4(f, t, steps, v_fn, L_diag, mask=None, xp: Backend = NUMPY):
         f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3             # :78
         k4 = h * v_fn(f + k3)                                        # :79
         f = f + k1 / 6 + k2 / 3 + k3 / 3 + k4 / 6                    # :80
+    return f
+
+
+def lawson_rk6(f, t, steps, v_fn, L_diag, mask=None, xp: Backend = NUMPY):
+    """Lawson integrating-factor sixth-order RK; restates timestepping.py:83-125
+    statement by statement (e = exp(h/6 L), applied after every stage)."""
+    h = t / steps                                                    # :105
+    e = xp.exp(h / 6 * L_diag)                                       # :106
+    if mask is not None:
+        e = e * mask                                                 # :108
+    for _ in range(steps):                                           # :125
+        k1 = h * v_fn(f)                                             # :110
+        f = e * f; k1 = e * k1                                       # :111
+        k2 = h * v_fn(f + k1 / 6)                                    # :112
+        k3 = h * v_fn(f + k1 / 12 + k2 / 12)                         # :113
+        f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3             # :114
+        k4 = h * v_fn(f - k2 * 4 / 33 + k3 * 5 / 11)                 # :115
+        f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3; k4 = e * k4   # :116
+        k5 = h * v_fn(f - k1 / 4 - k2 * 29 / 44 + k3 * 31 / 22)      # :117
+        f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3; k4 = e * k4; k5 = e * k5   # :118
+        k6 = h * v_fn(f + k1 * 3 / 11 + k2 * 8 / 33 - k3 * 4 / 11 + k4 / 11 + k5 * 14 / 33)   # :119
+        f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3; k4 = e * k4; k5 = e * k5; k6 = e * k6   # :120
+        k7 = h * v_fn(f - k1 * 17 / 48 - k2 * 5 / 12 + k3 + k4 - k5 * 13 / 12 + k6 * 11 / 16)   # :121
+        f = e * f; k1 = e * k1; k2 = e * k2; k3 = e * k3; k4 = e * k4; k5 = e * k5; k6 = e * k6; k7 = e * k7  # :122
+        k8 = h * v_fn(f + k1 * 20 / 39 + k2 * 12 / 39 - k3 * 31 / 39 - k4 / 39 + k5 * 34 / 39
+                      - k6 * 11 / 39 + k7 * 16 / 39)                 # :123
+        f = f + 13 / 200 * (k1 + k8) + 4 / 25 * (k3 + k7) + 11 / 40 * (k4 + k6)   # :124
+    return f
+
+
+def tdrk4(f, t, steps, v_fn, jac_fn):
+    """Two-derivative RK4; restates timestepping.py:127-149.  jac_fn(f, k) is the
+    Jacobian-vector product of v_fn at f along k (jax.jvp at :133)."""
+    h = t / steps                                                    # :132
+    for _ in range(steps):                                           # :148
+        k1 = h * v_fn(f)                                             # :137
+        a1 = h * jac_fn(f, k1)                                       # :138
+        f_temp = f + k1 / 2 + a1 / 8                                 # :140
+        k2 = h * v_fn(f_temp)                                        # :141
+        a2 = h * jac_fn(f_temp, k2)                                  # :142
+        f = f + k1 + a1 / 6 + a2 / 3                                 # :144
     return f
 
 
@@ -308,8 +386,8 @@ def rot180(f, xp: Backend = NUMPY):
 # ---------------------------------------------------------------------------
 
 def mismatch_RPO(input_dict, param_dict, mode, xp: Backend = NUMPY):
-    """Restates ``mismatch_RPO`` (loss_functions.py:9-96) for the RK4, Lawson_RK4
-    and Lawson_RK43 modes.  Returns (f0, f, info)."""
+    """Restates ``mismatch_RPO`` (loss_functions.py:9-96) for all five modes
+    (RK4, Lawson_RK4, Lawson_RK6, Lawson_RK43, TDRK4).  Returns (f0, f, info)."""
     f0 = input_dict["fields"]
     T = input_dict["T"]
     sx = input_dict["sx"]
@@ -329,6 +407,22 @@ def mismatch_RPO(input_dict, param_dict, mode, xp: Backend = NUMPY):
         f = f0
         for _ in range(nc):
             f = lawson_rk4(f, T / nc, ms, v_fn, L_diag, mask=param_dict["mask"], xp=xp)
+        info = None
+    elif mode == "Lawson_RK6":                                       # :66-71
+        v_fn = lambda f: state_vel(f, param_dict, False, xp)
+        L_diag = dissipation(param_dict, xp)
+        f = lawson_rk6(f0, T, int(param_dict["steps"]), v_fn, L_diag, mask=param_dict["mask"], xp=xp)
+        info = None
+    elif mode == "TDRK4":                                            # :78-85
+        nc, ms = int(param_dict["num_checkpoints"]), int(param_dict["ministeps"])
+        v_fn = lambda f: state_vel(f, param_dict, True, xp)
+        if xp is TORCH:   # jax.jvp of v_fn (timestepping.py:133)
+            jac_fn = lambda f, k: torch.func.jvp(v_fn, (f,), (k,))[1]
+        else:             # the same derivative written out (product rule of state_vel)
+            jac_fn = lambda f, k: state_vel_jvp(f, k, param_dict, True, xp)
+        f = f0
+        for _ in range(nc):
+            f = tdrk4(f, T / nc, ms, v_fn, jac_fn)
         info = None
     elif mode == "Lawson_RK43":                                      # :72-77
         vel_fn = lambda f: state_vel(f, param_dict, False, xp)

@@ -8,9 +8,13 @@
    reference's physics: RHS, forcing sign, dissipation, symmetries.
 2. Synthetic seeded cases at n=64 computed by the oracle (synthetic_n64.npz):
    state_vel, 64 Lawson-RK4 steps, objective and loss.
+3. Closure of all fifteen reference solutions under each fixed-step mode
+   (closure_modes.json: Lawson_RK4, TDRK4, RK4).  The reference does not store
+   which integrator converged a solution; the mode that closes one to rounding
+   level is the one it was converged with, which pins that mode's oracle.
 
 Run from the repository root (needs the reference checkout):
-    python tests/golden/make_golden.py /path/to/reference
+    python tests/golden/make_golden.py /path/to/reference [modes]
 """
 
 import json
@@ -79,7 +83,27 @@ def synthetic():
                         objective=obj["fields"], loss=loss)
 
 
+def closure_by_mode(ref, modes=("Lawson_RK4", "TDRK4", "RK4")):
+    rec = {}
+    for sub in ["Re40", "Re50"]:
+        for fn in sorted(os.listdir(os.path.join(ref, "solutions", sub))):
+            name = f"{sub}/{fn[:-4]}"
+            d = np.load(os.path.join(ref, "solutions", sub, fn), allow_pickle=True)
+            pd = param_dict_from(d)
+            inp = {"fields": d["fields"], "T": float(d["T"]), "sx": float(d["sx"])}
+            rec[name] = {"n": int(d["fields"].shape[-1]), "steps": int(d["steps"])}
+            for mode in modes:
+                out = O.objective_RPO(inp, pd, mode)
+                rec[name][mode] = float(np.linalg.norm(out["fields"]) / np.linalg.norm(d["fields"]))
+            print(name, rec[name], flush=True)
+    with open(os.path.join(HERE, "closure_modes.json"), "w") as f:
+        json.dump(rec, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    synthetic()
-    solutions(ref)
+    if len(sys.argv) > 2 and sys.argv[2] == "modes":
+        closure_by_mode(ref)
+    else:
+        synthetic()
+        solutions(ref)

@@ -86,3 +86,56 @@ def test_symmetry_equivariance(ny, rot):
     a = g(O.lawson_rk4(f0, 0.05, 10, v, L, pd["mask"]))
     b = O.lawson_rk4(g(f0), 0.05, 10, v, L, pd["mask"])
     assert rel_l2(np.fft.irfft2(a), np.fft.irfft2(b)) < 1e-12
+
+
+def test_lawson_rk6_sixth_order():
+    """Lawson_RK6 (timestepping.py:83-125) converges at order ~6."""
+    n = 64
+    pd = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+")
+    f0 = np.fft.rfft2(initial_condition(0, n, amp=3.0))
+    v = lambda f: O.state_vel(f, pd, False)
+    L = O.dissipation(pd)
+    t = 0.2
+    fine = O.lawson_rk6(f0, t, 256, v, L, pd["mask"])
+    steps = np.array([16, 24, 32])
+    err = [np.linalg.norm(np.fft.irfft2(O.lawson_rk6(f0, t, int(s), v, L, pd["mask"]) - fine)) for s in steps]
+    slope = np.polyfit(np.log(steps), np.log(err), 1)[0]
+    assert -7.0 < slope < -5.0, err
+
+
+def test_state_vel_jvp_matches_autodiff():
+    """The written-out forward derivative of state_vel equals torch.func.jvp of
+    its torch restatement (the two stand-ins for jax.jvp in tdrk4)."""
+    n = 64
+    pn = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+")
+    pt = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", xp=O.TORCH)
+    f = np.fft.rfft2(initial_condition(2, n))
+    k = np.fft.rfft2(initial_condition(3, n, amp=1.0))
+    for diss in (False, True):
+        a = O.state_vel_jvp(f, k, pn, diss)
+        b = torch.func.jvp(lambda x: O.state_vel(x, pt, diss, O.TORCH), (torch.from_numpy(f),),
+                           (torch.from_numpy(k),))[1].numpy()
+        assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
+
+
+def test_tdrk4_fourth_order_and_backends_agree():
+    """TDRK4 (timestepping.py:127-149) converges at order ~4; the numpy and torch
+    restatements agree."""
+    n = 64
+    kw = dict(num_checkpoints=1, ministeps=16, shift_reflect_ny=0, rot=False)
+    pd = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    f0 = np.fft.rfft2(initial_condition(0, n))
+    v = lambda f: O.state_vel(f, pd, True)
+    jac = lambda f, k: O.state_vel_jvp(f, k, pd, True)
+    t = 0.1
+    fine = O.tdrk4(f0, t, 512, v, jac)
+    steps = np.array([32, 64, 128])
+    err = [np.linalg.norm(np.fft.irfft2(O.tdrk4(f0, t, int(s), v, jac) - fine)) for s in steps]
+    slope = np.polyfit(np.log(steps), np.log(err), 1)[0]
+    assert -4.7 < slope < -3.3, err
+    pt = O.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", xp=O.TORCH, **kw)
+    u0 = initial_condition(4, n)
+    a = O.objective_RPO({"fields": u0, "T": 0.1, "sx": 0.2}, pd, "TDRK4")["fields"]
+    b = O.objective_RPO({"fields": torch.from_numpy(u0), "T": torch.tensor(0.1, dtype=torch.float64),
+                         "sx": torch.tensor(0.2, dtype=torch.float64)}, pt, "TDRK4", xp=O.TORCH)["fields"]
+    assert rel_l2(b.detach().numpy(), a) < 1e-13
