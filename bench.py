@@ -216,6 +216,19 @@ def plain_vs_batched(E, torch, dev, flush, prim, tan):
             "speedup_batch_vs_plain": (B / tb) * tb1}
 
 
+def tdrk4_matvecs(E, torch, dev, flush, prim, tan):
+    """Matvecs in TDRK4 mode (the reference Newton driver's default,
+    jax_scripts/newton.py:70) on the same base point and tangents: 40 x 32 fixed
+    steps over T=4.6, linearisation included, 64 tangents per batch."""
+    pd = E.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", num_checkpoints=40, ministeps=32,
+                           shift_reflect_ny=0, rot=False)
+    obj = E.Objective(pd, "TDRK4")
+    t, o = _timed(torch, flush, lambda: obj.linearize_jvp(prim, tan)[1])
+    B = tan["fields"].shape[0]
+    return {"matvecs_per_s": B / t, "seconds": t, "steps": 1280, "batch": B,
+            "finite": bool(torch.isfinite(o["fields"]).all())}
+
+
 def cpu_baseline(target_s=12.0, attempts_full=None):
     """The oracle (torch-CPU restatement, torch.func.jvp) on the host cores for a
     bounded sample: the first k attempts of the same adaptive JVP, scaled to one
@@ -484,6 +497,7 @@ def main():
     secondary = secondary_workloads(E, torch, dev, flush) if not args.no_secondary else {}
     if not args.no_secondary:
         secondary["config1_plain_vs_batched"] = plain_vs_batched(E, torch, dev, flush, prim, tan)
+        secondary["tdrk4_matvec_n128_f64"] = tdrk4_matvecs(E, torch, dev, flush, prim, tan)
 
     if rank == 0:
         clocks = clk.summary()

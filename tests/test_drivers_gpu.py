@@ -63,3 +63,21 @@ def test_mixed_precision_newton_tracks_fp64(cuda):
     for a, b in zip(r32[:2], [h["rel_err"] for h in h64]):
         assert abs(a - b) <= 0.02 * b, (h32, h64)
     assert abs(r32[-1] - e64) <= 0.02 * e64, (r32, e64)
+
+
+def test_newton_gmres_tdrk4_reference_default(cuda):
+    """The reference Newton driver's default configuration (mode "TDRK4",
+    use_transpose=True; jax_scripts/newton.py:70, :151-215) on the reference's
+    TW1 -- converged with TDRK4 -- perturbed off the orbit: one step shrinks
+    the residual sharply."""
+    d = np.load("tests/golden/solution_Re40_TW1.npz")
+    n = d["fields"].shape[-1]
+    pd = E.make_param_dict(n, float(d["nu"]), float(d["eta"]), b0=d["b0"], forcing="kolmogorov",
+                           num_checkpoints=int(d["num_checkpoints"]), ministeps=int(d["ministeps"]),
+                           shift_reflect_ny=int(d["shift_reflect_ny"]), rot=bool(d["rot"]))
+    u = torch.as_tensor(d["fields"] + 1e-4 * initial_condition(98, n, amp=1.0), device="cuda")
+    x = {"fields": E.dealias(u, pd), "T": float(d["T"]) * (1 + 1e-4), "sx": float(d["sx"])}
+    f0 = float(torch.linalg.norm(E.objective_RPO(x, pd, "TDRK4")["fields"]))
+    new, st = drivers.newton_gmres_update(x, pd, "TDRK4", inner=16, use_transpose=True)
+    f1 = float(torch.linalg.norm(E.objective_RPO(new, pd, "TDRK4")["fields"]))
+    assert f1 < 0.1 * f0, (f0, f1, st)
