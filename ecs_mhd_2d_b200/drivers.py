@@ -139,3 +139,47 @@ def mixed_precision_newton(input_dict, param_dict, mode, iters=3, inner=16, use_
     f = Objective(param_dict, mode)(_as_device_dict(x))
     hist.append({"final_rel_err": float(relative_error_RPO(_as_device_dict(x), f))})
     return x, hist
+
+
+def floquet_operator(input_dict, param_dict, mode="TDRK4", obj=None):
+    """J_fl(tangents): the Jacobian of the masked, symmetry-shifted flow map
+    f0 -> irfft2(mask . mismatch_RPO(f0)) that jax_scripts/floquet.py:40-56
+    differentiates (jax.jvp, vmapped over a block of tangents), at fixed T and sx.
+    objective_RPO's fields output is irfft2(f0 - g Phi_T(f0)), so the map's
+    derivative is dealias(t - d_objective(t)): one batched ecs_jvp per call.
+    Returns a function of tangents [B, 2, n, n] (device, FP64)."""
+    obj = obj or Objective(param_dict, mode)
+    x = _as_device_dict(input_dict)
+
+    def apply(tang):
+        B = tang.shape[0]
+        zero = torch.zeros(B, dtype=torch.float64)
+        d = obj.jvp(x, {"fields": tang.contiguous(), "T": zero, "sx": zero})
+        return dealias((tang - d["fields"]).contiguous(), param_dict)
+    return apply
+
+
+def floquet_power_iteration(input_dict, param_dict, mode="TDRK4", block_size=32, maxit=256, seed=0,
+                            tangents=None):
+    """Block power iteration for the leading Floquet multipliers of an RPO
+    (jax_scripts/floquet.py:58-99): `maxit` applications of J_fl to a block of
+    `block_size` tangents, each followed by a reduced QR re-orthonormalisation,
+    then R = Q J_fl(Q)^T (Schur factor estimate).  Seeded normal start vectors
+    (numpy PCG64 here; the reference uses jax.random).  Returns (R, Q) with Q
+    [block_size, 2, n, n]."""
+    import numpy as np
+    apply = floquet_operator(input_dict, param_dict, mode)
+    n = _as_device_dict(input_dict)["fields"].shape[-1]
+    if tangents is None:
+        tangents = torch.as_tensor(np.random.default_rng(seed).standard_normal((block_size, 2, n, n)), device="cuda")
+    q = tangents.to(device="cuda", dtype=torch.float64)
+    B = q.shape[0]
+
+    def orth(t):
+        Qm, _ = torch.linalg.qr(t.reshape(B, -1).T, mode="reduced")   # floquet.py:90-92
+        return Qm.T.reshape(B, 2, n, n).contiguous()
+
+    for _ in range(maxit):
+        q = orth(apply(q))
+    R = q.reshape(B, -1) @ apply(q).reshape(B, -1).T                     # floquet.py:95-98
+    return R, q

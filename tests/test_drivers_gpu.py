@@ -81,3 +81,31 @@ def test_newton_gmres_tdrk4_reference_default(cuda):
     new, st = drivers.newton_gmres_update(x, pd, "TDRK4", inner=16, use_transpose=True)
     f1 = float(torch.linalg.norm(E.objective_RPO(new, pd, "TDRK4")["fields"]))
     assert f1 < 0.1 * f0, (f0, f1, st)
+
+
+def test_floquet_neutral_directions_and_power_iteration(cuda):
+    """For the reference's TW1 (converged with TDRK4) the Floquet map of
+    jax_scripts/floquet.py has multiplier 1 along the flow and along the
+    x-shift (symmetry directions), to the orbit's closure accuracy; a short
+    block power iteration gives a finite Schur factor with those multipliers
+    among its eigenvalues' neighbourhood of 1."""
+    d = np.load("tests/golden/solution_Re40_TW1.npz")
+    n = d["fields"].shape[-1]
+    pd = E.make_param_dict(n, float(d["nu"]), float(d["eta"]), b0=d["b0"], forcing="kolmogorov",
+                           num_checkpoints=int(d["num_checkpoints"]), ministeps=int(d["ministeps"]),
+                           shift_reflect_ny=int(d["shift_reflect_ny"]), rot=bool(d["rot"]))
+    x = {"fields": torch.as_tensor(d["fields"], device="cuda"), "T": float(d["T"]), "sx": float(d["sx"])}
+    apply = drivers.floquet_operator(x, pd, "TDRK4")
+    f0 = torch.fft.rfft2(x["fields"])
+    kx = torch.fft.fftfreq(n, 1 / n, dtype=torch.float64, device="cuda").reshape(-1, 1)
+    vx = torch.fft.irfft2(1j * kx * f0, s=(n, n))                        # d/dx u0 (shift direction)
+    vt = E.state_vel(f0, pd, include_dissipation=True)                   # d/dt u0 (flow direction)
+    vt = torch.fft.irfft2(vt, s=(n, n))
+    for v in (vx, vt):
+        v = E.dealias(v.contiguous(), pd)
+        jv = apply(v.unsqueeze(0))[0]
+        assert float(torch.linalg.norm(jv - v) / torch.linalg.norm(v)) < 1e-6
+    R, Q = drivers.floquet_power_iteration(x, pd, "TDRK4", block_size=4, maxit=3, seed=0)
+    assert R.shape == (4, 4) and bool(torch.isfinite(R).all())
+    G = Q.reshape(4, -1) @ Q.reshape(4, -1).T
+    assert float(torch.linalg.norm(G - torch.eye(4, dtype=G.dtype, device=G.device))) < 1e-12
