@@ -7,7 +7,7 @@ reference's jax_scripts/lib modules.
 """
 
 from .mhd import construct_domain, dissipation, make_param_dict, state_vel  # noqa: F401
-from .timestepping import lawson_rk4  # noqa: F401
+from .timestepping import lawson_rk4, lawson_rk6, rk4, tdrk4, integrate  # noqa: F401
 from .loss_functions import objective_RPO, loss_RPO, dealias  # noqa: F401
 from .synthetic import initial_condition, unit_tangents  # noqa: F401
 from .autodiff import (Objective, compile_objective_and_Jacobian, vjp, loss_and_grad,  # noqa: F401

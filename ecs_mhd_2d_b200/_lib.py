@@ -72,6 +72,8 @@ SIGNATURES = {
                       ctypes.POINTER(EcsInfo), _I, _VP]),
     "ecs_linearize": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, ctypes.POINTER(EcsInfo), _VP]),
     "ecs_jvp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
+    "ecs_integrate": (_I, [_VP, _I, _VP, ctypes.c_double, _I, _I, _VP]),
+    "ecs_recurrence": (_I, [_VP, _VP, _I, _VP, _VP]),
     "ecs_linearize_jvp": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, ctypes.POINTER(EcsInfo),
                                _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
     "ecs_vjp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),

@@ -182,6 +182,19 @@ int ecs_lawson_rk4(ecs_ctx* ctx, void* f_hat, double t, int steps, int batch, vo
   return table_of(ctx)->lawson_rk4(ctx, f_hat, t, steps, batch, as_stream(stream));
 }
 
+int ecs_integrate(ecs_ctx* ctx, int mode, void* f_hat, double t, int steps, int batch, void* stream) {
+  ECS_CHECK_CTX(ctx, batch);
+  if (!f_hat) return set_err(ctx, ECS_ERR_INVALID, "null pointer");
+  if (steps < 1) return set_err(ctx, ECS_ERR_INVALID, "steps must be >= 1");
+  return table_of(ctx)->integrate(ctx, mode, f_hat, t, steps, batch, as_stream(stream));
+}
+
+int ecs_recurrence(ecs_ctx* ctx, const void* fs, int snapshots, double* dist, void* stream) {
+  if (!ctx) return ECS_ERR_INVALID;
+  if (!fs || !dist || snapshots < 1 || snapshots > 65535) return set_err(ctx, ECS_ERR_INVALID, "bad arguments");
+  return table_of(ctx)->recurrence(ctx, fs, snapshots, dist, as_stream(stream));
+}
+
 int ecs_objective(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T, const double* sx,
                   void* out_fields, double* out_T, double* out_sx, ecs_info* info, int batch, void* stream) {
   ECS_CHECK_CTX(ctx, batch);

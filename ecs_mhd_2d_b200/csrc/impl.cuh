@@ -442,6 +442,39 @@ struct Impl {
     return mode == ECS_MODE_RK4 ? (int)FX_RK4 : mode == ECS_MODE_LAWSON_RK6 ? (int)FX_RK6 : (int)FX_TD4;
   }
 
+  // Fixed-step integration of full rfft2 states f_hat [B][2][N][N/2+1] in place
+  // (timestepping.py rk4 / lawson_rk4 / lawson_rk6 / tdrk4 with the v_fn,
+  // L_diag and mask of mismatch_RPO's mode).
+  static int integrate_mode(ecs_ctx* c, int mode, cplx<R>* fhat, double t, int steps, int B, cudaStream_t s) {
+    if (mode == ECS_MODE_LAWSON_RK4) return lawson_rk4(c, fhat, t, steps, B, s);
+    if (mode != ECS_MODE_RK4 && mode != ECS_MODE_LAWSON_RK6 && mode != ECS_MODE_TDRK4)
+      return set_err(c, ECS_ERR_BAD_MODE, "ecs_integrate: fixed-step modes only");
+    const long VEC = 2L * K * M;
+    ++c->launches; k_fill<<<1, 256, 0, s>>>(c->Tbuf, t, B);
+    ++c->launches; k_gather_box<R><<<grid1d((long)B * VEC), 256, 0, s>>>(fhat, (cplx<R>*)c->F, N, B);
+    cudaError_t e = cudaMemcpy2DAsync((cplx<R>*)c->S43 + X_F * VEC, S_NSLOT * VEC * sizeof(cplx<R>), c->F,
+                                      VEC * sizeof(cplx<R>), VEC * sizeof(cplx<R>), B, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_err(c, e, "integrate");
+    ++c->launches;
+    k_fx_setup<R><<<grid1d((long)B * VEC), 256, 0, s>>>(c->Tbuf, 1, steps, 6, c->ctl, (R*)c->Etab, N, c->nu, c->eta, B);
+    int st = integrate_fx(c, fx_scheme(mode), B, steps, s);
+    if (st) return st;
+    e = cudaMemcpy2DAsync(c->F, VEC * sizeof(cplx<R>), (const cplx<R>*)c->S43 + X_F * VEC,
+                          S_NSLOT * VEC * sizeof(cplx<R>), VEC * sizeof(cplx<R>), B, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_err(c, e, "integrate");
+    const long nfull = (long)B * 2 * N * (N / 2 + 1);
+    ++c->launches;
+    if (carry_mode(mode)) k_scatter_box_keep<R><<<grid1d(nfull), 256, 0, s>>>((const cplx<R>*)c->F, fhat, N, B);
+    else k_scatter_box<R><<<grid1d(nfull), 256, 0, s>>>((const cplx<R>*)c->F, fhat, N, B);
+    return cuda_err(c, cudaGetLastError(), "integrate");
+  }
+
+  static int recurrence(ecs_ctx* c, const cplx<R>* fs, int S, double* dist, cudaStream_t s) {
+    const long len = 2L * N * (N / 2 + 1);
+    ++c->launches; k_recurrence<R><<<dim3(S, S), 256, 0, s>>>(fs, S, len, dist);
+    return cuda_err(c, cudaGetLastError(), "recurrence");
+  }
+
   static int rk4_setup(ecs_ctx* c, const double* T, int nc, int ms, int B, cudaStream_t s) {
     const long tot = (long)B * 2 * K * M;
     ++c->launches; k_rk4_setup<R><<<grid1d(tot), 256, 0, s>>>(T, nc, ms, c->ctl, (R*)c->Etab, N, c->nu, c->eta, B);
@@ -1815,6 +1848,10 @@ ImplTable make_table() {
     return I::linearize(c, cfg, (const R*)f, T, sx, (R*)o, info, s); };
   t.jvp = [](ecs_ctx* c, const void* df, const double* dT, const double* dsx, void* o, double* oT, double* osx, int B,
              cudaStream_t s) { return I::jvp(c, (const R*)df, dT, dsx, (R*)o, oT, osx, B, s); };
+  t.integrate = [](ecs_ctx* c, int mode, void* f, double t_, int steps, int B, cudaStream_t s) {
+    return I::integrate_mode(c, mode, (cplx<R>*)f, t_, steps, B, s); };
+  t.recurrence = [](ecs_ctx* c, const void* fs, int S, double* dist, cudaStream_t s) {
+    return I::recurrence(c, (const cplx<R>*)fs, S, dist, s); };
   t.linearize_jvp = [](ecs_ctx* c, const ecs_shoot_cfg* cfg, const void* f, const double* T, const double* sx, void* o,
                        ecs_info* info, const void* df, const double* dT, const double* dsx, void* od, double* oT,
                        double* osx, int B, cudaStream_t s) {

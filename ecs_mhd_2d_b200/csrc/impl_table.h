@@ -21,6 +21,8 @@ struct ImplTable {
   int (*linearize)(ecs_ctx*, const ecs_shoot_cfg*, const void*, const double*, const double*, void*, ecs_info*,
                    cudaStream_t);
   int (*jvp)(ecs_ctx*, const void*, const double*, const double*, void*, double*, double*, int, cudaStream_t);
+  int (*integrate)(ecs_ctx*, int, void*, double, int, int, cudaStream_t);
+  int (*recurrence)(ecs_ctx*, const void*, int, double*, cudaStream_t);
   int (*linearize_jvp)(ecs_ctx*, const ecs_shoot_cfg*, const void*, const double*, const double*, void*, ecs_info*,
                        const void*, const double*, const double*, void*, double*, double*, int, cudaStream_t);
   int (*vjp)(ecs_ctx*, const void*, const double*, const double*, void*, double*, double*, int, cudaStream_t);

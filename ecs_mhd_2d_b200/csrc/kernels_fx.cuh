@@ -567,6 +567,49 @@ __global__ void __launch_bounds__(128) k_col_tda(ColTdaParams<R> p) {
   col_adj_emit<R, N>(lam, p.G, b, c, ky, lane, s_tw);
 }
 
+// Box entries back into the full half spectrum, leaving every other entry as it is
+// (RK4 / TDRK4 carry the modes outside the box unchanged).
+template <typename R>
+__global__ void k_scatter_box_keep(const cplx<R>* box, cplx<R>* full, int n, int B) {
+  const Geom g = make_geom(n);
+  const int nh = n / 2 + 1;
+  const long total = (long)B * 2 * n * nh;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ky = i % nh; const long r = i / nh; const int pos = r % n; const long bc = r / n;
+    const int slot = (ky < g.K) ? pos_to_slot(pos, n, g.kmax, g.M) : -1;
+    if (slot >= 0) full[i] = box[(bc * g.K + ky) * g.M + slot];
+  }
+}
+
+// Recurrence matrix of snapshots (jax_scripts/generate_turbulence.py:150-160):
+// dist[j][i] = || |fs_j| - |fs_i| ||_2 over the len complex entries of a
+// snapshot (spectral magnitudes: blind to translations).  One block per pair
+// j >= i (the matrix is symmetric), FP64 accumulation, a fixed-order tree.
+template <typename R>
+__global__ void k_recurrence(const cplx<R>* fs, int S, long len, double* dist) {
+  const int i = blockIdx.x, j = blockIdx.y;
+  if (j < i) return;
+  const cplx<R>* a = fs + (size_t)j * len;
+  const cplx<R>* b = fs + (size_t)i * len;
+  double acc = 0.0;
+  for (long k = threadIdx.x; k < len; k += blockDim.x) {
+    const double d = hypot((double)a[k].x, (double)a[k].y) - hypot((double)b[k].x, (double)b[k].y);
+    acc += d * d;
+  }
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    const double r = sqrt(t);
+    dist[(size_t)j * S + i] = r;
+    dist[(size_t)i * S + j] = r;
+  }
+}
+
 // e = exp(h/div L) mask and h = (T/nc)/ms per batch element (timestepping.py:69-72, :105-108).
 template <typename R>
 __global__ void k_fx_setup(const double* T, int nc, int ms, int div, StepCtl* ctl, R* Etab, int n, double nu,

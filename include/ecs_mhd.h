@@ -113,6 +113,20 @@ int ecs_state_vel(ecs_ctx* ctx, const void* f_hat, void* dfdt_hat, int batch,
  * rfft2 layout, in place; L_diag = dissipation(param_dict). */
 int ecs_lawson_rk4(ecs_ctx* ctx, void* f_hat, double t, int steps, int batch, void* stream);
 
+/* Fixed-step integration in place of rfft2 states f_hat [batch][2][n][n/2+1]
+ * over time t in `steps` steps with the right-hand side, dissipation and mask
+ * of mismatch_RPO's `mode` (ECS_MODE_RK4, _LAWSON_RK4, _LAWSON_RK6, _TDRK4;
+ * jax_scripts/lib/timestepping.py:17-149).  Modes outside the 2/3 box are
+ * zeroed by the Lawson modes (masked integrating factor) and kept by RK4 and
+ * TDRK4 (masked right-hand side), as the reference does.  generate_turbulence.py
+ * drives Lawson_RK6 this way (:94, :112). */
+int ecs_integrate(ecs_ctx* ctx, int mode, void* f_hat, double t, int steps, int batch, void* stream);
+
+/* Recurrence matrix of `snapshots` rfft2 states fs [snapshots][2][n][n/2+1]:
+ * dist[j][i] = || |fs_j| - |fs_i| ||_2 (jax_scripts/generate_turbulence.py:150-160),
+ * dist a DEVICE double [snapshots][snapshots]. */
+int ecs_recurrence(ecs_ctx* ctx, const void* fs, int snapshots, double* dist, void* stream);
+
 /* objective_RPO (jax_scripts/lib/loss_functions.py:132-148):
  * out_fields = irfft2(f0 - g.Phi_T(f0)), out_T = pt, out_sx = px (both 0 in value). */
 int ecs_objective(ecs_ctx* ctx, const ecs_shoot_cfg* cfg, const void* fields, const double* T,
