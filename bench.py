@@ -229,6 +229,46 @@ def tdrk4_matvecs(E, torch, dev, flush, prim, tan):
             "finite": bool(torch.isfinite(o["fields"]).all())}
 
 
+def dns_generation(E, torch, dev, flush):
+    """DNS data generation in the reference script's configuration
+    (jax_scripts/generate_turbulence.py: n=128 FP64, dt=1/256, Lawson-RK6,
+    8192 transient steps, 256 snapshots of 64 steps, 256 x 256 recurrence):
+    one trajectory (as the script runs it) and 64 independent trajectories,
+    each timed over 1024 steps, and the recurrence matrix of 256 snapshots."""
+    from ecs_mhd_2d_b200 import turbulence
+    n, dt, S = 128, 1 / 256, 1024
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, b0=(0.0, 0.3), forcing="kolmogorov")
+    rng = np.random.default_rng(111111)
+    f1 = torch.as_tensor(np.fft.rfft2(10.0 * rng.standard_normal((1, 2, n, n))), device=dev) * pd["mask"].to(dev)
+    f1 = E.integrate(f1, dt * 512, 512, pd, "Lawson_RK6")              # leave the random initial data
+    f64 = f1.repeat(64, 1, 1, 1) * (1 + 1e-3 * torch.arange(64, device=dev).view(64, 1, 1, 1))
+    t1, _ = _timed(torch, flush, lambda: E.integrate(f1, dt * S, S, pd, "Lawson_RK6"))
+    t64, _ = _timed(torch, flush, lambda: E.integrate(f64, dt * S, S, pd, "Lawson_RK6"))
+    fs = E.integrate(f64, dt * 64, 64, pd, "Lawson_RK6").repeat(4, 1, 1, 1).contiguous()   # 256 snapshots
+    tr, _ = _timed(torch, flush, lambda: turbulence.recurrence(fs, pd))
+    script_steps = 8192 + 256 * 64
+    return {"rk6_steps_per_s_b1": S / t1, "rk6_state_steps_per_s_b64": 64 * S / t64,
+            "recurrence_256_ms": tr * 1e3, "script_steps": script_steps,
+            "script_estimate_s": script_steps * t1 / S + tr}
+
+
+def cpu_baseline_dns(steps=64):
+    """The oracle's Lawson-RK6 (numpy) on the host for a few steps of the same
+    128^2 FP64 DNS: steps per second of one trajectory."""
+    import oracle as O
+    n = 128
+    opd = O.make_param_dict(n, 1 / 40, 1 / 40, b0=(0.0, 0.3), forcing="kolmogorov")
+    f = np.fft.rfft2(10.0 * np.random.default_rng(111111).standard_normal((2, n, n))) * opd["mask"]
+    v = lambda x: O.state_vel(x, opd, False)
+    L = O.dissipation(opd)
+    O.lawson_rk6(f, 1 / 256, 1, v, L, opd["mask"])
+    t0 = time.perf_counter()
+    O.lawson_rk6(f, steps / 256, steps, v, L, opd["mask"])
+    t = time.perf_counter() - t0
+    return {"value": steps / t, "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} Lawson-RK6 steps of one 128^2 trajectory, {t:.2f} s, numpy oracle"}
+
+
 def cpu_baseline(target_s=12.0, attempts_full=None):
     """The oracle (torch-CPU restatement, torch.func.jvp) on the host cores for a
     bounded sample: the first k attempts of the same adaptive JVP, scaled to one
@@ -498,6 +538,7 @@ def main():
     if not args.no_secondary:
         secondary["config1_plain_vs_batched"] = plain_vs_batched(E, torch, dev, flush, prim, tan)
         secondary["tdrk4_matvec_n128_f64"] = tdrk4_matvecs(E, torch, dev, flush, prim, tan)
+        secondary["dns_generation_n128_f64"] = dns_generation(E, torch, dev, flush)
 
     if rank == 0:
         clocks = clk.summary()
@@ -507,6 +548,11 @@ def main():
                 cb = cpu_baseline(attempts_full=info.get("accepted", 0) + info.get("rejected", 0))
             except Exception as ex:  # the oracle is test infrastructure; report why it is missing
                 cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {ex}"}
+            if "dns_generation_n128_f64" in secondary:
+                try:
+                    secondary["dns_generation_n128_f64"]["cpu_baseline"] = cpu_baseline_dns()
+                except Exception as ex:
+                    secondary["dns_generation_n128_f64"]["cpu_baseline"] = {"value": None, "sample": f"failed: {ex}"}
         extra = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
                  "tangent_rk_steps_per_s": value * info.get("accepted", 0),
                  "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1},

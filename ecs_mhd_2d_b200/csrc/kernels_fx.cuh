@@ -581,7 +581,7 @@ __global__ void k_scatter_box_keep(const cplx<R>* box, cplx<R>* full, int n, int
   }
 }
 
-// Recurrence matrix of snapshots (jax_scripts/generate_turbulence.py:150-160):
+// Recurrence matrix of snapshots (jax_scripts/generate_turbulence.py:136-146):
 // dist[j][i] = || |fs_j| - |fs_i| ||_2 over the len complex entries of a
 // snapshot (spectral magnitudes: blind to translations).  One block per pair
 // j >= i (the matrix is symmetric), FP64 accumulation, a fixed-order tree.

@@ -16,7 +16,7 @@ from .timestepping import integrate
 
 def recurrence(fs, param_dict):
     """dist[j, i] = || |fs_j| - |fs_i| ||_2 for snapshots fs [S, 2, n, n//2+1]
-    (generate_turbulence.py:150-160), on the device (ecs_recurrence)."""
+    (generate_turbulence.py:136-146), on the device (ecs_recurrence)."""
     S, n = fs.shape[0], fs.shape[-2]
     rdt = torch.float64 if fs.dtype == torch.complex128 else torch.float32
     ctx = _ctx.get_context(param_dict, n, rdt, 1)
@@ -28,12 +28,12 @@ def recurrence(fs, param_dict):
 
 def generate_turbulence(n=128, dt=1 / 256, ministeps=64, steps=256, transient_steps=1024 * 2 * 4, nu=1 / 40,
                         eta=1 / 40, b0=(0.0, 0.3), seed=111111, amp=10.0, data_type=torch.float64, path=None):
-    """generate_turbulence.py:21-172.  Random initial fields amp * N(0, 1) [2, n, n]
-    (numpy PCG64 seeded with `seed`; the reference draws them with jax.random),
-    rfft2 and mask (:83-84); `transient_steps` Lawson-RK6 steps of dt (:93-99);
-    `steps` snapshots each `ministeps` steps apart (:110-131); the recurrence
-    matrix (:150-160).  With `path`, saves {"fs", "dist"} and the parameters as
-    the reference does (:175, dictionaryIO.save_dicts).  Returns (fs, dist,
+    """generate_turbulence.py:21-162.  Random initial fields amp * N(0, 1) [2, n, n]
+    (:53-55; numpy PCG64 seeded with `seed` where the reference draws them with
+    jax.random), rfft2 and mask (:77-79); `transient_steps` Lawson-RK6 steps of
+    dt (:84-94); `steps` snapshots each `ministeps` steps apart (:101-124); the
+    recurrence matrix (:136-146).  With `path`, saves {"fs", "dist"} and the
+    parameters as the reference does (:161-162, dictionaryIO.save_dicts).  Returns (fs, dist,
     param_dict); fs is [steps, 2, n, n//2+1] complex on the device."""
     pd = make_param_dict(n, nu, eta, b0=b0, forcing="kolmogorov", data_type=data_type)
     pd.update({"dt": dt, "ministeps": ministeps, "steps": steps})
@@ -46,7 +46,7 @@ def generate_turbulence(n=128, dt=1 / 256, ministeps=64, steps=256, transient_st
         f = integrate(f, dt * transient_steps, transient_steps, pd, "Lawson_RK6")
     fs = torch.empty((steps, 2, n, n // 2 + 1), dtype=ctype, device="cuda")
     for i in range(steps):
-        f = integrate(f, dt * ministeps, ministeps, pd, "Lawson_RK6")   # :112 one_step
+        f = integrate(f, dt * ministeps, ministeps, pd, "Lawson_RK6")   # :105 one_step
         fs[i] = f
     dist = recurrence(fs, pd)
     if path is not None:

@@ -119,11 +119,11 @@ int ecs_lawson_rk4(ecs_ctx* ctx, void* f_hat, double t, int steps, int batch, vo
  * jax_scripts/lib/timestepping.py:17-149).  Modes outside the 2/3 box are
  * zeroed by the Lawson modes (masked integrating factor) and kept by RK4 and
  * TDRK4 (masked right-hand side), as the reference does.  generate_turbulence.py
- * drives Lawson_RK6 this way (:94, :112). */
+ * drives Lawson_RK6 this way (:88, :105). */
 int ecs_integrate(ecs_ctx* ctx, int mode, void* f_hat, double t, int steps, int batch, void* stream);
 
 /* Recurrence matrix of `snapshots` rfft2 states fs [snapshots][2][n][n/2+1]:
- * dist[j][i] = || |fs_j| - |fs_i| ||_2 (jax_scripts/generate_turbulence.py:150-160),
+ * dist[j][i] = || |fs_j| - |fs_i| ||_2 (jax_scripts/generate_turbulence.py:136-146),
  * dist a DEVICE double [snapshots][snapshots]. */
 int ecs_recurrence(ecs_ctx* ctx, const void* fs, int snapshots, double* dist, void* stream);
 
