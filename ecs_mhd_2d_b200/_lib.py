@@ -78,6 +78,7 @@ SIGNATURES = {
                                _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
     "ecs_vjp": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
     "ecs_arnoldi_mgs": (_I, [_VP, ctypes.c_long, _I, _VP, _VP, ctypes.c_long, _VP]),
+    "ecs_arnoldi_mgs_reorth": (_I, [_VP, ctypes.c_long, _I, _VP, _VP, ctypes.c_long, _I, _VP]),
     "ecs_hessenberg_lstsq": (_I, [_VP, _I, _I, _VP, _VP, _VP]),
     "ecs_state_vel_noalloc": (_I, [_I, _D, _D, _D, _D, _VP, _VP, _VP, _I, _I, _VP]),
     "ecs_pool_reset": (_I, [_VP, _VP]),

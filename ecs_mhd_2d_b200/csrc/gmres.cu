@@ -41,8 +41,10 @@ __device__ double block_sum(double v, double* red) {
   return s;
 }
 
+// reorth extra sweeps j = 0..k subtract the projections again without
+// recording them (linalg.py:146-148, :260-262, :514-517, :534-537), before the norm.
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(TPB)
-k_arnoldi_mgs(double* Q, long ld, int k, const double* w_in, double* Hcol, long len) {
+k_arnoldi_mgs(double* Q, long ld, int k, const double* w_in, double* Hcol, long len, int reorth) {
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   extern __shared__ double s_w[];
@@ -53,21 +55,24 @@ k_arnoldi_mgs(double* Q, long ld, int k, const double* w_in, double* Hcol, long 
   const int cnt = (int)(hi > lo ? hi - lo : 0);
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_w[i] = w_in[lo + i];
   __syncthreads();
-  for (int j = 0; j <= k + 1; ++j) {
-    const bool norm_pass = (j == k + 1);
+  const int sweep = k + 1;                                  // projections per sweep
+  const int total = sweep > 0 ? (reorth + 1) * sweep + 1 : 1;
+  for (int it = 0; it < total; ++it) {
+    const bool norm_pass = (it == total - 1);
+    const int j = norm_pass ? k + 1 : it % sweep;
     const double* q = Q + (size_t)j * ld + lo;
     double v = 0.0;
     if (!norm_pass) for (int i = threadIdx.x; i < cnt; i += blockDim.x) v += s_w[i] * q[i];
     else for (int i = threadIdx.x; i < cnt; i += blockDim.x) v += s_w[i] * s_w[i];
     v = block_sum(v, red);
-    if (threadIdx.x == 0) part[j & 1] = v;
+    if (threadIdx.x == 0) part[it & 1] = v;
     cluster.sync();
     // every CTA sums the partials in rank order (same value everywhere)
     double hj = 0.0;
-    for (int r = 0; r < CL; ++r) hj += *cluster.map_shared_rank(&part[j & 1], r);
+    for (int r = 0; r < CL; ++r) hj += *cluster.map_shared_rank(&part[it & 1], r);
     if (!norm_pass) {
       for (int i = threadIdx.x; i < cnt; i += blockDim.x) s_w[i] -= hj * q[i];
-      if (rank == 0 && threadIdx.x == 0) Hcol[j] = hj;
+      if (it < sweep && rank == 0 && threadIdx.x == 0) Hcol[j] = hj;
     } else {
       const double nrm = sqrt(hj);
       if (rank == 0 && threadIdx.x == 0) Hcol[k + 1] = nrm;
@@ -125,7 +130,12 @@ __global__ void k_hessenberg_lstsq(const double* H, int ldh, int m, const double
 }  // namespace
 
 extern "C" int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, double* Hcol, long len, void* stream) {
-  if (!Q || !w || !Hcol || k < -1 || len < 1 || ld < len) return ECS_ERR_INVALID;
+  return ecs_arnoldi_mgs_reorth(Q, ld, k, w, Hcol, len, 0, stream);
+}
+
+extern "C" int ecs_arnoldi_mgs_reorth(double* Q, long ld, int k, const double* w, double* Hcol, long len, int reorth,
+                                      void* stream) {
+  if (!Q || !w || !Hcol || k < -1 || len < 1 || ld < len || reorth < 0 || reorth > 4) return ECS_ERR_INVALID;
   const long per = (len + CL - 1) / CL;
   if (per > MAXSLICE) return ECS_ERR_UNSUPPORTED;
   const size_t smem = (size_t)per * sizeof(double);
@@ -135,7 +145,7 @@ extern "C" int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, doubl
       return ECS_ERR_CUDA;
     configured = true;
   }
-  k_arnoldi_mgs<<<CL, TPB, smem, (cudaStream_t)stream>>>(Q, ld, k, w, Hcol, len);
+  k_arnoldi_mgs<<<CL, TPB, smem, (cudaStream_t)stream>>>(Q, ld, k, w, Hcol, len, reorth);
   return cudaGetLastError() == cudaSuccess ? ECS_OK : ECS_ERR_CUDA;
 }
 

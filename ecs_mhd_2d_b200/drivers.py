@@ -7,7 +7,7 @@ from __future__ import annotations
 import torch
 
 from .autodiff import Objective, loss_and_grad, vjp
-from .linalg import gmres
+from .linalg import block_gmres, gmres, newton_gmres_hookstep_v2
 from .loss_functions import dealias
 from .utils import flatten, line_search_unravel, relative_error_RPO, unflatten
 
@@ -67,6 +67,71 @@ def newton_gmres_update(input_dict, param_dict, mode, inner=16, use_transpose=Tr
     stats = {"rel_err": float(rel_err), "|f|": float(torch.linalg.norm(b)), "gmres_rel_res": float(gmres_res),
              "damp": damp, "T": new["T"], "sx": new["sx"]}
     return new, stats
+
+
+def newton_hookstep_iteration(input_dict, param_dict, mode, inner=64, s=100.0, obj=None):
+    """One iteration of the trust-region Newton driver
+    (jax_scripts/newton_hookstep_v2.py:95-121): objective, Krylov space of the
+    JVP at the current point, newton_gmres_hookstep_v2 with step bound s, then
+    dealias.  Returns (new_input_dict, s, stats) with the driver's printed
+    quantities (rel_err, |f|, rel_res, T, sx)."""
+    obj = obj or Objective(param_dict, mode)
+    x_dict = _as_device_dict(input_dict)
+    n = x_dict["fields"].shape[-1]
+    f = obj(x_dict)
+    f_vec = flatten(f)
+
+    def A(v):
+        t = unflatten(v, n)
+        return flatten(obj.jvp(x_dict, {"fields": t["fields"].contiguous(), "T": t["T"], "sx": t["sx"]}))
+
+    new, s, rel_res = newton_gmres_hookstep_v2(A, f_vec, inner, s, obj, x_dict)   # newton_hookstep_v2.py:108
+    rel_err = relative_error_RPO(new, f)                          # :112, |f| over the updated fields
+    new = {"fields": dealias(new["fields"].contiguous(), param_dict), "T": float(new["T"]),
+           "sx": float(new["sx"])}                                 # :116-119
+    stats = {"rel_err": float(rel_err), "|f|": float(torch.linalg.norm(f_vec)), "rel_res": float(rel_res),
+             "s": s, "T": new["T"], "sx": new["sx"]}
+    return new, s, stats
+
+
+def newton_block_gmres_update(input_dict, param_dict, mode, block=8, m=4, seed=0, do_line_search=True, obj=None):
+    """Newton update whose linear solve is block_gmres (jax_scripts/lib/
+    linalg.py:340-427) over {B, JB, ..., J^m B}: B holds the residual and
+    block-1 seeded random directions, and every application of J is ONE
+    batched JVP of `block` tangents, where sequential GMRES issues one tangent
+    per Krylov vector.  Line search and dealiasing as in newton_gmres_update.
+    Returns (new_input_dict, stats)."""
+    import numpy as np
+    obj = obj or Objective(param_dict, mode)
+    x_dict = _as_device_dict(input_dict)
+    n = x_dict["fields"].shape[-1]
+    f = obj(x_dict)
+    b = flatten(f)
+    nv = b.numel()
+    R = torch.as_tensor(np.random.default_rng(seed).standard_normal((nv, block - 1)), device=b.device)
+    B0 = torch.cat([b.reshape(nv, 1), R], dim=1)
+
+    def A(Bk):
+        s_ = Bk.shape[1]
+        t = Bk.t().contiguous()
+        out = obj.jvp(x_dict, {"fields": t[:, 1:-1].reshape(s_, 2, n, n).contiguous(), "T": t[:, 0].contiguous(),
+                               "sx": t[:, -1].contiguous()})
+        return torch.cat([out["T"].reshape(1, s_), out["fields"].reshape(s_, -1).t(), out["sx"].reshape(1, s_)], 0)
+
+    step = block_gmres(A, b, m, B0)
+    res = float(torch.linalg.norm(A(step.reshape(nv, 1)).reshape(-1) - b) / torch.linalg.norm(b))
+    x = flatten(x_dict)
+    unravel = lambda v: unflatten(v, n)
+    if do_line_search:
+        x, damp = line_search_unravel(x, step, obj, unravel, b, max_iters=20)
+    else:
+        damp = 1.0
+        x = x - step
+    new = unravel(x)
+    rel_err = relative_error_RPO(x_dict, f)
+    new = {"fields": dealias(new["fields"].contiguous(), param_dict), "T": float(new["T"]), "sx": float(new["sx"])}
+    return new, {"rel_err": float(rel_err), "|f|": float(torch.linalg.norm(b)), "block_gmres_rel_res": res,
+                 "damp": damp, "T": new["T"], "sx": new["sx"]}
 
 
 def init_adam(params):

@@ -179,6 +179,14 @@ int ecs_vjp(ecs_ctx* ctx, const void* c_fields, const double* c_T, const double*
  * w into Q[:,0] (linalg.py:58) and writes |w| to Hcol[0].  len <= 131200. */
 int ecs_arnoldi_mgs(double* Q, long ld, int k, const double* w, double* Hcol, long len, void* stream);
 
+/* ecs_arnoldi_mgs followed by `reorth` (0..4) more sweeps j = 0..k that
+ * subtract <w, Q[:,j]> Q[:,j] again without recording it, then the norm and
+ * Q[:,k+1] = w/|w| (the twice-re-orthogonalised Arnoldi and Golub-Kahan steps
+ * of newton_gmres_hookstep(_v2) and adjoint_GMRES, jax_scripts/lib/linalg.py:
+ * 137-153, 254-266, 502-540). */
+int ecs_arnoldi_mgs_reorth(double* Q, long ld, int k, const double* w, double* Hcol, long len, int reorth,
+                           void* stream);
+
 /* y = argmin |H y - b| for the (m+1) x m upper Hessenberg H (column-major,
  * leading dimension ldh >= m+1), m <= 128 (jnp.linalg.lstsq at linalg.py:93). */
 int ecs_hessenberg_lstsq(const double* H, int ldh, int m, const double* b, double* y, void* stream);
