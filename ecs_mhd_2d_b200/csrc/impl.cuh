@@ -30,13 +30,13 @@ constexpr int XT = 8;
 constexpr int COLWARPS = 4;
 
 // Row kernels with NG (or 3 adjoint) input and NH (or NHA adjoint) output tiles: 7 tiles of K x (X+1).
-template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (tw_smem(N) + 7 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
+template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (fft_smem(N, X) + 7 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 // Small batches use 2-row tiles: 4x more CTAs for the same rows.
 constexpr int XTS = 2;
 template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
-template <typename R, int N> size_t smem_row_tan2() { return (tw_smem(N) + 11 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
-template <typename R, int N> size_t smem_row_phys() { return (tw_smem(N) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
-template <typename R, int N, int X = XT> size_t smem_row_2f() { return (tw_smem(N) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
+template <typename R, int N> size_t smem_row_tan2() { return (fft_smem(N, XT) + 11 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N> size_t smem_row_phys() { return (fft_smem(N, XT) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
+template <typename R, int N, int X = XT> size_t smem_row_2f() { return (fft_smem(N, X) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
 // Launch a stepping kernel of batch B; with c->pdl set and B >= 8, with
 // programmatic stream serialization (the kernel waits on its predecessor

@@ -119,7 +119,7 @@ __device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int 
     fft_dif2<R, N, false>(v, r, s_tw, lane);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       const R m0 = prod_mult<R>(0, kx, ky), m1 = prod_mult<R>(1, kx, ky);
       v[j] = mk<R>(m0 * v[j].x + m1 * r[j].x, m0 * v[j].y + m1 * r[j].y);
     }
@@ -127,7 +127,7 @@ __device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int 
     col_load_fwd1<R, N>(H, NH, b, 2, ky, lane, s_tw, v);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       v[j] = cscale(v[j], prod_mult<R>(2, kx, ky));
     }
   }
@@ -145,7 +145,7 @@ __device__ __forceinline__ void col_inverse_uv(const cplx<R> (&x)[N / 32], cplx<
   cplx<R> wu[E], wv[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+    const int kx = pos_to_k(spec_pos<N>(lane, j), N);
     wu[j] = cscale(cimul(x[j], spectral_mu<R>(2, kx, ky)), inv_n2);
     wv[j] = cscale(cimul(x[j], spectral_mu<R>(3, kx, ky)), inv_n2);
   }
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     x[j] = mk<R>(0, 0);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   cplx<R>* s_H = s_G + NG * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_to_box(RowFwdParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_H = s_tw + tw_smem(N);
+  cplx<R>* s_H = s_tw + fft_smem(N, XT);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_to_box(RowFwdParams<R> p) {
   cplx<R> W[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int y = bitrev<N>(lane + 32 * j);
+    const int y = spec_pos<N>(lane, j);
     W[j] = mk<R>(u0[y], u1[y]);
   }
   fft_dit<R, N, false>(W, s_tw, lane);
@@ -500,7 +500,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(128) k_col_to_box(ColBoxParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(128) k_col_to_box(ColBoxParams<R> p) {
   cplx<R>* vout = p.V + (size_t)b * p.vstride + (size_t)fk * M;
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     if (slot >= 0) vout[slot] = v[j];
   }
 }
@@ -563,7 +563,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(128) k_col_from_box(ColFromBoxParams<R> p) {
   cplx<R> v[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int pos = bitrev<N>(lane + 32 * j);
+    const int pos = spec_pos<N>(lane, j);
     const int slot = pos_to_slot(pos, N, KMAX, M);
     v[j] = mk<R>(0, 0);
     if (slot < 0) continue;
@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_from_box(RowFromBoxParams<R> p)
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_from_box(RowFromBoxParams<R> p)
   cplx<R> z[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int q = bitrev<N>(lane + 32 * j);
+    const int q = spec_pos<N>(lane, j);
     z[j] = packed_pair<R, N, XT>(s_G, s_G + K * (XT + 1), q, w);
   }
   fft_dit<R, N, true>(z, s_tw, lane);

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   cplx<R>* s_H = s_G + 3 * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
     fft_dif2<R, N, false>(xb, v1, s_tw, lane);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       xb[j] = cadd(cimul(xb[j], -spectral_mu<R>(2, kx, ky)), cimul(v1[j], -spectral_mu<R>(3, kx, ky)));
     }
 #pragma unroll
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     lam[j] = mk<R>(0, 0);
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
     cplx<R> z0[E], z1[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       z0[j] = cscale(lam[j], prod_mult<R>(0, kx, ky));
       z1[j] = cscale(lam[j], prod_mult<R>(1, kx, ky));
     }
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   } else {
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const int kx = pos_to_k(bitrev<N>(lane + 32 * j), N);
+      const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       lam[j] = cscale(lam[j], prod_mult<R>(2, kx, ky));
     }
     col_inverse1<R, N>(lam, p.G, NG, b, 2, ky, lane, s_tw, R(1));

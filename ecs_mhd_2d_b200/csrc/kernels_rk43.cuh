@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     x[j] = mk<R>(0, 0);
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     cplx<R> v = mk<R>(0, 0);
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   __shared__ double s_max[XT];
   __shared__ int s_last;
   const int tiles = N / XT;

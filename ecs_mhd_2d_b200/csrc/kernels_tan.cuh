@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(128) k_col_regen(ColRegenParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   load_twiddles<R, N>(s_tw, p.tw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128) k_col_regen(ColRegenParams<R> p) {
   cplx<R> x[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     x[j] = slot >= 0 ? y[slot] : mk<R>(0, 0);
   }
   col_inverse_uv<R, N>(x, p.G, it, ch, ky, lane, s_tw);
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(XT * 32) k_row_phys(RowPhysParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   const int tiles = N / XT;
   const int it = blockIdx.x / tiles, x0 = (blockIdx.x - it * tiles) * XT;
   load_twiddles<R, N>(s_tw, p.tw);
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + tw_smem(N);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
   cplx<R>* s_H = s_G + NG * K * (XT + 1);
   const int tiles = N / XT;
   const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ cplx<R> s_tw[tw_smem(N)];
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     x[j] = mk<R>(0, 0);
-    const int slot = pos_to_slot(bitrev<N>(lane + 32 * j), N, KMAX, M);
+    const int slot = pos_to_slot(spec_pos<N>(lane, j), N, KMAX, M);
     if (slot < 0) continue;
     const int kx = slot_to_kx(slot, KMAX, M);
     const bool in_mask = !(kx == 0 && ky == 0);

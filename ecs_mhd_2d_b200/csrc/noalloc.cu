@@ -71,8 +71,8 @@ int na_setup_twiddles(unsigned char* base, size_t off) {
                                                                                                 : ECS_ERR_CUDA;
 }
 
-template <int N> size_t na_smem_rhs() { return (tw_smem(N) + (NG + NH) * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
-template <int N> size_t na_smem_2f() { return (tw_smem(N) + 2 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
+template <int N> size_t na_smem_rhs() { return (fft_smem(N, NA_XT) + (NG + NH) * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
+template <int N> size_t na_smem_2f() { return (fft_smem(N, NA_XT) + 2 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
 
 // One-time set-up on the current device (synchronous).
 int na_setup(unsigned char** out) {
