@@ -11,11 +11,12 @@
 // __shfl_xor_sync; spec_pos(l, j) = bitrev(l + 32 j).
 // N = 128: radix-4/4/4/2 on the digits of the position; after each local
 // radix-4 pass over the register index, the register digit is swapped with the
-// next lane digit through a per-warp shared-memory buffer (three exchanges with
-// bank-conflict-free, XOR-swizzled addresses), so every butterfly is local.
-// The transposed sequence (twiddles before butterflies, exchanges reversed)
-// is the DIT.  Fewer instructions than five shuffle stages, and the exchange
-// replaces shuffle traffic by 128-bit shared-memory accesses.
+// next lane digit through a per-warp shared-memory buffer (two exchanges with
+// bank-conflict-free, XOR-swizzled addresses), and the last lane digit with a
+// register digit by a pairwise shuffle swap fused with the radix-2 pass, so
+// every butterfly is local.  The transposed sequence (twiddles before
+// butterflies, exchanges reversed) is the DIT.  Fewer instructions than five
+// shuffle stages and less shared-memory/shuffle traffic.
 //
 // Both are unnormalised.  FWD uses exp(-2 pi i k/N), INV uses exp(+2 pi i k/N).
 // Twiddles come from a table tw[k] = exp(-2 pi i k / N), k in [0, N/2),
@@ -103,7 +104,8 @@ __device__ __forceinline__ void dit_shfl(cplx<R> (&v)[N / 32], const cplx<R>* __
 // over the next lane digit after exchange 2 (W_8^{p r1}), pass 4 the final
 // radix-2 after exchange 3.  Output: lane L, register t holds X[k] with
 // k = k1 + 4 q1 + 16 r1 + 64 r2, k1 = L >> 3, q1 = (L >> 1) & 3,
-// r1 = (L & 1) + 2 (t >> 1), r2 = t & 1.
+// r1 = (L & 1) + 2 (t >> 1), r2 = t & 1.  Exchange 3 (one digit) is a pairwise
+// shuffle swap fused with the radix-2 pass (r2_swap_dif / r2_swap_dit).
 // Radix-4 table at tw + 128 (tw[k] = W_128^k): [0, 96) W_128^{l k1} at
 // (k1-1)*32 + l; [96, 120) W_32^{m q1} at 96 + (q1-1)*8 + m; [120, 128)
 // W_8^{p r1} at 120 + 4p + r1.
@@ -130,14 +132,6 @@ __device__ __forceinline__ int x2_w(int lane, int r) { return (lane >> 3) * 32 +
 __device__ __forceinline__ int x2_r(int lane, int r) {
   const int p = lane & 1, q1 = (lane >> 1) & 3;
   return (lane >> 3) * 32 + q1 * 8 + ((2 * r + p) ^ (2 * q1));
-}
-__device__ __forceinline__ int x3_w(int lane, int r) {
-  const int p = lane & 1, q1 = (lane >> 1) & 3;
-  return (lane >> 3) * 32 + (2 * (r >> 1) + p) * 8 + 2 * q1 + (p ^ (r & 1));
-}
-__device__ __forceinline__ int x3_r(int lane, int r) {
-  const int r10 = lane & 1, q1 = (lane >> 1) & 3, p = r & 1, r11 = r >> 1;
-  return (lane >> 3) * 32 + (2 * r11 + p) * 8 + 2 * q1 + (p ^ r10);
 }
 
 template <typename R, int NT, int WF(int, int), int RF(int, int)>
@@ -178,21 +172,47 @@ __device__ __forceinline__ void r4_pass(cplx<R> (*const (&v)[NT])[4]) {
   for (int a = 0; a < NT; ++a) r4_dft<R, INV>((*v[a])[0], (*v[a])[1], (*v[a])[2], (*v[a])[3]);
 }
 
-template <typename R, int NT>
-__device__ __forceinline__ void r2_pass(cplx<R> (*const (&v)[NT])[4]) {
-#pragma unroll
-  for (int a = 0; a < NT; ++a)
-#pragma unroll
-    for (int h = 0; h < 4; h += 2) {
-      const cplx<R> u = (*v[a])[h], w = (*v[a])[h + 1];
-      (*v[a])[h] = cadd(u, w); (*v[a])[h + 1] = csub(u, w);
-    }
-}
-
 // The exchange buffer of the calling warp: after the tables, 2 * 128 entries per warp.
 template <typename R>
 __device__ __forceinline__ cplx<R>* r4_buf(const cplx<R>* tw) {
   return const_cast<cplx<R>*>(tw) + tw_smem(128) + (threadIdx.x >> 5) * fft_xbuf(128);
+}
+
+// Exchange 3 fused with the last radix-2 pass: lanes L and L^1 swap the
+// register digit r1 & 1 with the lane digit p (each sends one value of each
+// register pair), and the pair's butterfly sign follows the lane bit:
+// out(r2 = 0) = keep + recv, out(r2 = 1) = (1 - 2b) (keep - recv).
+template <typename R, int NT>
+__device__ __forceinline__ void r2_swap_dif(cplx<R> (*const (&v)[NT])[4], int lane) {
+  const bool b = lane & 1;
+  const R sg = b ? R(-1) : R(1);
+#pragma unroll
+  for (int a = 0; a < NT; ++a)
+#pragma unroll
+    for (int h = 0; h < 4; h += 2) {
+      const cplx<R> keep = b ? (*v[a])[h + 1] : (*v[a])[h];
+      const cplx<R> send = b ? (*v[a])[h] : (*v[a])[h + 1];
+      const cplx<R> recv = shfl_xor_c<R>(send, 1);
+      (*v[a])[h] = cadd(keep, recv);
+      (*v[a])[h + 1] = cscale(csub(keep, recv), sg);
+    }
+}
+
+// Transpose of r2_swap_dif: the radix-2 pass, then the lane/register digit swap.
+template <typename R, int NT>
+__device__ __forceinline__ void r2_swap_dit(cplx<R> (*const (&v)[NT])[4], int lane) {
+  const bool b = lane & 1;
+  const R sg = b ? R(-1) : R(1);
+#pragma unroll
+  for (int a = 0; a < NT; ++a)
+#pragma unroll
+    for (int h = 0; h < 4; h += 2) {
+      const cplx<R> x = (*v[a])[h], y = cscale((*v[a])[h + 1], sg);
+      const cplx<R> keep = cadd(x, y), send = csub(x, y);
+      const cplx<R> recv = shfl_xor_c<R>(send, 1);
+      (*v[a])[h] = b ? recv : keep;
+      (*v[a])[h + 1] = b ? keep : recv;
+    }
 }
 
 template <typename R, bool INV, int NT>
@@ -207,16 +227,14 @@ __device__ __forceinline__ void fft128_dif(cplx<R> (*const (&v)[NT])[4], const c
   r4_xchg<R, NT, x2_w, x2_r>(v, xb, lane);
   r4_pass<R, INV, NT>(v);
   r4_twiddle<R, INV, NT>(v, t4, 121, 1, (lane & 1) * 4);
-  r4_xchg<R, NT, x3_w, x3_r>(v, xb, lane);
-  r2_pass<R, NT>(v);
+  r2_swap_dif<R, NT>(v, lane);
 }
 
 template <typename R, bool INV, int NT>
 __device__ __forceinline__ void fft128_dit(cplx<R> (*const (&v)[NT])[4], const cplx<R>* tw, int lane) {
   const cplx<R>* t4 = tw + 128;
   cplx<R>* xb = r4_buf<R>(tw);
-  r2_pass<R, NT>(v);
-  r4_xchg<R, NT, x3_r, x3_w>(v, xb, lane);
+  r2_swap_dit<R, NT>(v, lane);
   r4_twiddle<R, INV, NT>(v, t4, 121, 1, (lane & 1) * 4);
   r4_pass<R, INV, NT>(v);
   r4_xchg<R, NT, x2_r, x2_w>(v, xb, lane);
