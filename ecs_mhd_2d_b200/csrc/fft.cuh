@@ -9,14 +9,11 @@
 // N = 64, 256: radix-2; stages whose butterfly span is >= 32 are
 // register-local, the five stages with span < 32 exchange values with
 // __shfl_xor_sync; spec_pos(l, j) = bitrev(l + 32 j).
-// N = 128: radix-4/4/4/2 on the digits of the position; after each local
-// radix-4 pass over the register index, the register digit is swapped with the
-// next lane digit through a per-warp shared-memory buffer (two exchanges with
-// bank-conflict-free, XOR-swizzled addresses), and the last lane digit with a
-// register digit by a pairwise shuffle swap fused with the radix-2 pass, so
-// every butterfly is local.  The transposed sequence (twiddles before
-// butterflies, exchanges reversed) is the DIT.  Fewer instructions than five
-// shuffle stages and less shared-memory/shuffle traffic.
+// N = 128: a radix-4 pass over the two register digits, then five radix-2
+// stages in which a lane digit is swapped with a finished register digit by
+// pairwise shuffles (each lane sends half of its values) and the butterfly is
+// local, with its sign taken from the lane bit; half the shuffle traffic of
+// the plain radix-2 stages.  The transposed sequence is the DIT.
 //
 // Both are unnormalised.  FWD uses exp(-2 pi i k/N), INV uses exp(+2 pi i k/N).
 // Twiddles come from a table tw[k] = exp(-2 pi i k / N), k in [0, N/2),
@@ -32,15 +29,14 @@
 namespace ecs {
 
 // Shared-memory twiddle entries and the offset of the stride-r sub-table.
-// N = 128 adds the radix-4 table (R4_TW entries) after the strided ones.
-constexpr int R4_TW = 128;
+// N = 128 adds the radix-4 pass's table (R4_TW entries) after the strided ones.
+constexpr int R4_TW = 96;
 __host__ __device__ constexpr int tw_smem(int N) { return N + (N == 128 ? R4_TW : 0); }
 __host__ __device__ constexpr int tw_off(int N, int r) { return N - N / r; }
-// Per-warp exchange buffers of the N = 128 transforms (two transforms of N
-// entries), placed after the tables; fft_smem(N, W) is the whole region of a
-// CTA of W warps, which every kernel that calls a transform reserves.
-__host__ __device__ constexpr int fft_xbuf(int N) { return N == 128 ? 2 * N : 0; }
-__host__ __device__ constexpr int fft_smem(int N, int W) { return tw_smem(N) + W * fft_xbuf(N); }
+// Shared-memory region of the transforms of a CTA of W warps (the tables; the
+// transforms need no per-warp buffers), which every kernel that calls a
+// transform reserves at its start.
+__host__ __device__ constexpr int fft_smem(int N, int /*warps*/) { return tw_smem(N); }
 
 template <int N> struct Log2E;
 template <> struct Log2E<64>  { static constexpr int v = 1; };
@@ -98,20 +94,23 @@ __device__ __forceinline__ void dit_shfl(cplx<R> (&v)[N / 32], const cplx<R>* __
 }
 
 // ---------------------------------------------------------------------------
-// N = 128: radix-4/4/4/2 with shared-memory digit exchanges.
-// Position e = l + 32 j with l = m + 8 i: pass 1 is the length-4 DFT over j
-// (twiddles W_128^{l k1}), pass 2 over i after exchange 1 (W_32^{m q1}), pass 3
-// over the next lane digit after exchange 2 (W_8^{p r1}), pass 4 the final
-// radix-2 after exchange 3.  Output: lane L, register t holds X[k] with
-// k = k1 + 4 q1 + 16 r1 + 64 r2, k1 = L >> 3, q1 = (L >> 1) & 3,
-// r1 = (L & 1) + 2 (t >> 1), r2 = t & 1.  Exchange 3 (one digit) is a pairwise
-// shuffle swap fused with the radix-2 pass (r2_swap_dif / r2_swap_dit).
-// Radix-4 table at tw + 128 (tw[k] = W_128^k): [0, 96) W_128^{l k1} at
-// (k1-1)*32 + l; [96, 120) W_32^{m q1} at 96 + (q1-1)*8 + m; [120, 128)
-// W_8^{p r1} at 120 + 4p + r1.
+// N = 128: one radix-4 pass over the register digits, then five half-swap
+// radix-2 stages over the lane digits.
+// Position e = l + 32 j.  The radix-4 pass is the length-4 DFT over j with the
+// twiddles W_128^{l k1} (table at tw + 128, entry (k1-1)*32 + l, k1 = 1..3).
+// Stage t (lane bit t, span S = 2^t) swaps lane bit t with a finished register
+// bit rb: the lane whose bit t is c keeps its two values whose register bit rb
+// is c and sends the other two to lane ^ S (8 32-bit shuffles), and the
+// butterfly over the new register bit is local, with its sign taken from c:
+// lower = keep + recv, upper = (1 - 2c)(keep - recv) W_{2S}^{l mod S}.  Stages
+// (t, rb) = (4,0) (3,1) (2,0) (1,1) (0,0).  Output: lane L, register t holds
+// X[k1 + 4 k2] with k1 = L4 + 2 L3, k2 = L2 + 2 L1 + 4 L0 + 8 t1 + 16 t0 (Li,
+// ti the bits of L and t).  The DIT is the transposed sequence.
 // ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ int spec128(int lane, int t) {
-  return (lane >> 3) + 4 * ((lane >> 1) & 3) + 16 * ((lane & 1) + 2 * (t >> 1)) + 64 * (t & 1);
+  const int k1 = ((lane >> 4) & 1) + 2 * ((lane >> 3) & 1);
+  const int k2 = ((lane >> 2) & 1) + 2 * ((lane >> 1) & 1) + 4 * (lane & 1) + 8 * ((t >> 1) & 1) + 16 * (t & 1);
+  return k1 + 4 * k2;
 }
 
 template <int N> __device__ __forceinline__ int spec_pos(int lane, int j) {
@@ -125,124 +124,111 @@ __device__ __forceinline__ void r4_dft(cplx<R>& a0, cplx<R>& a1, cplx<R>& a2, cp
   a0 = cadd(s02, s13); a1 = cadd(d02, d13); a2 = csub(s02, s13); a3 = csub(d02, d13);
 }
 
-// exchange address maps (entry index in a 128-entry buffer) for lane, register r
-__device__ __forceinline__ int x1_w(int lane, int r) { return r * 32 + lane; }
-__device__ __forceinline__ int x1_r(int lane, int r) { return (lane >> 3) * 32 + (lane & 7) + 8 * r; }
-__device__ __forceinline__ int x2_w(int lane, int r) { return (lane >> 3) * 32 + r * 8 + ((lane & 7) ^ (2 * r)); }
-__device__ __forceinline__ int x2_r(int lane, int r) {
-  const int p = lane & 1, q1 = (lane >> 1) & 3;
-  return (lane >> 3) * 32 + q1 * 8 + ((2 * r + p) ^ (2 * q1));
-}
-
-template <typename R, int NT, int WF(int, int), int RF(int, int)>
-__device__ __forceinline__ void r4_xchg(cplx<R> (*const (&v)[NT])[4], cplx<R>* xb, int lane) {
-#pragma unroll
-  for (int a = 0; a < NT; ++a)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) xb[a * 128 + WF(lane, r)] = (*v[a])[r];
-  __syncwarp();
-#pragma unroll
-  for (int a = 0; a < NT; ++a)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) (*v[a])[r] = xb[a * 128 + RF(lane, r)];
-  __syncwarp();
-}
-
-template <typename R, bool INV>
-__device__ __forceinline__ cplx<R> r4_tw(const cplx<R>* t4, int i) {
-  cplx<R> w = t4[i];
-  if (INV) w.y = -w.y;
-  return w;
-}
-
+// The radix-4 pass: DFT over the register index, then W_128^{l k1} on k1 = 1..3.
 template <typename R, bool INV, int NT>
-__device__ __forceinline__ void r4_twiddle(cplx<R> (*const (&v)[NT])[4], const cplx<R>* t4, int base, int stride,
-                                           int idx) {
+__device__ __forceinline__ void r4_first(cplx<R> (*const (&v)[NT])[4], const cplx<R>* t4, int lane) {
+#pragma unroll
+  for (int a = 0; a < NT; ++a) r4_dft<R, INV>((*v[a])[0], (*v[a])[1], (*v[a])[2], (*v[a])[3]);
 #pragma unroll
   for (int k = 1; k < 4; ++k) {
-    const cplx<R> w = r4_tw<R, INV>(t4, base + (k - 1) * stride + idx);
+    const cplx<R> w = twid<R, INV>(t4, (k - 1) * 32 + lane);
 #pragma unroll
     for (int a = 0; a < NT; ++a) (*v[a])[k] = cmul((*v[a])[k], w);
   }
 }
 
+// Transpose of r4_first: the twiddles, then the DFT over the register index.
 template <typename R, bool INV, int NT>
-__device__ __forceinline__ void r4_pass(cplx<R> (*const (&v)[NT])[4]) {
+__device__ __forceinline__ void r4_last(cplx<R> (*const (&v)[NT])[4], const cplx<R>* t4, int lane) {
+#pragma unroll
+  for (int k = 1; k < 4; ++k) {
+    const cplx<R> w = twid<R, INV>(t4, (k - 1) * 32 + lane);
+#pragma unroll
+    for (int a = 0; a < NT; ++a) (*v[a])[k] = cmul((*v[a])[k], w);
+  }
 #pragma unroll
   for (int a = 0; a < NT; ++a) r4_dft<R, INV>((*v[a])[0], (*v[a])[1], (*v[a])[2], (*v[a])[3]);
 }
 
-// The exchange buffer of the calling warp: after the tables, 2 * 128 entries per warp.
-template <typename R>
-__device__ __forceinline__ cplx<R>* r4_buf(const cplx<R>* tw) {
-  return const_cast<cplx<R>*>(tw) + tw_smem(128) + (threadIdx.x >> 5) * fft_xbuf(128);
+// (1 - 2c) W_{2S}^{lane mod S} for a half-swap stage of span S (W = 1 for S = 1).
+template <typename R, bool INV, int S>
+__device__ __forceinline__ cplx<R> hs_factor(const cplx<R>* tw, int lane, R sg) {
+  if constexpr (S > 2) {
+    const cplx<R> w = twid<R, INV>(tw + tw_off(128, 128 / (2 * S)), lane & (S - 1));
+    return mk<R>(sg * w.x, sg * w.y);
+  } else {
+    return mk<R>(sg, R(0));
+  }
 }
 
-// Exchange 3 fused with the last radix-2 pass: lanes L and L^1 swap the
-// register digit r1 & 1 with the lane digit p (each sends one value of each
-// register pair), and the pair's butterfly sign follows the lane bit:
-// out(r2 = 0) = keep + recv, out(r2 = 1) = (1 - 2b) (keep - recv).
-template <typename R, int NT>
-__device__ __forceinline__ void r2_swap_dif(cplx<R> (*const (&v)[NT])[4], int lane) {
-  const bool b = lane & 1;
-  const R sg = b ? R(-1) : R(1);
+template <typename R, bool INV, int NT, int T, int RB>
+__device__ __forceinline__ void hs_dif(cplx<R> (*const (&v)[NT])[4], const cplx<R>* tw, int lane) {
+  constexpr int S = 1 << T;
+  const bool c = (lane >> T) & 1;
+  const cplx<R> f = hs_factor<R, INV, S>(tw, lane, c ? R(-1) : R(1));
 #pragma unroll
   for (int a = 0; a < NT; ++a)
 #pragma unroll
-    for (int h = 0; h < 4; h += 2) {
-      const cplx<R> keep = b ? (*v[a])[h + 1] : (*v[a])[h];
-      const cplx<R> send = b ? (*v[a])[h] : (*v[a])[h + 1];
-      const cplx<R> recv = shfl_xor_c<R>(send, 1);
-      (*v[a])[h] = cadd(keep, recv);
-      (*v[a])[h + 1] = cscale(csub(keep, recv), sg);
+    for (int og = 0; og < 2; ++og) {
+      constexpr int o = 1 - RB;
+      const int r0 = og << o, r1 = (1 << RB) | (og << o);
+      const cplx<R> keep = c ? (*v[a])[r1] : (*v[a])[r0];
+      const cplx<R> send = c ? (*v[a])[r0] : (*v[a])[r1];
+      const cplx<R> recv = shfl_xor_c<R>(send, S);
+      (*v[a])[r0] = cadd(keep, recv);
+      cplx<R> d = csub(keep, recv);
+      if constexpr (S > 2) d = cmul(d, f);
+      else {
+        d = cscale(d, f.x);
+        if constexpr (S == 2) { if (lane & 1) d = mul_mi<R, INV>(d); }
+      }
+      (*v[a])[r1] = d;
     }
 }
 
-// Transpose of r2_swap_dif: the radix-2 pass, then the lane/register digit swap.
-template <typename R, int NT>
-__device__ __forceinline__ void r2_swap_dit(cplx<R> (*const (&v)[NT])[4], int lane) {
-  const bool b = lane & 1;
-  const R sg = b ? R(-1) : R(1);
+template <typename R, bool INV, int NT, int T, int RB>
+__device__ __forceinline__ void hs_dit(cplx<R> (*const (&v)[NT])[4], const cplx<R>* tw, int lane) {
+  constexpr int S = 1 << T;
+  const bool c = (lane >> T) & 1;
+  const cplx<R> f = hs_factor<R, INV, S>(tw, lane, c ? R(-1) : R(1));
 #pragma unroll
   for (int a = 0; a < NT; ++a)
 #pragma unroll
-    for (int h = 0; h < 4; h += 2) {
-      const cplx<R> x = (*v[a])[h], y = cscale((*v[a])[h + 1], sg);
+    for (int og = 0; og < 2; ++og) {
+      constexpr int o = 1 - RB;
+      const int r0 = og << o, r1 = (1 << RB) | (og << o);
+      cplx<R> y = (*v[a])[r1];
+      if constexpr (S > 2) y = cmul(y, f);
+      else {
+        if constexpr (S == 2) { if (lane & 1) y = mul_mi<R, INV>(y); }
+        y = cscale(y, f.x);
+      }
+      const cplx<R> x = (*v[a])[r0];
       const cplx<R> keep = cadd(x, y), send = csub(x, y);
-      const cplx<R> recv = shfl_xor_c<R>(send, 1);
-      (*v[a])[h] = b ? recv : keep;
-      (*v[a])[h + 1] = b ? keep : recv;
+      const cplx<R> recv = shfl_xor_c<R>(send, S);
+      (*v[a])[r0] = c ? recv : keep;
+      (*v[a])[r1] = c ? keep : recv;
     }
 }
 
 template <typename R, bool INV, int NT>
 __device__ __forceinline__ void fft128_dif(cplx<R> (*const (&v)[NT])[4], const cplx<R>* tw, int lane) {
-  const cplx<R>* t4 = tw + 128;
-  cplx<R>* xb = r4_buf<R>(tw);
-  r4_pass<R, INV, NT>(v);
-  r4_twiddle<R, INV, NT>(v, t4, 0, 32, lane);
-  r4_xchg<R, NT, x1_w, x1_r>(v, xb, lane);
-  r4_pass<R, INV, NT>(v);
-  r4_twiddle<R, INV, NT>(v, t4, 96, 8, lane & 7);
-  r4_xchg<R, NT, x2_w, x2_r>(v, xb, lane);
-  r4_pass<R, INV, NT>(v);
-  r4_twiddle<R, INV, NT>(v, t4, 121, 1, (lane & 1) * 4);
-  r2_swap_dif<R, NT>(v, lane);
+  r4_first<R, INV, NT>(v, tw + 128, lane);
+  hs_dif<R, INV, NT, 4, 0>(v, tw, lane);
+  hs_dif<R, INV, NT, 3, 1>(v, tw, lane);
+  hs_dif<R, INV, NT, 2, 0>(v, tw, lane);
+  hs_dif<R, INV, NT, 1, 1>(v, tw, lane);
+  hs_dif<R, INV, NT, 0, 0>(v, tw, lane);
 }
 
 template <typename R, bool INV, int NT>
 __device__ __forceinline__ void fft128_dit(cplx<R> (*const (&v)[NT])[4], const cplx<R>* tw, int lane) {
-  const cplx<R>* t4 = tw + 128;
-  cplx<R>* xb = r4_buf<R>(tw);
-  r2_swap_dit<R, NT>(v, lane);
-  r4_twiddle<R, INV, NT>(v, t4, 121, 1, (lane & 1) * 4);
-  r4_pass<R, INV, NT>(v);
-  r4_xchg<R, NT, x2_r, x2_w>(v, xb, lane);
-  r4_twiddle<R, INV, NT>(v, t4, 96, 8, lane & 7);
-  r4_pass<R, INV, NT>(v);
-  r4_xchg<R, NT, x1_r, x1_w>(v, xb, lane);
-  r4_twiddle<R, INV, NT>(v, t4, 0, 32, lane);
-  r4_pass<R, INV, NT>(v);
+  hs_dit<R, INV, NT, 0, 0>(v, tw, lane);
+  hs_dit<R, INV, NT, 1, 1>(v, tw, lane);
+  hs_dit<R, INV, NT, 2, 0>(v, tw, lane);
+  hs_dit<R, INV, NT, 3, 1>(v, tw, lane);
+  hs_dit<R, INV, NT, 4, 0>(v, tw, lane);
+  r4_last<R, INV, NT>(v, tw + 128, lane);
 }
 
 template <typename R, int N, bool INV>
@@ -435,12 +421,9 @@ __device__ __forceinline__ void load_twiddles(cplx<R>* s_tw, const cplx<R>* __re
     const int src = (i - off) * r;
     s_tw[i] = g_tw[src < N / 2 ? src : 0];
   }
-  if constexpr (N == 128) {   // radix-4 table: W_128^k with k < 128 from the half table
+  if constexpr (N == 128) {   // radix-4 table: W_128^{l k1} at (k1-1)*32 + l from the half table
     for (int i = threadIdx.x; i < R4_TW; i += blockDim.x) {
-      int k;
-      if (i < 96) k = ((i >> 5) + 1) * (i & 31);
-      else if (i < 120) k = 4 * (((i - 96) >> 3) + 1) * ((i - 96) & 7);
-      else k = 16 * ((i - 120) >> 2) * ((i - 120) & 3);
+      const int k = ((i >> 5) + 1) * (i & 31);
       cplx<R> w = g_tw[k & 63];
       if (k & 64) { w.x = -w.x; w.y = -w.y; }
       s_tw[N + i] = w;
