@@ -185,7 +185,7 @@ void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_
   RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B; p.phys_bstride = phys_bstride;
   if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
-  else if (c->rowtan_xt == 4)
+  else if (N == 128 && c->rowtan_xt == 4)   // 4-row tiles measured faster at n = 128 only
     launch_step(c, B, k_row_tan<R, N, 4>, dim3(B * (N / 4)), dim3(4 * 32), smem_row_rhs<R, N, 4>(), s, p);
   else launch_step(c, B, k_row_tan<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
 }
