@@ -95,6 +95,7 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   if (const char* v = getenv("ECS_PDL")) c->pdl = atoi(v) != 0 ? 1 : 0;
   if (const char* v = getenv("ECS_TGROUPS")) c->tgroups = std::max(1, std::min(ecs_ctx::MAXG, atoi(v)));
   if (const char* v = getenv("ECS_ROWTAN_XT")) c->rowtan_xt = atoi(v) == 4 ? 4 : 8;
+  if (const char* v = getenv("ECS_PDL_MINB")) c->pdl_minb = std::max(1, atoi(v));
   int st;
   const ecs::ImplTable* t = ecs::impl_table(dtype, n);
   st = t ? t->init(c, params) : ECS_ERR_UNSUPPORTED;

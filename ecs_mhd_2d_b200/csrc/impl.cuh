@@ -38,11 +38,12 @@ template <typename R, int N> size_t smem_row_tan2() { return (fft_smem(N, XT) + 
 template <typename R, int N> size_t smem_row_phys() { return (fft_smem(N, XT) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N, int X = XT> size_t smem_row_2f() { return (fft_smem(N, X) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 
-// Launch a stepping kernel of batch B; with c->pdl set and B >= 8, with
-// programmatic stream serialization (the kernel waits on its predecessor
-// itself, see pdl_wait).  Measured at n=128 FP64: the batch-64 tangent kernels
-// gain 5-7%, while single-state chains lose (their launches are already
-// overlapped inside CUDA graphs), hence the batch threshold.
+// Launch a stepping kernel of batch B; with c->pdl set, with programmatic
+// stream serialization (the kernel waits on its predecessor itself, see
+// pdl_wait), so that a kernel's launch and prologue overlap its predecessor's
+// tail.  Measured at n=128 FP64: the batch-64 tangent kernels gain 5-7%, and
+// single-state chains inside CUDA graphs gain 10-24% (gradient, plain JVP,
+// Lawson-RK4), except the pipelined linearisation's primal (see below).
 template <typename... P, typename... A>
 inline void launch_step(ecs_ctx* c, int B, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                         A... args) {
@@ -51,10 +52,25 @@ inline void launch_step(ecs_ctx* c, int B, void (*k)(P...), dim3 grid, dim3 bloc
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at; cfg.numAttrs = (c->pdl && B >= 8) ? 1 : 0;
+  // inside a PlainOrder scope small batches keep plain stream order (see PlainOrder)
+  const bool plain = c->plain_order > 0 && B < 8;
+  cfg.attrs = at; cfg.numAttrs = (c->pdl && B >= c->pdl_minb && !plain) ? 1 : 0;
   ++c->launches;
   cudaLaunchKernelEx(&cfg, k, args...);
 }
+
+// Scope in which batches below 8 launch without programmatic dependent launch:
+// the adaptive Lawson-RK4(3) solve and the fixed-step integrations measured
+// 5-10% slower with it at batch 1, and the batch-1 primal that runs beside the
+// tangent batch (pipelined linearisation) would park early-launched CTAs on
+// SMs that the tangents need.  Graphs captured inside the scope keep it.
+struct PlainOrder {
+  ecs_ctx* c;
+  explicit PlainOrder(ecs_ctx* c_) : c(c_) { ++c->plain_order; }
+  ~PlainOrder() { --c->plain_order; }
+  PlainOrder(const PlainOrder&) = delete;
+  PlainOrder& operator=(const PlainOrder&) = delete;
+};
 
 template <typename R, int N>
 int configure_kernels(ecs_ctx* c) {
@@ -388,6 +404,7 @@ struct Impl {
   // Fixed-step RK4 / Lawson-RK6 / TDRK4 over `steps` steps from slot X_F of S43
   // (h and e from fx_setup); 16-step CUDA graphs per scheme.
   static int integrate_fx(ecs_ctx* c, int scheme, int B, long steps, cudaStream_t s) {
+    PlainOrder plain_order(c);
     if (steps <= 0) return ECS_OK;
     constexpr int GS = 16;
     R* phys = nullptr;
@@ -502,6 +519,7 @@ struct Impl {
   static int rk43_solve(ecs_ctx* c, const ecs_shoot_cfg* cfg, const double* T, int B, cudaStream_t s,
                         cplx<R>* rec = nullptr, double* rec_h = nullptr, int* rec_acc = nullptr, int cap = 0,
                         bool launch = true) {
+    PlainOrder plain_order(c);
     const long amax = (long)cfg->checkpoints * cfg->max_steps_per_checkpoint;
     if (amax <= 0) return set_err(c, ECS_ERR_INVALID, "checkpoints * max_steps_per_checkpoint must be > 0");
     ++c->launches; k_rk43_setup<<<(B + 127) / 128, 128, 0, s>>>(T, cfg->h0, c->ctl, B);
@@ -1156,6 +1174,7 @@ struct Impl {
     auto primal_chunk = [&](long k) -> cudaError_t {
       void* const Gs = c->G; void* const Hs = c->H;
       c->G = c->Gp; c->H = c->Hp;
+      PlainOrder plain_order(c);
       if (k == 0) launch_col_rk4<R, N>(c, 1, COL_START, 1, 0, ps);
       for (long it = k * CS; it < std::min(steps, (k + 1) * CS); ++it) {
         cplx<R>* rs = rec + (size_t)it * Q_NREC * VEC;
