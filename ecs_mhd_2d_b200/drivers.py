@@ -134,6 +134,74 @@ def newton_block_gmres_update(input_dict, param_dict, mode, block=8, m=4, seed=0
                  "damp": damp, "T": new["T"], "sx": new["sx"]}
 
 
+def second_directional_derivative(obj, input_dict, v, eps=None):
+    """K(v) = d^2 objective[v, v] at input_dict for a flat direction v ([T,
+    fields, sx]), as the nested jax.jvp of jax_scripts/acceleration.py:127-129
+    computes it.  Here it is the central difference of two JVPs along v at
+    x +- eps v (each a linearisation and one tangent on the device), error
+    O(eps^2) (a few 1e-7 relative at the default eps = 1e-5 max(|x|, 1) / |v|),
+    except for the two phase conditions: they are linear in the state with
+    stop-gradient coefficients (loss_functions.py:113-130), so their second
+    derivative is exactly zero, while the difference would also differentiate
+    those coefficients; their entries are set to zero.  `obj` should be an
+    Objective of its own (its linearisations move to x +- eps v)."""
+    x_dict = _as_device_dict(input_dict)
+    n = x_dict["fields"].shape[-1]
+    x = flatten(x_dict)
+    v = v.to(torch.float64)
+    if eps is None:
+        eps = 1e-5 * max(float(torch.linalg.norm(x)), 1.0) / float(torch.linalg.norm(v))
+    t = unflatten(v, n)
+    tan = {"fields": t["fields"].contiguous(), "T": t["T"], "sx": t["sx"]}
+
+    def jv(xs):
+        d = unflatten(xs, n)
+        return flatten(obj.jvp({"fields": d["fields"].contiguous(), "T": float(d["T"]), "sx": float(d["sx"])}, tan))
+
+    k = (jv(x + eps * v) - jv(x - eps * v)) / (2 * eps)
+    k[0] = 0.0    # pt (flat order [pt, fields, px])
+    k[-1] = 0.0   # px
+    return k
+
+
+def geodesic_acceleration_update(input_dict, param_dict, mode, inner=16, obj=None, obj_k=None):
+    """One Newton-GMRES update with geodesic acceleration
+    (jax_scripts/acceleration.py:103-168): step1 solves J s = -f, step2 solves
+    J s = -K(step1)/2 with the second directional derivative K, both by GMRES
+    with the transpose preconditioner; x <- x + step1 + step2, then dealias.
+    K is the central difference of two JVPs (second_directional_derivative)
+    where the reference nests jax.jvp.  Returns (new_input_dict, stats)."""
+    obj = obj or Objective(param_dict, mode)
+    obj_k = obj_k or Objective(param_dict, mode)
+    x_dict = _as_device_dict(input_dict)
+    n = x_dict["fields"].shape[-1]
+    f = obj(x_dict)
+    b = -flatten(f)                                                    # acceleration.py:114
+
+    def J(v):                                                          # :117
+        t = unflatten(v, n)
+        return flatten(obj.jvp(x_dict, {"fields": t["fields"].contiguous(), "T": t["T"], "sx": t["sx"]}))
+
+    _, jacT = vjp(obj, x_dict)                                         # :120-121
+
+    def J_T(v):
+        t = unflatten(v, n)
+        g = jacT({"fields": t["fields"].contiguous(), "T": t["T"], "sx": t["sx"]})[0]
+        return flatten({"fields": g["fields"], "T": g["T"], "sx": g["sx"]})
+
+    step1, res1 = gmres(J, b, inner, 1, [J_T])                         # :124
+    r = -second_directional_derivative(obj_k, x_dict, step1) / 2       # :127-131
+    step2, res2 = gmres(J, r, inner, 1, [J_T])                         # :134
+    new = unflatten(flatten(x_dict) + step1 + step2, n)                # :137-142
+    rel_err = relative_error_RPO(new, f)                               # :148
+    new = {"fields": dealias(new["fields"].contiguous(), param_dict), "T": float(new["T"]),
+           "sx": float(new["sx"])}                                     # :163-167
+    stats = {"rel_err": float(rel_err), "|f|": float(torch.linalg.norm(b)), "gmres_rel_res": float(res1),
+             "gmres_rel_res_2": float(res2), "|step1|": float(torch.linalg.norm(step1)),
+             "|step2|": float(torch.linalg.norm(step2)), "T": new["T"], "sx": new["sx"]}
+    return new, stats
+
+
 def init_adam(params):
     """Zero moments (jax_scripts/lib/adam.py:7-20)."""
     return ({k: 0 * torch.as_tensor(v) for k, v in params.items()},
