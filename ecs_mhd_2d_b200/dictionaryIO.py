@@ -83,3 +83,38 @@ def recompute_grid_information(input_dict, param_dict):
     b0 = param_dict.get("b0", [0.0, 0.1])
     param_dict["b0"] = [float(b0[0]), float(b0[1])]
     return param_dict
+
+
+def change_resolution(f, n):
+    """A real field [..., m, m] resampled to [..., n, n] spectrally
+    (jax_scripts/upscale_state.py:29-47): fft2, the four corner blocks of
+    min(m, n)//2 wavenumbers copied (the Nyquist line is dropped), ifft2 scaled
+    by (n/m)^2, real part.  Runs on the tensor's device."""
+    f = torch.as_tensor(f)
+    m = f.shape[-1]
+    F = torch.fft.fft2(f.to(torch.float64))
+    F2 = torch.zeros(tuple(f.shape[:-2]) + (n, n), dtype=torch.complex128, device=f.device)
+    m2 = min(m, n) // 2
+    F2[..., :m2, :m2] = F[..., :m2, :m2]
+    F2[..., n - m2:, :m2] = F[..., m - m2:, :m2]
+    F2[..., :m2, n - m2:] = F[..., :m2, m - m2:]
+    F2[..., n - m2:, n - m2:] = F[..., m - m2:, m - m2:]
+    return (torch.fft.ifft2(F2) * (n / m) ** 2).real
+
+
+def upscale_state(input_dict, param_dict, n):
+    """A state and its parameters at resolution n (jax_scripts/upscale_state.py:48-63):
+    both field channels and the forcing resampled by change_resolution, the grid
+    tables rebuilt for n; T, sx and the other parameters unchanged.  Returns
+    new (input_dict, param_dict); save_dicts writes them in the reference's
+    format (the forcing is stored as its forcing_str, as the reference does)."""
+    fields = torch.as_tensor(input_dict["fields"])
+    inp = dict(input_dict)
+    inp["fields"] = change_resolution(fields, n).to(fields.dtype)
+    par = dict(param_dict)
+    dt = fields.dtype if fields.is_floating_point() else torch.float64
+    par.update(construct_domain(n, dt))
+    if "forcing" in param_dict:
+        fr = change_resolution(torch.as_tensor(param_dict["forcing"]), n)
+        par["forcing"] = fr.to(dtype=dt, device=par["x"].device)
+    return inp, par

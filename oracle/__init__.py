@@ -27,6 +27,6 @@ from .mhd_oracle import (  # noqa: F401
     rk4, lawson_rk4, lawson_rk6, tdrk4, lawson_rk43,
     shift_x, shift_reflect, rot180,
     mismatch_RPO, loss_RPO, phase_conditions, objective_RPO,
-    make_param_dict, ravel_dict, unravel_dict,
+    make_param_dict, ravel_dict, unravel_dict, change_resolution,
     gmres, line_search_unravel,
 )

@@ -494,6 +494,19 @@ def make_param_dict(n, nu, eta, b0=(0.0, 0.1), forcing="kolmogorov", xp: Backend
     return pd
 
 
+def change_resolution(f, n):
+    """Restates change_resolution (jax_scripts/upscale_state.py:29-47) in numpy."""
+    m = f.shape[-1]
+    F = np.fft.fft2(f)
+    F2 = np.zeros(f.shape[:-2] + (n, n), dtype=np.complex128)
+    m2 = min(m, n) // 2                                              # :36
+    F2[..., 0:m2, 0:m2] = F[..., 0:m2, 0:m2]                         # :40-43
+    F2[..., n - m2:, 0:m2] = F[..., -m2:, 0:m2]
+    F2[..., 0:m2, n - m2:] = F[..., 0:m2, -m2:]
+    F2[..., n - m2:, n - m2:] = F[..., -m2:, -m2:]
+    return np.real(np.fft.ifft2(F2) * (n / m) ** 2)                  # :45, :47
+
+
 def ravel_dict(d, xp: Backend = NUMPY):
     """Flatten {"T","fields","sx"} in jax ravel_pytree order (sorted keys): [T, fields, sx]."""
     if xp.is_torch:
