@@ -28,5 +28,6 @@ from .mhd_oracle import (  # noqa: F401
     shift_x, shift_reflect, rot180,
     mismatch_RPO, loss_RPO, phase_conditions, objective_RPO,
     make_param_dict, ravel_dict, unravel_dict, change_resolution,
+    compute_observables, laminar_flow,
     gmres, line_search_unravel,
 )

@@ -507,6 +507,30 @@ def change_resolution(f, n):
     return np.real(np.fft.ifft2(F2) * (n / m) ** 2)                  # :45, :47
 
 
+def compute_observables(f, param_dict):
+    """Restates compute_observables (jax_scripts/projection.py:19-46) in numpy."""
+    n = f.shape[-2]
+    u = np.fft.irfft2(1j * param_dict["to_u"] * f[0], s=(n, n))                # :32
+    v = np.fft.irfft2(1j * param_dict["to_v"] * f[0], s=(n, n))                # :33
+    force = np.fft.rfft2(param_dict["forcing"])                                 # :35
+    fx = np.fft.irfft2(1j * param_dict["to_u"] * force, s=(n, n))               # :36
+    fy = np.fft.irfft2(1j * param_dict["to_v"] * force, s=(n, n))               # :37
+    injection = np.mean(u * fx + v * fy)                                        # :40
+    d = np.mean(np.square(np.fft.irfft2(f, s=(n, n))), axis=(-1, -2))           # :43
+    return np.array([injection, param_dict["nu"] * d[0] + param_dict["eta"] * d[1]])   # :44-45
+
+
+def laminar_flow(param_dict):
+    """Restates laminar_flow (jax_scripts/projection.py:49-73)."""
+    alpha = param_dict["b0"][1]
+    L = np.sqrt(param_dict["eta"] * param_dict["nu"]) / alpha
+    k = 4.0
+    y = param_dict["y"]
+    U0 = param_dict["eta"] / (alpha * alpha * (1 + L * L * k * k))
+    B0 = 1.0 / (k * alpha * (1 + L * L * k * k))
+    return np.stack([-U0 * k * np.cos(k * y), B0 * k * np.sin(k * y)])
+
+
 def ravel_dict(d, xp: Backend = NUMPY):
     """Flatten {"T","fields","sx"} in jax ravel_pytree order (sorted keys): [T, fields, sx]."""
     if xp.is_torch:
