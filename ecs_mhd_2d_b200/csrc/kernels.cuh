@@ -318,13 +318,23 @@ __device__ __forceinline__ const R* phys_row(const R* base, int x) {
   return base + (size_t)x * NPH * N;
 }
 
-// Load a [nf][K][XT] tile of a [B][nf][K][N] array into shared memory with row pitch XT+1.
+// Load a [nf][K][XT] tile of a [B][nf][K][N] array into shared memory with row
+// pitch XT+1.  Asynchronous copies (cp.async: global -> shared without a
+// register round trip; 16 bytes per complex double, 8 per complex float);
+// each thread waits for its own copies before returning, and the caller's
+// __syncthreads then makes the whole tile visible.
 template <typename R, int N, int XT>
 __device__ __forceinline__ void load_tile(cplx<R>* s, const cplx<R>* __restrict__ g, int nfK, int x0) {
   for (int i = threadIdx.x; i < nfK * XT; i += blockDim.x) {
     const int xt = i % XT, r = i / XT;
-    s[r * (XT + 1) + xt] = g[(size_t)r * N + x0 + xt];
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(s + r * (XT + 1) + xt);
+    const cplx<R>* src = g + (size_t)r * N + x0 + xt;
+    if constexpr (sizeof(cplx<R>) == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 template <typename R, int N, int XT>
 __device__ __forceinline__ void store_tile(cplx<R>* __restrict__ g, const cplx<R>* s, int nfK, int x0) {
