@@ -24,8 +24,9 @@
 // output permutation spec_pos are listed below for each N.
 //
 // Twiddles come from a table tw[k] = exp(-2 pi i k / N), k in [0, N/2),
-// computed on the host in long double.  In shared memory it is expanded to one
-// contiguous sub-table per index stride r = 1, 2, 4, ...:
+// computed on the host in long double, and expanded on the host (twiddle_image)
+// into the shared-memory layout: one contiguous sub-table per index stride
+// r = 1, 2, 4, ...:
 //   s_tw[tw_off(N, r) + i] = tw[i r],  i < N / (2 r),  tw_off(N, r) = N - N / r,
 // so that the lanes of a stage read consecutive entries, followed by the
 // radix-E pass's table s_tw[N + (k1-1)*32 + l] = W_N^{l k1}, k1 = 1..E-1.
@@ -249,22 +250,39 @@ __device__ __forceinline__ void fft_dit2(cplx<R> (&a)[N / 32], cplx<R> (&b)[N / 
   fft_dit_n<R, INV, 2, N>(ptrs, tw, lane);
 }
 
-// Cooperative expansion of the N/2-entry twiddle table into the tw_smem(N)
-// shared entries: the strided sub-tables, then the radix-E pass's table.
-template <typename R, int N>
-__device__ __forceinline__ void load_twiddles(cplx<R>* s_tw, const cplx<R>* __restrict__ g_tw) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+// The shared-memory twiddle image (tw_smem(N) entries) built from the half
+// table half[k] = exp(-2 pi i k / N), k < N/2: the strided sub-tables, then the
+// radix-E pass's table W_N^{l k1} (k >= N/2 taken as -W_N^{k - N/2}).  Built
+// once on the host when a context is created.
+template <typename C, int N>
+__host__ __device__ inline void twiddle_image(const C* half, C* img) {
+  for (int i = 0; i < N; ++i) {
     int r = 1, off = 0;
     while (r < N / 2 && i >= off + N / (2 * r)) { off += N / (2 * r); r *= 2; }
     const int src = (i - off) * r;
-    s_tw[i] = g_tw[src < N / 2 ? src : 0];
+    img[i] = half[src < N / 2 ? src : 0];
   }
-  for (int i = threadIdx.x; i < tw_first(N); i += blockDim.x) {
-    const int k = ((i >> 5) + 1) * (i & 31);   // W_N^k, k < N (k >= N/2: -W_N^{k - N/2})
-    cplx<R> w = g_tw[k & (N / 2 - 1)];
+  for (int i = 0; i < tw_first(N); ++i) {
+    const int k = ((i >> 5) + 1) * (i & 31);
+    C w = half[k & (N / 2 - 1)];
     if (k & (N / 2)) { w.x = -w.x; w.y = -w.y; }
-    s_tw[N + i] = w;
+    img[N + i] = w;
   }
+}
+
+// Copy of the twiddle image into shared memory (cp.async: global -> shared
+// without a register round trip); each thread waits for its own copies and the
+// caller's __syncthreads makes the table visible.
+template <typename R, int N>
+__device__ __forceinline__ void load_twiddles(cplx<R>* s_tw, const cplx<R>* __restrict__ g_img) {
+  for (int i = threadIdx.x; i < tw_smem(N); i += blockDim.x) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(s_tw + i);
+    if constexpr (sizeof(cplx<R>) == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(g_img + i) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(g_img + i) : "memory");
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 }  // namespace ecs

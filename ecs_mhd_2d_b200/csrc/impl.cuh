@@ -1804,7 +1804,7 @@ int ctx_init(ecs_ctx* c, const ecs_params* prm) {
   c->ctl = (StepCtl*)dev_alloc(c, (size_t)B * sizeof(StepCtl), &st);
   c->rowsq = (double*)dev_alloc(c, (size_t)B * N * sizeof(double), &st);
   c->Tbuf = (double*)dev_alloc(c, (size_t)B * sizeof(double), &st);
-  c->tw = dev_alloc(c, (N / 2) * cb, &st);
+  c->tw = dev_alloc(c, (size_t)tw_smem(N) * cb, &st);   // the shared-memory twiddle image
   c->fhat = dev_alloc(c, (size_t)Geomc<N>::K * Geomc<N>::M * cb, &st);
   if (st) return st;
   if (cudaMallocHost((void**)&c->hcount, sizeof(int)) != cudaSuccess) return set_err(c, ECS_ERR_OOM, "pinned alloc");
@@ -1817,7 +1817,9 @@ int ctx_init(ecs_ctx* c, const ecs_params* prm) {
     long double a = twopi * (long double)k / (long double)N;
     tw[k] = mk<R>((R)cosl(a), (R)(-sinl(a)));
   }
-  cudaError_t e = cudaMemcpy(c->tw, tw.data(), tw.size() * cb, cudaMemcpyHostToDevice);
+  std::vector<cplx<R>> img(tw_smem(N));
+  twiddle_image<cplx<R>, N>(tw.data(), img.data());
+  cudaError_t e = cudaMemcpy(c->tw, img.data(), img.size() * cb, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_err(c, e, "twiddle upload");
   // forcing on the grid x_i = i/n * 2 * pi (mhd_jax.py:47), channel omega only
   std::vector<R> fr((size_t)2 * N * N, R(0));

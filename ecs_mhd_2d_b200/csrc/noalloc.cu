@@ -38,9 +38,9 @@ constexpr size_t CB = sizeof(double2);
 constexpr size_t al(size_t x) { return (x + 255) / 256 * 256; }
 
 // Byte layout of the static scratch (sized for n = 128, batch = 4).
-constexpr size_t OFF_TW64 = 0;                                                   // 32 twiddles
-constexpr size_t OFF_TW128 = al(OFF_TW64 + 32 * CB);                             // 64 twiddles
-constexpr size_t OFF_CTL = al(OFF_TW128 + 64 * CB);                              // step controls (zeroed)
+constexpr size_t OFF_TW64 = 0;                                                   // twiddle image, n = 64
+constexpr size_t OFF_TW128 = al(OFF_TW64 + tw_smem(64) * CB);                    // twiddle image, n = 128
+constexpr size_t OFF_CTL = al(OFF_TW128 + tw_smem(128) * CB);                    // step controls (zeroed)
 constexpr size_t OFF_FIELDS = al(OFF_CTL + NA_MAX_BATCH * sizeof(StepCtl));      // [forcing; 0] real [2][n][n]
 constexpr size_t OFF_FBOX = al(OFF_FIELDS + 2 * NA_MAX_N * NA_MAX_N * sizeof(double));   // forcing box [2][K][M]
 constexpr size_t OFF_F = al(OFF_FBOX + 2 * NA_K * NA_M * CB);                    // input box [B][2][K][M]
@@ -67,8 +67,10 @@ int na_setup_twiddles(unsigned char* base, size_t off) {
     const long double a = twopi * (long double)k / (long double)N;
     tw[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
   }
-  return cudaMemcpy(base + off, tw.data(), tw.size() * CB, cudaMemcpyHostToDevice) == cudaSuccess ? ECS_OK
-                                                                                                : ECS_ERR_CUDA;
+  std::vector<double2> img(tw_smem(N));
+  twiddle_image<double2, N>(tw.data(), img.data());
+  return cudaMemcpy(base + off, img.data(), img.size() * CB, cudaMemcpyHostToDevice) == cudaSuccess ? ECS_OK
+                                                                                                  : ECS_ERR_CUDA;
 }
 
 template <int N> size_t na_smem_rhs() { return (fft_smem(N, NA_XT) + (NG + NH) * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
