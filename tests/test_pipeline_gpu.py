@@ -92,3 +92,30 @@ def test_linearize_jvp_repeated_calls(cuda):
     first = obj.linearize_jvp(prim, tan)[1]["fields"].clone()
     for _ in range(2):
         assert torch.equal(obj.linearize_jvp(prim, tan)[1]["fields"], first)
+
+
+@pytest.mark.parametrize("env", [{"ECS_ROWTAN_XT": "8"}, {"ECS_PDL_MINB": "8"}, {"ECS_TGROUPS": "1"}])
+def test_tuning_switches_do_not_change_results(cuda, env, monkeypatch):
+    """The tuning switches (read when a context is created) change launch
+    shapes and ordering only: the objective and a batch of 64 tangents at
+    n = 128 are bit for bit those of the defaults."""
+    from ecs_mhd_2d_b200 import context
+    n, B = 128, 64
+    kw = dict(shift_reflect_ny=0, rot=False, adaptive_dict={"atol": 1e-7, "checkpoints": 2, "max_steps_per_checkpoint": 32})
+    pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", **kw)
+    prim, tan = _inputs(n, B)
+    prim["T"] = 0.3
+
+    def run():
+        context.clear_cache()
+        v, t = E.Objective(pd, "Lawson_RK43").linearize_jvp(prim, tan)
+        return v["fields"].cpu().numpy(), t["fields"].cpu().numpy(), t["T"].cpu().numpy()
+
+    base = run()
+    for k, val in env.items():
+        monkeypatch.setenv(k, val)
+    other = run()
+    monkeypatch.undo()
+    context.clear_cache()
+    for a, b in zip(base, other):
+        assert np.array_equal(a, b)
