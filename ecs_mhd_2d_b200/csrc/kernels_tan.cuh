@@ -122,14 +122,18 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
   // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
-  // the tile load and the inverse transforms
+  // the tile load and the inverse transforms (n <= 128); at n = 256 they would
+  // hold 4 E = 32 registers across the transform, so they are loaded after it
   const R* ph = phys_row<R, N>(p.phys + (size_t)b * p.phys_bstride, x);
   R pu[E], pv[E], pbx[E], pby[E];
+  auto load_phys = [&]() {
 #pragma unroll
-  for (int j = 0; j < E; ++j) {
-    const int e = lane + 32 * j;
-    pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
-  }
+    for (int j = 0; j < E; ++j) {
+      const int e = lane + 32 * j;
+      pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
+    }
+  };
+  if constexpr (N <= 128) load_phys();
   load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   cplx<R> duv[E], dbb[E];
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
     dbb[j] = packed_pair<R, N, XT>(s_G + 2 * K * (XT + 1), s_G + 3 * K * (XT + 1), q, w);
   }
   fft_dif2<R, N, true>(duv, dbb, s_tw, lane);
+  if constexpr (N > 128) load_phys();
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const R du = duv[j].x, dv = duv[j].y, dbx = dbb[j].x, dby = dbb[j].y;
