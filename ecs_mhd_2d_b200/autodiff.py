@@ -51,7 +51,7 @@ class Objective:
             ctx.ensure_batch(batch)
         else:
             ctx = _ctx.get_context(self.param_dict, n, fields.dtype, batch)
-        key = (id(ctx), ctx.handle.value if ctx.handle else None) + self._primal_key(input_dict["fields"]
+        key = (ctx.generation,) + self._primal_key(input_dict["fields"]
                                                                                     if isinstance(input_dict["fields"], torch.Tensor)
                                                                                     else fields, T[0], sx[0])
         if not force and key == self._key and self._ctx is ctx:
@@ -91,7 +91,7 @@ class Objective:
         ctx.call("ecs_linearize_jvp", self.cfg, _ctx.ptr(fields), _ctx.ptr(T), _ctx.ptr(sx), _ctx.ptr(out), info,
                  _ctx.ptr(dfields), _ctx.ptr(dT), _ctx.ptr(dsx), _ctx.ptr(dout), _ctx.ptr(oT), _ctx.ptr(osx), B,
                  _ctx.stream_ptr())
-        key = (id(ctx), ctx.handle.value if ctx.handle else None) + self._primal_key(
+        key = (ctx.generation,) + self._primal_key(
             primal_dict["fields"] if isinstance(primal_dict["fields"], torch.Tensor) else fields, T[0], sx[0])
         self._key, self._ctx = key, ctx
         self._fields_ref = (fields, T, sx)

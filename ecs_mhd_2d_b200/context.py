@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import hashlib
+import itertools
 
 import numpy as np
 import torch
@@ -42,8 +43,15 @@ def ptr(t: torch.Tensor):
     return ctypes.c_void_p(t.data_ptr())
 
 
+_GENERATION = itertools.count(1)
+
+
 class Context:
-    """Owns one ``ecs_ctx`` for (device, n, dtype, nu, eta, b0, forcing)."""
+    """Owns one ``ecs_ctx`` for (device, n, dtype, nu, eta, b0, forcing).
+
+    ``generation`` is unique to each native context this process creates
+    (growing the batch re-creates it, dropping any linearisation it held;
+    the freed handle's address may come back for the new one)."""
 
     def __init__(self, n, dtype, nu, eta, b0, forcing=None, max_batch=1):
         if not torch.cuda.is_available():
@@ -72,6 +80,7 @@ class Context:
         with torch.cuda.device(self.device):
             _lib.check(self.lib.ecs_ctx_create(self.n, self.code, ctypes.byref(prm), max_batch, ctypes.byref(h)))
         self.handle = h
+        self.generation = next(_GENERATION)
         self.max_batch = max_batch
         K, M = ctypes.c_int(), ctypes.c_int()
         _lib.check(self.lib.ecs_box_dims(self.handle, ctypes.byref(K), ctypes.byref(M)), self.handle)

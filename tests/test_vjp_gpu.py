@@ -127,3 +127,25 @@ def test_checkpointed_linearisation_matches_full_record(cuda):
     assert rel_l2(g1["fields"].cpu().numpy(), g0["fields"].cpu().numpy()) < 1e-14
     assert abs(float(g1["T"]) - float(g0["T"])) <= 1e-13 * abs(float(g0["T"]))
     assert abs(float(g1["sx"]) - float(g0["sx"])) <= 1e-13 * max(abs(float(g0["sx"])), 1.0)
+
+
+def test_vjp_after_context_growth(cuda):
+    """A linearisation at batch 1 followed by a batch of cotangents grows (re-creates)
+    the context, which drops the linearisation: the Objective must notice and
+    linearise again, even when the new native context reuses the old address."""
+    from ecs_mhd_2d_b200 import context
+    context.clear_cache()
+    n = 64
+    kw = CASES[0][1]
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", **kw)
+    obj = E.Objective(pd, "Lawson_RK4")
+    prim = {"fields": torch.as_tensor(initial_condition(3, n), device="cuda"), "T": 0.1, "sx": 0.35}
+    _, jacT = E.vjp(obj, prim)
+    rng = np.random.default_rng(6)
+    cot = {"fields": torch.as_tensor(rng.standard_normal((3, 2, n, n)), device="cuda"),
+           "T": torch.zeros(3, dtype=torch.float64), "sx": torch.zeros(3, dtype=torch.float64)}
+    g = jacT(cot)[0]
+    g1 = jacT({"fields": cot["fields"][1].contiguous(), "T": 0.0, "sx": 0.0})[0]
+    assert torch.isfinite(g["fields"]).all()
+    assert torch.allclose(g["fields"][1], g1["fields"], rtol=1e-13, atol=0)
+    context.clear_cache()
