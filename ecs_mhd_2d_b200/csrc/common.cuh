@@ -45,6 +45,15 @@ template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_c(cplx<R> v, i
   v.y = __shfl_xor_sync(0xffffffffu, v.y, m);
   return v;
 }
+// One complex value copied global -> shared with cp.async (no register round
+// trip; 16 bytes for double, 8 for float); completed by cp.async.wait_all.
+template <typename R> __device__ __forceinline__ void cp_async_c(cplx<R>* dst_smem, const cplx<R>* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  if constexpr (sizeof(cplx<R>) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 template <typename R> __device__ __forceinline__ cplx<R> shfl_c(cplx<R> v, int src) {
   v.x = __shfl_sync(0xffffffffu, v.x, src);
   v.y = __shfl_sync(0xffffffffu, v.y, src);

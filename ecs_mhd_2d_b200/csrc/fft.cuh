@@ -275,13 +275,7 @@ __host__ __device__ inline void twiddle_image(const C* half, C* img) {
 // caller's __syncthreads makes the table visible.
 template <typename R, int N>
 __device__ __forceinline__ void load_twiddles(cplx<R>* s_tw, const cplx<R>* __restrict__ g_img) {
-  for (int i = threadIdx.x; i < tw_smem(N); i += blockDim.x) {
-    const unsigned dst = (unsigned)__cvta_generic_to_shared(s_tw + i);
-    if constexpr (sizeof(cplx<R>) == 16)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(g_img + i) : "memory");
-    else
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(g_img + i) : "memory");
-  }
+  for (int i = threadIdx.x; i < tw_smem(N); i += blockDim.x) cp_async_c<R>(s_tw + i, g_img + i);
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 

@@ -327,12 +327,7 @@ template <typename R, int N, int XT>
 __device__ __forceinline__ void load_tile(cplx<R>* s, const cplx<R>* __restrict__ g, int nfK, int x0) {
   for (int i = threadIdx.x; i < nfK * XT; i += blockDim.x) {
     const int xt = i % XT, r = i / XT;
-    const unsigned dst = (unsigned)__cvta_generic_to_shared(s + r * (XT + 1) + xt);
-    const cplx<R>* src = g + (size_t)r * N + x0 + xt;
-    if constexpr (sizeof(cplx<R>) == 16)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-    else
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    cp_async_c<R>(s + r * (XT + 1) + xt, g + (size_t)r * N + x0 + xt);
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }

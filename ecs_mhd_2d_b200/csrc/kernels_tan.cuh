@@ -188,6 +188,27 @@ struct ColTanParams {
   int B, stage, produce;
 };
 
+// Record vectors (bits of Rk43Rec) and tangent slots (bits of Rk43Slot) that the
+// stage algebra of an adaptive stage reads; they are staged per column into
+// shared memory at the start (see k_col_tan).
+__host__ __device__ constexpr unsigned tan_qmask(int stage) {
+  return stage == T43_INIT ? (1u << RR_K1)
+       : stage == T43_A ? (1u << RR_X0) | (1u << RR_K1)
+       : stage == T43_B ? (1u << RR_K2)
+       : stage == T43_C ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_K2) | (1u << RR_K3)
+       : stage == T43_D ? (1u << RR_K4)
+       : stage == T43_E ? (1u << RR_K5) : 0u;
+}
+__host__ __device__ constexpr unsigned tan_dmask(int stage) {
+  return stage == T43_START ? (1u << S_X0)
+       : stage == T43_A ? (1u << S_X0) | (1u << S_K1)
+       : stage == T43_B ? (1u << S_XE)
+       : stage == T43_C ? (1u << S_XE) | (1u << S_K1E) | (1u << S_K2)
+       : stage == T43_D ? (1u << S_K1) | (1u << S_K2) | (1u << S_K3) | (1u << S_X2)
+       : stage == T43_E ? (1u << S_XF) : 0u;
+}
+__host__ __device__ constexpr int popc_c(unsigned m) { return m ? (int)(m & 1u) + popc_c(m >> 1) : 0; }
+
 template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr int E = N / 32;
@@ -208,8 +229,38 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr bool has_rhs = !(STAGE == TS_START || STAGE == T43_A || STAGE == T43_START);
   const R h = (R)p.h, t = (R)p.t;
   const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
+  // The record vectors and tangent slots the stage algebra reads, this column's
+  // rows of them (M entries each), copied into the warp's shared buffer with
+  // cp.async before the forward transform, so that their latency overlaps it
+  // without holding registers (adaptive stages, n <= 128: static shared memory).
+  constexpr unsigned QM = N <= 128 ? tan_qmask(STAGE) : 0u, DM = N <= 128 ? tan_dmask(STAGE) : 0u;
+  constexpr int NQ = popc_c(QM), NOP = NQ + popc_c(DM);
+  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
+  cplx<R>* my_op = s_op + (threadIdx.x >> 5) * NOP * M;
+  if constexpr (NOP > 0) {
+    const size_t row = ((size_t)ch * K + ky) * M;
+    int v = 0;
+#pragma unroll
+    for (int bit = 0; bit < 16; ++bit) {
+      if ((QM >> bit) & 1u) {
+        for (int s2 = lane; s2 < M; s2 += 32) cp_async_c<R>(my_op + v * M + s2, Q + bit * VEC + row + s2);
+        ++v;
+      }
+    }
+#pragma unroll
+    for (int bit = 0; bit < 16; ++bit) {
+      if ((DM >> bit) & 1u) {
+        for (int s2 = lane; s2 < M; s2 += 32) cp_async_c<R>(my_op + v * M + s2, D + bit * VEC + row + s2);
+        ++v;
+      }
+    }
+  }
   cplx<R> r[E];
   if (has_rhs) col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
+  if constexpr (NOP > 0) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+  }
   const R coeff = ch == 0 ? p.nu : p.eta;
   cplx<R> x[E];
 #pragma unroll
@@ -263,41 +314,50 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
       // Lawson-RK4(3): e = exp(t L h/2), de = e L h/2 dt; dk = dt v + t dv with v = k/t
       const R e = exp((t * L) * h / R(2));
       const R de = e * (L * h / R(2)) * dpar;
-      auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / t), cscale(dv, t)); };
+      // staged operands (shared memory) or, without staging, global memory
+      auto QV = [&](int q) -> cplx<R> {
+        if constexpr (NOP > 0) return my_op[popc_c(QM & ((1u << q) - 1u)) * M + slot];
+        else return Q[q * VEC + o];
+      };
+      auto DV = [&](int d) -> cplx<R> {
+        if constexpr (NOP > 0) return my_op[(NQ + popc_c(DM & ((1u << d) - 1u))) * M + slot];
+        else return D[d * VEC + o];
+      };
+      auto dk_of = [&](int q) { return cadd(cscale(QV(q), dpar / t), cscale(dv, t)); };
       switch (STAGE) {
-        case T43_START: xin = D[S_X0 * VEC + o]; break;
+        case T43_START: xin = DV(S_X0); break;
         case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
         case T43_A: {
-          const cplx<R> dxe = cadd(cscale(Q[RR_X0 * VEC + o], de), cscale(D[S_X0 * VEC + o], e));
-          const cplx<R> dk1e = cadd(cscale(Q[RR_K1 * VEC + o], de), cscale(D[S_K1 * VEC + o], e));
+          const cplx<R> dxe = cadd(cscale(QV(RR_X0), de), cscale(DV(S_X0), e));
+          const cplx<R> dk1e = cadd(cscale(QV(RR_K1), de), cscale(DV(S_K1), e));
           D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
           xin = cadd(dxe, cscale(cscale(dk1e, h), R(0.5)));
         } break;
         case T43_B: {
           const cplx<R> dk2 = dk_of(RR_K2);
           D[S_K2 * VEC + o] = dk2;
-          xin = cadd(D[S_XE * VEC + o], cscale(cscale(dk2, h), R(0.5)));
+          xin = cadd(DV(S_XE), cscale(cscale(dk2, h), R(0.5)));
         } break;
         case T43_C: {
           const cplx<R> dk3 = dk_of(RR_K3);
-          const cplx<R> xe = cscale(Q[RR_X0 * VEC + o], e), k1e = cscale(Q[RR_K1 * VEC + o], e);
-          const cplx<R> dx2 = cadd(cscale(xe, de), cscale(D[S_XE * VEC + o], e));
-          const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(D[S_K1E * VEC + o], e));
-          const cplx<R> dk2e = cadd(cscale(Q[RR_K2 * VEC + o], de), cscale(D[S_K2 * VEC + o], e));
-          const cplx<R> dk3e = cadd(cscale(Q[RR_K3 * VEC + o], de), cscale(dk3, e));
+          const cplx<R> xe = cscale(QV(RR_X0), e), k1e = cscale(QV(RR_K1), e);
+          const cplx<R> dx2 = cadd(cscale(xe, de), cscale(DV(S_XE), e));
+          const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(DV(S_K1E), e));
+          const cplx<R> dk2e = cadd(cscale(QV(RR_K2), de), cscale(DV(S_K2), e));
+          const cplx<R> dk3e = cadd(cscale(QV(RR_K3), de), cscale(dk3, e));
           D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
           xin = cadd(dx2, cscale(dk3e, h));
         } break;
         case T43_D: {
           const cplx<R> dk4 = dk_of(RR_K4);
-          const cplx<R> acc = cadd(cadd(cadd(cdiv_r(D[S_K1 * VEC + o], R(6)), cdiv_r(D[S_K2 * VEC + o], R(3))),
-                                        cdiv_r(D[S_K3 * VEC + o], R(3))), cdiv_r(dk4, R(6)));
-          xin = cadd(D[S_X2 * VEC + o], cscale(acc, h));
+          const cplx<R> acc = cadd(cadd(cadd(cdiv_r(DV(S_K1), R(6)), cdiv_r(DV(S_K2), R(3))),
+                                        cdiv_r(DV(S_K3), R(3))), cdiv_r(dk4, R(6)));
+          xin = cadd(DV(S_X2), cscale(acc, h));
           D[S_XF * VEC + o] = xin;
         } break;
         default: {   // T43_E: accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
           D[S_K1 * VEC + o] = dk_of(RR_K5);
-          D[S_X0 * VEC + o] = D[S_XF * VEC + o];
+          D[S_X0 * VEC + o] = DV(S_XF);
         } break;
       }
     }
