@@ -54,6 +54,16 @@ template <typename R> __device__ __forceinline__ void cp_async_c(cplx<R>* dst_sm
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+// One value of 4, 8 or 16 bytes copied global -> shared with cp.async.
+template <typename T> __device__ __forceinline__ void cp_async_v(T* dst_smem, const T* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  if constexpr (sizeof(T) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
 template <typename R> __device__ __forceinline__ cplx<R> shfl_c(cplx<R> v, int src) {
   v.x = __shfl_sync(0xffffffffu, v.x, src);
   v.y = __shfl_sync(0xffffffffu, v.y, src);

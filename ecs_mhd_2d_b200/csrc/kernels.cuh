@@ -228,10 +228,31 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   const int c = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
 
   if (p.use_done && p.ctl[b].done) return;
+  const size_t base = ((size_t)(b * 2 + c) * K + ky) * M;
+  // The rows of F (and A1, K2, the factor e) that the stage algebra reads,
+  // copied into the warp's shared buffers with cp.async before the forward
+  // transform, so that their latency overlaps it (n <= 128).
+  constexpr bool STG = N <= 128 && STAGE >= COL_RK4_S1 && STAGE <= COL_RK4_S4;
+  constexpr int NC = !STG ? 0 : STAGE == COL_RK4_S3 ? 3 : 1;                    // F (A1, K2)
+  constexpr int NRL = (STG && (STAGE == COL_RK4_S1 || STAGE == COL_RK4_S3)) ? 1 : 0;   // e
+  __shared__ __align__(16) cplx<R> s_rc[(NC > 0 ? NC : 1) * 4 * M];   // 4 warps per CTA
+  __shared__ __align__(16) R s_rr[(NRL > 0 ? NRL : 1) * 4 * M];
+  cplx<R>* my_c = s_rc + (threadIdx.x >> 5) * NC * M;
+  R* my_e = s_rr + (threadIdx.x >> 5) * NRL * M;
+  if constexpr (STG) {
+    for (int s2 = lane; s2 < M; s2 += 32) {
+      cp_async_v(my_c + s2, p.F + base + s2);
+      if constexpr (NC == 3) { cp_async_v(my_c + M + s2, p.A1 + base + s2); cp_async_v(my_c + 2 * M + s2, p.K2 + base + s2); }
+      if constexpr (NRL == 1) cp_async_v(my_e + s2, p.Etab + base + s2);
+    }
+  }
   cplx<R> r[E];
   if (STAGE != COL_START) col_load_rhs<R, N>(p.H, b, c, ky, lane, s_tw, r);
+  if constexpr (STG) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+  }
   const R h = (R)p.ctl[b].h;
-  const size_t base = ((size_t)(b * 2 + c) * K + ky) * M;
   cplx<R>* rb = p.rec ? p.rec + (size_t)b * p.rec_bstride : nullptr;
   cplx<R> x[E];
 #pragma unroll
@@ -249,13 +270,19 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
     const size_t i = base + slot;
     const size_t o = ((size_t)c * K + ky) * M + slot;
     auto put = [&](int q, cplx<R> a) { if (rb) rb[q * VEC + o] = a; };
+    // the staged (or, without staging, global) operands at this slot
+    [[maybe_unused]] const cplx<R> FV =
+        STG ? my_c[slot] : ((STAGE >= COL_RK4_S1 && STAGE <= COL_RK4_S4) ? p.F[i] : mk<R>(0, 0));
+    [[maybe_unused]] const cplx<R> A1V = NC == 3 ? my_c[M + slot] : (STAGE == COL_RK4_S3 ? p.A1[i] : mk<R>(0, 0));
+    [[maybe_unused]] const cplx<R> K2V = NC == 3 ? my_c[2 * M + slot] : (STAGE == COL_RK4_S3 ? p.K2[i] : mk<R>(0, 0));
+    [[maybe_unused]] const R EV = NRL == 1 ? my_e[slot] : ((STAGE == COL_RK4_S1 || STAGE == COL_RK4_S3) ? p.Etab[i] : R(0));
     switch (STAGE) {
       case COL_START: x[j] = p.F[i]; break;
       case COL_RK4_S1: {   // k1 = h v(f); f = e f; k1 = e k1; X2 = f + k1/2   (timestepping.py:74-76)
-        const R e = p.Etab[i];
+        const R e = EV;
         cplx<R> k1 = cscale(v, h);
-        put(Q_F, p.F[i]); put(Q_K1, k1);
-        const cplx<R> f = cscale(p.F[i], e);
+        put(Q_F, FV); put(Q_K1, k1);
+        const cplx<R> f = cscale(FV, e);
         k1 = cscale(k1, e);
         p.F[i] = f; p.A1[i] = k1;
         x[j] = cadd(f, cscale(k1, R(0.5)));
@@ -264,14 +291,14 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
       case COL_RK4_S2: {   // k2 = h v(X2); X3 = f + k2/2   (:76-77)
         const cplx<R> k2 = cscale(v, h);
         p.K2[i] = k2;
-        x[j] = cadd(p.F[i], cscale(k2, R(0.5)));
+        x[j] = cadd(FV, cscale(k2, R(0.5)));
         put(Q_K2, k2); put(Q_X3, x[j]);
       } break;
       case COL_RK4_S3: {   // k3; f,k1,k2,k3 *= e; X4 = f + k3; acc = f + k1/6 + k2/3 + k3/3   (:77-80)
-        const R e = p.Etab[i];
+        const R e = EV;
         cplx<R> k3 = cscale(v, h);
         put(Q_K3, k3);
-        const cplx<R> f = cscale(p.F[i], e), a = cscale(p.A1[i], e), q2 = cscale(p.K2[i], e);
+        const cplx<R> f = cscale(FV, e), a = cscale(A1V, e), q2 = cscale(K2V, e);
         k3 = cscale(k3, e);
         x[j] = cadd(f, k3);
         put(Q_X4, x[j]);
@@ -280,7 +307,7 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
       case COL_RK4_S4: {   // k4; f = acc + k4/6   (:79-80)
         const cplx<R> k4 = cscale(v, h);
         put(Q_K4, k4);
-        const cplx<R> f = cadd(p.F[i], cdiv_r(k4, R(6)));
+        const cplx<R> f = cadd(FV, cdiv_r(k4, R(6)));
         p.F[i] = f;
         x[j] = f;
       } break;
