@@ -42,6 +42,16 @@ struct Col43Params {
   int B, stage;
 };
 
+// Slots (bits of Rk43Slot) that the algebra of an attempt stage reads after its
+// forward transform; they are staged per column into shared memory.
+__host__ __device__ constexpr unsigned r43_smask(int stage) {
+  return stage == R43_B ? (1u << S_XE)
+       : stage == R43_C ? (1u << S_XE) | (1u << S_K1E) | (1u << S_K2)
+       : stage == R43_D ? (1u << S_K1) | (1u << S_K2) | (1u << S_K3) | (1u << S_X2)
+       : stage == R43_E ? (1u << S_K4) : 0u;
+}
+__host__ __device__ constexpr int popc_r43(unsigned m) { return m ? (int)(m & 1u) + popc_r43(m >> 1) : 0; }
+
 template <typename R, int N, int STAGE>
 __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   constexpr int E = N / 32;
@@ -64,8 +74,37 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   cplx<R>* rec = p.rec ? p.rec + ((size_t)b * p.cap + (c.attempts < p.cap ? c.attempts : p.cap - 1)) * RR_NREC * VEC
                        : nullptr;
   const bool has_rhs = STAGE != R43_A && STAGE != R43_START;
+  // The slot rows (and, for the vorticity, the forcing row) that the algebra
+  // reads after the forward transform, copied into the warp's shared buffer
+  // with cp.async before it, so that their latency overlaps it (n <= 128).
+  constexpr unsigned SM = N <= 128 ? r43_smask(STAGE) : 0u;
+  constexpr int NS = popc_r43(SM), NOP = NS > 0 ? NS + 1 : 0;   // + the forcing row
+  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
+  cplx<R>* my_op = s_op + (threadIdx.x >> 5) * NOP * M;
+  if constexpr (NOP > 0) {
+    const size_t row = ((size_t)ch * K + ky) * M;
+    int v = 0;
+#pragma unroll
+    for (int bit = 0; bit < 16; ++bit) {
+      if ((SM >> bit) & 1u) {
+        for (int s2 = lane; s2 < M; s2 += 32) cp_async_v(my_op + v * M + s2, S + bit * VEC + row + s2);
+        ++v;
+      }
+    }
+    if (ch == 0)
+      for (int s2 = lane; s2 < M; s2 += 32) cp_async_v(my_op + NS * M + s2, p.fhat + ky * M + s2);
+  }
   cplx<R> r[E];
   if (has_rhs) col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
+  if constexpr (NOP > 0) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncwarp();
+  }
+  // staged (or, without staging, global) slot values at a slot
+  auto SV = [&](int q, size_t o, int slot) -> cplx<R> {
+    if constexpr (NOP > 0) return my_op[popc_r43(SM & ((1u << q) - 1u)) * M + slot];
+    else return S[q * VEC + o];
+  };
   const R coeff = ch == 0 ? p.nu : p.eta;
   cplx<R> x[E];
 #pragma unroll
@@ -77,7 +116,10 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
     cplx<R> v = mk<R>(0, 0);
     if (has_rhs) {
       v = r[j];                                                        // zero at (0,0)
-      if (ch == 0 && !(kx == 0 && ky == 0)) v = cadd(v, p.fhat[ky * M + slot]);
+      if (ch == 0 && !(kx == 0 && ky == 0)) {
+        if constexpr (NOP > 0) v = cadd(v, my_op[NS * M + slot]);
+        else v = cadd(v, p.fhat[ky * M + slot]);
+      }
     }
     const size_t o = ((size_t)ch * K + ky) * M + slot;
     const R L = diss_L<R>(kx, ky, coeff);
@@ -100,15 +142,15 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       case R43_B: {                                  // :270-271
         S[S_K2 * VEC + o] = kv;
         if (rec) rec[RR_K2 * VEC + o] = kv;
-        xin = cadd(S[S_XE * VEC + o], cscale(cscale(kv, h), R(0.5)));
+        xin = cadd(SV(S_XE, o, slot), cscale(cscale(kv, h), R(0.5)));
         if (rec) rec[RR_Y3 * VEC + o] = xin;
       } break;
       case R43_C: {                                  // :271-280
         if (rec) rec[RR_K3 * VEC + o] = kv;
         const R e = exp((t * L) * h / R(2));
-        const cplx<R> x2 = cscale(S[S_XE * VEC + o], e);
-        const cplx<R> k1ee = cscale(S[S_K1E * VEC + o], e);
-        const cplx<R> k2e = cscale(S[S_K2 * VEC + o], e);
+        const cplx<R> x2 = cscale(SV(S_XE, o, slot), e);
+        const cplx<R> k1ee = cscale(SV(S_K1E, o, slot), e);
+        const cplx<R> k2e = cscale(SV(S_K2, o, slot), e);
         const cplx<R> k3e = cscale(kv, e);
         S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
         S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
@@ -118,16 +160,16 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       case R43_D: {                                  // :280-281
         S[S_K4 * VEC + o] = kv;
         if (rec) rec[RR_K4 * VEC + o] = kv;
-        const cplx<R> acc = cadd(cadd(cadd(cdiv_r(S[S_K1 * VEC + o], R(6)), cdiv_r(S[S_K2 * VEC + o], R(3))),
-                                      cdiv_r(S[S_K3 * VEC + o], R(3))), cdiv_r(kv, R(6)));
-        xin = cadd(S[S_X2 * VEC + o], cscale(acc, h));
+        const cplx<R> acc = cadd(cadd(cadd(cdiv_r(SV(S_K1, o, slot), R(6)), cdiv_r(SV(S_K2, o, slot), R(3))),
+                                      cdiv_r(SV(S_K3, o, slot), R(3))), cdiv_r(kv, R(6)));
+        xin = cadd(SV(S_X2, o, slot), cscale(acc, h));
         S[S_XF * VEC + o] = xin;
         if (rec) rec[RR_XF * VEC + o] = xin;
       } break;
       default: {                                     // R43_E: :282, :288
         S[S_K5 * VEC + o] = kv;
         if (rec) rec[RR_K5 * VEC + o] = kv;
-        xin = cdiv_r(cscale(csub(kv, S[S_K4 * VEC + o]), h), R(6));
+        xin = cdiv_r(cscale(csub(kv, SV(S_K4, o, slot)), h), R(6));
       } break;
     }
     x[j] = xin;
