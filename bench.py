@@ -453,7 +453,7 @@ def main():
     h2d = u0_pin.numel() * 8 + tf_pin.numel() * 8 + 2 * BATCH * 8 + 16
     d2h = out_pin.numel() * 8 + 2 * BATCH * 8
     e2e_times = []
-    for _ in range(args.steps):
+    for it in range(args.warmup + args.steps):   # the same untimed warm-up as the device-resident loop
         flush.zero_()
         torch.cuda.synchronize()
         barrier()
@@ -467,7 +467,8 @@ def main():
         oT_pin.copy_(o["T"], non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
-        e2e_times.append(e0.elapsed_time(e1))
+        if it >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
     te = max_over_ranks(sum(e2e_times), world, dev)
     e2e_value = whole_job_rate(world, BATCH * args.steps, te / 1e3)
 
