@@ -14,7 +14,7 @@ import torch
 
 from . import _lib
 from . import context as _ctx
-from .loss_functions import objective_RPO, prep_inputs, shoot_cfg
+from .loss_functions import _empty_like_out, grid_of, objective_RPO, prep_inputs, shoot_cfg
 
 
 class Objective:
@@ -76,8 +76,12 @@ class Objective:
         fields, T, sx, _ = prep_inputs(primal_dict)
         if fields.shape[0] != 1:
             raise ValueError("linearize_jvp takes one primal point")
-        dfields, dT, dsx, batched = prep_inputs(tangent_dict)
+        dfields, dT, dsx, batched = prep_inputs(tangent_dict, n=fields.shape[-1], dtype=fields.dtype,
+                                                what="tangent fields")
         B, n = dfields.shape[0], fields.shape[-1]
+        if B == 0:
+            self.linearize(primal_dict)
+            return self.last_value, _empty_like_out(dfields)
         if self._own_ctx is not None:
             ctx = self._own_ctx
             ctx.ensure_batch(B)
@@ -104,8 +108,11 @@ class Objective:
 
     def jvp(self, primal_dict, tangent_dict):
         """Tangent of objective_RPO at primal_dict; tangent_dict may carry a leading batch dim."""
-        dfields, dT, dsx, batched = prep_inputs(tangent_dict)
+        n, dtype = grid_of(primal_dict)
+        dfields, dT, dsx, batched = prep_inputs(tangent_dict, n=n, dtype=dtype, what="tangent fields")
         B = dfields.shape[0]
+        if B == 0:
+            return _empty_like_out(dfields)
         ctx = self.linearize(primal_dict, batch=B)
         out = torch.empty_like(dfields)
         oT = torch.empty(B, dtype=torch.float64, device=dfields.device)
@@ -134,8 +141,11 @@ def compile_objective_and_Jacobian(input_dict, param_dict, obj):
 
 
 def _vjp_call(obj, primal_dict, cot):
-    cf, cT, csx, batched = prep_inputs(cot)
+    n, dtype = grid_of(primal_dict)
+    cf, cT, csx, batched = prep_inputs(cot, n=n, dtype=dtype, what="cotangent fields")
     B = cf.shape[0]
+    if B == 0:
+        return _empty_like_out(cf)
     ctx = obj.linearize(primal_dict, batch=B)
     g = torch.empty_like(cf)
     gT = torch.empty(B, dtype=torch.float64, device=cf.device)

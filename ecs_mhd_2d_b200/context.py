@@ -43,6 +43,27 @@ def ptr(t: torch.Tensor):
     return ctypes.c_void_p(t.data_ptr())
 
 
+# Shape checks run on the host before any pointer reaches a kernel: the
+# kernels take sizes from the context (n) and the call (batch), so a tensor
+# of another shape would be read or written past its end.
+
+def check_fields(f, what="fields", n=None):
+    """A real state [2, n, n] or a batch [B, 2, n, n]; with `n`, of that side."""
+    if f.dim() not in (3, 4) or f.shape[-3] != 2 or f.shape[-1] != f.shape[-2]:
+        raise ValueError(f"{what} must be [2, n, n] or [B, 2, n, n], got {tuple(f.shape)}")
+    if n is not None and f.shape[-1] != n:
+        raise ValueError(f"{what} has grid side {f.shape[-1]}, the primal has {n}")
+
+
+def check_spectral(f, what="state"):
+    """rfft2 coefficients [..., 2, n, n//2+1] (complex); returns n."""
+    if not torch.is_complex(f):
+        raise TypeError(f"{what} must be the rfft2 coefficients (complex), got {f.dtype}")
+    if f.dim() < 3 or f.shape[-3] != 2 or f.shape[-1] != f.shape[-2] // 2 + 1:
+        raise ValueError(f"{what} must be [..., 2, n, n//2+1], got {tuple(f.shape)}")
+    return f.shape[-2]
+
+
 _GENERATION = itertools.count(1)
 
 
@@ -119,6 +140,8 @@ def _forcing_key(forcing):
 def get_context(param_dict, n, dtype, batch=1):
     """Context for the physics in ``param_dict`` (nu, eta, b0, forcing)."""
     fk = _forcing_key(param_dict.get("forcing"))
+    if fk is not None and fk[1].size != int(n) * int(n):
+        raise ValueError(f"param_dict['forcing'] has shape {fk[1].shape}, the fields are {n}x{n}")
     key = (torch.cuda.current_device(), int(n), dtype, float(param_dict["nu"]), float(param_dict["eta"]),
            float(param_dict["b0"][0]), float(param_dict["b0"][1]), None if fk is None else fk[0])
     ctx = _CACHE.get(key)

@@ -33,6 +33,8 @@ def gmres(A, b, inner, outer=1, preconditioner_list=()):
     """Returns (x, rel_res) with the reference's semantics: left preconditioners
     applied in order, MGS Arnoldi without re-orthogonalisation, no restarts
     (`outer` is accepted and unused, as in linalg.py:12-98)."""
+    if not 1 <= inner <= 128:
+        raise ValueError(f"gmres: inner must be in [1, 128] (the projected solve is one CTA), got {inner}")
     b = b.to(torch.float64).contiguous()
     n = b.numel()
     dev = b.device
@@ -46,23 +48,29 @@ def gmres(A, b, inner, outer=1, preconditioner_list=()):
     H = torch.zeros((inner, inner + 1), dtype=torch.float64, device=dev)   # column-major (inner+1) x inner
     h0 = torch.zeros(inner + 2, dtype=torch.float64, device=dev)
     b = precond(b).to(torch.float64).contiguous()
-    vp = lambda t: ctypes.c_void_p(t.data_ptr())
-    _lib_call("ecs_arnoldi_mgs", vp(Q), n, -1, vp(b), vp(h0), n, stream_ptr())   # Q[:,0] = b/|b|
+    _lib_call("ecs_arnoldi_mgs", _vp(Q), n, -1, _vp(b, n), _vp(h0), n, stream_ptr())   # Q[:,0] = b/|b|
     for k in range(inner):
         Aq = precond(A(Q[k])).to(torch.float64).contiguous()
         col = torch.zeros(inner + 2, dtype=torch.float64, device=dev)
-        _lib_call("ecs_arnoldi_mgs", vp(Q), n, k, vp(Aq), vp(col), n, stream_ptr())
+        _lib_call("ecs_arnoldi_mgs", _vp(Q), n, k, _vp(Aq, n), _vp(col), n, stream_ptr())
         H[k, : min(k + 2, inner + 1)] = col[: min(k + 2, inner + 1)]
     b2 = torch.mv(Q, b)                        # Q^T b   (linalg.py:92)
     y = torch.empty(inner, dtype=torch.float64, device=dev)
     Hc = H.contiguous()
-    _lib_call("ecs_hessenberg_lstsq", vp(Hc), inner + 1, inner, vp(b2), vp(y), stream_ptr())
+    _lib_call("ecs_hessenberg_lstsq", _vp(Hc), inner + 1, inner, _vp(b2), _vp(y), stream_ptr())
     x = torch.mv(Q[:inner].t(), y)             # Q[:, :inner] y  (linalg.py:94)
     rel_res = torch.linalg.norm(precond(A(x)) - b) / torch.linalg.norm(b)
     return x, rel_res
 
 
-def _vp(t):
+def _vp(t, numel=None):
+    """Device pointer of a contiguous FP64 CUDA tensor; with `numel`, the
+    tensor must hold exactly that many values (a Krylov vector of the basis's
+    length), since the kernels read as many as the basis is long."""
+    if not (t.is_cuda and t.is_contiguous() and t.dtype == torch.float64):
+        raise ValueError(f"Krylov vectors must be contiguous FP64 CUDA tensors, got {t.dtype} on {t.device}")
+    if numel is not None and t.numel() != numel:
+        raise ValueError(f"vector has {t.numel()} values, the Krylov basis has length {numel}")
     return ctypes.c_void_p(t.data_ptr())
 
 
@@ -71,7 +79,9 @@ def _orth(Q, k, w, hcol, reorth):
     receives w/|w|, hcol[0..k] the first sweep's projections, hcol[k+1] = |w|."""
     n = Q.shape[1]
     w = w.to(torch.float64).contiguous()
-    _lib_call("ecs_arnoldi_mgs_reorth", _vp(Q), n, k, _vp(w), _vp(hcol), n, reorth, stream_ptr())
+    if not (-1 <= k < Q.shape[0] - 1) or hcol.numel() < k + 2:
+        raise ValueError(f"_orth: step {k} outside a basis of {Q.shape[0]} vectors (or hcol too short)")
+    _lib_call("ecs_arnoldi_mgs_reorth", _vp(Q), n, k, _vp(w, n), _vp(hcol), n, reorth, stream_ptr())
 
 
 def _bisection(g, lower, upper, maxit):

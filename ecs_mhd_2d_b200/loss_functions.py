@@ -38,36 +38,61 @@ def shoot_cfg(param_dict, mode):
     return c
 
 
-def prep_inputs(input_dict):
+def prep_inputs(input_dict, n=None, dtype=None, what="fields"):
     """Batched, contiguous device tensors (fields [B,2,n,n], T [B], sx [B]) and
-    whether the input carried a batch dimension."""
+    whether the input carried a batch dimension.  The shapes are checked on the
+    host first: fields [2, n, n] or [B, 2, n, n] (side `n` when given, e.g. a
+    tangent's against its primal), T and sx one value or B values.  `dtype`
+    converts the fields (a tangent takes its primal's precision)."""
     f = input_dict["fields"]
     if not isinstance(f, torch.Tensor):
         f = torch.as_tensor(f)
+    _ctx.check_fields(f, what, n)
     batched = f.dim() == 4
     fb = (f if batched else f.unsqueeze(0))
-    if fb.dtype not in (torch.float64, torch.float32):
+    if dtype is not None:
+        fb = fb.to(dtype)
+    elif fb.dtype not in (torch.float64, torch.float32):
         fb = fb.to(torch.float64)
-    fb = fb.to("cuda").contiguous()
     B = fb.shape[0]
 
-    def scal(v):
-        t = torch.as_tensor(v, dtype=torch.float64)
-        t = t.reshape(-1).to("cuda")
-        if t.numel() == 1 and B > 1:
-            t = t.expand(B)
-        return t.contiguous()
+    def scal(v, name):
+        t = torch.as_tensor(v, dtype=torch.float64).reshape(-1)
+        if t.numel() != B and t.numel() != 1:
+            raise ValueError(f"{name} has {t.numel()} values for a batch of {B}")
+        return t
 
-    return fb, scal(input_dict["T"]), scal(input_dict["sx"]), batched
+    def dev(t):
+        t = t.to("cuda")
+        return (t.expand(B) if t.numel() == 1 and B != 1 else t).contiguous()
+
+    T, sx = scal(input_dict["T"], "T"), scal(input_dict["sx"], "sx")   # both checked before any copy
+    return fb.to("cuda").contiguous(), dev(T), dev(sx), batched
+
+
+def grid_of(input_dict):
+    """(n, dtype) that prep_inputs gives the fields of input_dict, without copying them."""
+    f = input_dict["fields"]
+    if not isinstance(f, torch.Tensor):
+        f = torch.as_tensor(f)
+    _ctx.check_fields(f)
+    return f.shape[-1], (f.dtype if f.dtype in (torch.float64, torch.float32) else torch.float64)
+
+
+def _empty_like_out(fields):
+    z = torch.empty(0, dtype=torch.float64, device=fields.device)
+    return {"fields": torch.empty_like(fields), "T": z, "sx": z.clone()}
 
 
 def objective_RPO(input_dict, param_dict, mode):
     """{"fields": irfft2(f0 - g.Phi_T(f0)), "T": pt, "sx": px} (loss_functions.py:132-148).
     pt and px are phase conditions whose value is exactly 0 (:128-129)."""
+    cfg = shoot_cfg(param_dict, mode)
     fields, T, sx, batched = prep_inputs(input_dict)
     B, n = fields.shape[0], fields.shape[-1]
+    if B == 0:
+        return _empty_like_out(fields)
     ctx = _ctx.get_context(param_dict, n, fields.dtype, B)
-    cfg = shoot_cfg(param_dict, mode)
     out = torch.empty_like(fields)
     oT = torch.empty(B, dtype=torch.float64, device=fields.device)
     osx = torch.empty(B, dtype=torch.float64, device=fields.device)
@@ -81,10 +106,12 @@ def objective_RPO(input_dict, param_dict, mode):
 
 def loss_RPO(input_dict, param_dict, mode):
     """(mean(irfft2(f - f0)^2), info) (loss_functions.py:99-111)."""
+    cfg = shoot_cfg(param_dict, mode)
     fields, T, sx, batched = prep_inputs(input_dict)
     B, n = fields.shape[0], fields.shape[-1]
+    if B == 0:
+        return torch.empty(0, dtype=torch.float64, device=fields.device), []
     ctx = _ctx.get_context(param_dict, n, fields.dtype, B)
-    cfg = shoot_cfg(param_dict, mode)
     loss = torch.empty(B, dtype=torch.float64, device=fields.device)
     info = (_lib.EcsInfo * B)()
     ctx.call("ecs_loss", cfg, _ctx.ptr(fields), _ctx.ptr(T), _ctx.ptr(sx), _ctx.ptr(loss), info, B,
@@ -98,9 +125,12 @@ def loss_RPO(input_dict, param_dict, mode):
 
 def dealias(fields, param_dict):
     """irfft2(mask * rfft2(fields)) (newton.py:211-214, adjoint_descent.py:111-114)."""
+    _ctx.check_fields(fields)
     f = fields if fields.dim() == 4 else fields.unsqueeze(0)
     f = f.contiguous()
     B, n = f.shape[0], f.shape[-1]
+    if B == 0:
+        return torch.empty_like(fields)
     ctx = _ctx.get_context(param_dict, n, f.dtype, B)
     out = torch.empty_like(f)
     ctx.call("ecs_dealias", _ctx.ptr(f), _ctx.ptr(out), B, _ctx.stream_ptr())

@@ -78,13 +78,13 @@ def dissipation(param_dict):
 def state_vel(fields, param_dict, include_dissipation):
     """Time derivative of the rfft2 state [..., 2, n, n//2+1] (mhd_jax.py:105-175),
     computed by the fused column/row kernels (ecs_state_vel)."""
-    if not torch.is_complex(fields):
-        raise TypeError("state_vel expects the rfft2 coefficients (complex)")
-    n = fields.shape[-2]
+    n = _ctx.check_spectral(fields, "state_vel input")
     rdt = torch.float64 if fields.dtype == torch.complex128 else torch.float32
     lead = fields.shape[:-3]
     f = fields.reshape(-1, 2, n, n // 2 + 1).contiguous()
     B = f.shape[0]
+    if B == 0:
+        return torch.empty_like(fields)
     ctx = _ctx.get_context(param_dict, n, rdt, B)
     out = torch.empty_like(f)
     ctx.call("ecs_state_vel", _ctx.ptr(f), _ctx.ptr(out), B, int(bool(include_dissipation)), _ctx.stream_ptr())

@@ -18,11 +18,13 @@ def lawson_rk4(f, t, steps, param_dict):
     steps with the mask applied to the integrating factor
     (timestepping.py:46-81 with v_fn = state_vel(., include_dissipation=False),
     L_diag = dissipation(param_dict), mask = param_dict["mask"])."""
-    n = f.shape[-2]
+    n = _ctx.check_spectral(f)
     rdt = torch.float64 if f.dtype == torch.complex128 else torch.float32
     lead = f.shape[:-3]
     out = f.reshape(-1, 2, n, n // 2 + 1).contiguous().clone()
     B = out.shape[0]
+    if B == 0:
+        return out.reshape(f.shape)
     ctx = _ctx.get_context(param_dict, n, rdt, B)
     ctx.call("ecs_lawson_rk4", _ctx.ptr(out), float(t), int(steps), B, _ctx.stream_ptr())
     return out.reshape(*lead, 2, n, n // 2 + 1)
@@ -38,11 +40,13 @@ def integrate(f, t, steps, param_dict, mode):
              "Lawson_RK6": _lib.ECS_MODE_LAWSON_RK6, "TDRK4": _lib.ECS_MODE_TDRK4}
     if mode not in codes:
         raise ValueError(f"integrate: fixed-step mode expected, got {mode}")
-    n = f.shape[-2]
+    n = _ctx.check_spectral(f)
     rdt = torch.float64 if f.dtype == torch.complex128 else torch.float32
     lead = f.shape[:-3]
     out = f.reshape(-1, 2, n, n // 2 + 1).contiguous().clone()
     B = out.shape[0]
+    if B == 0:
+        return out.reshape(f.shape)
     ctx = _ctx.get_context(param_dict, n, rdt, B)
     ctx.call("ecs_integrate", codes[mode], _ctx.ptr(out), float(t), int(steps), B, _ctx.stream_ptr())
     return out.reshape(*lead, 2, n, n // 2 + 1)

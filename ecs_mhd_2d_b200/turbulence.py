@@ -17,7 +17,12 @@ from .timestepping import integrate
 def recurrence(fs, param_dict):
     """dist[j, i] = || |fs_j| - |fs_i| ||_2 for snapshots fs [S, 2, n, n//2+1]
     (generate_turbulence.py:136-146), on the device (ecs_recurrence)."""
-    S, n = fs.shape[0], fs.shape[-2]
+    n = _ctx.check_spectral(fs, "snapshots")
+    if fs.dim() != 4:
+        raise ValueError(f"snapshots must be [S, 2, n, n//2+1], got {tuple(fs.shape)}")
+    S = fs.shape[0]
+    if S == 0:
+        return torch.empty((0, 0), dtype=torch.float64, device=fs.device)
     rdt = torch.float64 if fs.dtype == torch.complex128 else torch.float32
     ctx = _ctx.get_context(param_dict, n, rdt, 1)
     fs = fs.contiguous()
