@@ -53,7 +53,7 @@ def test_empty_batches(setup):
     # the primal value still comes back with an empty tangent batch
     val, tan = obj.linearize_jvp(x, empty)
     ref = E.objective_RPO(x, pd, "Lawson_RK4")
-    assert _rel(val["fields"], ref["fields"]) < 1e-13 and tan["fields"].shape == (0, 2, n, n)
+    assert _rel(val["fields"], ref["fields"]) < 1e-12 and tan["fields"].shape == (0, 2, n, n)
 
 
 def test_tangent_precision_follows_the_primal(setup):
