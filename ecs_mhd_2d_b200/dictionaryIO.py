@@ -49,6 +49,31 @@ def load_dicts(filename, device=None):
     return inp, par
 
 
+def inspect_dict(d):
+    """One line per key: shape, dtype and size in KB of array values, the type
+    otherwise (inspect_dict of jax_scripts/test_solution_file_structure.py:17-25,
+    returned as a list of lines instead of printed)."""
+    lines = []
+    for key, value in d.items():
+        if isinstance(value, torch.Tensor):
+            value = value.detach().cpu().numpy()
+        if hasattr(value, "size") and hasattr(value, "dtype"):
+            kb = value.size * value.dtype.itemsize / 1024
+            lines.append(f"Key: {key}, shape: {value.shape}, dtype: {value.dtype}, size: {kb:.2f} KB")
+        else:
+            lines.append(f"Key: {key}, type: {type(value)}, size: unknown")
+    return lines
+
+
+def describe_file(filename):
+    """The two sections that test_solution_file_structure.py:27-31 prints for a
+    state file: "input_dict:" and "param_dict:" with inspect_dict's lines."""
+    inp, par = load_dicts(filename)
+    inp = {k: (v.numpy() if isinstance(v, torch.Tensor) else v) for k, v in inp.items()}
+    par = {k: (v.numpy() if isinstance(v, torch.Tensor) else v) for k, v in par.items()}
+    return "\n".join(["input_dict:"] + inspect_dict(inp) + ["", "param_dict:"] + inspect_dict(par))
+
+
 def remove_grid_information(param_dict):
     """Drop the grid tensors before saving (dictionaryIO.py:52-60)."""
     pd = dict(param_dict)

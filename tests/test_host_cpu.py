@@ -36,6 +36,19 @@ def test_save_load_round_trip(tmp_path):
     assert "forcing" not in dictionaryIO.remove_grid_information(p2)
 
 
+def test_describe_state_file(tmp_path):
+    inp = {"fields": torch.zeros(2, 64, 64, dtype=torch.float64), "T": torch.tensor(4.6, dtype=torch.float64),
+           "sx": torch.tensor(0.1, dtype=torch.float64)}
+    par = {"nu": 0.025, "forcing_str": "lambda x,y : -4*jnp.cos(4*y)", "steps": 640}
+    fn = str(tmp_path / "state.npz")
+    dictionaryIO.save_dicts(fn, inp, par)
+    text = dictionaryIO.describe_file(fn).splitlines()
+    assert text[0] == "input_dict:" and text[4] == "" and text[5] == "param_dict:"
+    assert text[1] == "Key: fields, shape: (2, 64, 64), dtype: float64, size: 64.00 KB"
+    assert text[2] == "Key: T, shape: (), dtype: float64, size: 0.01 KB"
+    assert text[7].startswith("Key: forcing_str, ") and len(text) == 9
+
+
 def test_line_search_halves_until_improvement():
     target = torch.tensor([1.0, 2.0, 3.0], dtype=torch.float64)
     obj = lambda d: {"fields": d["fields"] - target.reshape(1, 1, 3)[..., :1].expand(2, 1, 1), "T": d["T"] * 0,
