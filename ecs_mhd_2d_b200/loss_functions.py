@@ -35,6 +35,11 @@ def shoot_cfg(param_dict, mode):
     c.max_steps_per_checkpoint = int(ad.get("max_steps_per_checkpoint", 1024))
     c.checkpoints = int(ad.get("checkpoints", 1))
     c.ckpt_every = int(param_dict.get("ckpt_every", 0))
+    for name in ("num_checkpoints", "ministeps", "checkpoints", "max_steps_per_checkpoint"):
+        if getattr(c, name) < 1:
+            raise ValueError(f"{name} must be >= 1, got {getattr(c, name)}")
+    if c.ckpt_every < 0:
+        raise ValueError(f"ckpt_every must be >= 0, got {c.ckpt_every}")
     return c
 
 

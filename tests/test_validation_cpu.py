@@ -28,6 +28,16 @@ def test_unknown_mode_is_an_error(pd64):
         E.integrate(torch.zeros(2, 64, 33, dtype=torch.complex128), 0.1, 1, pd64, "Lawson_RK43")
 
 
+@pytest.mark.parametrize("key,val", [("num_checkpoints", 0), ("ministeps", -1), ("ckpt_every", -2),
+                                     ("adaptive_dict", {"checkpoints": 0}),
+                                     ("adaptive_dict", {"max_steps_per_checkpoint": -4})])
+def test_step_counts_checked(key, val):
+    pd = E.make_param_dict(64, 1 / 40, 1 / 40, forcing="kolmogorov+", **{key: val})
+    with pytest.raises(ValueError, match=">= "):
+        E.objective_RPO({"fields": torch.zeros(2, 64, 64), "T": 1.0, "sx": 0.0}, pd,
+                        "Lawson_RK43" if key == "adaptive_dict" else "Lawson_RK4")
+
+
 @pytest.mark.parametrize("shape", [(2, 64, 32), (3, 64, 64), (64, 64), (1, 1, 2, 64, 64), (4, 2, 64, 63)])
 def test_fields_shape_checked(pd64, shape):
     x = {"fields": torch.zeros(shape), "T": 1.0, "sx": 0.0}
