@@ -40,3 +40,36 @@ def test_invalid_arguments_rejected_without_gpu(built_lib):
     assert lib.ecs_ctx_create(64, 7, ctypes.byref(prm), 1, ctypes.byref(h)) == 6    # unsupported dtype
     assert lib.ecs_ctx_create(64, 0, ctypes.byref(prm), 0, ctypes.byref(h)) == 1    # bad batch
     assert lib.ecs_to_box(None, None, None, 1, None) == 1
+
+
+def test_status_codes_before_any_device_work(built_lib):
+    """Each entry point refuses bad scalars with its documented status before it
+    touches the device (so these run without a GPU)."""
+    from ecs_mhd_2d_b200 import _lib
+    lib = _lib.load()
+    buf = (ctypes.c_double * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    dp = ctypes.cast(buf, ctypes.POINTER(ctypes.c_double))
+    INVALID, UNSUPPORTED, TOO_LARGE = 1, 6, 7
+    # Arnoldi / Hessenberg: step index, lengths, re-orthogonalisation sweeps, m <= 128
+    assert lib.ecs_arnoldi_mgs(dp, 8, -2, dp, dp, 8, None) == INVALID
+    assert lib.ecs_arnoldi_mgs(dp, 4, 0, dp, dp, 8, None) == INVALID          # ld < len
+    assert lib.ecs_arnoldi_mgs(dp, 8, 0, dp, dp, 0, None) == INVALID          # empty vectors
+    assert lib.ecs_arnoldi_mgs_reorth(dp, 8, 0, dp, dp, 8, 5, None) == INVALID
+    assert lib.ecs_arnoldi_mgs(None, 8, 0, dp, dp, 8, None) == INVALID
+    assert lib.ecs_hessenberg_lstsq(dp, 130, 129, dp, dp, None) == INVALID
+    assert lib.ecs_hessenberg_lstsq(dp, 4, 4, dp, dp, None) == INVALID       # ldh < m + 1
+    assert lib.ecs_hessenberg_lstsq(dp, 2, 0, dp, dp, None) == INVALID
+    # allocation-free state_vel: n and batch limits of its fixed scratch
+    assert lib.ecs_state_vel_noalloc(256, 0.02, 0.02, 0.0, 0.1, dp, p, p, 1, 0, None) == TOO_LARGE
+    assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, dp, p, p, 5, 0, None) == TOO_LARGE
+    assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, dp, p, p, 0, 0, None) == TOO_LARGE
+    assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, None, p, p, 1, 0, None) == INVALID
+    # entry points given no context
+    assert lib.ecs_objective(None, None, p, dp, dp, p, dp, dp, None, 1, None) == INVALID
+    assert lib.ecs_jvp(None, p, dp, dp, p, dp, dp, 1, None) == INVALID
+    assert lib.ecs_vjp(None, p, dp, dp, p, dp, dp, 1, None) == INVALID
+    assert lib.ecs_ctx_create(256, 1, None, 1, None) == INVALID
+    prm = _lib.EcsParams()
+    h = ctypes.c_void_p()
+    assert lib.ecs_ctx_create(512, 0, ctypes.byref(prm), 1, ctypes.byref(h)) == UNSUPPORTED
