@@ -2,7 +2,9 @@
 launch, a tangent batch of one precision pushed through a primal of the
 other is converted to the primal's precision, and grid sizes or modes that
 the library does not provide end in an error status, not a launch.  The
-non-empty results are compared with the same calls on well-formed inputs."""
+non-empty results are compared with the same calls on well-formed inputs.
+This file sorts after the parity tests so that a run stopping at the first
+failure has run those first."""
 import numpy as np
 import pytest
 import torch
