@@ -15,7 +15,10 @@
 // or different host threads on one device) race and corrupt each other.
 // The first call on each device performs a one-time set-up (symbol address
 // lookup, twiddle upload, kernel attributes) with synchronous CUDA calls, so
-// that first call should come before any stream capture.
+// that first call should come before any stream capture.  The device address
+// found then is kept for the life of the process, per device ordinal: the entry
+// point assumes the CUDA runtime's primary context of that device and no
+// cudaDeviceReset afterwards (a reset frees the module memory behind it).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -23,6 +26,7 @@
 #include <vector>
 
 #include "../../include/ecs_mhd.h"
+#include "api_internal.cuh"
 #include "kernels.cuh"
 
 namespace {
@@ -49,7 +53,6 @@ constexpr size_t OFF_G = al(OFF_OUT + NA_MAX_BATCH * 2 * NA_K * NA_M * CB);     
 constexpr size_t OFF_H = al(OFF_G + NA_MAX_BATCH * NG * NA_K * NA_MAX_N * CB);   // [B][NH][K][n]
 constexpr size_t NA_BYTES = al(OFF_H + NA_MAX_BATCH * NH * NA_K * NA_MAX_N * CB);
 
-std::mutex g_mutex;
 unsigned char* g_base[128] = {};   // device address of the scratch array, per device ordinal
 
 }  // namespace
@@ -76,11 +79,13 @@ int na_setup_twiddles(unsigned char* base, size_t off) {
 template <int N> size_t na_smem_rhs() { return (fft_smem(N, NA_XT) + (NG + NH) * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
 template <int N> size_t na_smem_2f() { return (fft_smem(N, NA_XT) + 2 * ((N - 1) / 3 + 1) * (NA_XT + 1)) * CB; }
 
-// One-time set-up on the current device (synchronous).
+// One-time set-up on the current device (synchronous).  It holds the mutex that
+// context set-up and every graph capture of this library take, so its
+// legacy-stream copies never land inside another thread's capture.
 int na_setup(unsigned char** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return ECS_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_mutex);
+  std::lock_guard<std::mutex> lock(ecs::capture_mutex());
   if (!g_base[dev]) {
     void* p = nullptr;
     // In host code g_noalloc_scratch names a host-side stand-in; the kernels
@@ -118,21 +123,21 @@ int na_state_vel(unsigned char* base, double nu, double eta, double b0x, double 
   if (e == cudaSuccess) e = cudaMemsetAsync(fields + (size_t)N * N, 0, (size_t)N * N * sizeof(double), s);
   if (e != cudaSuccess) return ECS_ERR_CUDA;
   // forcing spectrum on the box, mask[0,0] = False
-  RowFwdParams<double> rf; rf.fields = fields; rf.H = H; rf.tw = tw; rf.B = 1;
+  RowFwdParams<double> rf{}; rf.fields = fields; rf.H = H; rf.tw = tw; rf.B = 1;
   k_row_to_box<double, N, NA_XT><<<N / NA_XT, NA_XT * 32, na_smem_2f<N>(), s>>>(rf);
-  ColBoxParams<double> cbp; cbp.H = H; cbp.V = fbox; cbp.tw = tw; cbp.vstride = 2L * K * M; cbp.B = 1; cbp.nf = 2;
+  ColBoxParams<double> cbp{}; cbp.H = H; cbp.V = fbox; cbp.tw = tw; cbp.vstride = 2L * K * M; cbp.B = 1; cbp.nf = 2;
   k_col_to_box<double, N><<<(2 * K + 3) / 4, 128, 0, s>>>(cbp);
   if (cudaMemsetAsync(fbox, 0, CB, s) != cudaSuccess) return ECS_ERR_CUDA;
   // state_vel: gather box, column inverse, row products, column forward, scatter
   const long nbox = (long)B * 2 * K * M;
   k_gather_box<double><<<(int)((nbox + 255) / 256), 256, 0, s>>>(f_hat, F, N, B);
-  ColParams<double> cp;
+  ColParams<double> cp{};
   cp.H = H; cp.G = G; cp.F = F; cp.A1 = nullptr; cp.K2 = nullptr; cp.OUT = OUT; cp.Etab = nullptr; cp.ctl = ctl;
   cp.fhat = fbox; cp.tw = tw; cp.nu = nu; cp.eta = eta; cp.B = B; cp.stage = COL_START; cp.produce = 1;
   cp.diss = 0; cp.rec = nullptr; cp.rec_bstride = 0;
   const int cols = B * K * 2;   // one warp per (batch, ky, channel)
   k_col_rk4<double, N, COL_START><<<(cols + 3) / 4, 128, 0, s>>>(cp);
-  RowParams<double> rp;
+  RowParams<double> rp{};
   rp.G = G; rp.H = H; rp.ctl = nullptr; rp.phys = nullptr; rp.phys_bstride = 0;
   rp.tw = tw; rp.b0x = b0x; rp.b0y = b0y; rp.B = B;
   k_row_rhs<double, N, NA_XT><<<B * (N / NA_XT), NA_XT * 32, na_smem_rhs<N>(), s>>>(rp);
@@ -149,8 +154,9 @@ extern "C" int ecs_state_vel_noalloc(int n, double nu, double eta, double b0x, d
                                      const void* f_hat, void* dfdt_hat, int batch, int include_dissipation,
                                      void* stream) {
   if (!forcing || !f_hat || !dfdt_hat) return ECS_ERR_INVALID;
+  if (batch < 1) return ECS_ERR_INVALID;
   if (n != 64 && n != 128) return ECS_ERR_TOO_LARGE;
-  if (batch < 1 || batch > NA_MAX_BATCH) return ECS_ERR_TOO_LARGE;
+  if (batch > NA_MAX_BATCH) return ECS_ERR_TOO_LARGE;
   unsigned char* base = nullptr;
   const int st = na_setup(&base);
   if (st) return st;

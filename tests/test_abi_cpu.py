@@ -63,7 +63,7 @@ def test_status_codes_before_any_device_work(built_lib):
     # allocation-free state_vel: n and batch limits of its fixed scratch
     assert lib.ecs_state_vel_noalloc(256, 0.02, 0.02, 0.0, 0.1, dp, p, p, 1, 0, None) == TOO_LARGE
     assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, dp, p, p, 5, 0, None) == TOO_LARGE
-    assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, dp, p, p, 0, 0, None) == TOO_LARGE
+    assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, dp, p, p, 0, 0, None) == INVALID
     assert lib.ecs_state_vel_noalloc(64, 0.02, 0.02, 0.0, 0.1, None, p, p, 1, 0, None) == INVALID
     # entry points given no context
     assert lib.ecs_objective(None, None, p, dp, dp, p, dp, dp, None, 1, None) == INVALID

@@ -44,6 +44,35 @@ def test_noalloc_state_vel_matches_state_vel_twice(cuda):
         assert rel_l2(out.cpu().numpy(), want.cpu().numpy()) < TOL_RHS
 
 
+def test_noalloc_allocates_no_device_memory(cuda):
+    """After a first call per size (the one-time set-up, and the lazy loading of
+    the kernels), further calls leave the device's free memory unchanged: the
+    entry point takes nothing from the device's allocator.  Every tensor is
+    created before the first measurement."""
+    lib = _lib.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cases = []
+    for n, B in ((128, 4), (64, 2)):
+        pd = E.make_param_dict(n, 1 / 40, 1 / 40, b0=(0.0, 0.1), forcing="kolmogorov+")
+        f = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(b, n) for b in range(B)])), device="cuda")
+        forcing = pd["forcing"].to(device="cuda", dtype=torch.float64).contiguous()
+        cases.append((n, B, f.contiguous(), forcing, torch.empty_like(f)))
+
+    def call(i, diss):
+        n, B, f, forcing, out = cases[i]
+        return lib.ecs_state_vel_noalloc(n, 1 / 40, 1 / 40, 0.0, 0.1, _p(forcing), _p(f), _p(out), B, diss, stream)
+
+    for i in range(2):
+        for diss in (0, 1):
+            assert call(i, diss) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for it in range(6):
+        assert call(it % 2, (it // 2) % 2) == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0, it
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
     lib = _lib.load()
     f = torch.zeros((5, 2, 128, 65), dtype=torch.complex128, device="cuda")
