@@ -13,8 +13,15 @@
    which integrator converged a solution; the mode that closes one to rounding
    level is the one it was converged with, which pins that mode's oracle.
 
-Run from the repository root (needs the reference checkout):
-    python tests/golden/make_golden.py /path/to/reference [modes]
+4. The headline matvec at its full horizon (headline_jvp_n128.npz): the
+   objective value and the JVP of tangent 0 of the benchmark's 64-tangent
+   batch, at the benchmark's own workload (n=128 FP64, Re=50, Lawson_RK43 atol
+   1e-8, T=4.6, sx=0.12, seed-0 amplitude-2 state), by torch.func.jvp of the
+   oracle's torch form (minutes of CPU time, hence a fixture).
+
+Run from the repository root:
+    python tests/golden/make_golden.py /path/to/reference [modes]   (1-3: needs the reference checkout)
+    python tests/golden/make_golden.py headline                      (4: the oracle only)
 """
 
 import json
@@ -83,6 +90,30 @@ def synthetic():
                         objective=obj["fields"], loss=loss)
 
 
+def headline_jvp():
+    import torch
+    from torch.func import jvp
+    from ecs_mhd_2d_b200.synthetic import unit_tangents
+    torch.set_num_threads(os.cpu_count() or 1)
+    n, T, sx, B = 128, 4.6, 0.12, 64
+    ad = {"atol": 1e-8, "checkpoints": 64, "max_steps_per_checkpoint": 64}
+    kw = dict(forcing="kolmogorov+", shift_reflect_ny=0, rot=False, adaptive_dict=ad)
+    u0 = initial_condition(0, n, amp=2.0)
+    t0 = unit_tangents(0, n, B)[0]
+    _, _, info = O.mismatch_RPO({"fields": u0, "T": T, "sx": sx}, O.make_param_dict(n, 1 / 50, 1 / 50, **kw),
+                                "Lawson_RK43")
+    pdt = O.make_param_dict(n, 1 / 50, 1 / 50, xp=O.TORCH, **kw)
+    f = lambda d: O.objective_RPO(d, pdt, "Lawson_RK43", xp=O.TORCH)
+    prim = {"fields": torch.from_numpy(u0), "T": torch.tensor(T, dtype=torch.float64),
+            "sx": torch.tensor(sx, dtype=torch.float64)}
+    tan = {"fields": torch.from_numpy(np.ascontiguousarray(t0[1:-1].reshape(2, n, n))),
+           "T": torch.tensor(t0[0], dtype=torch.float64), "sx": torch.tensor(t0[-1], dtype=torch.float64)}
+    val, out = jvp(f, (prim,), (tan,))
+    np.savez_compressed(os.path.join(HERE, "headline_jvp_n128.npz"), objective=val["fields"].numpy(),
+                        jvp_fields=out["fields"].numpy(), jvp_T=out["T"].numpy(), jvp_sx=out["sx"].numpy(),
+                        accepted=info["accepted"], rejected=info["rejected"], T=T, sx=sx, tangent_index=0)
+
+
 def closure_by_mode(ref, modes=("Lawson_RK4", "TDRK4", "RK4")):
     rec = {}
     for sub in ["Re40", "Re50"]:
@@ -101,8 +132,12 @@ def closure_by_mode(ref, modes=("Lawson_RK4", "TDRK4", "RK4")):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if len(sys.argv) > 2 and sys.argv[2] == "modes":
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py (/path/to/reference [modes] | headline)")
+    ref = sys.argv[1]
+    if ref == "headline":
+        headline_jvp()
+    elif len(sys.argv) > 2 and sys.argv[2] == "modes":
         closure_by_mode(ref)
     else:
         synthetic()

@@ -65,6 +65,36 @@ def test_mixed_precision_newton_tracks_fp64(cuda):
     assert abs(r32[-1] - e64) <= 0.02 * e64, (r32, e64)
 
 
+def test_mixed_precision_newton_reaches_1e10_at_n256(cuda):
+    """The mixed-precision target at 256^2 (Re=50): the reference's RPO2
+    (solutions/Re50/RPO2.npz, 768 Lawson-RK4 steps) perturbed by 1e-7, four
+    Newton-GMRES steps with FP32 stepping and FP32 JVP/VJP products (FP64
+    residuals, Arnoldi and Hessenberg least squares), then two FP64 refinement
+    steps (jax_scripts/newton.py:151-215); 32 Krylov vectors on the normal
+    equations cut the residual about 7x per step here.  The final relative residual
+    |objective| / |fields| is <= 1e-10 as evaluated by the FP64 numpy oracle,
+    and the device's FP64 residual agrees with the oracle's to 1e-12
+    (absolute, on a relative residual)."""
+    import oracle as O
+    d = np.load("tests/golden/solution_Re50_RPO2.npz")
+    n = d["fields"].shape[-1]
+    kw = dict(num_checkpoints=int(d["num_checkpoints"]), ministeps=int(d["ministeps"]),
+              shift_reflect_ny=int(d["shift_reflect_ny"]), rot=bool(d["rot"]))
+    pd = E.make_param_dict(n, float(d["nu"]), float(d["eta"]), b0=d["b0"], forcing="kolmogorov", **kw)
+    u = E.dealias(torch.as_tensor(d["fields"] + 1e-7 * initial_condition(98, n, amp=1.0), device="cuda"), pd)
+    x0 = {"fields": u, "T": float(d["T"]) * (1 + 1e-7), "sx": float(d["sx"])}
+    r0 = float(relative_error_RPO(x0, E.objective_RPO(x0, pd, "Lawson_RK4")))
+    x, hist = drivers.mixed_precision_newton(x0, pd, "Lawson_RK4", iters=4, inner=32, refine=2)
+    assert [h["jacobian"] for h in hist[:-1]] == ["fp32"] * 4 + ["fp64"] * 2
+    r_dev = hist[-1]["final_rel_err"]
+    opd = O.make_param_dict(n, float(d["nu"]), float(d["eta"]), b0=tuple(d["b0"]), forcing="kolmogorov", **kw)
+    xh = {"fields": x["fields"].cpu().numpy(), "T": float(x["T"]), "sx": float(x["sx"])}
+    fo = O.objective_RPO(xh, opd, "Lawson_RK4")["fields"]
+    r_orc = float(np.linalg.norm(fo) / np.linalg.norm(xh["fields"]))
+    assert r0 > 1e-8 and r_orc <= 1e-10, (r0, r_orc, hist)
+    assert abs(r_dev - r_orc) <= 1e-12, (r_dev, r_orc)
+
+
 def test_newton_gmres_tdrk4_reference_default(cuda):
     """The reference Newton driver's default configuration (mode "TDRK4",
     use_transpose=True; jax_scripts/newton.py:70, :151-215) on the reference's
