@@ -8,6 +8,7 @@ rot, ...) with two key lists, "input_keys" and "param_keys".
 
 from __future__ import annotations
 
+import ast
 import math
 
 import numpy as np
@@ -82,19 +83,55 @@ def remove_grid_information(param_dict):
     return pd
 
 
-class _NumpyAsJnp:
-    """The names a reference forcing_str uses (jnp.cos, jnp.sin, jnp.pi, ...)."""
-    cos, sin, exp, tanh, sqrt = np.cos, np.sin, np.exp, np.tanh, np.sqrt
-    pi = math.pi
+_FORCING_FUNCS = {"cos": np.cos, "sin": np.sin, "exp": np.exp, "tanh": np.tanh, "sqrt": np.sqrt,
+                  "cosh": np.cosh, "sinh": np.sinh, "abs": np.abs}
+_FORCING_CONSTS = {"pi": math.pi}
+_FORCING_BINOPS = {ast.Add: np.add, ast.Sub: np.subtract, ast.Mult: np.multiply, ast.Div: np.divide,
+                   ast.Pow: np.power}
+
+
+def _forcing_eval(node, env):
+    """Evaluate one node of a forcing expression: numbers, the two coordinates,
+    + - * / **, unary minus, and jnp./np. math functions and pi; anything else
+    is refused."""
+    if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)) and not isinstance(node.value, bool):
+        return float(node.value)
+    if isinstance(node, ast.Name) and node.id in env:
+        return env[node.id]
+    if isinstance(node, ast.BinOp) and type(node.op) in _FORCING_BINOPS:
+        return _FORCING_BINOPS[type(node.op)](_forcing_eval(node.left, env), _forcing_eval(node.right, env))
+    if isinstance(node, ast.UnaryOp) and isinstance(node.op, (ast.USub, ast.UAdd)):
+        v = _forcing_eval(node.operand, env)
+        return -v if isinstance(node.op, ast.USub) else v
+    if (isinstance(node, ast.Attribute) and isinstance(node.value, ast.Name) and node.value.id in ("jnp", "np")
+            and node.attr in _FORCING_CONSTS):
+        return _FORCING_CONSTS[node.attr]
+    if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute) and isinstance(node.func.value, ast.Name)
+            and node.func.value.id in ("jnp", "np") and node.func.attr in _FORCING_FUNCS
+            and len(node.args) == 1 and not node.keywords):
+        return _FORCING_FUNCS[node.func.attr](_forcing_eval(node.args[0], env))
+    raise ValueError(f"forcing_str: unsupported expression {ast.dump(node)[:80]}")
 
 
 def forcing_from_string(forcing_str, n):
-    """Evaluate a reference forcing string such as 'lambda x,y : -4*jnp.cos(4*y)'
-    on the grid of construct_domain, with only numpy math in scope."""
+    """The reference's forcing string, e.g. 'lambda x,y : -4*jnp.cos(4*y)'
+    (jax_scripts/lib/dictionaryIO.py:74 evaluates it), on the grid of
+    construct_domain.  The string is parsed, not executed: a lambda of two
+    arguments whose body uses numbers, the arguments, + - * / **, and the
+    jnp./np. functions cos sin exp tanh sqrt cosh sinh abs and the constant pi."""
     grid = np.arange(n, dtype=np.float64) / n * 2 * PI_LITERAL
     x, y = np.meshgrid(grid, grid, indexing="ij")
-    fn = eval(str(forcing_str), {"__builtins__": {}, "jnp": _NumpyAsJnp, "np": _NumpyAsJnp})
-    return np.asarray(fn(x, y), dtype=np.float64)
+    try:
+        tree = ast.parse(str(forcing_str).strip(), mode="eval")
+    except SyntaxError as ex:
+        raise ValueError(f"forcing_str: not an expression: {forcing_str!r}") from ex
+    lam = tree.body
+    if (not isinstance(lam, ast.Lambda) or len(lam.args.args) != 2 or lam.args.vararg or lam.args.kwarg
+            or lam.args.kwonlyargs or lam.args.defaults or lam.args.posonlyargs):
+        raise ValueError(f"forcing_str: expected 'lambda x,y : <expression>', got {forcing_str!r}")
+    names = [a.arg for a in lam.args.args]
+    val = _forcing_eval(lam.body, {names[0]: x, names[1]: y})
+    return np.broadcast_to(np.asarray(val, dtype=np.float64), (n, n)).copy()
 
 
 def recompute_grid_information(input_dict, param_dict):

@@ -21,6 +21,25 @@ def test_forcing_string_of_the_reference_files():
     assert np.array_equal(fr, -4 * np.cos(4 * np.meshgrid(y, y, indexing="ij")[1]))
 
 
+def test_forcing_string_is_parsed_not_executed():
+    """Other arithmetic forms evaluate; anything beyond numbers, the two
+    coordinates, + - * / ** and jnp./np. math is refused before it runs."""
+    fr = dictionaryIO.forcing_from_string("lambda a, b: 2*jnp.sin(3*a)**2 - np.exp(-b/jnp.pi)", 16)
+    g = np.arange(16) / 16 * 2 * 3.14159265358979323846
+    x, y = np.meshgrid(g, g, indexing="ij")
+    assert np.allclose(fr, 2 * np.sin(3 * x) ** 2 - np.exp(-y / np.pi), rtol=0, atol=1e-15)
+    assert np.array_equal(dictionaryIO.forcing_from_string("lambda x,y: 3", 4), np.full((4, 4), 3.0))
+    bad = ["__import__('os').system('true')", "lambda x,y: x.__class__", "lambda x,y: open('f')",
+           "lambda x: x", "lambda x,y: jnp.linalg.norm(x)", "lambda x,y: [x]", "lambda x,y: jnp.cos(x, y)",
+           "lambda x,y: True", "lambda x,y: 'a'"]
+    for s in bad:
+        try:
+            dictionaryIO.forcing_from_string(s, 4)
+        except ValueError:
+            continue
+        raise AssertionError(f"accepted {s!r}")
+
+
 def test_save_load_round_trip(tmp_path):
     inp = {"fields": torch.randn(2, 64, 64, dtype=torch.float64), "T": torch.tensor(4.6, dtype=torch.float64),
            "sx": torch.tensor(0.1, dtype=torch.float64)}
