@@ -60,6 +60,10 @@ SIGNATURES = {
     "ecs_last_error": (ctypes.c_char_p, [_VP]),
     "ecs_launch_count": (ctypes.c_longlong, [_VP]),
     "ecs_bench_kernel": (_I, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), _VP]),
+    "ecs_jvp_multi": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I,
+                           _VP]),
+    "ecs_kernel_timing": (_I, [_VP, _I, ctypes.POINTER(_D), ctypes.POINTER(_I), ctypes.POINTER(_D),
+                               ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ecs_box_dims": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ecs_to_box": (_I, [_VP, _VP, _VP, _I, _VP]),
     "ecs_from_box": (_I, [_VP, _VP, _VP, _I, _VP]),

@@ -102,6 +102,9 @@ class Context:
             _lib.check(self.lib.ecs_ctx_create(self.n, self.code, ctypes.byref(prm), max_batch, ctypes.byref(h)))
         self.handle = h
         self.generation = next(_GENERATION)
+        # the native context holds one linearisation (trajectory record); this
+        # token names the Objective call that made the current one
+        self.lin_token = None
         self.max_batch = max_batch
         K, M = ctypes.c_int(), ctypes.c_int()
         _lib.check(self.lib.ecs_box_dims(self.handle, ctypes.byref(K), ctypes.byref(M)), self.handle)
@@ -135,6 +138,13 @@ def _forcing_key(forcing):
     a = np.ascontiguousarray(forcing.detach().cpu().numpy() if isinstance(forcing, torch.Tensor) else forcing,
                              dtype=np.float64)
     return hashlib.sha1(a.tobytes()).hexdigest(), a
+
+
+def physics_key(param_dict):
+    """(nu, eta, b0, forcing digest): what a context fixes besides grid and dtype."""
+    fk = _forcing_key(param_dict.get("forcing"))
+    return (float(param_dict["nu"]), float(param_dict["eta"]), float(param_dict["b0"][0]),
+            float(param_dict["b0"][1]), None if fk is None else fk[0])
 
 
 def get_context(param_dict, n, dtype, batch=1):

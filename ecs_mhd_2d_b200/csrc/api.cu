@@ -126,6 +126,8 @@ static int ctx_destroy_locked(ecs_ctx* ctx) {
     for (cudaEvent_t e : ctx->tjoin[g]) if (e) cudaEventDestroy(e);
   }
   if (ctx->tfork) cudaEventDestroy(ctx->tfork);
+  for (cudaEvent_t e : ctx->kt.ev) cudaEventDestroy(e);
+  if (ctx->mj.g.exec) cudaGraphExecDestroy(ctx->mj.g.exec);
   if (ctx->Gp) cudaFree(ctx->Gp);
   if (ctx->Gx) cudaFree(ctx->Gx);
   if (ctx->Hp) cudaFree(ctx->Hp);
@@ -254,6 +256,72 @@ int ecs_bench_kernel(ecs_ctx* ctx, int which, int batch, int iters, float* ms, d
   ECS_CHECK_CTX(ctx, batch);
   if (!ms || !bytes || iters < 1 || which < 0 || which > 1) return set_err(ctx, ECS_ERR_INVALID, "bad arguments");
   return table_of(ctx)->bench_kernel(ctx, which, batch, iters, ms, bytes, as_stream(stream));
+}
+
+int ecs_jvp_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, const double* T, const double* sx,
+                  void* out_fields, const void* dfields, const double* dT, const double* dsx, void* out_dfields,
+                  double* out_dT, double* out_dsx, int batch, void* stream) {
+  ECS_CHECK_CTX(ctx, batch);
+  if (!cfgs || !fields || !T || !sx || !dfields || !dT || !dsx || !out_dfields || !out_dT || !out_dsx)
+    return set_err(ctx, ECS_ERR_INVALID, "null pointer");
+  return table_of(ctx)->jvp_multi(ctx, cfgs, fields, T, sx, out_fields, dfields, dT, dsx, out_dfields, out_dT, out_dsx,
+                                  batch, as_stream(stream));
+}
+
+namespace ecs {
+static cudaEvent_t kt_event(ecs_ctx* c) {
+  auto& k = c->kt;
+  if (k.used == k.ev.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) { k.on = 0; return nullptr; }
+    k.ev.push_back(e);
+  }
+  return k.ev[k.used++];
+}
+
+void kt_begin(ecs_ctx* c, cudaStream_t s) {
+  if (!c->kt.on) return;
+  cudaEvent_t e = kt_event(c);
+  if (e) cudaEventRecord(e, s);
+}
+
+void kt_end(ecs_ctx* c, int kind, int batch, cudaStream_t s) {
+  if (!c->kt.on) return;
+  cudaEvent_t e = kt_event(c);
+  if (!e) return;
+  cudaEventRecord(e, s);
+  c->kt.kind.push_back(kind);
+  c->kt.batch = batch;
+}
+}  // namespace ecs
+
+int ecs_kernel_timing(ecs_ctx* ctx, int enable, double* row_ms, int* row_n, double* col_ms, int* col_n,
+                      int* group_batch) {
+  if (!ctx) return ECS_ERR_INVALID;
+  auto& k = ctx->kt;
+  if (enable) {
+    k.on = 1; k.used = 0; k.batch = 0; k.kind.clear();
+    return ECS_OK;
+  }
+  k.on = 0;
+  double sum[2] = {0, 0};
+  int cnt[2] = {0, 0};
+  for (size_t i = 0; i < k.kind.size(); ++i) {
+    if (2 * i + 1 >= k.used) break;
+    float ms = 0;
+    cudaError_t e = cudaEventSynchronize(k.ev[2 * i + 1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, k.ev[2 * i], k.ev[2 * i + 1]);
+    if (e != cudaSuccess) return set_err(ctx, ECS_ERR_CUDA, cudaGetErrorString(e));
+    sum[k.kind[i]] += ms;
+    ++cnt[k.kind[i]];
+  }
+  if (row_ms) *row_ms = cnt[0] ? sum[0] / cnt[0] : 0.0;
+  if (row_n) *row_n = cnt[0];
+  if (col_ms) *col_ms = cnt[1] ? sum[1] / cnt[1] : 0.0;
+  if (col_n) *col_n = cnt[1];
+  if (group_batch) *group_batch = k.batch;
+  k.used = 0; k.kind.clear();
+  return ECS_OK;
 }
 
 int ecs_pool_reset(ecs_ctx* ctx, void* stream) {

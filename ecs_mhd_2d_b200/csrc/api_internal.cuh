@@ -104,6 +104,24 @@ struct ecs_ctx {
   // 16-step graphs of the other fixed-step modes (RK4, Lawson-RK6, TDRK4)
   struct GraphFx { cudaGraphExec_t exec = nullptr; int B = 0; void* phys = nullptr; long long nodes = 0; } gfx[3];
   void* fxphys = nullptr; size_t fxphys_bytes = 0;   // TDRK4: recorded u, v, B_x, B_y per batch element
+  // several candidates' Lawson-RK4 matvecs in one forward-mode sweep
+  // (ecs_jvp_multi): the tangents' own G/H, the primal physical fields of the
+  // current stage, the current step's record, the phase fields, dT scales
+  struct Multi {
+    void* G = nullptr; void* H = nullptr; void* phys = nullptr; void* rec = nullptr;
+    void* vt = nullptr; void* vx = nullptr; double* dscale = nullptr; double* dT = nullptr;
+    // the 8-step graph bakes in B and the tangent-slot buffer D (which grows)
+    struct Graph { cudaGraphExec_t exec = nullptr; int B = 0; void* D = nullptr; long long nodes = 0; } g;
+  } mj;
+  // in-step timing of the batched tangent kernels (ecs_kernel_timing): CUDA
+  // events around tangent group 0's row-pass and column-pass launches inside
+  // the attempt loop of ecs_linearize_jvp, on that group's stream
+  struct KernelTiming {
+    int on = 0, batch = 0;
+    std::vector<cudaEvent_t> ev;    // event pool, created on demand
+    std::vector<int> kind;          // per recorded pair: 0 row pass, 1 column pass
+    size_t used = 0;                // events recorded (two per pair)
+  } kt;
   std::string err;
 };
 
@@ -121,6 +139,10 @@ int set_err(ecs_ctx* c, int code, const std::string& msg);
 // device-wide synchronisation while another thread captures is an error.
 std::mutex& capture_mutex();
 int cuda_err(ecs_ctx* c, cudaError_t e, const char* where);
+// Kernel timing marks (no-ops unless ecs_kernel_timing enabled them): an event
+// before a launch, and one after it naming its kind (0 row pass, 1 column pass).
+void kt_begin(ecs_ctx* c, cudaStream_t s);
+void kt_end(ecs_ctx* c, int kind, int batch, cudaStream_t s);
 void* dev_alloc(ecs_ctx* c, size_t bytes, int* st);
 // (re)allocate a growable device buffer owned by the context (not in allocs)
 int grow(ecs_ctx* c, void** p, size_t* have, size_t need);

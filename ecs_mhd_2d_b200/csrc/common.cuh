@@ -40,6 +40,28 @@ template <typename C, typename R> __device__ __forceinline__ C cimul(C z, R mu) 
 }
 template <typename C, typename R> __device__ __forceinline__ C cdiv_r(C a, R s) { a.x = a.x / s; a.y = a.y / s; return a; }
 
+// x / D for a positive integer constant D, correctly rounded, without a
+// division instruction.  A power of two is an exact multiplication.  Otherwise
+// (odd part of D at least 3): q0 = x RN(1/D); the residual r = x - q0 D is
+// exact in one FMA; q = RN(q0 + r RN(1/D)) is one more FMA (Markstein's
+// correction step, P. Markstein, IBM J. Res. Dev. 34(1), 1990).  q is RN(x/D)
+// for normal x: q0 + r RN(1/D) differs from x/D by at most ~2^-52 ulp, and x/D
+// is never a rounding midpoint (D times a 54-bit odd midpoint significand has
+// more than 53 significant bits), being at least ulp/(2D) away from one.  So
+// the stepper algebra keeps the operation order and the results of x / D.
+template <int D, typename R> __device__ __forceinline__ R div_k(R x) {
+  static_assert(D > 0, "positive divisor");
+  constexpr R inv = R(1) / R(D);
+  if constexpr ((D & (D - 1)) == 0) {
+    return x * inv;
+  } else {
+    const R q0 = x * inv;
+    const R r = fma(-q0, R(D), x);
+    return fma(r, inv, q0);
+  }
+}
+template <int D, typename C> __device__ __forceinline__ C cdiv_k(C a) { a.x = div_k<D>(a.x); a.y = div_k<D>(a.y); return a; }
+
 template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_c(cplx<R> v, int m) {
   v.x = __shfl_xor_sync(0xffffffffu, v.x, m);
   v.y = __shfl_xor_sync(0xffffffffu, v.y, m);

@@ -128,7 +128,7 @@ void launch_row_from_box(ecs_ctx* c, const cplx<R>* G2, R* out, const R* base, d
 template <typename R, int N>
 void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStream_t s, cplx<R>* rec = nullptr,
                     long rec_bstride = 0, int use_done = 0) {
-  ColParams<R> p;
+  ColParams<R> p{};
   p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.F = (cplx<R>*)c->F; p.A1 = (cplx<R>*)c->A1;
   p.K2 = (cplx<R>*)c->K2; p.OUT = (cplx<R>*)c->OUT; p.Etab = (const R*)c->Etab; p.ctl = c->ctl;
   p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.nu = (R)c->nu; p.eta = (R)c->eta;
@@ -149,7 +149,7 @@ void launch_col_rk4(ecs_ctx* c, int B, int stage, int produce, int diss, cudaStr
 template <typename R, int N>
 void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = nullptr, R* phys = nullptr,
                     long phys_bstride = 0) {
-  RowParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.tw = (const cplx<R>*)c->tw; p.ctl = ctl;
+  RowParams<R> p{}; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.tw = (const cplx<R>*)c->tw; p.ctl = ctl;
   p.phys = phys; p.phys_bstride = phys_bstride;
   p.b0x = (R)c->b0x; p.b0y = (R)c->b0y; p.B = B;
   if (small_rows<N>(B)) launch_step(c, B, k_row_rhs<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
@@ -158,7 +158,7 @@ void launch_row_rhs(ecs_ctx* c, int B, cudaStream_t s, const StepCtl* ctl = null
 
 template <typename R, int N>
 void launch_col_rk43(ecs_ctx* c, int B, int stage, cudaStream_t s, cplx<R>* rec = nullptr, int cap = 0) {
-  Col43Params<R> p;
+  Col43Params<R> p{};
   p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.S = (cplx<R>*)c->S43; p.ctl = c->ctl;
   p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.rec = rec; p.cap = cap;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
@@ -197,8 +197,9 @@ void launch_regen(ecs_ctx* c, const cplx<R>* rec, const long* items, int nitems,
 }
 
 template <typename R, int N>
-void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_bstride = 0) {
-  RowTanParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_bstride = 0,
+                    const StepCtl* ctl = nullptr) {
+  RowTanParams<R> p{}; p.ctl = ctl; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B; p.phys_bstride = phys_bstride;
   if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
   else if (N == 128 && c->rowtan_xt == 4)   // 4-row tiles measured faster at n = 128 only
@@ -208,8 +209,9 @@ void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_
 
 template <typename R, int N>
 void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* rec, const double* dT, double t,
-                    double h, double dscale, int nslot, cudaStream_t s) {
-  ColTanParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
+                    double h, double dscale, int nslot, cudaStream_t s, const StepCtl* ctl = nullptr,
+                    long rec_bstride = 0, const double* dscale_b = nullptr, const R* etab = nullptr) {
+  ColTanParams<R> p{}; p.ctl = ctl; p.rec_bstride = rec_bstride; p.dscale_b = dscale_b; p.etab = etab; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
   p.rec = rec; p.dT = dT; p.t = t; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage; p.produce = produce;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
@@ -1052,8 +1054,7 @@ struct Impl {
         const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
         const double h = L.hs[a];
         if (!L.acc[a]) {
-          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, t, h, (R)c->nu,
-                                                                (R)c->eta, N, B);
+          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, N, B);
           continue;
         }
         launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
@@ -1315,14 +1316,19 @@ struct Impl {
         const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
         const double h = hh[a - a_lo];
         if (!acc[a - a_lo]) {
-          ++c->launches; k_tan_reject<R><<<grid1d((long)Bg * VEC), 256, 0, st>>>((cplx<R>*)c->D, nslot, ra, dTg, 1.0, t, h,
-                                                                                 (R)c->nu, (R)c->eta, N, Bg);
+          ++c->launches; k_tan_reject<R><<<grid1d((long)Bg * VEC), 256, 0, st>>>((cplx<R>*)c->D, nslot, ra, dTg, 1.0, N, Bg);
           continue;
         }
+        const bool kt = g == 0 && c->kt.on;
+        if (kt) kt_begin(c, st);
         launch_col_tan<R, N>(c, Bg, T43_A, 1, ra, dTg, t, h, 1.0, nslot, st);
+        if (kt) kt_end(c, 1, Bg, st);
         for (int k = 0; k < 4; ++k) {
+          if (kt) kt_begin(c, st);
           launch_row_tan<R, N>(c, Bg, phys(item_of[a - a_lo] + k), st);
+          if (kt) { kt_end(c, 0, Bg, st); kt_begin(c, st); }
           launch_col_tan<R, N>(c, Bg, T43_B + k, 1, ra, dTg, t, h, 1.0, nslot, st);
+          if (kt) kt_end(c, 1, Bg, st);
         }
       }
       c->G = G0; c->H = H0; c->D = D0;
@@ -1619,7 +1625,7 @@ struct Impl {
           const double h = L.hs[a];
           if (!L.acc[a]) {
             const int cols = B * K;
-            ++c->launches; k_adj_reject<R><<<(cols + 3) / 4, 128, 0, s>>>((cplx<R>*)c->D, nslot, ra, c->hacc, t, h, (R)c->nu, (R)c->eta, N, B);
+            ++c->launches; k_adj_reject<R><<<(cols + 3) / 4, 128, 0, s>>>((cplx<R>*)c->D, nslot, ra, c->hacc, N, B);
             continue;
           }
           launch_col_adj<R, N>(c, B, AJ43_PRE, ra, nullptr, t, h, nslot, s);
@@ -1742,6 +1748,151 @@ struct Impl {
     ps.active = 0;
     ++c->launches; k_pool_init<<<1, 32, 0, s>>>(c->ctl, slot, 1, 0);
     return cuda_err(c, cudaGetLastError(), "pool_retire");
+  }
+
+  // ---------------------------------------------------------------------
+  // Several candidates' Lawson-RK4 objectives and one JVP each, in one
+  // forward-mode sweep (ecs_jvp_multi): B independent jax.jvp calls of
+  // objective_RPO (jax_scripts/lib/utils.py:108) batched across candidates.
+  // The B primal solves step together as the slot pool's do (own T, h,
+  // symmetry, step budget per candidate: control block b), and each stage's
+  // tangent pass follows that stage's primal pass: the primal row pass writes
+  // the stage's physical fields u, v, B_x, B_y per candidate, the primal
+  // column pass the step's record vectors (one step, overwritten each step),
+  // and the tangent row and column passes read them.  Nothing else is kept,
+  // so device memory does not grow with the horizon.  A candidate whose budget
+  // is spent is skipped by every later launch.  Steps run as 8-step CUDA
+  // graphs (per-candidate data is read from the control blocks).
+  // ---------------------------------------------------------------------
+  static int ensure_multi(ecs_ctx* c) {
+    auto& m = c->mj;
+    if (m.G) return ECS_OK;
+    const size_t B = (size_t)c->max_batch, VEC = 2UL * K * M, cb = sizeof(cplx<R>), rb = sizeof(R);
+    int st = ECS_OK;
+    m.G = dev_alloc(c, B * NG * K * N * cb, &st);
+    m.H = dev_alloc(c, B * NH * K * N * cb, &st);
+    m.phys = dev_alloc(c, B * N * NPH * N * rb, &st);
+    m.rec = dev_alloc(c, B * Q_NREC * VEC * cb, &st);
+    m.vt = dev_alloc(c, B * 2 * N * N * rb, &st);
+    m.vx = dev_alloc(c, B * 2 * N * N * rb, &st);
+    m.dscale = (double*)dev_alloc(c, B * sizeof(double), &st);
+    m.dT = (double*)dev_alloc(c, B * sizeof(double), &st);
+    return st;
+  }
+
+  static int jvp_multi(ecs_ctx* c, const ecs_shoot_cfg* cfgs, const R* fields, const double* T, const double* sx,
+                       R* out_fields, const R* dfields, const double* dT, const double* dsx, R* out, double* odT,
+                       double* odsx, int B, cudaStream_t s) {
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>), fe = 2UL * N * N;
+    const long pstride = (long)N * NPH * N, rstride = (long)Q_NREC * VEC;
+    const int nslot = (int)D_NS4;
+    std::vector<double> dscale(B);
+    long smax = 0;
+    for (int b = 0; b < B; ++b) {
+      if (cfgs[b].mode != ECS_MODE_LAWSON_RK4) return set_err(c, ECS_ERR_BAD_MODE, "ecs_jvp_multi runs Lawson_RK4");
+      const long steps = (long)cfgs[b].num_checkpoints * cfgs[b].ministeps;
+      if (cfgs[b].num_checkpoints <= 0 || cfgs[b].ministeps <= 0 || steps > (1L << 30))
+        return set_err(c, ECS_ERR_INVALID, "num_checkpoints and ministeps must be > 0");
+      smax = std::max(smax, steps);
+      dscale[b] = 1.0 / ((double)cfgs[b].num_checkpoints * (double)cfgs[b].ministeps);
+    }
+    int st = ensure_multi(c);
+    if (!st) st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (st) return st;
+    auto& m = c->mj;
+    c->pool.clear();   // the control blocks are reused: a slot pool on this context starts over
+    cudaError_t e = cudaMemcpyAsync(m.dscale, dscale.data(), B * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m.dT, dT, B * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_err(c, e, "jvp_multi scales");
+    dT = m.dT;   // the captured steps read the context's copy
+    // primal and tangent start states (boxes of rfft2(fields), rfft2(dfields))
+    st = to_box(c, fields, (cplx<R>*)c->F, B, s);
+    if (st) return st;
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)D_F * VEC, B, 2, s, (long)nslot * VEC);
+    // per candidate: h = (T/nc)/ms, e = exp(h/2 L) mask, step budget
+    for (int b = 0; b < B; ++b) {
+      ++c->launches;
+      k_rk4_setup<R><<<grid1d((long)VEC), 256, 0, s>>>(T + b, cfgs[b].num_checkpoints, cfgs[b].ministeps, c->ctl + b,
+                                                       (R*)c->Etab + (size_t)b * VEC, N, c->nu, c->eta, 1);
+      ++c->launches;
+      k_pool_init<<<1, 32, 0, s>>>(c->ctl, b, 1, (int)((long)cfgs[b].num_checkpoints * cfgs[b].ministeps));
+    }
+    // phase fields (stop-gradient, loss_functions.py:113-130): vt = irfft2(state_vel(f0)), vx = irfft2(i kx f0)
+    launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
+    launch_row_rhs<R, N>(c, B, s);
+    launch_col_rk4<R, N>(c, B, COL_PLAIN, 0, 1, s);
+    st = from_box(c, (const cplx<R>*)c->OUT, (R*)m.vt, B, s);
+    if (st) return st;
+    launch_col_from_box<R, N>(c, (const cplx<R>*)c->F, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 1, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, (R*)m.vx, nullptr, nullptr, B, 0, s);
+    // the sweep: per stage, the primal pass on (G, H), then the tangent pass on the tangents' (G, H)
+    void* const G0 = c->G; void* const H0 = c->H;
+    auto tangent_bufs = [&](bool on) { c->G = on ? m.G : G0; c->H = on ? m.H : H0; };
+    auto start = [&](cudaStream_t st_) {
+      launch_col_rk4<R, N>(c, B, COL_START, 1, 0, st_, nullptr, 0, 1);
+      tangent_bufs(true);
+      launch_col_tan<R, N>(c, B, TS_START, 1, (const cplx<R>*)m.rec, dT, 0.0, 0.0, 0.0, nslot, st_, c->ctl, rstride,
+                           m.dscale, (const R*)c->Etab);
+      tangent_bufs(false);
+    };
+    auto one_step = [&](cudaStream_t st_) {
+      for (int q = 1; q <= 4; ++q) {
+        launch_row_rhs<R, N>(c, B, st_, c->ctl, (R*)m.phys, pstride);
+        launch_col_rk4<R, N>(c, B, q, 1, 0, st_, (cplx<R>*)m.rec, rstride, 1);
+        tangent_bufs(true);
+        launch_row_tan<R, N>(c, B, (const R*)m.phys, st_, pstride, c->ctl);
+        launch_col_tan<R, N>(c, B, q, 1, (const cplx<R>*)m.rec, dT, 0.0, 0.0, 0.0, nslot, st_, c->ctl, rstride,
+                             m.dscale, (const R*)c->Etab);
+        tangent_bufs(false);
+      }
+      ++c->launches; k_pool_count<<<(B + 127) / 128, 128, 0, st_>>>(c->ctl, B);
+    };
+    constexpr int GS = 8;
+    auto& gk = m.g;
+    if (gk.exec && (gk.B != B || gk.D != c->D)) { cudaGraphExecDestroy(gk.exec); gk.exec = nullptr; }
+    if (!gk.exec && smax >= GS) {
+      const long long l0 = c->launches;
+      cudaGraph_t graph = nullptr;
+      std::lock_guard<std::mutex> capture_guard(capture_mutex());   // no set-up of another context meanwhile
+      e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int a = 0; a < GS; ++a) one_step(c->cap_stream);
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&gk.exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) { gk.exec = nullptr; return cuda_err(c, e, "jvp_multi graph capture"); }
+      gk.B = B; gk.D = c->D;
+      gk.nodes = c->launches - l0;
+      c->launches = l0;
+    }
+    start(s);
+    long it = 0;
+    for (; gk.exec && it + GS <= smax; it += GS) {
+      e = cudaGraphLaunch(gk.exec, s);
+      if (e != cudaSuccess) return cuda_err(c, e, "jvp_multi graph launch");
+      c->launches += gk.nodes;
+    }
+    for (; it < smax; ++it) one_step(s);
+    // per candidate: objective residual, tangent residual, phase-condition tangents
+    for (int b = 0; b < B; ++b) {
+      const cplx<R>* phi = (const cplx<R>*)c->F + (size_t)b * VEC;
+      if (out_fields) {
+        st = residual(c, &cfgs[b], fields + (size_t)b * fe, phi, nullptr, sx + b, 1, out_fields + (size_t)b * fe, s, 1);
+        if (st) return st;
+      }
+      ++c->launches;
+      k_tan_shift<R><<<grid1d((long)VEC), 256, 0, s>>>((const cplx<R>*)c->D + ((size_t)b * nslot + D_F) * VEC,
+                                                       (long)nslot * VEC, phi, dsx + b, (cplx<R>*)c->V, N, 1);
+      st = residual(c, &cfgs[b], dfields + (size_t)b * fe, (const cplx<R>*)c->V, nullptr, sx + b, 1,
+                    out + (size_t)b * fe, s, 1);
+      if (st) return st;
+      ++c->launches;
+      k_phase_dot<R><<<1, 256, 0, s>>>((const R*)m.vt + (size_t)b * fe, (const R*)m.vx + (size_t)b * fe,
+                                       dfields + (size_t)b * fe, odT + b, odsx + b, N);
+    }
+    return cuda_err(c, cudaGetLastError(), "jvp_multi");
   }
 
   // Time `iters` launches of one hot kernel on the current workspace (after a
@@ -1884,6 +2035,10 @@ ImplTable make_table() {
              cudaStream_t s) { return I::vjp(c, (const R*)cf, cT, csx, (R*)g, gT, gsx, B, s); };
   t.bench_kernel = [](ecs_ctx* c, int which, int B, int iters, float* ms, double* bytes, cudaStream_t s) {
     return I::bench_kernel(c, which, B, iters, ms, bytes, s); };
+  t.jvp_multi = [](ecs_ctx* c, const ecs_shoot_cfg* cfgs, const void* f, const double* T, const double* sx, void* o,
+                   const void* df, const double* dT, const double* dsx, void* od, double* oT, double* osx, int B,
+                   cudaStream_t s) {
+    return I::jvp_multi(c, cfgs, (const R*)f, T, sx, (R*)o, (const R*)df, dT, dsx, (R*)od, oT, osx, B, s); };
   t.pool_reset = [](ecs_ctx* c, cudaStream_t s) { return I::pool_reset(c, s); };
   t.pool_admit = [](ecs_ctx* c, int slot, const ecs_shoot_cfg* cfg, const void* f, double T, double sx,
                     cudaStream_t s) { return I::pool_admit(c, slot, cfg, (const R*)f, T, sx, s); };

@@ -302,12 +302,12 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
         k3 = cscale(k3, e);
         x[j] = cadd(f, k3);
         put(Q_X4, x[j]);
-        p.F[i] = cadd(cadd(cadd(f, cdiv_r(a, R(6))), cdiv_r(q2, R(3))), cdiv_r(k3, R(3)));
+        p.F[i] = cadd(cadd(cadd(f, cdiv_k<6>(a)), cdiv_k<3>(q2)), cdiv_k<3>(k3));
       } break;
       case COL_RK4_S4: {   // k4; f = acc + k4/6   (:79-80)
         const cplx<R> k4 = cscale(v, h);
         put(Q_K4, k4);
-        const cplx<R> f = cadd(FV, cdiv_r(k4, R(6)));
+        const cplx<R> f = cadd(FV, cdiv_k<6>(k4));
         p.F[i] = f;
         x[j] = f;
       } break;

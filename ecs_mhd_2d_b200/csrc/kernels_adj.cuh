@@ -178,9 +178,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
       switch (STAGE) {
         case AJ_PRE: {
           const cplx<R> ob = J[J_OB * VEC + o];
-          J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_r(ob, R(6));
-          J[J_K2 * VEC + o] = cdiv_r(ob, R(3)); J[J_B3 * VEC + o] = cdiv_r(ob, R(3));
-          kb = cdiv_r(ob, R(6));                                   // k4bar
+          J[J_F2 * VEC + o] = ob; J[J_A1 * VEC + o] = cdiv_k<6>(ob);
+          J[J_K2 * VEC + o] = cdiv_k<3>(ob); J[J_B3 * VEC + o] = cdiv_k<3>(ob);
+          kb = cdiv_k<6>(ob);                                   // k4bar
           hpart += ip(kb, Q[Q_K4 * VEC + o]) / (double)h;
         } break;
         case AJ_S4: {
@@ -214,9 +214,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
           const cplx<R> fb = cadd(J[J_OB * VEC + o], Xb);
           J[J_OB * VEC + o] = fb;
           if (p.rec_prev) {
-            J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_r(fb, R(6));
-            J[J_K2 * VEC + o] = cdiv_r(fb, R(3)); J[J_B3 * VEC + o] = cdiv_r(fb, R(3));
-            kb = cdiv_r(fb, R(6));
+            J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_k<6>(fb);
+            J[J_K2 * VEC + o] = cdiv_k<3>(fb); J[J_B3 * VEC + o] = cdiv_k<3>(fb);
+            kb = cdiv_k<6>(fb);
             hpart += ip(kb, p.rec_prev[Q_K4 * VEC + o]) / (double)h;
           } else {
             feed = false;
@@ -225,8 +225,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
       }
       kb = cscale(kb, h);
     } else {
-      const R e = exp((t * L) * h / R(2));
-      const R dedt = e * (L * h / R(2));
+      const cplx<R> eg = Q[RR_E * VEC + o];   // (e, e L h/2) of the attempt, e = exp(t L h/2)
+      const R e = eg.x;
+      const R dedt = eg.y;
       switch (STAGE) {
         case AJ43_PRE:      // from (xbar_f, k5bar) in (X0, K1) slots: RHS5 input = k5bar
         case AJ43_IPRE: {   // initial k1 = t v(x0): input = k1bar
@@ -236,10 +237,10 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
         case AJ43_S5: {     // xbar_f += Xbar5; distribute to x2, k1'', k2', k3', k4
           const cplx<R> xfb = cadd(J[JJ_X0 * VEC + o], Xb);
           J[JJ_X2 * VEC + o] = xfb;
-          J[JJ_K1PP * VEC + o] = cdiv_r(cscale(xfb, h), R(6));
-          J[JJ_K2P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
-          J[JJ_K3P * VEC + o] = cdiv_r(cscale(xfb, h), R(3));
-          kb = cdiv_r(cscale(xfb, h), R(6));                       // k4bar
+          J[JJ_K1PP * VEC + o] = cdiv_k<6>(cscale(xfb, h));
+          J[JJ_K2P * VEC + o] = cdiv_k<3>(cscale(xfb, h));
+          J[JJ_K3P * VEC + o] = cdiv_k<3>(cscale(xfb, h));
+          kb = cdiv_k<6>(cscale(xfb, h));                       // k4bar
           hpart += ip(kb, Q[RR_K4 * VEC + o]) / (double)t;
         } break;
         case AJ43_S4: {     // Y4 = x2 + h k3'
@@ -309,10 +310,9 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   }
 }
 
-// Rejected Lawson-RK4(3) attempt in reverse: k1_next = e (e k1).
+// Rejected Lawson-RK4(3) attempt in reverse: k1_next = e (e k1) ((e, e L h/2) from the attempt's record).
 template <typename R>
-__global__ void k_adj_reject(cplx<R>* J, int nslot, const cplx<R>* rec, double* hacc, double t, double h, R nu, R eta,
-                             int n, int B) {
+__global__ void k_adj_reject(cplx<R>* J, int nslot, const cplx<R>* rec, double* hacc, int n, int B) {
   const Geom g = make_geom(n);
   const size_t VEC = (size_t)2 * g.K * g.M;
   // one warp per (b, ky) column so that hacc[b][ky] has a single writer
@@ -325,10 +325,9 @@ __global__ void k_adj_reject(cplx<R>* J, int nslot, const cplx<R>* rec, double* 
   for (int ch = 0; ch < 2; ++ch)
     for (int slot = lane; slot < g.M; slot += 32) {
       const size_t o = ((size_t)ch * g.K + ky) * g.M + slot;
-      const int kx = slot_to_kx(slot, g.kmax, g.M);
-      const R L = diss_L<R>(kx, ky, ch == 0 ? nu : eta);
-      const R e = exp(((R)t * L) * (R)h / R(2));
-      const R dedt = e * (L * (R)h / R(2));
+      const cplx<R> eg = rec[RR_E * VEC + o];   // (e, e L h/2) of the attempt
+      const R e = eg.x;
+      const R dedt = eg.y;
       const cplx<R> k1 = rec[RR_K1 * VEC + o], k1e = cscale(k1, e);
       const cplx<R> kppb = Jb[JJ_K1 * VEC + o];
       const cplx<R> kpb = cscale(kppb, e);

@@ -87,16 +87,16 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
       // v_fn includes dissipation L x at the stage input x (loss_functions.py:53, mhd_jax.py:171-173)
       const cplx<R> f = Q(X_F);
       cplx<R> xs = f;
-      if (STAGE == 2) xs = cadd(f, cdiv_r(Q(X_K1), R(2)));
-      if (STAGE == 3) xs = cadd(f, cdiv_r(Q(X_K1 + 1), R(2)));
+      if (STAGE == 2) xs = cadd(f, cdiv_k<2>(Q(X_K1)));
+      if (STAGE == 3) xs = cadd(f, cdiv_k<2>(Q(X_K1 + 1)));
       if (STAGE == 4) xs = cadd(f, Q(X_K1 + 2));
       const cplx<R> k = cscale(cadd(v, cscale(xs, L)), h);            // timestepping.py:40-43
       if (STAGE < 4) {
         Q(X_K1 + STAGE - 1) = k;
-        xin = STAGE < 3 ? cadd(f, cdiv_r(k, R(2))) : cadd(f, k);
+        xin = STAGE < 3 ? cadd(f, cdiv_k<2>(k)) : cadd(f, k);
       } else {
-        const cplx<R> fn = cadd(cadd(cadd(cadd(f, cdiv_r(Q(X_K1), R(6))), cdiv_r(Q(X_K1 + 1), R(3))),
-                                     cdiv_r(Q(X_K1 + 2), R(3))), cdiv_r(k, R(6)));   // :44
+        const cplx<R> fn = cadd(cadd(cadd(cadd(f, cdiv_k<6>(Q(X_K1))), cdiv_k<3>(Q(X_K1 + 1))),
+                                     cdiv_k<3>(Q(X_K1 + 2))), cdiv_k<6>(k));   // :44
         Q(X_F) = fn;
         xin = fn;
       }
@@ -111,40 +111,40 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
       switch (STAGE) {
         case 1:   // :110-112
           K_(1) = k; scale_all(1);
-          xin = cadd(Q(X_F), cdiv_r(K_(1), R(6)));
+          xin = cadd(Q(X_F), cdiv_k<6>(K_(1)));
           break;
         case 2:   // :113
           K_(2) = k;
-          xin = cadd(cadd(Q(X_F), cdiv_r(K_(1), R(12))), cdiv_r(K_(2), R(12)));
+          xin = cadd(cadd(Q(X_F), cdiv_k<12>(K_(1))), cdiv_k<12>(K_(2)));
           break;
         case 3:   // :114-115
           K_(3) = k; scale_all(3);
-          xin = cadd(csub(Q(X_F), cdiv_r(cscale(K_(2), R(4)), R(33))), cdiv_r(cscale(K_(3), R(5)), R(11)));
+          xin = cadd(csub(Q(X_F), cdiv_k<33>(cscale(K_(2), R(4)))), cdiv_k<11>(cscale(K_(3), R(5))));
           break;
         case 4:   // :116-117
           K_(4) = k; scale_all(4);
-          xin = cadd(csub(csub(Q(X_F), cdiv_r(K_(1), R(4))), cdiv_r(cscale(K_(2), R(29)), R(44))),
-                     cdiv_r(cscale(K_(3), R(31)), R(22)));
+          xin = cadd(csub(csub(Q(X_F), cdiv_k<4>(K_(1))), cdiv_k<44>(cscale(K_(2), R(29)))),
+                     cdiv_k<22>(cscale(K_(3), R(31))));
           break;
         case 5:   // :118-119
           K_(5) = k; scale_all(5);
-          xin = cadd(cadd(csub(cadd(cadd(Q(X_F), cdiv_r(cscale(K_(1), R(3)), R(11))), cdiv_r(cscale(K_(2), R(8)), R(33))),
-                               cdiv_r(cscale(K_(3), R(4)), R(11))), cdiv_r(K_(4), R(11))),
-                     cdiv_r(cscale(K_(5), R(14)), R(33)));
+          xin = cadd(cadd(csub(cadd(cadd(Q(X_F), cdiv_k<11>(cscale(K_(1), R(3)))), cdiv_k<33>(cscale(K_(2), R(8)))),
+                               cdiv_k<11>(cscale(K_(3), R(4)))), cdiv_k<11>(K_(4))),
+                     cdiv_k<33>(cscale(K_(5), R(14))));
           break;
         case 6:   // :120-121
           K_(6) = k; scale_all(6);
-          xin = cadd(csub(cadd(cadd(csub(csub(Q(X_F), cdiv_r(cscale(K_(1), R(17)), R(48))), cdiv_r(cscale(K_(2), R(5)), R(12))),
-                                    K_(3)), K_(4)), cdiv_r(cscale(K_(5), R(13)), R(12))),
-                     cdiv_r(cscale(K_(6), R(11)), R(16)));
+          xin = cadd(csub(cadd(cadd(csub(csub(Q(X_F), cdiv_k<48>(cscale(K_(1), R(17)))), cdiv_k<12>(cscale(K_(2), R(5)))),
+                                    K_(3)), K_(4)), cdiv_k<12>(cscale(K_(5), R(13)))),
+                     cdiv_k<16>(cscale(K_(6), R(11))));
           break;
         case 7:   // :122-123
           K_(7) = k; scale_all(7);
-          xin = cadd(csub(cadd(csub(csub(cadd(cadd(Q(X_F), cdiv_r(cscale(K_(1), R(20)), R(39))),
-                                                  cdiv_r(cscale(K_(2), R(12)), R(39))),
-                                             cdiv_r(cscale(K_(3), R(31)), R(39))), cdiv_r(K_(4), R(39))),
-                                   cdiv_r(cscale(K_(5), R(34)), R(39))), cdiv_r(cscale(K_(6), R(11)), R(39))),
-                     cdiv_r(cscale(K_(7), R(16)), R(39)));
+          xin = cadd(csub(cadd(csub(csub(cadd(cadd(Q(X_F), cdiv_k<39>(cscale(K_(1), R(20)))),
+                                                  cdiv_k<39>(cscale(K_(2), R(12)))),
+                                             cdiv_k<39>(cscale(K_(3), R(31)))), cdiv_k<39>(K_(4))),
+                                   cdiv_k<39>(cscale(K_(5), R(34)))), cdiv_k<39>(cscale(K_(6), R(11)))),
+                     cdiv_k<39>(cscale(K_(7), R(16))));
           break;
         default: {   // 8: :124
           const R c1 = R(13) / R(200), c3 = R(4) / R(25), c4 = R(11) / R(40);
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
           const cplx<R> k1 = Q(X_K1);
           const cplx<R> a1 = cscale(cadd(v, cscale(k1, L)), h);
           Q(X_A1) = a1;
-          const cplx<R> ft = cadd(cadd(Q(X_F), cdiv_r(k1, R(2))), cdiv_r(a1, R(8)));
+          const cplx<R> ft = cadd(cadd(Q(X_F), cdiv_k<2>(k1)), cdiv_k<8>(a1));
           Q(X_FT) = ft;
           if (p.rec) { p.rec[TR_A1 * VEC + o] = a1; p.rec[TR_FT * VEC + o] = ft; }
           xin = ft;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
         default: {  // a2 = h jac(f_temp, k2); f = f + k1 + a1/6 + a2/3
           const cplx<R> a2 = cscale(cadd(v, cscale(Q(X_K2T), L)), h);
           if (p.rec) p.rec[TR_A2 * VEC + o] = a2;
-          const cplx<R> fn = cadd(cadd(cadd(Q(X_F), Q(X_K1)), cdiv_r(Q(X_A1), R(6))), cdiv_r(a2, R(3)));
+          const cplx<R> fn = cadd(cadd(cadd(Q(X_F), Q(X_K1)), cdiv_k<6>(Q(X_A1))), cdiv_k<3>(a2));
           Q(X_F) = fn;
           xin = fn;
         } break;
@@ -334,14 +334,14 @@ __global__ void __launch_bounds__(128) k_col_tdj(ColTdjParams<R> p) {
         const cplx<R> dk1 = Dq(DT_K1);
         const cplx<R> da1 = dk(TR_A1, dk1);
         Dq(DT_A1) = da1;
-        const cplx<R> dft = cadd(cadd(Dq(DT_F), cdiv_r(dk1, R(2))), cdiv_r(da1, R(8)));
+        const cplx<R> dft = cadd(cadd(Dq(DT_F), cdiv_k<2>(dk1)), cdiv_k<8>(da1));
         Dq(DT_FT) = dft;
         xin = dft;
       } break;
       case 3: { const cplx<R> dk2 = dk(TR_K2, Dq(DT_FT)); Dq(DT_K2) = dk2; xin = dk2; } break;
       default: {
         const cplx<R> da2 = dk(TR_A2, Dq(DT_K2));
-        const cplx<R> dfn = cadd(cadd(cadd(Dq(DT_F), Dq(DT_K1)), cdiv_r(Dq(DT_A1), R(6))), cdiv_r(da2, R(3)));
+        const cplx<R> dfn = cadd(cadd(cadd(Dq(DT_F), Dq(DT_K1)), cdiv_k<6>(Dq(DT_A1))), cdiv_k<3>(da2));
         Dq(DT_F) = dfn;
         xin = dfn;
       } break;
@@ -527,8 +527,8 @@ __global__ void __launch_bounds__(128) k_col_tda(ColTdaParams<R> p) {
     switch (STAGE) {
       case TA_SEED: {
         const cplx<R> fb = Jq(JT_F);
-        const cplx<R> a2b = cdiv_r(fb, R(3));
-        Jq(JT_A2) = a2b; Jq(JT_K1) = fb; Jq(JT_A1) = cdiv_r(fb, R(6));
+        const cplx<R> a2b = cdiv_k<3>(fb);
+        Jq(JT_A2) = a2b; Jq(JT_K1) = fb; Jq(JT_A1) = cdiv_k<6>(fb);
         hpart += ip(a2b, Q[TR_A2 * VEC + o]) / (double)h;
         kb = a2b;
       } break;
@@ -541,8 +541,8 @@ __global__ void __launch_bounds__(128) k_col_tda(ColTdaParams<R> p) {
       case TA_C: {
         const cplx<R> ftb = cadd(cadd(Jq(JT_FT), xa[j]), cscale(Jq(JT_K2), h * L));
         Jq(JT_F) = cadd(Jq(JT_F), ftb);
-        Jq(JT_K1) = cadd(Jq(JT_K1), cdiv_r(ftb, R(2)));
-        const cplx<R> a1b = cadd(Jq(JT_A1), cdiv_r(ftb, R(8)));
+        Jq(JT_K1) = cadd(Jq(JT_K1), cdiv_k<2>(ftb));
+        const cplx<R> a1b = cadd(Jq(JT_A1), cdiv_k<8>(ftb));
         Jq(JT_A1) = a1b;
         hpart += ip(a1b, Q[TR_A1 * VEC + o]) / (double)h;
         kb = a1b;

@@ -13,10 +13,15 @@
 namespace ecs {
 
 // Per-candidate state slots of the stepper, each a box vector [2][K][M].
-enum Rk43Slot { S_X0 = 0, S_K1, S_XE, S_K1E, S_K2, S_K3, S_X2, S_K4, S_XF, S_K5, S_NSLOT };
+// S_E holds (e, e L h/2) of the current attempt, e = exp(t L h/2) (written at
+// stage A, read at stage C).
+enum Rk43Slot { S_X0 = 0, S_K1, S_XE, S_K1E, S_K2, S_K3, S_X2, S_K4, S_XF, S_K5, S_E, S_NSLOT };
 // Trajectory record per attempt (primal values needed by tangent/adjoint):
-// start state, carried k1 (before twiddles), k2..k5 and the stage inputs.
-enum Rk43Rec { RR_X0 = 0, RR_K1, RR_K2, RR_K3, RR_K4, RR_K5, RR_Y2, RR_Y3, RR_Y4, RR_XF, RR_NREC };
+// start state, carried k1 (before twiddles), k2..k5, the stage inputs, and the
+// attempt's integrating factor as (e, e L h/2) with e = exp(t L h/2), computed
+// once here so that the tangent and adjoint passes do not recompute it per
+// tangent (the same expression, so the same values).
+enum Rk43Rec { RR_X0 = 0, RR_K1, RR_K2, RR_K3, RR_K4, RR_K5, RR_Y2, RR_Y3, RR_Y4, RR_XF, RR_E, RR_NREC };
 
 enum Rk43Stage : int {
   R43_START = 6,  // no RHS input; inverse transforms of x0
@@ -46,7 +51,7 @@ struct Col43Params {
 // forward transform; they are staged per column into shared memory.
 __host__ __device__ constexpr unsigned r43_smask(int stage) {
   return stage == R43_B ? (1u << S_XE)
-       : stage == R43_C ? (1u << S_XE) | (1u << S_K1E) | (1u << S_K2)
+       : stage == R43_C ? (1u << S_XE) | (1u << S_K1E) | (1u << S_K2) | (1u << S_E)
        : stage == R43_D ? (1u << S_K1) | (1u << S_K2) | (1u << S_K3) | (1u << S_X2)
        : stage == R43_E ? (1u << S_K4) : 0u;
 }
@@ -134,6 +139,9 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
         if (pend) { S[S_X0 * VEC + o] = xs; S[S_K1 * VEC + o] = ks; }
         if (rec) { rec[RR_X0 * VEC + o] = xs; rec[RR_K1 * VEC + o] = ks; }
         const R e = exp((t * L) * h / R(2));         // e = exp(mod_L * h/2), not masked (:263)
+        const cplx<R> eg = mk<R>(e, e * (L * h * R(0.5)));
+        S[S_E * VEC + o] = eg;
+        if (rec) rec[RR_E * VEC + o] = eg;
         const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
         S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
         xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
@@ -147,7 +155,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       } break;
       case R43_C: {                                  // :271-280
         if (rec) rec[RR_K3 * VEC + o] = kv;
-        const R e = exp((t * L) * h / R(2));
+        const R e = SV(S_E, o, slot).x;
         const cplx<R> x2 = cscale(SV(S_XE, o, slot), e);
         const cplx<R> k1ee = cscale(SV(S_K1E, o, slot), e);
         const cplx<R> k2e = cscale(SV(S_K2, o, slot), e);
@@ -160,8 +168,8 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       case R43_D: {                                  // :280-281
         S[S_K4 * VEC + o] = kv;
         if (rec) rec[RR_K4 * VEC + o] = kv;
-        const cplx<R> acc = cadd(cadd(cadd(cdiv_r(SV(S_K1, o, slot), R(6)), cdiv_r(SV(S_K2, o, slot), R(3))),
-                                      cdiv_r(SV(S_K3, o, slot), R(3))), cdiv_r(kv, R(6)));
+        const cplx<R> acc = cadd(cadd(cadd(cdiv_k<6>(SV(S_K1, o, slot)), cdiv_k<3>(SV(S_K2, o, slot))),
+                                      cdiv_k<3>(SV(S_K3, o, slot))), cdiv_k<6>(kv));
         xin = cadd(SV(S_X2, o, slot), cscale(acc, h));
         S[S_XF * VEC + o] = xin;
         if (rec) rec[RR_XF * VEC + o] = xin;
@@ -169,7 +177,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
       default: {                                     // R43_E: :282, :288
         S[S_K5 * VEC + o] = kv;
         if (rec) rec[RR_K5 * VEC + o] = kv;
-        xin = cdiv_r(cscale(csub(kv, SV(S_K4, o, slot)), h), R(6));
+        xin = cdiv_k<6>(cscale(csub(kv, SV(S_K4, o, slot)), h));
       } break;
     }
     x[j] = xin;

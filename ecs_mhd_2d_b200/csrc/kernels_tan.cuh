@@ -103,6 +103,7 @@ struct RowTanParams {
   const R* phys;        // primal physical fields of this stage: phys + b * phys_bstride is [N][NPH][N]
   long phys_bstride;    // 0: one primal shared by the batch
   const cplx<R>* tw;
+  const StepCtl* ctl;   // optional per-candidate control: batch elements whose ctl.done is set are skipped
   int B;
 };
 
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
+  if (p.ctl && p.ctl[b].done) return;   // the whole CTA belongs to batch element b
   // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
   // the tile load and the inverse transforms (n <= 128); at n = 256 they would
   // hold 4 E = 32 registers across the transform, so they are loaded after it
@@ -186,6 +188,14 @@ struct ColTanParams {
   const cplx<R>* tw;
   R nu, eta;
   int B, stage, produce;
+  // Several candidates, one tangent each (ecs_jvp_multi; Lawson-RK4 stages):
+  // ctl[b] gives candidate b's step size h and done flag (skipped once done),
+  // rec + b * rec_bstride its record, dscale_b[b] its dT scale, and
+  // etab + b * 2 K M its factor exp(h/2 L) mask.  All null/0 for one candidate.
+  const StepCtl* ctl;
+  long rec_bstride;
+  const double* dscale_b;
+  const R* etab;
 };
 
 // Record vectors (bits of Rk43Rec) and tangent slots (bits of Rk43Slot) that the
@@ -193,9 +203,9 @@ struct ColTanParams {
 // shared memory at the start (see k_col_tan).
 __host__ __device__ constexpr unsigned tan_qmask(int stage) {
   return stage == T43_INIT ? (1u << RR_K1)
-       : stage == T43_A ? (1u << RR_X0) | (1u << RR_K1)
+       : stage == T43_A ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_E)
        : stage == T43_B ? (1u << RR_K2)
-       : stage == T43_C ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_K2) | (1u << RR_K3)
+       : stage == T43_C ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_K2) | (1u << RR_K3) | (1u << RR_E)
        : stage == T43_D ? (1u << RR_K4)
        : stage == T43_E ? (1u << RR_K5) : 0u;
 }
@@ -223,12 +233,13 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (colid >= p.B * K * 2) return;
   const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
+  if (p.ctl && p.ctl[b].done) return;
   cplx<R>* D = p.D + (size_t)b * p.nslot * VEC;
-  const cplx<R>* Q = p.rec;
+  const cplx<R>* Q = p.rec + (size_t)b * p.rec_bstride;
   constexpr bool rk43 = STAGE >= T43_INIT;
   constexpr bool has_rhs = !(STAGE == TS_START || STAGE == T43_A || STAGE == T43_START);
-  const R h = (R)p.h, t = (R)p.t;
-  const R dpar = (R)(p.dT[b] * p.dscale);   // dh (RK4) or dt (RK4(3))
+  const R h = p.ctl ? (R)p.ctl[b].h : (R)p.h, t = (R)p.t;
+  const R dpar = (R)(p.dT[b] * (p.dscale_b ? p.dscale_b[b] : p.dscale));   // dh (RK4) or dt (RK4(3))
   // The record vectors and tangent slots the stage algebra reads, this column's
   // rows of them (M entries each), copied into the warp's shared buffer with
   // cp.async before the forward transform, so that their latency overlaps it
@@ -277,7 +288,7 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
     cplx<R> xin = mk<R>(0, 0);
     if (!rk43) {
       // Lawson-RK4: e = exp(h/2 L) mask, de = e L dh/2; dk = dh v + h dv with v = k/h
-      const R e = in_mask ? exp(h / R(2) * L) : R(0);
+      const R e = p.etab ? p.etab[(size_t)b * VEC + o] : in_mask ? exp(h / R(2) * L) : R(0);
       const R de = e * L * (dpar / R(2));
       auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv, h)); };
       switch (STAGE) {
@@ -302,23 +313,25 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
           const cplx<R> db2 = cadd(cscale(Q[Q_K2 * VEC + o], de), cscale(D[D_K2 * VEC + o], e));
           const cplx<R> db3 = cadd(cscale(Q[Q_K3 * VEC + o], de), cscale(dk3, e));
           xin = cadd(df2, db3);
-          D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_r(db1, R(6))), cdiv_r(db2, R(3))), cdiv_r(db3, R(3)));
+          D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_k<6>(db1)), cdiv_k<3>(db2)), cdiv_k<3>(db3));
         } break;
         default: {   // T4_S4
           const cplx<R> dk4 = dk_of(Q_K4);
-          xin = cadd(D[D_F * VEC + o], cdiv_r(dk4, R(6)));
+          xin = cadd(D[D_F * VEC + o], cdiv_k<6>(dk4));
           D[D_F * VEC + o] = xin;
         } break;
       }
     } else {
       // Lawson-RK4(3): e = exp(t L h/2), de = e L h/2 dt; dk = dt v + t dv with v = k/t
-      const R e = exp((t * L) * h / R(2));
-      const R de = e * (L * h / R(2)) * dpar;
       // staged operands (shared memory) or, without staging, global memory
       auto QV = [&](int q) -> cplx<R> {
         if constexpr (NOP > 0) return my_op[popc_c(QM & ((1u << q) - 1u)) * M + slot];
         else return Q[q * VEC + o];
       };
+      // (e, e L h/2) of this attempt from the primal record (stages A and C use them)
+      const cplx<R> eg = (STAGE == T43_A || STAGE == T43_C) ? QV(RR_E) : mk<R>(0, 0);
+      const R e = eg.x;
+      const R de = eg.y * dpar;
       auto DV = [&](int d) -> cplx<R> {
         if constexpr (NOP > 0) return my_op[(NQ + popc_c(DM & ((1u << d) - 1u))) * M + slot];
         else return D[d * VEC + o];
@@ -350,8 +363,8 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
         } break;
         case T43_D: {
           const cplx<R> dk4 = dk_of(RR_K4);
-          const cplx<R> acc = cadd(cadd(cadd(cdiv_r(DV(S_K1), R(6)), cdiv_r(DV(S_K2), R(3))),
-                                        cdiv_r(DV(S_K3), R(3))), cdiv_r(dk4, R(6)));
+          const cplx<R> acc = cadd(cadd(cadd(cdiv_k<6>(DV(S_K1)), cdiv_k<3>(DV(S_K2))),
+                                        cdiv_k<3>(DV(S_K3))), cdiv_k<6>(dk4));
           xin = cadd(DV(S_X2), cscale(acc, h));
           D[S_XF * VEC + o] = xin;
         } break;
@@ -368,21 +381,19 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
 }
 
 // Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);
-// its tangent is d(e (e k1)) with e' = e L h/2 dt.
+// its tangent is d(e (e k1)) with e' = e L h/2 dt ((e, e L h/2) from the attempt's record).
 template <typename R>
-__global__ void k_tan_reject(cplx<R>* D, int nslot, const cplx<R>* rec, const double* dT, double dscale, double t,
-                             double h, R nu, R eta, int n, int B) {
+__global__ void k_tan_reject(cplx<R>* D, int nslot, const cplx<R>* rec, const double* dT, double dscale, int n,
+                             int B) {
   const Geom g = make_geom(n);
   const size_t VEC = (size_t)2 * g.K * g.M;
   const long total = (long)B * VEC;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
     const int b = (int)(i / VEC);
     const size_t o = i - (size_t)b * VEC;
-    const int slot = o % g.M; const int ky = (o / g.M) % g.K; const int ch = (int)(o / ((size_t)g.K * g.M));
-    const int kx = slot_to_kx(slot, g.kmax, g.M);
-    const R L = diss_L<R>(kx, ky, ch == 0 ? nu : eta);
-    const R e = exp(((R)t * L) * (R)h / R(2));
-    const R de = e * (L * (R)h / R(2)) * (R)(dT[b] * dscale);
+    const cplx<R> eg = rec[RR_E * VEC + o];   // (e, e L h/2) of the attempt
+    const R e = eg.x;
+    const R de = eg.y * (R)(dT[b] * dscale);
     cplx<R>* Db = D + (size_t)b * nslot * VEC;
     const cplx<R> k1 = rec[RR_K1 * VEC + o];
     const cplx<R> k1e = cscale(k1, e);

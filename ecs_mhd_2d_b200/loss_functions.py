@@ -89,15 +89,20 @@ def _empty_like_out(fields):
     return {"fields": torch.empty_like(fields), "T": z, "sx": z.clone()}
 
 
-def objective_RPO(input_dict, param_dict, mode):
+def objective_RPO(input_dict, param_dict, mode, ctx=None):
     """{"fields": irfft2(f0 - g.Phi_T(f0)), "T": pt, "sx": px} (loss_functions.py:132-148).
-    pt and px are phase conditions whose value is exactly 0 (:128-129)."""
+    pt and px are phase conditions whose value is exactly 0 (:128-129).
+    `ctx` pins a private context (e.g. a serving worker thread's); by default
+    the shared per-physics context."""
     cfg = shoot_cfg(param_dict, mode)
     fields, T, sx, batched = prep_inputs(input_dict)
     B, n = fields.shape[0], fields.shape[-1]
     if B == 0:
         return _empty_like_out(fields)
-    ctx = _ctx.get_context(param_dict, n, fields.dtype, B)
+    if ctx is None:
+        ctx = _ctx.get_context(param_dict, n, fields.dtype, B)
+    else:
+        ctx.ensure_batch(B)
     out = torch.empty_like(fields)
     oT = torch.empty(B, dtype=torch.float64, device=fields.device)
     osx = torch.empty(B, dtype=torch.float64, device=fields.device)

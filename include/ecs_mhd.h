@@ -88,6 +88,33 @@ long long ecs_launch_count(const ecs_ctx* ctx);
  * per launch (instrumentation for roofline reporting; no reference counterpart). */
 int ecs_bench_kernel(ecs_ctx* ctx, int which, int batch, int iters, float* ms, double* bytes, void* stream);
 
+/* Newton-GMRES matvecs of `batch` different candidates in one call: for each
+ * candidate b the objective (objective_RPO, jax_scripts/lib/loss_functions.py:132-148)
+ * and its JVP for one tangent, as `batch` separate jax.jvp(obj, (x_b,), (v_b,))
+ * calls would give them (jax_scripts/lib/utils.py:108, once per Arnoldi step
+ * of jax_scripts/newton.py:165).  Mode Lawson_RK4 only; cfgs[b] (HOST array)
+ * gives candidate b's num_checkpoints, ministeps, shift_reflect_ny and rot, so
+ * candidates may differ in horizon, T, sx and symmetry (not in grid, dtype or
+ * physics, which the context fixes).  Forward mode: the primal solves and their
+ * tangents step together and no trajectory is kept (the context's linearisation
+ * is untouched; a slot pool on the context restarts).  Device arrays: fields,
+ * dfields, out_fields (may be NULL), out_dfields [batch][2][n][n]; T, sx, dT,
+ * dsx, out_dT, out_dsx [batch] (double).  batch <= max_batch. */
+int ecs_jvp_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, const double* T, const double* sx,
+                  void* out_fields, const void* dfields, const double* dT, const double* dsx, void* out_dfields,
+                  double* out_dT, double* out_dsx, int batch, void* stream);
+
+/* In-step timing of the batched tangent kernels (instrumentation for roofline
+ * reporting; no reference counterpart).  enable = 1: the following
+ * ecs_linearize_jvp calls (adaptive mode, pipelined path) record CUDA events
+ * around tangent group 0's row-pass and column-pass launches of every accepted
+ * attempt, on that group's stream, so each launch is timed in the launch shape
+ * of the real sweep (the other groups run beside it).  enable = 0: stop, wait
+ * for those events and return the mean duration (ms) and count per kind, and
+ * group 0's batch.  Output pointers are HOST memory and may be NULL. */
+int ecs_kernel_timing(ecs_ctx* ctx, int enable, double* row_ms, int* row_n, double* col_ms, int* col_n,
+                      int* group_batch);
+
 /* Context with grid tables and workspace for grids n in {64,128,256}
  * (replaces mhd_jax.construct_domain, jax_scripts/lib/mhd_jax.py:20-94, and
  * dictionaryIO.recompute_grid_information, jax_scripts/lib/dictionaryIO.py:64-78).
@@ -218,10 +245,12 @@ int ecs_pool_retire(ecs_ctx* ctx, int slot, void* out_fields, double* loss, void
  * physics is passed directly, with `forcing` a DEVICE real [n][n] array on the
  * grid of construct_domain.  All scratch comes from one fixed ~3.8 MB device
  * array in the library, held on every GPU that loads it until exit.
- * Limits: n in {64, 128}, batch <= 4, else ECS_ERR_TOO_LARGE.  Calls share the
- * array, so calls that overlap on the GPU race; each call re-initialises what
- * must start at zero.  The first call on a device does a one-time synchronous
- * set-up, so make it before any stream capture. */
+ * Limits: n in {64, 128}, batch <= 4, else ECS_ERR_TOO_LARGE (batch < 1:
+ * ECS_ERR_INVALID).  Calls share the array, so calls that overlap on the GPU
+ * race; each call re-initialises what must start at zero.  The first call on a
+ * device does a one-time synchronous set-up, so make it before any stream
+ * capture; the device address it looks up is kept, which assumes the runtime's
+ * primary context and no cudaDeviceReset afterwards. */
 int ecs_state_vel_noalloc(int n, double nu, double eta, double b0x, double b0y, const double* forcing,
                           const void* f_hat, void* dfdt_hat, int batch, int include_dissipation, void* stream);
 

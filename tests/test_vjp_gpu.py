@@ -105,6 +105,69 @@ def test_autograd_function(cuda):
     assert abs(float(T.grad) - float(g["T"])) <= 1e-12 * abs(float(g["T"]))
 
 
+def test_autograd_forward_and_backward_split(cuda):
+    """The adjoint sweep runs in backward only (as jax.value_and_grad splits it,
+    jax_scripts/adjoint_descent.py:91): under torch.no_grad the op launches
+    exactly what the plain loss_RPO launches; with grad enabled backward adds
+    the adjoint launches; the upstream gradient scales the result; the
+    normalised loss matches loss_and_grad(normalized=True)."""
+    from ecs_mhd_2d_b200 import context
+    n = 64
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", num_checkpoints=2, ministeps=8,
+                           shift_reflect_ny=1, rot=False, ckpt_every=4)
+    u0h = initial_condition(9, n)
+    inp = {"fields": torch.as_tensor(u0h, device="cuda"), "T": 0.15, "sx": 0.3}
+    ctx = context.get_context(pd, n, torch.float64, 1)
+    count = lambda: (torch.cuda.synchronize(), ctx.lib.ecs_launch_count(ctx.handle))[1]
+
+    c0 = count()
+    lp, _ = E.loss_RPO(inp, pd, "Lawson_RK4")
+    plain = count() - c0
+    u0 = torch.as_tensor(u0h, device="cuda").requires_grad_(True)
+    T = torch.tensor(0.15, dtype=torch.float64, device="cuda", requires_grad=True)
+    sx = torch.tensor(0.3, dtype=torch.float64, device="cuda", requires_grad=True)
+    with torch.no_grad():
+        c0 = count()
+        ln = E.loss_rpo_autograd(u0, T, sx, pd, "Lawson_RK4")
+        assert count() - c0 == plain
+    assert float(ln) == pytest.approx(float(lp), rel=1e-14)
+
+    c0 = count()
+    loss = E.loss_rpo_autograd(u0, T, sx, pd, "Lawson_RK4")
+    c1 = count()
+    (3.0 * loss).backward()
+    assert count() > c1
+    assert float(loss) == pytest.approx(float(lp), rel=1e-14)
+    (l2, _), g = E.loss_and_grad({"fields": u0.detach(), "T": 0.15, "sx": 0.3}, pd, "Lawson_RK4")
+    assert torch.allclose(u0.grad, 3.0 * g["fields"], rtol=1e-13, atol=1e-14 * float(g["fields"].abs().max()))
+    assert float(T.grad) == pytest.approx(3.0 * float(g["T"]), rel=1e-12)
+    assert float(sx.grad) == pytest.approx(3.0 * float(g["sx"]), rel=1e-12, abs=1e-14)
+
+    u0.grad = T.grad = sx.grad = None
+    lossn = E.loss_rpo_autograd(u0, T, sx, pd, "Lawson_RK4", normalized=True)
+    lossn.backward()
+    (ln2, _), gn = E.loss_and_grad({"fields": u0.detach(), "T": 0.15, "sx": 0.3}, pd, "Lawson_RK4", normalized=True)
+    assert float(lossn) == pytest.approx(float(ln2), rel=1e-13)
+    assert torch.allclose(u0.grad, gn["fields"], rtol=1e-12, atol=1e-14 * float(gn["fields"].abs().max()))
+    assert float(T.grad) == pytest.approx(float(gn["T"]), rel=1e-12)
+
+
+def test_shared_context_linearisations_do_not_mix(cuda):
+    """Two Objectives on the same cached context: a linearisation made by one
+    replaces the other's trajectory record, so the other must re-linearise
+    before its next JVP instead of reusing the record."""
+    n = 64
+    pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", num_checkpoints=1, ministeps=8,
+                           shift_reflect_ny=0, rot=False)
+    a, b = E.Objective(pd, "Lawson_RK4"), E.Objective(pd, "Lawson_RK4")
+    pa = {"fields": torch.as_tensor(initial_condition(1, n), device="cuda"), "T": 0.05, "sx": 0.0}
+    pb = {"fields": torch.as_tensor(initial_condition(2, n), device="cuda"), "T": 0.07, "sx": 0.1}
+    v = {"fields": torch.as_tensor(initial_condition(3, n), device="cuda"), "T": 0.1, "sx": 0.2}
+    ja = a.jvp(pa, v)["fields"].clone()
+    b.jvp(pb, v)
+    assert torch.equal(a.jvp(pa, v)["fields"], ja)
+
+
 def test_checkpointed_linearisation_matches_full_record(cuda):
     """Keeping every 5th state and recomputing segments (jax.checkpoint per
     segment, loss_functions.py:63) gives the same JVP and VJP as the full record."""
