@@ -46,14 +46,14 @@ METRIC = "GMRES matvecs/s (JVP of objective_RPO, Lawson_RK43 atol 1e-8, T=4.6) a
 UNIT = "matvec/s"
 
 
-def workload_config(extra=None):
-    cfg = {"workload": "newton_gmres_matvec_batch", "n": N, "dtype": "f64", "Re": RE, "forcing": "+4cos(4y)",
-           "b0": [0.0, 0.1], "T": T0, "sx": SX0, "mode": "Lawson_RK43", "atol": ATOL,
-           "checkpoints_x_max_steps": list(CAP), "tangents_per_step": BATCH, "ic": f"seed {IC_SEED}, amp {IC_AMP}",
-           "l2": "flushed (256 MiB write) between timed steps", "parallelism": "replicas"}
-    if extra:
-        cfg.update(extra)
-    return cfg
+def workload_config():
+    """The workload both arms run (identical in both lines; measured results go
+    to other keys)."""
+    return {"workload": "newton_gmres_matvec_batch", "n": N, "dtype": "f64", "Re": RE, "forcing": "+4cos(4y)",
+            "b0": [0.0, 0.1], "T": T0, "sx": SX0, "mode": "Lawson_RK43", "atol": ATOL,
+            "checkpoints_x_max_steps": list(CAP), "krylov_batch": BATCH, "ic": f"seed {IC_SEED}, amp {IC_AMP}",
+            "tangents": f"unit_tangents(seed rank, n, {BATCH})",
+            "l2": "device arm: flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
 
 
 def param_dict(E):
@@ -192,6 +192,27 @@ def secondary_workloads(E, torch, dev, flush):
     f3 = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(500 + b, n3, amp=IC_AMP) for b in range(64)])),
                          dtype=torch.complex64, device=dev)
     tsb, _ = _timed(torch, flush, lambda: E.lawson_rk4(f3, 256 * 4.6 / 2048, 256, pd3s))
+    # the precision target: Newton-GMRES with FP32 Jacobian products and FP64
+    # residuals/Arnoldi/least squares, then FP64 refinement, from the reference's
+    # 256^2 RPO2 (Re=50, 768 steps) perturbed by 1e-7
+    from ecs_mhd_2d_b200 import drivers
+    from ecs_mhd_2d_b200.utils import relative_error_RPO
+    d = np.load(os.path.join(ROOT, "tests", "golden", "solution_Re50_RPO2.npz"))
+    kw = dict(num_checkpoints=int(d["num_checkpoints"]), ministeps=int(d["ministeps"]),
+              shift_reflect_ny=int(d["shift_reflect_ny"]), rot=bool(d["rot"]))
+    pdr = E.make_param_dict(n3, float(d["nu"]), float(d["eta"]), b0=d["b0"], forcing="kolmogorov", **kw)
+    u = E.dealias(torch.as_tensor(d["fields"] + 1e-7 * initial_condition(98, n3, amp=1.0), device=dev), pdr)
+    x0 = {"fields": u, "T": float(d["T"]) * (1 + 1e-7), "sx": float(d["sx"])}
+    r0 = float(relative_error_RPO(x0, E.objective_RPO(x0, pdr, "Lawson_RK4")))
+    torch.cuda.synchronize()
+    tn0 = time.perf_counter()
+    _, hist = drivers.mixed_precision_newton(x0, pdr, "Lawson_RK4", iters=4, inner=32, refine=2)
+    torch.cuda.synchronize()
+    out["config3_newton_n256"] = {"start_rel_residual": r0, "final_rel_residual_fp64": hist[-1]["final_rel_err"],
+                                  "per_step_rel_residual": [h.get("rel_err") for h in hist[:-1]],
+                                  "jacobian": [h.get("jacobian") for h in hist[:-1]], "inner": 32,
+                                  "seconds": time.perf_counter() - tn0,
+                                  "base": "reference RPO2 (solutions/Re50/RPO2.npz), 768 Lawson-RK4 steps, +1e-7"}
     out["config3_mixed_n256"] = {"fp32_batch64_state_steps_per_s": 64 * 256 / tsb,
                                  "fp32_objective_steps_per_s": 2048 / t32, "fp64_objective_steps_per_s": 2048 / t64,
                                  "fp32_vs_fp64_objective_rel_err": err, "matvec_batch": Bt, "steps": 2048,
@@ -304,61 +325,249 @@ def cpu_baseline(target_s=12.0, attempts_full=None):
                       f"scaled by {full} attempts per full matvec; restated oracle on CPU (torch.func.jvp), not JAX"}
 
 
-def run_reference(args, rank):
+REF_BUDGET_S = 150.0   # the reference arm starts no new timed step after this much timed CPU work
+
+
+def oracle_matvec_fn():
+    """One complete matvec of the workload as the reference computes it: jax.jvp
+    of objective_RPO at the base point for one tangent (jax_scripts/lib/utils.py:108,
+    called once per Arnoldi step by jax_scripts/newton.py:165), i.e. the adaptive
+    primal solve and the tangent together.  Here torch.func.jvp of the oracle's
+    torch form on the host cores.  Returns f(i, cap=None): the matvec of tangent
+    i of the batch (cap: attempt cap override, for short warm-up runs)."""
+    import torch
+    from torch.func import jvp
+    import oracle as O
+    torch.set_num_threads(os.cpu_count() or 1)
+    u0, tv = host_inputs(0)
+
+    def f(i, cap=None):
+        ad = {"atol": ATOL, "checkpoints": CAP[0] if cap is None else 1,
+              "max_steps_per_checkpoint": CAP[1] if cap is None else cap}
+        pdt = O.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", xp=O.TORCH, shift_reflect_ny=0,
+                                rot=False, adaptive_dict=ad)
+        prim = {"fields": torch.from_numpy(u0), "T": torch.tensor(T0, dtype=torch.float64),
+                "sx": torch.tensor(SX0, dtype=torch.float64)}
+        t = tv[i % BATCH]
+        tan = {"fields": torch.from_numpy(np.ascontiguousarray(t[1:-1].reshape(2, N, N))),
+               "T": torch.tensor(t[0]), "sx": torch.tensor(t[-1])}
+        jvp(lambda d: O.objective_RPO(d, pdt, "Lawson_RK43", xp=O.TORCH), (prim,), (tan,))
+    return f
+
+
+def run_reference(args, rank, budget_s=None):
+    """The reference arm: the reference's CPU algorithm (the oracle; jax is not
+    installable here) on this workload, one complete single-tangent matvec per
+    step.  W warm-up steps are short (10-attempt) JVPs that build the FFT plans;
+    then up to K complete matvecs are timed, stopping early once the timed work
+    passes the budget (the line's steps / warmup are the counts actually run)."""
     if rank != 0:
         return
-    ref_attempts = 1988   # attempts of this workload's adaptive solve: 1983 accepted + 5 rejected (CUDA path and oracle)
-    cb = cpu_baseline(attempts_full=ref_attempts)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": BATCH / cb["value"] * 1e3,
+    budget_s = REF_BUDGET_S if budget_s is None else budget_s
+    f = oracle_matvec_fn()
+    for i in range(args.warmup):
+        f(i, cap=10)
+    times = []
+    while len(times) < max(1, args.steps):
+        t0 = time.perf_counter()
+        f(len(times))
+        times.append(time.perf_counter() - t0)
+        if sum(times) + statistics.mean(times) > budget_s:
+            break
+    total = sum(times)
+    value = len(times) / total
+    import torch
+    cores = torch.get_num_threads()
+    sample = (f"{len(times)} complete matvecs (jax.jvp semantics: adaptive primal solve + 1 tangent, "
+              f"torch.func.jvp of the oracle) of the workload, {total:.1f} s; restated oracle on CPU, not JAX")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": len(times), "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded initial condition and tangents)", "config": workload_config(),
-            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                                        "d2h_bytes_per_step": 0}}
+            "step": {"matvecs": 1, "what": "one jax.jvp of objective_RPO (primal solve + one tangent)",
+                     "requested_steps": args.steps, "warmup_what": "10-attempt JVPs (FFT plans)",
+                     "budget_s": budget_s},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args, rank, local, world):
+def serving_workload(requests=512, rate=40.0, seed=0):
     """Serving workload: a seeded Poisson stream of mixed requests {forward
     shooting, GMRES matvec, adjoint gradient} x n in {64,128,256} x horizons
-    256-2048 steps x Re in {40,50}; n=256 runs FP32 stepping, the rest FP64.
-    Each rank serves its own stream (replicas); value = all requests / max time."""
+    256-2048 steps x Re in {40,50}; n=256 runs FP32 stepping, the rest FP64, a
+    quarter of the FP64 requests the adaptive Lawson_RK43 stepper.  Returns
+    throughput, p50/p99 latency overall and per kind, and the batch sizes of
+    the matvec sweeps."""
     import torch
-    import torch.distributed as dist
-    from ecs_mhd_2d_b200 import build as _build, serving
-    _build.build()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
-    warm = serving.poisson_requests(9, rate=1000.0, seed=1000 + rank, horizons=(64,))
+    from ecs_mhd_2d_b200 import serving
+    warm = serving.poisson_requests(9, rate=1000.0, seed=1000 + seed, horizons=(64,))
     serving.Server(slots=8, chunk_steps=32).run(warm)
-    reqs = serving.poisson_requests(args.requests, rate=args.rate, seed=rank)
+    reqs = serving.poisson_requests(requests, rate=rate, seed=seed)
     srv = serving.Server(hbm_budget=96 << 30, slots=16, chunk_steps=32, workers_per_group=4)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = srv.run(reqs)
     torch.cuda.synchronize()
-    wall = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    wall = time.perf_counter() - t0
     lat = np.array([r.latency for r in res])
     by = {}
     for k in ("forward", "matvec", "gradient"):
         lk = np.array([r.latency for r in res if r.kind == k])
         if lk.size:
             by[k] = {"count": int(lk.size), "p50_s": float(np.percentile(lk, 50)), "p99_s": float(np.percentile(lk, 99))}
+    sweeps = [x for bt in srv.batchers.values() for x in bt.sweeps]
+    return {"requests": len(res), "wall_s": wall, "requests_per_s": len(res) / wall,
+            "arrival_rate_per_s": rate, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "by_kind": by,
+            "adaptive_requests": sum(r.mode == "Lawson_RK43" for r in reqs),
+            "matvec_sweeps": len(sweeps), "matvec_batch_mean": float(np.mean(sweeps)) if sweeps else None,
+            "matvec_batch_max": max(sweeps) if sweeps else None, "slots_per_pool": 16, "workers_per_group": 4}
+
+
+def run_serving(args, rank, local, world):
+    """`--workload serving`: the serving workload alone, one line; each rank
+    serves its own stream (replicas); value = all requests / max time."""
+    import torch
+    import torch.distributed as dist
+    from ecs_mhd_2d_b200 import build as _build
+    _build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    out = serving_workload(args.requests, args.rate, seed=rank)
+    wall = max_over_ranks(out["wall_s"], world, "cuda")
     if rank == 0:
-        line = {"metric": "serving throughput (mixed shooting requests)", "value": whole_job_rate(world, len(res), wall),
+        line = {"metric": "serving throughput (mixed shooting requests)", "value": whole_job_rate(world, out["requests"], wall),
                 "unit": "requests/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": wall * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
                 "data": "synthetic Poisson stream (seeded)",
-                "config": {"workload": "serving_poisson_mixed", "requests": len(res), "arrival_rate_per_s": args.rate,
-                           "n": [64, 128, 256], "horizons": [256, 512, 1024, 2048], "Re": [40, 50],
-                           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-                           "by_kind": by, "slots_per_pool": 16, "workers_per_group": 4}}
+                "config": {"workload": "serving_poisson_mixed", "requests": out["requests"],
+                           "arrival_rate_per_s": args.rate, "n": [64, 128, 256], "horizons": [256, 512, 1024, 2048],
+                           "Re": [40, 50]},
+                "details": out}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_kernels(rank, local, B=64):
+    """Profiling case: each hot kernel family once or a few times at n=128 FP64
+    with a batch of 64 (the working sets of the batched passes are 30-60 MB,
+    below the 126 MB L2, so DRAM counts of these launches are lower bounds):
+    Lawson-RK4 stepping (k_col_rk4, k_row_rhs), the adaptive solve (k_col_rk43,
+    k_row_err), linearisation + JVP batch (k_col_regen, k_row_phys, k_col_tan,
+    k_row_tan), VJP batch (k_col_adj, k_row_adj), an Arnoldi step
+    (k_arnoldi_mgs) and a multi-candidate matvec sweep.  Prints one JSON line
+    with the seconds taken."""
+    import torch
+    import ecs_mhd_2d_b200 as E
+    from ecs_mhd_2d_b200 import build as _build, linalg
+    from ecs_mhd_2d_b200.synthetic import initial_condition
+    _build.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    pd = E.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", num_checkpoints=1, ministeps=8,
+                           shift_reflect_ny=0, rot=False)
+    f = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(b, N, amp=IC_AMP) for b in range(B)])), device=dev)
+    E.lawson_rk4(f, 0.016, 8, pd)
+    ad = {"atol": 1e-8, "checkpoints": 2, "max_steps_per_checkpoint": 16}
+    pda = E.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", shift_reflect_ny=0, rot=False, adaptive_dict=ad)
+    u0, tv = host_inputs(rank)
+    fields = torch.as_tensor(np.stack([initial_condition(b, N, amp=IC_AMP) for b in range(B)]), device=dev)
+    E.objective_RPO({"fields": fields, "T": torch.full((B,), 0.05, dtype=torch.float64), "sx": 0.1}, pda, "Lawson_RK43")
+    prim = {"fields": torch.as_tensor(u0, device=dev), "T": 0.05, "sx": SX0}
+    tan = {"fields": torch.as_tensor(tv[:, 1:-1].reshape(BATCH, 2, N, N), device=dev).contiguous(),
+           "T": torch.as_tensor(tv[:, 0]), "sx": torch.as_tensor(tv[:, -1])}
+    obj = E.Objective(pda, "Lawson_RK43")
+    obj.linearize_jvp(prim, tan)
+    _, jacT = E.vjp(obj, prim)
+    jacT(tan)
+    x = torch.as_tensor(tv[0], device=dev)
+    linalg.gmres(lambda v: v * 1.5 + 0.1 * torch.roll(v, 1), x, 8)
+    pds = [E.make_param_dict(N, 1 / RE, 1 / RE, forcing="kolmogorov+", num_checkpoints=2, ministeps=8,
+                             shift_reflect_ny=0, rot=False) for _ in range(16)]
+    prims = [{"fields": fields[b], "T": 0.03, "sx": 0.1} for b in range(16)]
+    tans = [{"fields": tan["fields"][b], "T": 0.1, "sx": 0.2} for b in range(16)]
+    E.jvp_multi(prims, tans, pds)
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": "kernels", "seconds": time.perf_counter() - t0}), flush=True)
+
+
+def tangent_kernel_bytes(K, M, Bg, n=N, w=8):
+    """Algorithmic bytes of one launch of the tangent row and column passes for a
+    group of Bg tangents in the box layout (n=128 FP64: K=43, M=85): the row
+    pass reads G (4 fields of K x n complex) and writes H (3 fields) per
+    tangent and reads the shared primal fields (4 real n x n); the column pass
+    reads H, writes G and reads/writes two box vectors of 2 K M complex per
+    tangent, plus one shared record vector."""
+    cb = 2 * w
+    vec = 2 * K * M
+    row = Bg * (4 + 3) * K * n * cb + n * 4 * n * w
+    col = Bg * (3 * K * n * cb + 4 * K * n * cb + 2 * vec * cb) + vec * cb
+    return row, col
+
+
+# bytes of one tangent right-hand side of one tangent in the full-spectrum HBM
+# model: 2 x B_rhs, B_rhs = 2 S + 4 Nr w with S = 4 Ns w (n=128 FP64: 1,056,768 B)
+def tangent_rhs_model_bytes(n=N, w=8):
+    ns, nr = n * (n // 2 + 1), n * n
+    return 2 * (2 * 4 * ns * w + 4 * nr * w)
+
+
+def kernel_roofline(E, torch, ctx, obj, prim, tan, flush, info):
+    """Roofline row of the dominant tangent kernel, from one instrumented step."""
+    import ctypes
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured (MEASURED_PEAKS.json hbm_gbs, copy)" if "hbm_gbs" in peaks else "fallback"
+    flush.zero_()
+    torch.cuda.synchronize()
+    ctx.call("ecs_kernel_timing", 1, None, None, None, None, None)
+    obj.linearize_jvp(prim, tan)
+    torch.cuda.synchronize()
+    rms, rn, cms, cn, bg = ctypes.c_double(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    ctx.call("ecs_kernel_timing", 0, ctypes.byref(rms), ctypes.byref(rn), ctypes.byref(cms), ctypes.byref(cn),
+               ctypes.byref(bg))
+    Bg = bg.value
+    rb, cbytes = tangent_kernel_bytes(ctx.K, ctx.M, Bg)
+    kern = {"k_row_tan": {"ms_per_launch": rms.value, "launches": rn.value, "bytes_per_launch": rb},
+            "k_col_tan": {"ms_per_launch": cms.value, "launches": cn.value, "bytes_per_launch": cbytes}}
+    for k in kern.values():
+        k["GBps"] = k["bytes_per_launch"] / (k["ms_per_launch"] / 1e3) / 1e9 if k["ms_per_launch"] > 0 else None
+        k["frac"] = k["GBps"] / hbm_peak if k["GBps"] else None
+        k["total_ms"] = k["ms_per_launch"] * k["launches"]
+    dom_name = max(kern, key=lambda k: kern[k]["total_ms"])
+    dom = kern[dom_name]
+    traffic, traffic_src = None, None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            t = json.load(open(tfile))[dom_name]
+            traffic = t["fixed_bytes"] + t["bytes_per_tangent"] * Bg
+            traffic_src = t["source"]
+        except Exception:
+            traffic = None
+    pair_ms = rms.value + cms.value
+    model = Bg * tangent_rhs_model_bytes()
+    return {"bound": "hbm", "kernel": dom_name, "achieved": dom["GBps"], "peak": hbm_peak, "unit": "GB/s",
+            "frac": dom["frac"], "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_src,
+            "algorithmic_bytes_per_launch": dom["bytes_per_launch"], "ms_per_launch": dom["ms_per_launch"],
+            "how": "CUDA events around tangent group 0's launches in one instrumented step "
+                   f"(group of {Bg} tangents; the other groups run beside it); bytes: box layout",
+            "group_batch": Bg, "kernels": kern,
+            "tangent_rhs_model": {"bytes_per_pair": model, "pair_ms": pair_ms,
+                                  "GBps": model / (pair_ms / 1e3) / 1e9 if pair_ms > 0 else None,
+                                  "frac": (model / (pair_ms / 1e3) / 1e9) / hbm_peak if pair_ms > 0 else None,
+                                  "what": "one row + one column launch = one tangent RHS per tangent; "
+                                          "bytes = group x 2 x B_rhs of the full-spectrum HBM model"}}
 
 
 def main():
@@ -369,8 +578,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the config 0/2/3 side measurements")
-    ap.add_argument("--workload", default="matvec", choices=["matvec", "serving"],
-                    help="matvec: the headline 128^2 matvec batch; serving: 512 mixed Poisson requests")
+    ap.add_argument("--workload", default="matvec", choices=["matvec", "serving", "kernels"],
+                    help="matvec: the headline 128^2 matvec batch; serving: 512 mixed Poisson requests; "
+                         "kernels: one short pass over every hot kernel family (profiling case)")
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--T", type=float, default=None, help="profiling only: shorter horizon (small ncu case)")
@@ -391,6 +601,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args, rank, local, world)
+        return
+    if args.workload == "kernels":
+        run_kernels(rank, local)
         return
 
     import torch
@@ -485,39 +698,11 @@ def main():
     phase_ms = {"linearize": _ev_ms(lambda: obj.linearize(prim, force=True, batch=BATCH)),
                 "jvp": _ev_ms(lambda: obj.jvp(prim, tan))}
 
-    # roofline of the dominant kernel, timed live on this stream
-    step()
-    torch.cuda.synchronize()
-    import ctypes
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    kern = []
-    for which, name in ((0, "k_row_tan"), (1, "k_col_tan")):
-        ms, by = ctypes.c_float(), ctypes.c_double()
-        ctx.call("ecs_bench_kernel", which, BATCH, 20, ctypes.byref(ms), ctypes.byref(by), C.stream_ptr())
-        kern.append((name, ms.value, by.value))
-    acc = info.get("accepted", 0)
-    # launches per step: 4 row + 5 column tangent kernels per accepted attempt
-    shares = {name: ms * (4 if name == "k_row_tan" else 5) * acc for name, ms, _ in kern}
-    dom = max(kern, key=lambda k: shares[k[0]])
-    achieved = dom[2] / (dom[1] / 1e3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(dom[0])
-        except Exception:
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": dom[2], "ms_per_launch": dom[1],
-                "kernel_ms": {k[0]: k[1] for k in kern},
-                "share_of_step_est": {k: v / ms_per_step for k, v in shares.items()}}
+    # roofline of the dominant kernel in the step's own launch shape: one more
+    # (untimed) step with CUDA events around tangent group 0's row-pass and
+    # column-pass launches of every accepted attempt, on that group's stream
+    # (the other groups run beside it, as in the timed steps)
+    roofline = kernel_roofline(E, torch, ctx, obj, prim, tan, flush, info)
 
     # secondary: Lawson-RK4 state-steps/s at 128^2 FP64 (batch 64 and a single state)
     def rk4_rate(B, S=64):
@@ -540,6 +725,7 @@ def main():
         secondary["config1_plain_vs_batched"] = plain_vs_batched(E, torch, dev, flush, prim, tan)
         secondary["tdrk4_matvec_n128_f64"] = tdrk4_matvecs(E, torch, dev, flush, prim, tan)
         secondary["dns_generation_n128_f64"] = dns_generation(E, torch, dev, flush)
+        secondary["serving_poisson_512"] = serving_workload(args.requests, args.rate, seed=rank)
 
     if rank == 0:
         clocks = clk.summary()
@@ -554,17 +740,19 @@ def main():
                     secondary["dns_generation_n128_f64"]["cpu_baseline"] = cpu_baseline_dns()
                 except Exception as ex:
                     secondary["dns_generation_n128_f64"]["cpu_baseline"] = {"value": None, "sample": f"failed: {ex}"}
-        extra = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
-                 "tangent_rk_steps_per_s": value * info.get("accepted", 0),
-                 "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1},
-                 "phase_ms": phase_ms,
-                 "secondary": secondary}
+        details = {"adaptive_info": info, "rk_attempts_per_matvec": info.get("accepted", 0) + info.get("rejected", 0),
+                   "tangent_rk_steps_per_s": value * info.get("accepted", 0),
+                   "lawson_rk4_state_steps_per_s": {"batch64": rk4_b64, "batch1": rk4_b1},
+                   "phase_ms": phase_ms, "secondary": secondary}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial condition and tangents)",
-                "config": workload_config(extra),
+                "config": workload_config(),
+                "step": {"matvecs": BATCH, "what": "one jax.jvp of objective_RPO with a batch of 64 tangents "
+                                                   "(primal solve + 64 tangents, overlapped)"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline, "cpu_baseline": cb}
+                "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline, "cpu_baseline": cb,
+                "details": details}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -9,8 +9,13 @@ their own grid n, horizon (steps), Reynolds number, T, sx and state.
   (ecs_pool_*): every slot has its own step size and budget, finished slots are
   skipped, and new requests are admitted at step boundaries while the other
   slots keep running — continuous batching, not a queue.
-* Matvec and gradient requests run on worker threads, each with a private
-  context and CUDA stream, so several linearisations proceed concurrently.
+* Matvec requests in Lawson_RK4 mode go to their group's batcher: whatever
+  has queued while its previous sweep ran (up to its batch size) becomes the
+  next sweep, one forward-mode pass over all those candidates (ecs_jvp_multi:
+  each candidate with its own state, T, sx, horizon and tangent).
+* Gradient requests, and every request in adaptive Lawson_RK43 mode, run on
+  worker threads, each with a private context and CUDA stream, so several
+  linearisations proceed concurrently.
 * Admission is by HBM footprint: a request is admitted only while the
   estimated device memory of all live contexts and records stays within the
   budget; otherwise it waits.
@@ -31,8 +36,8 @@ import torch
 
 from . import _lib
 from . import context as C
-from .autodiff import Objective, loss_and_grad
-from .loss_functions import shoot_cfg
+from .autodiff import Objective, jvp_multi, loss_and_grad
+from .loss_functions import objective_RPO, shoot_cfg
 from .mhd import make_param_dict
 
 
@@ -49,6 +54,8 @@ class Request:
     tangent: np.ndarray = None  # matvec: flat [T, fields, sx] (host)
     arrival: float = 0.0       # seconds after the start of the run
     dtype: torch.dtype = torch.float64
+    mode: str = "Lawson_RK4"   # or "Lawson_RK43" (adaptive, tolerance atol; T as for the fixed-step horizon)
+    atol: float = 1e-6
 
 
 @dataclasses.dataclass
@@ -76,10 +83,15 @@ def _ckpt(req):
     return 0 if req.kind == "matvec" else _nc_ms(req.steps)[1]
 
 
+ADAPTIVE_CAP = (64, 64)   # checkpoints x max_steps_per_checkpoint of adaptive requests
+
+
 def _param_dict(req, dtype):
     nc, ms = _nc_ms(req.steps)
+    ad = {"atol": req.atol, "checkpoints": ADAPTIVE_CAP[0], "max_steps_per_checkpoint": ADAPTIVE_CAP[1]}
     return make_param_dict(req.n, 1.0 / req.Re, 1.0 / req.Re, forcing="kolmogorov+", data_type=dtype,
-                           num_checkpoints=nc, ministeps=ms, shift_reflect_ny=0, rot=False, ckpt_every=_ckpt(req))
+                           num_checkpoints=nc, ministeps=ms, shift_reflect_ny=0, rot=False, ckpt_every=_ckpt(req),
+                           adaptive_dict=ad)
 
 
 def context_bytes(n, dtype, batch):
@@ -93,13 +105,25 @@ def context_bytes(n, dtype, batch):
             + 10 * box * cb + (64 << 20))
 
 
-def record_bytes(n, dtype, steps, ckpt):
+def record_bytes(n, dtype, steps, ckpt, mode="Lawson_RK4"):
     K, M = (n - 1) // 3 + 1, 2 * ((n - 1) // 3) + 1
     cb = 16 if dtype == torch.float64 else 8
     vec = 2 * K * M * cb
-    seg = ckpt if ckpt else steps
     regen = 384 << 20
+    if mode == "Lawson_RK43":   # 11 record vectors per attempt up to the attempt cap
+        return ADAPTIVE_CAP[0] * ADAPTIVE_CAP[1] * 11 * vec + regen
+    seg = ckpt if ckpt else steps
     return seg * 8 * vec + (steps // max(seg, 1) + 1) * vec + regen
+
+
+def multi_bytes(n, dtype, batch):
+    """Device bytes of ecs_jvp_multi's buffers beyond the context workspace:
+    tangent G/H, one stage's physical fields, one step's record, phase fields,
+    tangent slots."""
+    K, M = (n - 1) // 3 + 1, 2 * ((n - 1) // 3) + 1
+    rb = 8 if dtype == torch.float64 else 4
+    cb = 2 * rb
+    return batch * (7 * K * n * cb + 4 * n * n * rb + 8 * 2 * K * M * cb + 4 * n * n * rb + 3 * 2 * K * M * cb)
 
 
 class ForwardPool:
@@ -197,13 +221,85 @@ class Worker(threading.Thread):
             self.busy = False
 
 
+class MatvecBatcher(threading.Thread):
+    """Lawson_RK4 matvec requests of one (n, dtype, Re) group: each sweep takes
+    every request queued so far (up to `batch`) and runs them as one
+    ecs_jvp_multi call on a private context and stream, so requests that arrive
+    during a sweep join the next one."""
+
+    def __init__(self, n, dtype, Re, results, now_fn, batch=16):
+        super().__init__(daemon=True)
+        self.n, self.dtype, self.Re, self.batch = n, dtype, Re, batch
+        self.inbox = queue.Queue()
+        self.results, self.now_fn = results, now_fn
+        self.queued = 0
+        self.bytes = context_bytes(n, dtype, batch) + multi_bytes(n, dtype, batch)
+        self.error = None
+        self.sweeps = []   # batch size of every sweep run
+
+    def run(self):
+        torch.cuda.set_device(0)
+        stream = torch.cuda.Stream()
+        pd0 = make_param_dict(self.n, 1.0 / self.Re, 1.0 / self.Re, forcing="kolmogorov+", data_type=self.dtype)
+        fk = C._forcing_key(pd0["forcing"])
+        ctx = C.Context(self.n, self.dtype, 1.0 / self.Re, 1.0 / self.Re, pd0["b0"], fk[1], max_batch=self.batch)
+        while True:
+            item = self.inbox.get()
+            if item is None:
+                break
+            items = [item]
+            while len(items) < self.batch:
+                try:
+                    nxt = self.inbox.get_nowait()
+                except queue.Empty:
+                    break
+                if nxt is None:
+                    self.inbox.put(None)
+                    break
+                items.append(nxt)
+            try:
+                outs = run_matvec_batch([r for r, _ in items], ctx, stream)
+                self.sweeps.append(len(items))
+                t = self.now_fn()
+                for (req, t_admit), out in zip(items, outs):
+                    self.results.put(Result(req.rid, req.kind, out, req.arrival, t_admit, t))
+            except Exception as ex:   # surfaced by Server.run
+                self.error = ex
+                self.results.put(None)
+            self.queued -= len(items)
+
+
+def run_matvec_batch(reqs, ctx, stream):
+    """Lawson_RK4 matvec requests of one group in one ecs_jvp_multi sweep."""
+    with torch.cuda.stream(stream):
+        prims, tans, pds = [], [], []
+        for req in reqs:
+            n = req.n
+            prims.append({"fields": torch.as_tensor(req.fields, dtype=req.dtype).to("cuda").contiguous(),
+                          "T": req.T, "sx": req.sx})
+            tv = req.tangent
+            tans.append({"fields": torch.as_tensor(tv[1:-1].reshape(2, n, n), dtype=req.dtype).to("cuda").contiguous(),
+                         "T": float(tv[0]), "sx": float(tv[-1])})
+            pds.append(_param_dict(req, req.dtype))
+        _, jv = jvp_multi(prims, tans, pds, "Lawson_RK4", ctx=ctx)
+        outs = [{"fields": j["fields"].clone(), "T": float(j["T"]), "sx": float(j["sx"])} for j in jv]
+        stream.synchronize()
+    return outs
+
+
 def run_adjoint_request(req, ctx, stream):
-    """One matvec or gradient request on context `ctx` and `stream`."""
+    """One request on a single-candidate context `ctx` and `stream`: a matvec
+    (JVP), a gradient (loss and its gradient by the adjoint), or, in adaptive
+    mode, a forward shooting."""
     pd = _param_dict(req, req.dtype)
     with torch.cuda.stream(stream):
         x = {"fields": torch.as_tensor(req.fields, dtype=req.dtype).to("cuda").contiguous(), "T": req.T, "sx": req.sx}
-        if req.kind == "matvec":
-            obj = Objective(pd, "Lawson_RK4", ctx=ctx)
+        if req.kind == "forward":   # loss_RPO = mean(irfft2(f - f0)^2) of the same residual
+            res = objective_RPO(x, pd, req.mode, ctx=ctx)["fields"]
+            loss = torch.sum(res.double() ** 2) / (2 * req.n * req.n)
+            out = {"fields": res.clone(), "loss": float(loss)}
+        elif req.kind == "matvec":
+            obj = Objective(pd, req.mode, ctx=ctx)
             n = req.n
             tv = req.tangent
             tan = {"fields": torch.as_tensor(tv[1:-1].reshape(2, n, n), dtype=req.dtype).to("cuda").contiguous(),
@@ -211,7 +307,7 @@ def run_adjoint_request(req, ctx, stream):
             _, o = obj.linearize_jvp(x, tan)
             out = {"fields": o["fields"].clone(), "T": float(o["T"]), "sx": float(o["sx"])}
         else:
-            (loss, info), g = loss_and_grad(x, pd, "Lawson_RK4", ctx=ctx)
+            (loss, info), g = loss_and_grad(x, pd, req.mode, ctx=ctx)
             out = {"loss": float(loss), "fields": g["fields"].clone(), "T": float(g["T"]), "sx": float(g["sx"])}
         stream.synchronize()
     return out
@@ -221,11 +317,11 @@ class Server:
     def __init__(self, hbm_budget=64 << 30, slots=16, chunk_steps=32, workers_per_group=4):
         self.budget, self.slots, self.chunk = hbm_budget, slots, chunk_steps
         self.workers_per_group = workers_per_group
-        self.pools, self.workers = {}, {}
+        self.pools, self.workers, self.batchers = {}, {}, {}
         self.results = queue.Queue()
 
     def _used(self):
-        return (sum(p.bytes for p in self.pools.values())
+        return (sum(p.bytes for p in self.pools.values()) + sum(b.bytes for b in self.batchers.values())
                 + sum(w.bytes + w.req_bytes for ws in self.workers.values() for w in ws))
 
     def run(self, requests, time_scale=1.0):
@@ -258,18 +354,34 @@ class Server:
                 except queue.Empty:
                     break
                 if res is None:
-                    raise RuntimeError([w.error for ws in self.workers.values() for w in ws if w.error])
+                    raise RuntimeError([w.error for ws in self.workers.values() for w in ws if w.error]
+                                       + [b.error for b in self.batchers.values() if b.error])
                 results[res.rid] = res
             if not any(p.active() for p in self.pools.values()) and len(results) < total:
                 time.sleep(0.0005)
         for ws in self.workers.values():
             for w in ws:
                 w.inbox.put(None)
+        for b in self.batchers.values():
+            b.inbox.put(None)
         return [results[k] for k in sorted(results)]
 
     def _admit(self, r, t):
         key = (r.n, r.dtype, r.Re)
-        if r.kind == "forward":
+        if r.kind == "matvec" and r.mode == "Lawson_RK4":
+            bt = self.batchers.get(key)
+            if bt is None:
+                need = context_bytes(r.n, r.dtype, self.slots) + multi_bytes(r.n, r.dtype, self.slots)
+                if self._used() + need > self.budget:
+                    return False
+                bt = self.batchers[key] = MatvecBatcher(r.n, r.dtype, r.Re, self.results, self._now, batch=self.slots)
+                bt.start()
+            if bt.queued >= 2 * bt.batch:   # bounded backlog: the rest waits for admission
+                return False
+            bt.queued += 1
+            bt.inbox.put((r, t))
+            return True
+        if r.kind == "forward" and r.mode == "Lawson_RK4":
             pool = self.pools.get(key)
             if pool is None:
                 need = context_bytes(r.n, r.dtype, self.slots)
@@ -282,7 +394,7 @@ class Server:
             return True
         ws = self.workers.setdefault(key, [])
         idle = [w for w in ws if not w.busy]
-        need = record_bytes(r.n, r.dtype, r.steps, _ckpt(r))
+        need = record_bytes(r.n, r.dtype, r.steps, _ckpt(r), r.mode)
         if not idle:
             if len(ws) >= self.workers_per_group:
                 return False
@@ -302,8 +414,12 @@ class Server:
 
 
 def poisson_requests(count, rate, seed=0, ns=(64, 128, 256), horizons=(256, 512, 1024, 2048), Res=(40.0, 50.0),
-                     kinds=("forward", "matvec", "gradient"), fp32_for_256=True):
-    """Seeded Poisson stream of mixed requests (the serving workload)."""
+                     kinds=("forward", "matvec", "gradient"), fp32_for_256=True, adaptive_fraction=0.25,
+                     adaptive_atol=1e-6):
+    """Seeded Poisson stream of mixed requests (the serving workload).  A
+    fraction of the FP64 requests (n < 256) runs the adaptive Lawson_RK43
+    stepper with tolerance `adaptive_atol`; the rest, and every FP32 request,
+    Lawson_RK4."""
     from .synthetic import initial_condition, unit_tangents
     rng = np.random.default_rng(seed)
     t, out = 0.0, []
@@ -318,5 +434,7 @@ def poisson_requests(count, rate, seed=0, ns=(64, 128, 256), horizons=(256, 512,
                       arrival=t, dtype=torch.float32 if (fp32_for_256 and n == 256) else torch.float64)
         if kind == "matvec":
             req.tangent = unit_tangents(int(rng.integers(1 << 30)), n, 1)[0]
+        if rng.uniform() < adaptive_fraction and req.dtype == torch.float64:
+            req.mode, req.atol = "Lawson_RK43", adaptive_atol
         out.append(req)
     return out

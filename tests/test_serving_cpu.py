@@ -26,6 +26,10 @@ def test_poisson_stream_is_seeded_and_mixed():
         assert (r.tangent is not None) == (r.kind == "matvec")
         if r.kind == "matvec":
             assert r.tangent.shape == (2 * r.n * r.n + 2,) and abs(np.linalg.norm(r.tangent) - 1) < 1e-12
+        assert r.mode in ("Lawson_RK4", "Lawson_RK43")
+        if r.mode == "Lawson_RK43":
+            assert r.dtype == torch.float64
+    assert {r.mode for r in a} == {"Lawson_RK4", "Lawson_RK43"}
 
 
 def test_checkpoint_segments():

@@ -1,7 +1,9 @@
 """Continuous-batching server: every request's result is the same alone and in
-the mix (bitwise for these deterministic kernels; the bound written is 1e-12),
-requests that arrive while others run are admitted into free slots, and the
-slot pool keeps serving requests of different horizons side by side."""
+the mix (the bound written is 1e-12: batched matvecs take the primal fields
+from another pass of the same arithmetic than a single-candidate call),
+requests that arrive while others run are admitted into free slots, the slot
+pool keeps serving requests of different horizons side by side, and matvec
+requests that queue up together are swept as one batch."""
 import numpy as np
 import pytest
 import torch
@@ -17,7 +19,7 @@ TOL = 1e-12
 def alone(req):
     pd = serving._param_dict(req, req.dtype)
     x = {"fields": torch.as_tensor(req.fields, dtype=req.dtype, device="cuda"), "T": req.T, "sx": req.sx}
-    if req.kind == "forward":
+    if req.kind == "forward" and req.mode == "Lawson_RK4":
         out = E.objective_RPO(x, pd, "Lawson_RK4")
         loss, _ = E.loss_RPO(x, pd, "Lawson_RK4")
         return {"fields": out["fields"], "loss": float(loss)}
@@ -28,7 +30,8 @@ def alone(req):
 
 def test_results_identical_alone_and_in_the_mix(cuda):
     reqs = serving.poisson_requests(14, rate=400.0, seed=3, ns=(64, 128), horizons=(64, 96, 160),
-                                    Res=(40.0, 50.0))
+                                    Res=(40.0, 50.0), adaptive_fraction=0.3)
+    assert {r.mode for r in reqs} == {"Lawson_RK4", "Lawson_RK43"}
     srv = serving.Server(hbm_budget=24 << 30, slots=4, chunk_steps=16, workers_per_group=2)
     res = srv.run(reqs)
     assert [r.rid for r in res] == list(range(len(reqs)))
@@ -64,3 +67,19 @@ def test_pool_mixes_horizons(cuda):
     assert [d.rid for d in done] == [1]
     a = alone(r1)
     assert rel_l2(done[0].out["fields"].cpu().numpy(), a["fields"].cpu().numpy()) <= TOL
+
+
+def test_matvec_burst_is_batched(cuda):
+    """Eight matvec requests of one group arriving together: the batcher sweeps
+    several of them in one ecs_jvp_multi call, and every result equals the
+    request run alone."""
+    reqs = serving.poisson_requests(8, rate=1e5, seed=11, ns=(64,), horizons=(64, 96, 128), Res=(40.0,),
+                                    kinds=("matvec",), adaptive_fraction=0.0)
+    srv = serving.Server(hbm_budget=16 << 30, slots=8, chunk_steps=16, workers_per_group=1)
+    res = srv.run(reqs)
+    sweeps = [b.sweeps for b in srv.batchers.values()]
+    assert len(sweeps) == 1 and sum(sweeps[0]) == 8 and max(sweeps[0]) > 1, sweeps
+    for req, r in zip(reqs, res):
+        a = alone(req)
+        assert rel_l2(r.out["fields"].cpu().numpy(), a["fields"].cpu().numpy()) <= TOL
+        assert abs(r.out["T"] - float(a["T"])) <= TOL * max(abs(float(a["T"])), 1e-30) + 1e-18
