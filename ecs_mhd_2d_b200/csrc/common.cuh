@@ -60,6 +60,19 @@ template <int D, typename R> __device__ __forceinline__ R div_k(R x) {
     return fma(r, inv, q0);
   }
 }
+// a sa + b sb with each product and the sum rounded on their own (never
+// contracted into an FMA), so that the same formula compiled into different
+// kernels gives the same bits.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+template <typename C, typename R> __device__ __forceinline__ C lin2_rn(C a, R sa, C b, R sb) {
+  C r;
+  r.x = add_rn(mul_rn(a.x, sa), mul_rn(b.x, sb));
+  r.y = add_rn(mul_rn(a.y, sa), mul_rn(b.y, sb));
+  return r;
+}
 template <int D, typename C> __device__ __forceinline__ C cdiv_k(C a) { a.x = div_k<D>(a.x); a.y = div_k<D>(a.y); return a; }
 
 template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_c(cplx<R> v, int m) {

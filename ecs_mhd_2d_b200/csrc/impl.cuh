@@ -210,8 +210,10 @@ void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_
 template <typename R, int N>
 void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* rec, const double* dT, double t,
                     double h, double dscale, int nslot, cudaStream_t s, const StepCtl* ctl = nullptr,
-                    long rec_bstride = 0, const double* dscale_b = nullptr, const R* etab = nullptr) {
-  ColTanParams<R> p{}; p.ctl = ctl; p.rec_bstride = rec_bstride; p.dscale_b = dscale_b; p.etab = etab; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
+                    long rec_bstride = 0, const double* dscale_b = nullptr, const R* etab = nullptr,
+                    const cplx<R>* rec2 = nullptr) {
+  ColTanParams<R> p{}; p.ctl = ctl; p.rec_bstride = rec_bstride; p.dscale_b = dscale_b; p.etab = etab;
+  p.rec2 = rec2; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D; p.nslot = nslot;
   p.rec = rec; p.dT = dT; p.t = t; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage; p.produce = produce;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
@@ -228,6 +230,7 @@ void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* re
     case T43_B: launch_step(c, B, k_col_tan<R, N, T43_B>, g, bl, 0, s, p); break;
     case T43_C: launch_step(c, B, k_col_tan<R, N, T43_C>, g, bl, 0, s, p); break;
     case T43_D: launch_step(c, B, k_col_tan<R, N, T43_D>, g, bl, 0, s, p); break;
+    case T43_EA: launch_step(c, B, k_col_tan<R, N, T43_EA>, g, bl, 0, s, p); break;
     default: launch_step(c, B, k_col_tan<R, N, T43_E>, g, bl, 0, s, p); break;
   }
 }
@@ -1050,18 +1053,26 @@ struct Impl {
       launch_col_tan<R, N>(c, B, T43_START, 1, rec, dT, t, 0.0, 1.0, nslot, s);
       launch_row_tan<R, N>(c, B, phys_of(0), s);
       launch_col_tan<R, N>(c, B, T43_INIT, 0, rec, dT, t, 0.0, 1.0, nslot, s);
+      bool a_started = false;   // the E pass of the previous attempt ran this one's A pass (T43_EA)
       for (long a = 0; a < L.nrec; ++a) {
         const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
         const double h = L.hs[a];
         if (!L.acc[a]) {
           ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, N, B);
+          a_started = false;
           continue;
         }
-        launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
+        if (!a_started) launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
+        const bool merge = a + 1 < L.nrec && L.acc[a + 1];
         for (int k = 0; k < 4; ++k) {
           launch_row_tan<R, N>(c, B, phys_of(item_of[a] + k), s);
-          launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
+          if (k == 3 && merge)
+            launch_col_tan<R, N>(c, B, T43_EA, 1, ra, dT, t, L.hs[a + 1], 1.0, nslot, s, nullptr, 0, nullptr, nullptr,
+                                 ra + (size_t)RR_NREC * VEC);
+          else
+            launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
         }
+        a_started = merge;
       }
     }
     return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
@@ -1312,24 +1323,37 @@ struct Impl {
         launch_row_tan<R, N>(c, Bg, phys(0), st);
         launch_col_tan<R, N>(c, Bg, T43_INIT, 0, rec, dTg, t, 0.0, 1.0, nslot, st);
       }
+      // The E column pass of an accepted attempt and the A column pass of the
+      // next one, when that one is accepted and in this chunk, run as one
+      // launch (T43_EA: the same arithmetic, in registers instead of slots).
+      bool a_started = false;
       for (long a = a_lo; a < a_hi; ++a) {
         const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
         const double h = hh[a - a_lo];
         if (!acc[a - a_lo]) {
           ++c->launches; k_tan_reject<R><<<grid1d((long)Bg * VEC), 256, 0, st>>>((cplx<R>*)c->D, nslot, ra, dTg, 1.0, N, Bg);
+          a_started = false;
           continue;
         }
         const bool kt = g == 0 && c->kt.on;
-        if (kt) kt_begin(c, st);
-        launch_col_tan<R, N>(c, Bg, T43_A, 1, ra, dTg, t, h, 1.0, nslot, st);
-        if (kt) kt_end(c, 1, Bg, st);
+        if (!a_started) {
+          if (kt) kt_begin(c, st);
+          launch_col_tan<R, N>(c, Bg, T43_A, 1, ra, dTg, t, h, 1.0, nslot, st);
+          if (kt) kt_end(c, 1, Bg, st);
+        }
+        const bool merge = a + 1 < a_hi && acc[a + 1 - a_lo];
         for (int k = 0; k < 4; ++k) {
           if (kt) kt_begin(c, st);
           launch_row_tan<R, N>(c, Bg, phys(item_of[a - a_lo] + k), st);
           if (kt) { kt_end(c, 0, Bg, st); kt_begin(c, st); }
-          launch_col_tan<R, N>(c, Bg, T43_B + k, 1, ra, dTg, t, h, 1.0, nslot, st);
+          if (k == 3 && merge)
+            launch_col_tan<R, N>(c, Bg, T43_EA, 1, ra, dTg, t, hh[a + 1 - a_lo], 1.0, nslot, st, nullptr, 0, nullptr,
+                                 nullptr, ra + (size_t)RR_NREC * VEC);
+          else
+            launch_col_tan<R, N>(c, Bg, T43_B + k, 1, ra, dTg, t, h, 1.0, nslot, st);
           if (kt) kt_end(c, 1, Bg, st);
         }
+        a_started = merge;
       }
       c->G = G0; c->H = H0; c->D = D0;
     };

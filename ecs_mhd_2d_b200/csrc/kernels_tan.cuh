@@ -171,6 +171,7 @@ enum TanStage : int {
   T4_S1 = 1, T4_S2, T4_S3, T4_S4,   // Lawson-RK4 stages
   T43_INIT = 10, T43_A, T43_B, T43_C, T43_D, T43_E,   // Lawson-RK4(3) stages
   T43_START = 16,                // inverse transforms of dX0 (before T43_INIT)
+  T43_EA = 17,                   // T43_E of an attempt, then T43_A of the next (accepted) attempt, one launch
 };
 // Tangent slots (Lawson-RK4 uses the first three).
 enum TanSlot { D_F = 0, D_A1, D_K2, D_NS4 = 3 };
@@ -196,6 +197,7 @@ struct ColTanParams {
   long rec_bstride;
   const double* dscale_b;
   const R* etab;
+  const cplx<R>* rec2;  // T43_EA: the next attempt's record (h is the next attempt's step)
 };
 
 // Record vectors (bits of Rk43Rec) and tangent slots (bits of Rk43Slot) that the
@@ -207,7 +209,11 @@ __host__ __device__ constexpr unsigned tan_qmask(int stage) {
        : stage == T43_B ? (1u << RR_K2)
        : stage == T43_C ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_K2) | (1u << RR_K3) | (1u << RR_E)
        : stage == T43_D ? (1u << RR_K4)
-       : stage == T43_E ? (1u << RR_K5) : 0u;
+       : stage == T43_E || stage == T43_EA ? (1u << RR_K5) : 0u;
+}
+// Record vectors of the next attempt read by T43_EA (from rec2).
+__host__ __device__ constexpr unsigned tan_qmask2(int stage) {
+  return stage == T43_EA ? (1u << RR_X0) | (1u << RR_K1) | (1u << RR_E) : 0u;
 }
 __host__ __device__ constexpr unsigned tan_dmask(int stage) {
   return stage == T43_START ? (1u << S_X0)
@@ -215,7 +221,7 @@ __host__ __device__ constexpr unsigned tan_dmask(int stage) {
        : stage == T43_B ? (1u << S_XE)
        : stage == T43_C ? (1u << S_XE) | (1u << S_K1E) | (1u << S_K2)
        : stage == T43_D ? (1u << S_K1) | (1u << S_K2) | (1u << S_K3) | (1u << S_X2)
-       : stage == T43_E ? (1u << S_XF) : 0u;
+       : stage == T43_E || stage == T43_EA ? (1u << S_XF) : 0u;
 }
 __host__ __device__ constexpr int popc_c(unsigned m) { return m ? (int)(m & 1u) + popc_c(m >> 1) : 0; }
 
@@ -245,7 +251,9 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   // cp.async before the forward transform, so that their latency overlaps it
   // without holding registers (adaptive stages, n <= 128: static shared memory).
   constexpr unsigned QM = N <= 128 ? tan_qmask(STAGE) : 0u, DM = N <= 128 ? tan_dmask(STAGE) : 0u;
-  constexpr int NQ = popc_c(QM), NOP = NQ + popc_c(DM);
+  constexpr unsigned QM2 = N <= 128 ? tan_qmask2(STAGE) : 0u;
+  constexpr int NQ = popc_c(QM), NQ2 = popc_c(QM2), NOP = NQ + NQ2 + popc_c(DM);
+  const cplx<R>* Q2 = p.rec2;
   __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
   cplx<R>* my_op = s_op + (threadIdx.x >> 5) * NOP * M;
   if constexpr (NOP > 0) {
@@ -255,6 +263,13 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
     for (int bit = 0; bit < 16; ++bit) {
       if ((QM >> bit) & 1u) {
         for (int s2 = lane; s2 < M; s2 += 32) cp_async_c<R>(my_op + v * M + s2, Q + bit * VEC + row + s2);
+        ++v;
+      }
+    }
+#pragma unroll
+    for (int bit = 0; bit < 16; ++bit) {
+      if ((QM2 >> bit) & 1u) {
+        for (int s2 = lane; s2 < M; s2 += 32) cp_async_c<R>(my_op + v * M + s2, Q2 + bit * VEC + row + s2);
         ++v;
       }
     }
@@ -330,22 +345,32 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
       };
       // (e, e L h/2) of this attempt from the primal record (stages A and C use them)
       const cplx<R> eg = (STAGE == T43_A || STAGE == T43_C) ? QV(RR_E) : mk<R>(0, 0);
-      const R e = eg.x;
-      const R de = eg.y * dpar;
+      [[maybe_unused]] const R e = eg.x;
+      [[maybe_unused]] const R de = eg.y * dpar;
+      auto Q2V = [&](int q) -> cplx<R> {
+        if constexpr (NOP > 0) return my_op[(NQ + popc_c(QM2 & ((1u << q) - 1u))) * M + slot];
+        else return Q2[q * VEC + o];
+      };
       auto DV = [&](int d) -> cplx<R> {
-        if constexpr (NOP > 0) return my_op[(NQ + popc_c(DM & ((1u << d) - 1u))) * M + slot];
+        if constexpr (NOP > 0) return my_op[(NQ + NQ2 + popc_c(DM & ((1u << d) - 1u))) * M + slot];
         else return D[d * VEC + o];
       };
       auto dk_of = [&](int q) { return cadd(cscale(QV(q), dpar / t), cscale(dv, t)); };
+      // the A and E algebra, written with explicitly rounded operations: the
+      // merged pass T43_EA computes exactly what T43_E followed by T43_A does
+      auto stage_e = [&]() { return lin2_rn(QV(RR_K5), dpar / t, dv, t); };   // dk5
+      auto stage_a = [&](cplx<R> x0, cplx<R> k1, cplx<R> eg_, cplx<R> dx0, cplx<R> dk1, R h_) {
+        const R e_ = eg_.x, de_ = mul_rn(eg_.y, dpar);
+        const cplx<R> dxe = lin2_rn(x0, de_, dx0, e_), dk1e = lin2_rn(k1, de_, dk1, e_);
+        D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
+        cplx<R> half = cscale(dk1e, h_);
+        half.x = mul_rn(half.x, R(0.5)); half.y = mul_rn(half.y, R(0.5));
+        return mk<R>(add_rn(dxe.x, half.x), add_rn(dxe.y, half.y));
+      };
       switch (STAGE) {
         case T43_START: xin = DV(S_X0); break;
         case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
-        case T43_A: {
-          const cplx<R> dxe = cadd(cscale(QV(RR_X0), de), cscale(DV(S_X0), e));
-          const cplx<R> dk1e = cadd(cscale(QV(RR_K1), de), cscale(DV(S_K1), e));
-          D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
-          xin = cadd(dxe, cscale(cscale(dk1e, h), R(0.5)));
-        } break;
+        case T43_A: xin = stage_a(QV(RR_X0), QV(RR_K1), eg, DV(S_X0), DV(S_K1), h); break;
         case T43_B: {
           const cplx<R> dk2 = dk_of(RR_K2);
           D[S_K2 * VEC + o] = dk2;
@@ -368,9 +393,15 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
           xin = cadd(DV(S_X2), cscale(acc, h));
           D[S_XF * VEC + o] = xin;
         } break;
-        default: {   // T43_E: accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
-          D[S_K1 * VEC + o] = dk_of(RR_K5);
+        case T43_E: {   // accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
+          D[S_K1 * VEC + o] = stage_e();
           D[S_X0 * VEC + o] = DV(S_XF);
+        } break;
+        default: {      // T43_EA: T43_E, then T43_A of the next attempt on the promoted values
+          const cplx<R> dk1 = stage_e(), dx0 = DV(S_XF);
+          D[S_K1 * VEC + o] = dk1;
+          D[S_X0 * VEC + o] = dx0;
+          xin = stage_a(Q2V(RR_X0), Q2V(RR_K1), Q2V(RR_E), dx0, dk1, h);
         } break;
       }
     }
