@@ -9,6 +9,7 @@
 #include "kernels_tan.cuh"
 #include "kernels_adj.cuh"
 #include "kernels_fx.cuh"
+#include "kernels_fxl.cuh"
 #include "api_internal.cuh"
 #include "impl_table.h"
 
@@ -310,6 +311,43 @@ void launch_col_tdj(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* re
   p.nslot = nslot; p.rec = rec; p.dT = dT; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.produce = produce;
   launch_col_tdj_sw<R, N>(c, B, stage, s, p, std::make_integer_sequence<int, 5>{});
+}
+
+template <typename R, int N, int SCHEME, int... ST>
+void launch_col_fxt_sw(ecs_ctx* c, int B, int stage, cudaStream_t s, const ColFxtParams<R>& p,
+                       std::integer_sequence<int, ST...>) {
+  const int cols = B * Geomc<N>::K * 2;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ((stage == ST ? launch_step(c, B, k_col_fxt<R, N, SCHEME, ST>, g, bl, 0, s, p) : void()), ...);
+}
+
+// Tangent column pass of the RK4 / Lawson-RK6 linearisation (kernels_fxl.cuh).
+template <typename R, int N>
+void launch_col_fxt(ecs_ctx* c, int B, int scheme, int stage, int produce, const cplx<R>* rec, const double* dT,
+                    double h, double dscale, cudaStream_t s) {
+  ColFxtParams<R> p{}; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.D = (cplx<R>*)c->D;
+  p.nslot = fxt_nslot(scheme); p.rec = rec; p.dT = dT; p.h = h; p.dscale = dscale; p.tw = (const cplx<R>*)c->tw;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.produce = produce;
+  if (scheme == FX_RK6) launch_col_fxt_sw<R, N, FX_RK6>(c, B, stage, s, p, std::make_integer_sequence<int, 9>{});
+  else launch_col_fxt_sw<R, N, FX_RK4>(c, B, stage, s, p, std::make_integer_sequence<int, 5>{});
+}
+
+template <typename R, int N, int SCHEME, int... ST>
+void launch_col_fxa_sw(ecs_ctx* c, int B, int stage, cudaStream_t s, const ColFxaParams<R>& p,
+                       std::integer_sequence<int, ST...>) {
+  const int cols = B * Geomc<N>::K * 2;
+  const dim3 g((cols + COLWARPS - 1) / COLWARPS), bl(COLWARPS * 32);
+  ((stage == ST ? launch_step(c, B, k_col_fxa<R, N, SCHEME, ST>, g, bl, 0, s, p) : void()), ...);
+}
+
+// Adjoint column pass of the RK4 / Lawson-RK6 linearisation; stage S + 1 seeds a step.
+template <typename R, int N>
+void launch_col_fxa(ecs_ctx* c, int B, int scheme, int stage, const cplx<R>* rec, double h, cudaStream_t s) {
+  ColFxaParams<R> p{}; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.J = (cplx<R>*)c->D;
+  p.nslot = fxa_nslot(scheme); p.rec = rec; p.hacc = c->hacc; p.h = h; p.tw = (const cplx<R>*)c->tw;
+  p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B;
+  if (scheme == FX_RK6) launch_col_fxa_sw<R, N, FX_RK6>(c, B, stage, s, p, std::make_integer_sequence<int, 10>{});
+  else launch_col_fxa_sw<R, N, FX_RK4>(c, B, stage, s, p, std::make_integer_sequence<int, 6>{});
 }
 
 inline int grid1d(long total, int threads = 256) {
@@ -853,13 +891,138 @@ struct Impl {
     return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
   }
 
+  // ---------------------------------------------------------------------
+  // Classic RK4 and Lawson-RK6 (kernels_fxl.cuh): linearisation = the batch-1
+  // forward solve with a record per step [f0, k_1..k_S, x_2..x_S]; the JVP
+  // sweep runs the tangent stages forward over it, the VJP sweep the adjoint
+  // stages backward, both with the primal physical fields of every stage input
+  // regenerated in chunks from the record and shared by the batch.
+  // ---------------------------------------------------------------------
+  static bool fxl_mode(int mode) { return mode == ECS_MODE_RK4 || mode == ECS_MODE_LAWSON_RK6; }
+
+  static int linearize_fxl(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
+                           R* out_fields, ecs_info* info, cudaStream_t s) {
+    auto& L = c->lin;
+    const int scheme = fx_scheme(cfg->mode), S = fxl_stages(scheme), NR = fxr_n(scheme);
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    const long steps = (long)cfg->num_checkpoints * cfg->ministeps;
+    if (steps <= 0) return set_err(c, ECS_ERR_INVALID, "steps must be > 0");
+    int st = lin_prologue(c, cfg, fields, T, sx, s);
+    if (!st) st = grow(c, &L.rec, &L.rec_bytes, (size_t)steps * NR * vb);
+    if (st) return st;
+    PlainOrder plain_order(c);
+    cudaMemcpyAsync((cplx<R>*)c->S43 + X_F * VEC, L.f0box, vb, cudaMemcpyDeviceToDevice, s);
+    ++c->launches;
+    k_fx_setup<R><<<grid1d((long)VEC), 256, 0, s>>>(T, cfg->num_checkpoints, cfg->ministeps, 6, c->ctl, (R*)c->Etab, N,
+                                                    c->nu, c->eta, 1);
+    cplx<R>* rec = (cplx<R>*)L.rec;
+    launch_col_fx<R, N>(c, 1, scheme, 0, 1, s);
+    for (long it = 0; it < steps; ++it) {
+      cplx<R>* rs = rec + (size_t)it * NR * VEC;
+      for (int q = 1; q <= S; ++q) {
+        launch_row_rhs<R, N>(c, 1, s);
+        launch_col_fx<R, N>(c, 1, scheme, q, (q == S && it == steps - 1) ? 0 : 1, s, rs);
+      }
+    }
+    cudaMemcpyAsync(L.phi, (cplx<R>*)c->S43 + X_F * VEC, vb, cudaMemcpyDeviceToDevice, s);
+    L.seg = 0;
+    L.nrec = steps;
+    L.h = (double)(R)((L.T / (double)cfg->num_checkpoints) / (double)cfg->ministeps);
+    L.acc.clear(); L.hs.clear();
+    if (info) { info->completed = 1; info->s = 1.0; info->accepted = (int)steps; info->rejected = 0; info->fevals = (int)(S * steps); }
+    if (out_fields) {
+      st = residual(c, cfg, fields, (const cplx<R>*)L.phi, (const cplx<R>*)L.f0box, L.dsx, 1, out_fields, s, 1);
+      if (st) return st;
+    }
+    L.valid = 1;
+    return cuda_err(c, cudaGetLastError(), "linearize (RK4 / Lawson-RK6)");
+  }
+
+  // Regeneration plan of the fixed-step linearisation: per step, the S stage inputs.
+  static std::vector<long> fxl_items(int scheme, long steps) {
+    const int S = fxl_stages(scheme), NR = fxr_n(scheme);
+    std::vector<long> items;
+    items.reserve((size_t)(S * steps));
+    for (long it = 0; it < steps; ++it)
+      for (int q = 1; q <= S; ++q) items.push_back(it * NR + (q == 1 ? fxr_f() : fxr_x(scheme, q)));
+    return items;
+  }
+
+  static int jvp_fxl(ecs_ctx* c, const R* dfields, const double* dT, const double* dsx, R* out, double* odT,
+                     double* odsx, int B, cudaStream_t s) {
+    auto& L = c->lin;
+    const int scheme = fx_scheme(L.mode), S = fxl_stages(scheme), NR = fxr_n(scheme), nslot = fxt_nslot(scheme);
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
+    int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = ensure_regen(c);
+    if (st) return st;
+    launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)FT_F * VEC, B, 2, s, (long)nslot * VEC);
+    const long steps = L.nrec;
+    const std::vector<long> items = fxl_items(scheme, steps);
+    st = upload_items(c, items, s);
+    if (st) return st;
+    const long ci = (long)chunk_items();
+    long chunk_lo = -1;
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    auto phys_of = [&](long item) -> const R* {
+      if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+        chunk_lo = item;
+        const long cnt = std::min<long>(ci, (long)items.size() - item);
+        launch_regen<R, N>(c, rec, c->items + item, (int)cnt, s);
+      }
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
+    };
+    const double dscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
+    launch_col_fxt<R, N>(c, B, scheme, 0, 1, rec, dT, L.h, dscale, s);
+    for (long it = 0; it < steps; ++it) {
+      const cplx<R>* ra = rec + (size_t)it * NR * VEC;
+      for (int q = 1; q <= S; ++q) {
+        launch_row_tan<R, N>(c, B, phys_of(it * S + q - 1), s);
+        launch_col_fxt<R, N>(c, B, scheme, q, (q == S && it == steps - 1) ? 0 : 1, ra, dT, L.h, dscale, s);
+      }
+    }
+    return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
+  }
+
+  static int vjp_fxl_sweep(ecs_ctx* c, int B, cudaStream_t s) {
+    auto& L = c->lin;
+    const int scheme = fx_scheme(L.mode), S = fxl_stages(scheme), NR = fxr_n(scheme);
+    const size_t VEC = 2UL * K * M;
+    const long steps = L.nrec;
+    const std::vector<long> items = fxl_items(scheme, steps);
+    int st = upload_items(c, items, s);
+    if (st) return st;
+    const long ci = (long)chunk_items();
+    long chunk_lo = -1;
+    const cplx<R>* rec = (const cplx<R>*)L.rec;
+    auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
+      if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+        chunk_lo = std::max<long>(0, item - ci + 1);
+        const long cnt = std::min<long>(ci, (long)items.size() - chunk_lo);
+        launch_regen<R, N>(c, rec, c->items + chunk_lo, (int)cnt, s);
+      }
+      return (const R*)c->Phys + (size_t)(item - chunk_lo) * N * NPH * N;
+    };
+    for (long it = steps - 1; it >= 0; --it) {
+      const cplx<R>* ra = rec + (size_t)it * NR * VEC;
+      launch_col_fxa<R, N>(c, B, scheme, S + 1, ra, L.h, s);
+      for (int q = S; q >= 1; --q) {
+        launch_row_adj<R, N>(c, B, phys_of(it * S + q - 1), s);
+        launch_col_fxa<R, N>(c, B, scheme, q, ra, L.h, s);
+      }
+    }
+    return cuda_err(c, cudaGetLastError(), "vjp (RK4 / Lawson-RK6)");
+  }
+
   static int linearize(ecs_ctx* c, const ecs_shoot_cfg* cfg, const R* fields, const double* T, const double* sx,
                        R* out_fields, ecs_info* info, cudaStream_t s) {
     auto& L = c->lin;
     const bool rk43 = cfg->mode == ECS_MODE_LAWSON_RK43;
     if (cfg->mode == ECS_MODE_TDRK4) return linearize_td(c, cfg, fields, T, sx, out_fields, info, s);
+    if (fxl_mode(cfg->mode)) return linearize_fxl(c, cfg, fields, T, sx, out_fields, info, s);
     if (cfg->mode != ECS_MODE_LAWSON_RK4 && !rk43)
-      return set_err(c, ECS_ERR_BAD_MODE, "linearisation (JVP/VJP) supports Lawson_RK4, Lawson_RK43 and TDRK4");
+      return set_err(c, ECS_ERR_BAD_MODE, "unknown mode");
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
     int st = lin_prologue(c, cfg, fields, T, sx, s);
     if (st) return st;
@@ -977,6 +1140,7 @@ struct Impl {
     auto& L = c->lin;
     if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
     if (L.mode == ECS_MODE_TDRK4) return jvp_td(c, dfields, dT, dsx, out, odT, odsx, B, s);
+    if (fxl_mode(L.mode)) return jvp_fxl(c, dfields, dT, dsx, out, odT, odsx, B, s);
     const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43;
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
     const int nslot = rk43 ? (int)S_NSLOT : (int)D_NS4;
@@ -1083,10 +1247,10 @@ struct Impl {
   static int jvp_finish(ecs_ctx* c, const R* dfields, const double* dsx, R* out, double* odT, double* odsx, int B,
                         cudaStream_t s) {
     auto& L = c->lin;
-    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4;
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4, fxl = fxl_mode(L.mode);
     const size_t VEC = 2UL * K * M;
-    const int nslot = rk43 ? (int)S_NSLOT : td ? (int)DT_NSLOT : (int)D_NS4;
-    const int fslot = rk43 ? (int)S_X0 : td ? (int)DT_F : (int)D_F;
+    const int nslot = rk43 ? (int)S_NSLOT : td ? (int)DT_NSLOT : fxl ? fxt_nslot(fx_scheme(L.mode)) : (int)D_NS4;
+    const int fslot = rk43 ? (int)S_X0 : td ? (int)DT_F : fxl ? (int)FT_F : (int)D_F;
     ++c->launches; k_tan_shift<R><<<grid1d((long)B * VEC), 256, 0, s>>>((const cplx<R>*)c->D + (size_t)fslot * VEC,
                                                          (long)nslot * VEC, (const cplx<R>*)L.phi, dsx,
                                                          (cplx<R>*)c->V, N, B);
@@ -1511,10 +1675,10 @@ struct Impl {
                  double* gsx, int B, cudaStream_t s) {
     auto& L = c->lin;
     if (!L.valid) return set_err(c, ECS_ERR_INVALID, "no linearisation: call ecs_linearize first");
-    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4;
+    const bool rk43 = L.mode == ECS_MODE_LAWSON_RK43, td = L.mode == ECS_MODE_TDRK4, fxl = fxl_mode(L.mode);
     const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>);
-    const int nslot = rk43 ? (int)JJ_NS43 : td ? (int)JT_NSLOT : (int)J_NS4;
-    const int fslot = rk43 ? (int)JJ_X0 : td ? (int)JT_F : (int)J_OB;   // cotangent of the final / initial state
+    const int nslot = rk43 ? (int)JJ_NS43 : td ? (int)JT_NSLOT : fxl ? fxa_nslot(fx_scheme(L.mode)) : (int)J_NS4;
+    const int fslot = rk43 ? (int)JJ_X0 : td ? (int)JT_F : fxl ? (int)FA_F : (int)J_OB;   // cotangent of the final / initial state
     int st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
     if (!st) st = ensure_regen(c);
     if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * 2 * sizeof(double));
@@ -1531,8 +1695,8 @@ struct Impl {
                                      (cplx<R>*)c->D + (size_t)fslot * VEC, (long)nslot * VEC,
                                      gsx, N);
     double tscale = 1.0;
-    if (td) {
-      st = vjp_td_sweep(c, B, nslot, s);
+    if (td || fxl) {
+      st = td ? vjp_td_sweep(c, B, nslot, s) : vjp_fxl_sweep(c, B, s);
       if (st) return st;
       tscale = 1.0 / ((double)L.cfg.num_checkpoints * (double)L.cfg.ministeps);
     } else {

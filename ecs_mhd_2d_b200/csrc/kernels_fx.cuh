@@ -35,7 +35,8 @@ struct ColFxParams {
   const cplx<R>* tw;
   R nu, eta;
   int B, produce;
-  cplx<R>* rec;         // TDRK4 linearisation (batch 1): record [TR_NREC][2][K][M] of this step, or null
+  cplx<R>* rec;         // linearisation (batch 1): record of this step, or null: TDRK4 [TR_NREC][2][K][M];
+                        // RK4 / Lawson-RK6 [f0, k_1..k_S, x_2..x_S] (see kernels_fxl.cuh)
 };
 
 template <int SCHEME, int STAGE> struct FxTraits {
@@ -91,9 +92,14 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
       if (STAGE == 3) xs = cadd(f, cdiv_k<2>(Q(X_K1 + 1)));
       if (STAGE == 4) xs = cadd(f, Q(X_K1 + 2));
       const cplx<R> k = cscale(cadd(v, cscale(xs, L)), h);            // timestepping.py:40-43
+      if (p.rec) {   // record: f0, k_s, x_{s+1}
+        if (STAGE == 1) p.rec[o] = f;
+        p.rec[STAGE * VEC + o] = k;
+      }
       if (STAGE < 4) {
         Q(X_K1 + STAGE - 1) = k;
         xin = STAGE < 3 ? cadd(f, cdiv_k<2>(k)) : cadd(f, k);
+        if (p.rec) p.rec[(4 + STAGE) * VEC + o] = xin;
       } else {
         const cplx<R> fn = cadd(cadd(cadd(cadd(f, cdiv_k<6>(Q(X_K1))), cdiv_k<3>(Q(X_K1 + 1))),
                                      cdiv_k<3>(Q(X_K1 + 2))), cdiv_k<6>(k));   // :44
@@ -108,6 +114,10 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
         Q(X_F) = cscale(Q(X_F), e);
         for (int s = 1; s <= upto; ++s) K_(s) = cscale(K_(s), e);
       };
+      if (p.rec) {   // record: f0, k_s (before any factor)
+        if (STAGE == 1) p.rec[o] = Q(X_F);
+        p.rec[STAGE * VEC + o] = k;
+      }
       switch (STAGE) {
         case 1:   // :110-112
           K_(1) = k; scale_all(1);
@@ -154,6 +164,7 @@ __global__ void __launch_bounds__(128) k_col_fx(ColFxParams<R> p) {
           xin = fn;
         } break;
       }
+      if (p.rec && STAGE < 8) p.rec[(8 + STAGE) * VEC + o] = xin;   // the stage input x_{s+1}
     } else {   // FX_TD4, timestepping.py:137-144; v_fn and its derivative include dissipation
       switch (STAGE) {
         case 1: {   // k1 = h v(f); next: the transforms of k1 (tangent input of jac(f, k1))

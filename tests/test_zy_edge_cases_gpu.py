@@ -95,8 +95,10 @@ def test_unsupported_grid_and_mode_are_status_errors(setup):
     with pytest.raises(_lib.EcsError) as ei:
         E.objective_RPO(x96, pd96, "Lawson_RK4")
     assert ei.value.code == 6                         # ECS_ERR_UNSUPPORTED
+    obj = autodiff.Objective(pd, "Lawson_RK4")
+    obj.cfg.mode = 42                                 # a mode code the library does not know
     with pytest.raises(_lib.EcsError) as ei:
-        autodiff.Objective(pd, "RK4").linearize(x)    # no tangent/adjoint kernels for classic RK4
+        obj.linearize(x)
     assert ei.value.code == 3                         # ECS_ERR_BAD_MODE
 
 
