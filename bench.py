@@ -416,13 +416,16 @@ def serving_workload(requests=512, rate=40.0, seed=0):
         lk = np.array([r.latency for r in res if r.kind == k])
         if lk.size:
             by[k] = {"count": int(lk.size), "p50_s": float(np.percentile(lk, 50)), "p99_s": float(np.percentile(lk, 99))}
-    sweeps = [x for bt in srv.batchers.values() for x in bt.sweeps]
+    sweeps = {}
+    for k in ("matvec", "gradient"):
+        sw = [x for bt in srv.batchers.values() if bt.kind == k for x in bt.sweeps]
+        sweeps[k] = {"sweeps": len(sw), "batch_mean": float(np.mean(sw)) if sw else None,
+                     "batch_max": max(sw) if sw else None}
     return {"requests": len(res), "wall_s": wall, "requests_per_s": len(res) / wall,
             "arrival_rate_per_s": rate, "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "by_kind": by,
             "adaptive_requests": sum(r.mode == "Lawson_RK43" for r in reqs),
-            "matvec_sweeps": len(sweeps), "matvec_batch_mean": float(np.mean(sweeps)) if sweeps else None,
-            "matvec_batch_max": max(sweeps) if sweeps else None, "slots_per_pool": 16, "workers_per_group": 4}
+            "batched_sweeps": sweeps, "slots_per_pool": 16, "workers_per_group": 4}
 
 
 def run_serving(args, rank, local, world):

@@ -11,6 +11,6 @@ from .timestepping import lawson_rk4, lawson_rk6, rk4, tdrk4, integrate  # noqa:
 from .loss_functions import objective_RPO, loss_RPO, dealias  # noqa: F401
 from .synthetic import initial_condition, unit_tangents  # noqa: F401
 from .autodiff import (Objective, compile_objective_and_Jacobian, vjp, loss_and_grad,  # noqa: F401
-                       loss_rpo_autograd, jvp_multi)
+                       loss_rpo_autograd, jvp_multi, loss_grad_multi)
 
 __version__ = "0.1.0"

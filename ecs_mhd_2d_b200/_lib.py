@@ -62,6 +62,7 @@ SIGNATURES = {
     "ecs_bench_kernel": (_I, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), _VP]),
     "ecs_jvp_multi": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I,
                            _VP]),
+    "ecs_loss_grad_multi": (_I, [_VP, ctypes.POINTER(EcsShootCfg), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
     "ecs_kernel_timing": (_I, [_VP, _I, ctypes.POINTER(_D), ctypes.POINTER(_I), ctypes.POINTER(_D),
                                ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ecs_box_dims": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

@@ -182,6 +182,47 @@ def jvp_multi(primals, tangents, param_dicts, mode="Lawson_RK4", ctx=None):
     return values, jvps
 
 
+def loss_grad_multi(inputs, param_dicts, mode="Lawson_RK4", ctx=None):
+    """loss_RPO and its gradient for several candidates in one device sweep:
+    [jax.value_and_grad(loss_RPO)(x_b) for each b] (jax_scripts/adjoint_descent.py:91,
+    loss_functions.py:99-111), batched across candidates (ecs_loss_grad_multi;
+    Lawson_RK4 only).  The param dicts share the grid, dtype and physics and may
+    differ in num_checkpoints, ministeps, shift_reflect_ny and rot.  Returns a
+    list of (loss, grad) with grad a {"fields", "T", "sx"} dict."""
+    if mode != "Lawson_RK4":
+        raise ValueError(f"loss_grad_multi runs Lawson_RK4, got {mode}")
+    if len(inputs) != len(param_dicts):
+        raise ValueError("loss_grad_multi: inputs and param_dicts differ in length")
+    B = len(inputs)
+    if B == 0:
+        return []
+    xs = [prep_inputs(x) for x in inputs]
+    n, dtype = xs[0][0].shape[-1], xs[0][0].dtype
+    for (f, _, _, _) in xs:
+        if f.shape != (1, 2, n, n) or f.dtype != dtype:
+            raise ValueError("loss_grad_multi: every input is one state of the same grid and dtype")
+    key = _ctx.physics_key(param_dicts[0])
+    if any(_ctx.physics_key(pd) != key for pd in param_dicts[1:]):
+        raise ValueError("loss_grad_multi: the candidates' param dicts differ in grid or physics")
+    cfgs = (_lib.EcsShootCfg * B)()
+    for b, pd in enumerate(param_dicts):
+        cfgs[b] = shoot_cfg(pd, mode)
+    if ctx is None:
+        ctx = _ctx.get_context(param_dicts[0], n, dtype, B)
+    else:
+        ctx.ensure_batch(B)
+    fields = torch.cat([x[0] for x in xs]).contiguous()
+    T = torch.cat([x[1] for x in xs]).contiguous()
+    sx = torch.cat([x[2] for x in xs]).contiguous()
+    loss = torch.empty(B, dtype=torch.float64, device=fields.device)
+    g = torch.empty_like(fields)
+    gT = torch.empty(B, dtype=torch.float64, device=fields.device)
+    gsx = torch.empty(B, dtype=torch.float64, device=fields.device)
+    ctx.call("ecs_loss_grad_multi", cfgs, _ctx.ptr(fields), _ctx.ptr(T), _ctx.ptr(sx), _ctx.ptr(loss), _ctx.ptr(g),
+             _ctx.ptr(gT), _ctx.ptr(gsx), B, _ctx.stream_ptr())
+    return [(loss[b], {"fields": g[b], "T": gT[b], "sx": gsx[b]}) for b in range(B)]
+
+
 def _as_objective(obj, param_dict):
     if isinstance(obj, Objective):
         return obj

@@ -128,6 +128,7 @@ static int ctx_destroy_locked(ecs_ctx* ctx) {
   if (ctx->tfork) cudaEventDestroy(ctx->tfork);
   for (cudaEvent_t e : ctx->kt.ev) cudaEventDestroy(e);
   if (ctx->mj.g.exec) cudaGraphExecDestroy(ctx->mj.g.exec);
+  for (void* p : {ctx->mj.ckpt, ctx->mj.grec, ctx->mj.gphys, ctx->mj.res}) if (p) cudaFree(p);
   if (ctx->Gp) cudaFree(ctx->Gp);
   if (ctx->Gx) cudaFree(ctx->Gx);
   if (ctx->Hp) cudaFree(ctx->Hp);
@@ -266,6 +267,15 @@ int ecs_jvp_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, c
     return set_err(ctx, ECS_ERR_INVALID, "null pointer");
   return table_of(ctx)->jvp_multi(ctx, cfgs, fields, T, sx, out_fields, dfields, dT, dsx, out_dfields, out_dT, out_dsx,
                                   batch, as_stream(stream));
+}
+
+int ecs_loss_grad_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, const double* T,
+                        const double* sx, double* loss, void* g_fields, double* g_T, double* g_sx, int batch,
+                        void* stream) {
+  ECS_CHECK_CTX(ctx, batch);
+  if (!cfgs || !fields || !T || !sx || !loss || !g_fields || !g_T || !g_sx)
+    return set_err(ctx, ECS_ERR_INVALID, "null pointer");
+  return table_of(ctx)->loss_grad_multi(ctx, cfgs, fields, T, sx, loss, g_fields, g_T, g_sx, batch, as_stream(stream));
 }
 
 namespace ecs {

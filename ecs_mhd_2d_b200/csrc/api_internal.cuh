@@ -112,6 +112,13 @@ struct ecs_ctx {
     void* vt = nullptr; void* vx = nullptr; double* dscale = nullptr; double* dT = nullptr;
     // the 8-step graph bakes in B and the tangent-slot buffer D (which grows)
     struct Graph { cudaGraphExec_t exec = nullptr; int B = 0; void* D = nullptr; long long nodes = 0; } g;
+    // several candidates' gradients (ecs_loss_grad_multi): segment start states,
+    // one segment's record and stage fields, residuals, per-candidate segment counts
+    void* ckpt = nullptr; size_t ckpt_bytes = 0;
+    void* grec = nullptr; size_t grec_bytes = 0;
+    void* gphys = nullptr; size_t gphys_bytes = 0;
+    void* res = nullptr; size_t res_bytes = 0;
+    int* nseg = nullptr;
   } mj;
   // in-step timing of the batched tangent kernels (ecs_kernel_timing): CUDA
   // events around tangent group 0's row-pass and column-pass launches inside

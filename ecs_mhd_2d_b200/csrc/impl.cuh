@@ -14,6 +14,7 @@
 #include "impl_table.h"
 
 #include <algorithm>
+#include <numeric>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -237,8 +238,10 @@ void launch_col_tan(ecs_ctx* c, int B, int stage, int produce, const cplx<R>* re
 }
 
 template <typename R, int N>
-void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
-  RowAdjParams<R> p; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_bstride = 0,
+                    const StepCtl* ctl = nullptr) {
+  RowAdjParams<R> p{}; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
+  p.phys_bstride = phys_bstride; p.ctl = ctl;
   p.B = B;
   if (small_rows<N>(B)) launch_step(c, B, k_row_adj<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
   else launch_step(c, B, k_row_adj<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
@@ -246,8 +249,8 @@ void launch_row_adj(ecs_ctx* c, int B, const R* phys, cudaStream_t s) {
 
 template <typename R, int N>
 void launch_col_adj(ecs_ctx* c, int B, int stage, const cplx<R>* rec, const cplx<R>* rec_prev, double t, double h,
-                    int nslot, cudaStream_t s) {
-  ColAdjParams<R> p; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.J = (cplx<R>*)c->D; p.nslot = nslot;
+                    int nslot, cudaStream_t s, const StepCtl* ctl = nullptr, long rec_bstride = 0) {
+  ColAdjParams<R> p{}; p.ctl = ctl; p.rec_bstride = rec_bstride; p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.J = (cplx<R>*)c->D; p.nslot = nslot;
   p.rec = rec; p.rec_prev = rec_prev; p.hacc = c->hacc; p.t = t; p.h = h; p.tw = (const cplx<R>*)c->tw;
   p.nu = (R)c->nu; p.eta = (R)c->eta; p.B = B; p.stage = stage;
   const int cols = B * Geomc<N>::K * 2;   // one warp per (batch, ky, channel)
@@ -2083,6 +2086,146 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "jvp_multi");
   }
 
+  // ---------------------------------------------------------------------
+  // Several candidates' loss_RPO and its gradient in one adjoint sweep
+  // (ecs_loss_grad_multi): B independent jax.value_and_grad(loss_RPO) calls
+  // (jax_scripts/adjoint_descent.py:91), Lawson_RK4.  The B forward solves step
+  // together (per-candidate h, symmetry and step budget in the control
+  // blocks), keeping each candidate's state every SEG steps (SEG divides every
+  // candidate's step count).  The reverse sweep is aligned at each candidate's
+  // end: in reverse segment r candidate b recomputes its segment
+  // nseg_b - 1 - r from its checkpoint (with the record and the stage fields
+  // of all SEG steps kept), then the adjoint passes sweep it backwards;
+  // candidates without such a segment are skipped.  Loss mean(out^2) over
+  // 2 n^2 entries, cotangent out / n^2 (loss_functions.py:99-111).
+  // ---------------------------------------------------------------------
+  static int loss_grad_multi(ecs_ctx* c, const ecs_shoot_cfg* cfgs, const R* fields, const double* T,
+                             const double* sx, double* loss, R* gfields, double* gT, double* gsx, int B,
+                             cudaStream_t s) {
+    const size_t VEC = 2UL * K * M, vb = VEC * sizeof(cplx<R>), fe = 2UL * N * N;
+    const long pstride = (long)N * NPH * N;
+    const int nslot = (int)J_NS4;
+    std::vector<long> steps(B);
+    std::vector<int> nseg(B);
+    long smax = 0, seg = 0;
+    for (int b = 0; b < B; ++b) {
+      if (cfgs[b].mode != ECS_MODE_LAWSON_RK4) return set_err(c, ECS_ERR_BAD_MODE, "ecs_loss_grad_multi runs Lawson_RK4");
+      steps[b] = (long)cfgs[b].num_checkpoints * cfgs[b].ministeps;
+      if (cfgs[b].num_checkpoints <= 0 || cfgs[b].ministeps <= 0 || steps[b] > (1L << 30))
+        return set_err(c, ECS_ERR_INVALID, "num_checkpoints and ministeps must be > 0");
+      smax = std::max(smax, steps[b]);
+      seg = std::gcd(seg, steps[b]);
+    }
+    seg = std::min(seg, 32L);
+    while (seg > 1) {   // SEG must divide every step count
+      bool ok = true;
+      for (int b = 0; b < B; ++b) ok = ok && steps[b] % seg == 0;
+      if (ok) break;
+      --seg;
+    }
+    for (int b = 0; b < B; ++b) nseg[b] = (int)(steps[b] / seg);
+    const long nsegmax = smax / seg;
+    int st = ensure_multi(c);
+    auto& m = c->mj;
+    if (!st) st = grow(c, &c->D, &c->D_bytes, (size_t)B * nslot * vb);
+    if (!st) st = grow(c, (void**)&c->hacc, &c->hacc_bytes, (size_t)B * K * 2 * sizeof(double));
+    if (!st) st = grow(c, &m.ckpt, &m.ckpt_bytes, (size_t)nsegmax * B * vb);
+    if (!st) st = grow(c, &m.grec, &m.grec_bytes, (size_t)B * seg * Q_NREC * vb);
+    if (!st) st = grow(c, &m.gphys, &m.gphys_bytes, (size_t)seg * 4 * B * pstride * sizeof(R));
+    if (!st) st = grow(c, &m.res, &m.res_bytes, (size_t)2 * B * fe * sizeof(R));
+    if (!st && !m.nseg) m.nseg = (int*)dev_alloc(c, (size_t)c->max_batch * sizeof(int), &st);
+    if (st) return st;
+    c->pool.clear();   // the control blocks are reused: a slot pool on this context starts over
+    cudaError_t e = cudaMemcpyAsync(m.nseg, nseg.data(), B * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_err(c, e, "loss_grad_multi segments");
+    cplx<R>* F = (cplx<R>*)c->F;
+    st = to_box(c, fields, F, B, s);
+    if (st) return st;
+    for (int b = 0; b < B; ++b) {
+      ++c->launches;
+      k_rk4_setup<R><<<grid1d((long)VEC), 256, 0, s>>>(T + b, cfgs[b].num_checkpoints, cfgs[b].ministeps, c->ctl + b,
+                                                       (R*)c->Etab + (size_t)b * VEC, N, c->nu, c->eta, 1);
+      ++c->launches; k_pool_init<<<1, 32, 0, s>>>(c->ctl, b, 1, (int)steps[b]);
+    }
+    // forward solves with a checkpoint every SEG steps (the loss has no phase-condition part)
+    cplx<R>* ckpt = (cplx<R>*)m.ckpt;
+    launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s, nullptr, 0, 1);
+    for (long it = 0; it < smax; ++it) {
+      if (it % seg == 0) {
+        e = cudaMemcpyAsync(ckpt + (size_t)(it / seg) * B * VEC, F, B * vb, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_err(c, e, "loss_grad_multi checkpoint");
+      }
+      for (int q = 1; q <= 4; ++q) {
+        launch_row_rhs<R, N>(c, B, s, c->ctl);
+        launch_col_rk4<R, N>(c, B, q, 1, 0, s, nullptr, 0, 1);
+      }
+      ++c->launches; k_pool_count<<<(B + 127) / 128, 128, 0, s>>>(c->ctl, B);
+    }
+    // residuals out_b = fields_b - irfft2(sym(shift(phi_b))), losses, cotangents out_b / n^2
+    R* res = (R*)m.res;
+    R* cot = res + (size_t)B * fe;
+    for (int b = 0; b < B; ++b) {
+      st = residual(c, &cfgs[b], fields + (size_t)b * fe, F + (size_t)b * VEC, nullptr, sx + b, 1, res + (size_t)b * fe,
+                    s, 1);
+      if (st) return st;
+      ++c->launches; k_rowsq<R><<<N, 32, 0, s>>>(res + (size_t)b * fe, c->rowsq, N);
+      ++c->launches; k_reduce_rows<<<1, 128, 0, s>>>(c->rowsq, loss + b, N, 1, 1.0 / (2.0 * N * N));
+    }
+    e = cudaMemsetAsync(cot, 0, B * fe * sizeof(R), s);   // cot = res / n^2 (exact: n^2 is a power of two)
+    if (e != cudaSuccess) return cuda_err(c, e, "loss_grad_multi cotangent");
+    ++c->launches; k_axpy<R><<<grid1d((long)B * fe), 256, 0, s>>>(cot, res, R(1) / (R(N) * R(N)), (long)B * fe);
+    // head: Ybar = -(c/n^2) rfft2(cot) on the box; Phibar = sym^T(Ybar) and sxbar per candidate
+    cudaMemsetAsync(c->D, 0, (size_t)B * nslot * vb, s);
+    cudaMemsetAsync(c->hacc, 0, (size_t)B * K * 2 * sizeof(double), s);
+    launch_row_to_box<R, N>(c, cot, (cplx<R>*)c->H, B, s);
+    launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->V, B, 2, s);
+    ++c->launches; k_box_scale_c<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->V, (long)VEC, N, B, R(-1) / (R(N) * R(N)));
+    for (int b = 0; b < B; ++b) {
+      const int odd = (cfgs[b].shift_reflect_ny % 2 + 2) % 2 == 1;
+      const double sy = (cfgs[b].shift_reflect_ny * 2 * M_PI) / 8;
+      ++c->launches;
+      k_adj_head<R><<<1, 256, 0, s>>>((const cplx<R>*)c->V + (size_t)b * VEC, (const cplx<R>*)F + (size_t)b * VEC,
+                                      sx + b, 1, sy, odd, cfgs[b].rot, (cplx<R>*)c->D + ((size_t)b * nslot + J_OB) * VEC,
+                                      (long)nslot * VEC, gsx + b, N);
+    }
+    // reverse segments
+    cplx<R>* grec = (cplx<R>*)m.grec;
+    R* gphys = (R*)m.gphys;
+    const long rstride = (long)seg * Q_NREC * VEC;
+    for (long r = 0; r < nsegmax; ++r) {
+      ++c->launches;
+      k_grad_segment<R><<<grid1d((long)B * VEC), 256, 0, s>>>(F, ckpt, m.nseg, (int)r, c->ctl, (long)VEC, B);
+      launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s, nullptr, 0, 1);
+      for (long it = 0; it < seg; ++it) {
+        for (int q = 1; q <= 4; ++q) {
+          launch_row_rhs<R, N>(c, B, s, c->ctl, gphys + (size_t)(it * 4 + q - 1) * B * pstride, pstride);
+          launch_col_rk4<R, N>(c, B, q, (q == 4 && it == seg - 1) ? 0 : 1, 0, s, grec + (size_t)it * Q_NREC * VEC,
+                               rstride, 1);
+        }
+      }
+      launch_col_adj<R, N>(c, B, AJ_PRE, grec + (size_t)(seg - 1) * Q_NREC * VEC, nullptr, 0.0, 0.0, nslot, s,
+                           c->ctl, rstride);
+      for (long it = seg - 1; it >= 0; --it) {
+        const cplx<R>* ra = grec + (size_t)it * Q_NREC * VEC;
+        const cplx<R>* rp = it > 0 ? grec + (size_t)(it - 1) * Q_NREC * VEC : nullptr;
+        for (int k = 4; k >= 1; --k) {
+          launch_row_adj<R, N>(c, B, gphys + (size_t)(it * 4 + k - 1) * B * pstride, s, pstride, c->ctl);
+          launch_col_adj<R, N>(c, B, k, ra, rp, 0.0, 0.0, nslot, s, c->ctl, rstride);
+        }
+      }
+    }
+    // tail per candidate: gfields = cot + to_box^T(fbar0) + phase terms; gT from the h accumulators
+    ++c->launches; k_box_to_fields_adj<R><<<grid1d((long)B * VEC), 256, 0, s>>>(
+        (const cplx<R>*)c->D + (size_t)J_OB * VEC, (long)nslot * VEC, (cplx<R>*)c->V, N, B);
+    launch_col_from_box<R, N>(c, (const cplx<R>*)c->V, (cplx<R>*)c->G, B, nullptr, 0, 0, 0, 0, s);
+    launch_row_from_box<R, N>(c, (const cplx<R>*)c->G, gfields, cot, nullptr, B, 2, s);
+    for (int b = 0; b < B; ++b) {
+      const double tscale = 1.0 / ((double)cfgs[b].num_checkpoints * (double)cfgs[b].ministeps);
+      ++c->launches; k_reduce_hacc<<<1, 128, 0, s>>>(c->hacc + (size_t)b * K * 2, K, tscale, gT + b, 1);
+    }
+    return cuda_err(c, cudaGetLastError(), "loss_grad_multi");
+  }
+
   // Time `iters` launches of one hot kernel on the current workspace (after a
   // jvp call) with CUDA events on stream s; returns ms per launch and the
   // kernel's algorithmic bytes per launch.
@@ -2227,6 +2370,9 @@ ImplTable make_table() {
                    const void* df, const double* dT, const double* dsx, void* od, double* oT, double* osx, int B,
                    cudaStream_t s) {
     return I::jvp_multi(c, cfgs, (const R*)f, T, sx, (R*)o, (const R*)df, dT, dsx, (R*)od, oT, osx, B, s); };
+  t.loss_grad_multi = [](ecs_ctx* c, const ecs_shoot_cfg* cfgs, const void* f, const double* T, const double* sx,
+                         double* loss, void* g, double* gT, double* gsx, int B, cudaStream_t s) {
+    return I::loss_grad_multi(c, cfgs, (const R*)f, T, sx, loss, (R*)g, gT, gsx, B, s); };
   t.pool_reset = [](ecs_ctx* c, cudaStream_t s) { return I::pool_reset(c, s); };
   t.pool_admit = [](ecs_ctx* c, int slot, const ecs_shoot_cfg* cfg, const void* f, double T, double sx,
                     cudaStream_t s) { return I::pool_admit(c, slot, cfg, (const R*)f, T, sx, s); };

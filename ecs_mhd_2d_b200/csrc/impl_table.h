@@ -29,6 +29,8 @@ struct ImplTable {
   int (*bench_kernel)(ecs_ctx*, int, int, int, float*, double*, cudaStream_t);
   int (*jvp_multi)(ecs_ctx*, const ecs_shoot_cfg*, const void*, const double*, const double*, void*, const void*,
                    const double*, const double*, void*, double*, double*, int, cudaStream_t);
+  int (*loss_grad_multi)(ecs_ctx*, const ecs_shoot_cfg*, const void*, const double*, const double*, double*, void*,
+                         double*, double*, int, cudaStream_t);
   int (*pool_reset)(ecs_ctx*, cudaStream_t);
   int (*pool_admit)(ecs_ctx*, int, const ecs_shoot_cfg*, const void*, double, double, cudaStream_t);
   int (*pool_advance)(ecs_ctx*, int, cudaStream_t);

@@ -31,7 +31,9 @@ template <typename R>
 struct RowAdjParams {
   const cplx<R>* G;     // [B][NG][K][N]: fields 0..2 hold the inverse columns of the P1, P2, P3 cotangents (/c_ky)
   cplx<R>* H;           // [B][NHA][K][N]: rfft2 rows of the 4 adjoint fields
-  const R* phys;        // primal physical fields of this stage [N][NPH][N]
+  const R* phys;        // primal physical fields of this stage: phys + b * phys_bstride is [N][NPH][N]
+  long phys_bstride;    // 0: one primal shared by the batch
+  const StepCtl* ctl;   // optional per-candidate control: batch elements whose ctl.done is set are skipped
   const cplx<R>* tw;
   int B;
 };
@@ -51,7 +53,8 @@ __global__ void __launch_bounds__(XT * 32) k_row_adj(RowAdjParams<R> p) {
   pdl_trigger();
   load_twiddles<R, N>(s_tw, p.tw);
   pdl_wait();
-  const R* ph = phys_row<R, N>(p.phys, x);
+  if (p.ctl && p.ctl[b].done) return;   // the whole CTA belongs to batch element b
+  const R* ph = phys_row<R, N>(p.phys + (size_t)b * p.phys_bstride, x);
   R pu[E], pv[E], pbx[E], pby[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
@@ -110,6 +113,10 @@ struct ColAdjParams {
   const cplx<R>* tw;
   R nu, eta;
   int B, stage;
+  // Several candidates (Lawson-RK4 stages): ctl[b] gives candidate b's step h
+  // and done flag (skipped once done); rec / rec_prev + b * rec_bstride its record.
+  const StepCtl* ctl;
+  long rec_bstride;
 };
 
 __device__ __forceinline__ double rdot2(double ax, double ay, double bx, double by) { return ax * bx + ay * by; }
@@ -128,9 +135,11 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
   const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (colid >= p.B * K * 2) return;
   const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
+  if (p.ctl && p.ctl[b].done) return;
   cplx<R>* J = p.J + (size_t)b * p.nslot * VEC;
-  const cplx<R>* Q = p.rec;
-  const R h = (R)p.h, t = (R)p.t;
+  const cplx<R>* Q = p.rec + (size_t)b * p.rec_bstride;
+  const cplx<R>* Qp = p.rec_prev ? p.rec_prev + (size_t)b * p.rec_bstride : nullptr;
+  const R h = p.ctl ? (R)p.ctl[b].h : (R)p.h, t = (R)p.t;
   constexpr bool rk43 = STAGE >= AJ43_INIT;
   constexpr bool has_rhs = !(STAGE == AJ_PRE || STAGE == AJ43_PRE || STAGE == AJ43_IPRE);
   const R cky = ky == 0 ? R(1) : R(2);
@@ -213,11 +222,11 @@ __global__ void __launch_bounds__(128) k_col_adj(ColAdjParams<R> p) {
         default: {   // AJ_S1: fbar += X1bar; then seed the previous step (if any)
           const cplx<R> fb = cadd(J[J_OB * VEC + o], Xb);
           J[J_OB * VEC + o] = fb;
-          if (p.rec_prev) {
+          if (Qp) {
             J[J_F2 * VEC + o] = fb; J[J_A1 * VEC + o] = cdiv_k<6>(fb);
             J[J_K2 * VEC + o] = cdiv_k<3>(fb); J[J_B3 * VEC + o] = cdiv_k<3>(fb);
             kb = cdiv_k<6>(fb);
-            hpart += ip(kb, p.rec_prev[Q_K4 * VEC + o]) / (double)h;
+            hpart += ip(kb, Qp[Q_K4 * VEC + o]) / (double)h;
           } else {
             feed = false;
           }
@@ -431,6 +440,22 @@ static __global__ void k_reduce_hacc(const double* hacc, int K, double scale, do
   double s = 0.0;
   for (int k = 0; k < 2 * K; ++k) s += hacc[(size_t)b * 2 * K + k];
   out[b] = s * scale;
+}
+
+// Reverse segment r of several candidates' gradient sweeps, aligned at each
+// candidate's end: candidate b (nseg[b] segments) works on its segment
+// g = nseg[b] - 1 - r, whose start state is ckpt[g][b]; a candidate with g < 0
+// is done (skipped by every launch of the segment).
+template <typename R>
+__global__ void k_grad_segment(cplx<R>* F, const cplx<R>* ckpt, const int* nseg, int r, StepCtl* ctl, long vec,
+                               int B) {
+  const long total = (long)B * vec;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / vec);
+    const int g = nseg[b] - 1 - r;
+    if (i % vec == 0) ctl[b].done = g < 0 ? 1 : 0;
+    if (g >= 0) F[i] = ckpt[((size_t)g * B + b) * vec + (i % vec)];
+  }
 }
 
 }  // namespace ecs

@@ -9,13 +9,15 @@ their own grid n, horizon (steps), Reynolds number, T, sx and state.
   (ecs_pool_*): every slot has its own step size and budget, finished slots are
   skipped, and new requests are admitted at step boundaries while the other
   slots keep running — continuous batching, not a queue.
-* Matvec requests in Lawson_RK4 mode go to their group's batcher: whatever
-  has queued while its previous sweep ran (up to its batch size) becomes the
-  next sweep, one forward-mode pass over all those candidates (ecs_jvp_multi:
-  each candidate with its own state, T, sx, horizon and tangent).
-* Gradient requests, and every request in adaptive Lawson_RK43 mode, run on
-  worker threads, each with a private context and CUDA stream, so several
-  linearisations proceed concurrently.
+* Matvec and gradient requests in Lawson_RK4 mode go to their group's
+  batchers: whatever has queued while a batcher's previous sweep ran (up to its
+  batch size) becomes the next sweep over all those candidates, each with its
+  own state, T, sx and horizon — one forward-mode pass for matvecs
+  (ecs_jvp_multi), one forward pass and one adjoint pass for gradients
+  (ecs_loss_grad_multi).
+* Requests in adaptive Lawson_RK43 mode run on worker threads, each with a
+  private context and CUDA stream, so several linearisations proceed
+  concurrently (adaptive candidates do not step in lockstep).
 * Admission is by HBM footprint: a request is admitted only while the
   estimated device memory of all live contexts and records stays within the
   budget; otherwise it waits.
@@ -36,7 +38,7 @@ import torch
 
 from . import _lib
 from . import context as C
-from .autodiff import Objective, jvp_multi, loss_and_grad
+from .autodiff import Objective, jvp_multi, loss_and_grad, loss_grad_multi
 from .loss_functions import objective_RPO, shoot_cfg
 from .mhd import make_param_dict
 
@@ -114,6 +116,15 @@ def record_bytes(n, dtype, steps, ckpt, mode="Lawson_RK4"):
         return ADAPTIVE_CAP[0] * ADAPTIVE_CAP[1] * 11 * vec + regen
     seg = ckpt if ckpt else steps
     return seg * 8 * vec + (steps // max(seg, 1) + 1) * vec + regen
+
+
+def grad_multi_bytes(n, dtype, batch, max_steps=2048, seg=32):
+    """Device bytes of ecs_loss_grad_multi's buffers beyond multi_bytes:
+    segment start states, one segment's record and stage fields, residuals."""
+    K, M = (n - 1) // 3 + 1, 2 * ((n - 1) // 3) + 1
+    rb = 8 if dtype == torch.float64 else 4
+    vec = 2 * K * M * 2 * rb
+    return batch * ((max_steps // seg) * vec + seg * 8 * vec + seg * 4 * n * 4 * n * rb + 4 * n * n * rb)
 
 
 def multi_bytes(n, dtype, batch):
@@ -221,19 +232,22 @@ class Worker(threading.Thread):
             self.busy = False
 
 
-class MatvecBatcher(threading.Thread):
-    """Lawson_RK4 matvec requests of one (n, dtype, Re) group: each sweep takes
-    every request queued so far (up to `batch`) and runs them as one
-    ecs_jvp_multi call on a private context and stream, so requests that arrive
-    during a sweep join the next one."""
+class Batcher(threading.Thread):
+    """Lawson_RK4 requests of one kind ("matvec" or "gradient") and one (n,
+    dtype, Re) group: each sweep takes every request queued so far (up to
+    `batch`) and runs them as one ecs_jvp_multi or ecs_loss_grad_multi call on a
+    private context and stream, so requests that arrive during a sweep join the
+    next one."""
 
-    def __init__(self, n, dtype, Re, results, now_fn, batch=16):
+    def __init__(self, kind, n, dtype, Re, results, now_fn, batch=16):
         super().__init__(daemon=True)
-        self.n, self.dtype, self.Re, self.batch = n, dtype, Re, batch
+        self.kind, self.n, self.dtype, self.Re, self.batch = kind, n, dtype, Re, batch
         self.inbox = queue.Queue()
         self.results, self.now_fn = results, now_fn
         self.queued = 0
         self.bytes = context_bytes(n, dtype, batch) + multi_bytes(n, dtype, batch)
+        if kind == "gradient":
+            self.bytes += grad_multi_bytes(n, dtype, batch)
         self.error = None
         self.sweeps = []   # batch size of every sweep run
 
@@ -258,7 +272,8 @@ class MatvecBatcher(threading.Thread):
                     break
                 items.append(nxt)
             try:
-                outs = run_matvec_batch([r for r, _ in items], ctx, stream)
+                run = run_matvec_batch if self.kind == "matvec" else run_gradient_batch
+                outs = run([r for r, _ in items], ctx, stream)
                 self.sweeps.append(len(items))
                 t = self.now_fn()
                 for (req, t_admit), out in zip(items, outs):
@@ -283,6 +298,18 @@ def run_matvec_batch(reqs, ctx, stream):
             pds.append(_param_dict(req, req.dtype))
         _, jv = jvp_multi(prims, tans, pds, "Lawson_RK4", ctx=ctx)
         outs = [{"fields": j["fields"].clone(), "T": float(j["T"]), "sx": float(j["sx"])} for j in jv]
+        stream.synchronize()
+    return outs
+
+
+def run_gradient_batch(reqs, ctx, stream):
+    """Lawson_RK4 gradient requests of one group in one ecs_loss_grad_multi sweep."""
+    with torch.cuda.stream(stream):
+        xs = [{"fields": torch.as_tensor(r.fields, dtype=r.dtype).to("cuda").contiguous(), "T": r.T, "sx": r.sx}
+              for r in reqs]
+        res = loss_grad_multi(xs, [_param_dict(r, r.dtype) for r in reqs], "Lawson_RK4", ctx=ctx)
+        outs = [{"loss": float(l), "fields": g["fields"].clone(), "T": float(g["T"]), "sx": float(g["sx"])}
+                for l, g in res]
         stream.synchronize()
     return outs
 
@@ -368,13 +395,17 @@ class Server:
 
     def _admit(self, r, t):
         key = (r.n, r.dtype, r.Re)
-        if r.kind == "matvec" and r.mode == "Lawson_RK4":
-            bt = self.batchers.get(key)
+        if r.kind in ("matvec", "gradient") and r.mode == "Lawson_RK4":
+            bkey = (r.kind,) + key
+            bt = self.batchers.get(bkey)
             if bt is None:
                 need = context_bytes(r.n, r.dtype, self.slots) + multi_bytes(r.n, r.dtype, self.slots)
+                if r.kind == "gradient":
+                    need += grad_multi_bytes(r.n, r.dtype, self.slots)
                 if self._used() + need > self.budget:
                     return False
-                bt = self.batchers[key] = MatvecBatcher(r.n, r.dtype, r.Re, self.results, self._now, batch=self.slots)
+                bt = self.batchers[bkey] = Batcher(r.kind, r.n, r.dtype, r.Re, self.results, self._now,
+                                                   batch=self.slots)
                 bt.start()
             if bt.queued >= 2 * bt.batch:   # bounded backlog: the rest waits for admission
                 return False

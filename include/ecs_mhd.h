@@ -104,6 +104,20 @@ int ecs_jvp_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, c
                   void* out_fields, const void* dfields, const double* dT, const double* dsx, void* out_dfields,
                   double* out_dT, double* out_dsx, int batch, void* stream);
 
+/* loss_RPO and its gradient for `batch` different candidates in one call, as
+ * `batch` separate jax.value_and_grad(loss_RPO) calls give them
+ * (jax_scripts/adjoint_descent.py:91; loss_functions.py:99-111).  Mode
+ * Lawson_RK4 only; cfgs[b] (HOST array) gives candidate b's num_checkpoints,
+ * ministeps, shift_reflect_ny and rot.  The forward solves step together and
+ * keep a state every SEG steps (SEG, at most 32, divides every candidate's
+ * step count); the adjoint sweep runs backwards over one recomputed segment
+ * at a time, aligned at each candidate's end.  Device arrays: fields,
+ * g_fields [batch][2][n][n]; T, sx, loss, g_T, g_sx [batch] (double).  The
+ * context's linearisation is untouched; a slot pool on the context restarts. */
+int ecs_loss_grad_multi(ecs_ctx* ctx, const ecs_shoot_cfg* cfgs, const void* fields, const double* T,
+                        const double* sx, double* loss, void* g_fields, double* g_T, double* g_sx, int batch,
+                        void* stream);
+
 /* In-step timing of the batched tangent kernels (instrumentation for roofline
  * reporting; no reference counterpart).  enable = 1: the following
  * ecs_linearize_jvp calls (adaptive mode, pipelined path) record CUDA events

@@ -1,14 +1,18 @@
-"""Matvecs of several candidates in one sweep (ecs_jvp_multi): every
+"""Matvecs and gradients of several candidates in one sweep
+(ecs_jvp_multi, ecs_loss_grad_multi).  Matvecs: every
 candidate's objective and JVP equal those of its own single-candidate call
 (Objective.linearize_jvp: the primal record then a tangent sweep), to 1e-13
 relative (the two paths take the primal physical fields from different passes
 of the same arithmetic), and match torch.func.jvp of the oracle to 1e-12.
 Candidates differ in horizon, step count, T, sx, symmetry, state and tangent;
-the longest runs past the others, which must stop at their own budget."""
+the longest runs past the others, which must stop at their own budget.
+Gradients: every candidate's loss and gradient equal its own loss_and_grad
+call and torch.func.vjp of the oracle's loss_RPO to 1e-12, with different
+step counts (the reverse sweep is aligned at each candidate's end)."""
 import numpy as np
 import pytest
 import torch
-from torch.func import jvp as tjvp
+from torch.func import jvp as tjvp, vjp as tvjp
 
 import oracle as O
 import ecs_mhd_2d_b200 as E
@@ -101,3 +105,57 @@ def test_jvp_multi_fp32(cuda):
          "sx": torch.tensor(tans[b]["sx"], dtype=torch.float64)}
     _, wt = tjvp(f, (p,), (t,))
     assert rel_l2(jv[b]["fields"].double().cpu().numpy(), wt["fields"].numpy()) < 5e-5
+
+
+GCANDS = [  # (num_checkpoints, ministeps, T, sx, shift_reflect_ny, rot): step counts 16, 24, 32, 8 (segments of 8)
+    (2, 8, 0.08, 0.3, 0, False),
+    (3, 8, 0.12, -0.2, 1, True),
+    (4, 8, 0.15, 0.7, 3, False),
+    (1, 8, 0.03, 0.0, 2, False),
+]
+
+
+def _gsetup(n, cands, re=40.0):
+    xs, pds, opds = [], [], []
+    for i, (nc, ms, T, sx, ny, rot) in enumerate(cands):
+        kw = dict(num_checkpoints=nc, ministeps=ms, shift_reflect_ny=ny, rot=rot)
+        pds.append(E.make_param_dict(n, 1 / re, 1 / re, forcing="kolmogorov+", **kw))
+        opds.append(O.make_param_dict(n, 1 / re, 1 / re, forcing="kolmogorov+", xp=O.TORCH, **kw))
+        xs.append({"fields": torch.as_tensor(initial_condition(40 + i, n, amp=6.0), device="cuda"), "T": T, "sx": sx})
+    return xs, pds, opds
+
+
+@pytest.mark.parametrize("n,cands", [(64, GCANDS), (128, GCANDS[:3]), (64, CANDS)])
+def test_loss_grad_multi_equals_single_candidate_calls(cuda, n, cands):
+    """Each candidate's loss and gradient equal its own loss_and_grad call
+    (the single-candidate adjoint) to 1e-12; the third case has step counts
+    16, 24, 5, 32, 24 (segments of one step)."""
+    xs, pds, _ = _gsetup(n, cands)
+    res = E.loss_grad_multi(xs, pds)
+    for b in range(len(cands)):
+        (l1, _), g1 = E.loss_and_grad(xs[b], pds[b], "Lawson_RK4")
+        lb, gb = res[b]
+        assert abs(float(lb) - float(l1)) <= 1e-12 * abs(float(l1)), b
+        assert rel_l2(gb["fields"].cpu().numpy(), g1["fields"].cpu().numpy()) < 1e-12, b
+        for k in ("T", "sx"):
+            w = float(g1[k])
+            assert abs(float(gb[k]) - w) <= 1e-12 * max(abs(w), 1.0), (k, b)
+
+
+def test_loss_grad_multi_matches_oracle(cuda):
+    """Against torch.func.vjp of the oracle's loss_RPO (as jax.value_and_grad): 1e-12."""
+    n = 64
+    xs, pds, opds = _gsetup(n, GCANDS)
+    res = E.loss_grad_multi(xs, pds)
+    for b in (1, 2):
+        f = lambda d: O.loss_RPO(d, opds[b], "Lawson_RK4", xp=O.TORCH)[0]
+        p = {"fields": xs[b]["fields"].cpu(), "T": torch.tensor(xs[b]["T"], dtype=torch.float64),
+             "sx": torch.tensor(xs[b]["sx"], dtype=torch.float64)}
+        lw, fn = tvjp(f, p)
+        gw = fn(torch.tensor(1.0, dtype=torch.float64))[0]
+        lb, gb = res[b]
+        assert abs(float(lb) - float(lw)) <= 1e-12 * abs(float(lw))
+        assert rel_l2(gb["fields"].cpu().numpy(), gw["fields"].numpy()) < 1e-12, b
+        for k in ("T", "sx"):
+            w = float(gw[k])
+            assert abs(float(gb[k]) - w) <= 1e-12 * max(abs(w), 1.0), (k, b)
