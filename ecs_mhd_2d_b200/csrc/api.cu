@@ -96,6 +96,9 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   if (const char* v = getenv("ECS_TGROUPS")) c->tgroups = std::max(1, std::min(ecs_ctx::MAXG, atoi(v)));
   if (const char* v = getenv("ECS_ROWTAN_XT")) c->rowtan_xt = atoi(v) == 4 ? 4 : 8;
   if (const char* v = getenv("ECS_PDL_MINB")) c->pdl_minb = std::max(1, atoi(v));
+  if (const char* v = getenv("ECS_CHAIN_MAXB")) c->chain_maxb = std::max(0, atoi(v));
+  if (const char* v = getenv("ECS_RK4CHAIN_MAXB")) c->rk4chain_maxb = std::max(0, atoi(v));
+  if (const char* v = getenv("ECS_REGEN_ITEMS")) c->regen_items = atoi(v) > 0 ? std::max(8, atoi(v)) : 0;
   int st;
   const ecs::ImplTable* t = ecs::impl_table(dtype, n);
   st = t ? t->init(c, params) : ECS_ERR_UNSUPPORTED;
@@ -142,6 +145,7 @@ static int ctx_destroy_locked(ecs_ctx* ctx) {
   if (ctx->lin.rec_h) cudaFree(ctx->lin.rec_h);
   if (ctx->lin.rec_acc) cudaFree(ctx->lin.rec_acc);
   if (ctx->D) cudaFree(ctx->D);
+  if (ctx->chain_ops) cudaFree(ctx->chain_ops);
   if (ctx->Greg) cudaFree(ctx->Greg);
   if (ctx->Phys) cudaFree(ctx->Phys);
   if (ctx->items) cudaFree(ctx->items);

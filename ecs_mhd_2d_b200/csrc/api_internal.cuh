@@ -40,6 +40,9 @@ struct ecs_ctx {
   int pdl_minb = 1;                 // smallest batch launched with programmatic dependent launch (ECS_PDL_MINB)
   int plain_order = 0;              // depth of PlainOrder scopes (no programmatic launch below batch 8)
   int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)
+  int regen_items = 0;              // stage inputs per regeneration chunk (ECS_REGEN_ITEMS, at least 8; 0: about 384 MiB)
+  int rk4chain_maxb = 8;            // largest batch of Lawson-RK4 stepping run as one cluster-resident launch (ECS_RK4CHAIN_MAXB; 0: graphs of launches)
+  int chain_maxb = 64;              // largest batch of the adaptive tangent sweep run as one cluster-resident pass list (ECS_CHAIN_MAXB; 0: launch per pass)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;
@@ -64,6 +67,7 @@ struct ecs_ctx {
   void* D = nullptr; size_t D_bytes = 0;          // tangent or adjoint slots
   void* Greg = nullptr; void* Phys = nullptr; size_t reg_items = 0;   // regenerated primal fields
   long* items = nullptr; size_t items_cap = 0;
+  void* chain_ops = nullptr; size_t chain_ops_bytes = 0;   // pass list of the cluster-resident tangent sweep
   double* hacc = nullptr; size_t hacc_bytes = 0;   // adjoint dL/dh accumulators [B][K]
   // CUDA graph of a chunk of adaptive attempts (replayed on the caller's stream)
   cudaStream_t cap_stream = nullptr;

@@ -10,6 +10,7 @@
 #include "kernels_adj.cuh"
 #include "kernels_fx.cuh"
 #include "kernels_fxl.cuh"
+#include "kernels_chain.cuh"
 #include "api_internal.cuh"
 #include "impl_table.h"
 
@@ -91,6 +92,10 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, 4>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
+  if constexpr (N <= 128)
+    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N>());
+  if constexpr (N <= 128)
+    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N>());
   if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
   return ECS_OK;
 }
@@ -406,8 +411,31 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "state_vel");
   }
 
+  // Lawson-RK4 steps of the box states in c->F as one cluster-resident launch
+  // (k_rk4_chain), after the COL_START pass; no inverse transforms after the last stage.
+  static int rk4_chain(ecs_ctx* c, int B, long steps, cudaStream_t s) {
+    if constexpr (N <= 128) {
+      Rk4ChainParams<R> P{};
+      ColParams<R>& p = P.col;
+      p.H = (const cplx<R>*)c->H; p.G = (cplx<R>*)c->G; p.F = (cplx<R>*)c->F; p.A1 = (cplx<R>*)c->A1;
+      p.K2 = (cplx<R>*)c->K2; p.OUT = (cplx<R>*)c->OUT; p.Etab = (const R*)c->Etab; p.ctl = c->ctl;
+      p.fhat = (const cplx<R>*)c->fhat; p.tw = (const cplx<R>*)c->tw; p.nu = (R)c->nu; p.eta = (R)c->eta;
+      p.B = B;
+      RowParams<R>& q = P.row;
+      q.G = (const cplx<R>*)c->G; q.H = (cplx<R>*)c->H; q.tw = (const cplx<R>*)c->tw;
+      q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.B = B;
+      P.steps = steps; P.last_produce = 0;
+      launch_step(c, B, k_rk4_chain<R, N>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N>(), s, P);
+      return cuda_err(c, cudaGetLastError(), "rk4 chain");
+    } else {
+      (void)B; (void)steps; (void)s;
+      return set_err(c, ECS_ERR_UNSUPPORTED, "rk4 chain: n > 128");
+    }
+  }
+
   // Lawson-RK4 over `steps` steps of the box state in c->F (ctl/Etab prepared).
-  // Chunks of GS steps are captured once into a CUDA graph and replayed.
+  // Chunks of GS steps are captured once into a CUDA graph and replayed; batches
+  // up to c->rk4chain_maxb at n <= 128 run as one cluster-resident launch.
   static int integrate_rk4(ecs_ctx* c, int B, long steps, cudaStream_t s) {
     if (steps <= 0) return ECS_OK;
     constexpr int GS = 16;
@@ -436,6 +464,7 @@ struct Impl {
       gk.B = B;
     }
     launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
+    if (N <= 128 && B <= c->rk4chain_maxb) return rk4_chain(c, B, steps, s);
     long it = 0;
     while (steps - it > GS) {   // the final step (no inverse transforms) is launched directly
       cudaError_t e = cudaGraphLaunch(gk.exec, s);
@@ -852,7 +881,7 @@ struct Impl {
     launch_row_to_box<R, N>(c, dfields, (cplx<R>*)c->H, B, s);
     launch_col_to_box<R, N>(c, (const cplx<R>*)c->H, (cplx<R>*)c->D + (size_t)DT_F * VEC, B, 2, s, (long)nslot * VEC);
     const long steps = L.nrec;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     const long CS = std::max(1L, std::min(64L, ci / 4));   // steps per regeneration chunk (4 items each)
     // items: per chunk, the states [f, f_temp] of its steps, then the derivatives [k1, k2]
     std::vector<long> items;
@@ -965,7 +994,7 @@ struct Impl {
     const std::vector<long> items = fxl_items(scheme, steps);
     st = upload_items(c, items, s);
     if (st) return st;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     long chunk_lo = -1;
     const cplx<R>* rec = (const cplx<R>*)L.rec;
     auto phys_of = [&](long item) -> const R* {
@@ -996,7 +1025,7 @@ struct Impl {
     const std::vector<long> items = fxl_items(scheme, steps);
     int st = upload_items(c, items, s);
     if (st) return st;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     long chunk_lo = -1;
     const cplx<R>* rec = (const cplx<R>*)L.rec;
     auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
@@ -1114,14 +1143,16 @@ struct Impl {
                     "items upload");
   }
 
-  static size_t chunk_items() {
+  // Stage inputs regenerated per chunk (about 384 MiB of buffers; ECS_REGEN_ITEMS overrides).
+  static size_t chunk_items(const ecs_ctx* ctx) {
+    if (ctx->regen_items > 0) return (size_t)ctx->regen_items;
     const size_t per = (size_t)NG * K * N * sizeof(cplx<R>) + (size_t)N * NPH * N * sizeof(R);
     size_t c = ((size_t)384 << 20) / per;
     return c < 8 ? 8 : (c > 512 ? 512 : c);
   }
 
   static int ensure_regen(ecs_ctx* c) {
-    const size_t ci = chunk_items();
+    const size_t ci = chunk_items(c);
     if (c->reg_items >= ci && c->Greg) return ECS_OK;
     size_t have1 = c->Greg ? 1 : 0, have2 = have1;
     (void)have2;
@@ -1174,7 +1205,7 @@ struct Impl {
     }
     st = upload_items(c, items, s);
     if (st) return st;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     long chunk_lo = -1;
     auto phys_of = [&](long item) -> const R* {
       if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
@@ -1216,33 +1247,113 @@ struct Impl {
         }
       }
     } else {
-      const double t = L.T;
-      launch_col_tan<R, N>(c, B, T43_START, 1, rec, dT, t, 0.0, 1.0, nslot, s);
-      launch_row_tan<R, N>(c, B, phys_of(0), s);
-      launch_col_tan<R, N>(c, B, T43_INIT, 0, rec, dT, t, 0.0, 1.0, nslot, s);
-      bool a_started = false;   // the E pass of the previous attempt ran this one's A pass (T43_EA)
-      for (long a = 0; a < L.nrec; ++a) {
-        const cplx<R>* ra = rec + (size_t)a * RR_NREC * VEC;
-        const double h = L.hs[a];
-        if (!L.acc[a]) {
-          ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, N, B);
-          a_started = false;
-          continue;
+      const std::vector<ChainOp> ops = rk43_tangent_ops(L, item_of);
+      if (use_chain(c, B)) {
+        st = run_chain(c, ops, ci, (long)items.size(), B, nslot, dT, s);
+        if (st) return st;
+      } else {
+        for (const ChainOp& op : ops) {
+          const cplx<R>* ra = rec + (size_t)op.rec * VEC;
+          if (op.kind == CH_ROW) {
+            launch_row_tan<R, N>(c, B, phys_of(op.item), s);
+          } else if (op.kind == CH_REJECT) {
+            ++c->launches; k_tan_reject<R><<<grid1d((long)B * VEC), 256, 0, s>>>((cplx<R>*)c->D, nslot, ra, dT, 1.0, N, B);
+          } else {
+            launch_col_tan<R, N>(c, B, op.stage, op.produce, ra, dT, L.T, op.h, 1.0, nslot, s, nullptr, 0, nullptr,
+                                 nullptr, op.stage == T43_EA ? rec + (size_t)op.rec2 * VEC : nullptr);
+          }
         }
-        if (!a_started) launch_col_tan<R, N>(c, B, T43_A, 1, ra, dT, t, h, 1.0, nslot, s);
-        const bool merge = a + 1 < L.nrec && L.acc[a + 1];
-        for (int k = 0; k < 4; ++k) {
-          launch_row_tan<R, N>(c, B, phys_of(item_of[a] + k), s);
-          if (k == 3 && merge)
-            launch_col_tan<R, N>(c, B, T43_EA, 1, ra, dT, t, L.hs[a + 1], 1.0, nslot, s, nullptr, 0, nullptr, nullptr,
-                                 ra + (size_t)RR_NREC * VEC);
-          else
-            launch_col_tan<R, N>(c, B, T43_B + k, 1, ra, dT, t, h, 1.0, nslot, s);
-        }
-        a_started = merge;
       }
     }
     return jvp_finish(c, dfields, dsx, out, odT, odsx, B, s);
+  }
+
+  // The passes of the adaptive tangent sweep in launch order: inverse transforms
+  // of dX0, the row pass at x0 and the initial dk1, then per accepted attempt
+  // the stages A..E with a row pass before B..E (E of an attempt followed by an
+  // accepted attempt runs that attempt's A too: T43_EA), per rejected attempt
+  // the update of the carried dk1.  Row-pass items index the regeneration plan
+  // (item_of: first item of each accepted attempt; item 0 is x0 of attempt 0).
+  static std::vector<ChainOp> rk43_tangent_ops(const ecs_ctx::Lin& L, const std::vector<long>& item_of) {
+    std::vector<ChainOp> ops;
+    ops.reserve((size_t)L.nrec * 8 + 4);
+    auto col = [&](int stage, int produce, long a, double h, long a2 = 0) {
+      ChainOp o{}; o.kind = CH_COL; o.stage = stage; o.produce = produce;
+      o.rec = a * RR_NREC; o.rec2 = a2 * RR_NREC; o.h = h; ops.push_back(o);
+    };
+    auto row = [&](long item) { ChainOp o{}; o.kind = CH_ROW; o.item = item; ops.push_back(o); };
+    col(T43_START, 1, 0, 0.0);
+    row(0);
+    col(T43_INIT, 0, 0, 0.0);
+    bool a_started = false;   // the E pass of the previous attempt ran this one's A pass (T43_EA)
+    for (long a = 0; a < L.nrec; ++a) {
+      const double h = L.hs[a];
+      if (!L.acc[a]) {
+        ChainOp o{}; o.kind = CH_REJECT; o.rec = a * RR_NREC; ops.push_back(o);
+        a_started = false;
+        continue;
+      }
+      if (!a_started) col(T43_A, 1, a, h);
+      const bool merge = a + 1 < L.nrec && L.acc[a + 1];
+      for (int k = 0; k < 4; ++k) {
+        row(item_of[a] + k);
+        if (k == 3 && merge) col(T43_EA, 1, a, L.hs[a + 1], a + 1);
+        else col(T43_B + k, 1, a, h);
+      }
+      a_started = merge;
+    }
+    return ops;
+  }
+
+  // Batches that the adaptive tangent sweep runs through the cluster-resident
+  // pass list (k_tan_chain): n <= 128, batch up to c->chain_maxb.
+  static bool use_chain(const ecs_ctx* c, int B) { return N <= 128 && B <= c->chain_maxb; }
+
+  // The pass list through k_tan_chain: one launch per regeneration chunk (the
+  // row passes of a launch read the chunk's physical fields), with the chunk's
+  // regeneration launched before it on the same stream.
+  static int run_chain(ecs_ctx* c, const std::vector<ChainOp>& ops, long ci, long nitems, int B, int nslot,
+                       const double* dT, cudaStream_t s) {
+    if constexpr (N <= 128) {
+      auto& L = c->lin;
+      int st = grow(c, &c->chain_ops, &c->chain_ops_bytes, ops.size() * sizeof(ChainOp));
+      if (st) return st;
+      st = cuda_err(c, cudaMemcpyAsync(c->chain_ops, ops.data(), ops.size() * sizeof(ChainOp), cudaMemcpyHostToDevice, s),
+                    "pass list upload");
+      if (st) return st;
+      ChainParams<R> P{};
+      ColTanParams<R>& cp = P.col;
+      cp.H = (const cplx<R>*)c->H; cp.G = (cplx<R>*)c->G; cp.D = (cplx<R>*)c->D; cp.nslot = nslot;
+      cp.dT = dT; cp.t = L.T; cp.dscale = 1.0; cp.tw = (const cplx<R>*)c->tw; cp.nu = (R)c->nu; cp.eta = (R)c->eta;
+      cp.B = B;
+      P.row.G = (const cplx<R>*)c->G; P.row.H = (cplx<R>*)c->H; P.row.tw = (const cplx<R>*)c->tw; P.row.B = B;
+      P.rec = (const cplx<R>*)L.rec;
+      P.ops = (const ChainOp*)c->chain_ops;
+      long chunk_lo = -1;
+      size_t start = 0;
+      auto flush = [&](size_t end) {
+        if (end <= start) return;
+        P.op0 = (int)start; P.op1 = (int)end;
+        P.phys = (const R*)c->Phys; P.item0 = chunk_lo < 0 ? 0 : chunk_lo;
+        launch_step(c, B, k_tan_chain<R, N>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N>(), s, P);
+        start = end;
+      };
+      for (size_t i = 0; i < ops.size(); ++i) {
+        if (ops[i].kind != CH_ROW) continue;
+        const long item = ops[i].item;
+        if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
+          flush(i);
+          chunk_lo = item;
+          const long cnt = std::min<long>(ci, nitems - item);
+          launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + item, (int)cnt, s);
+        }
+      }
+      flush(ops.size());
+      return cuda_err(c, cudaGetLastError(), "tangent pass list");
+    } else {
+      (void)ops; (void)ci; (void)nitems; (void)B; (void)nslot; (void)dT; (void)s;
+      return set_err(c, ECS_ERR_UNSUPPORTED, "pass list: n > 128");
+    }
   }
 
   // JVP output from the final tangent state:
@@ -1347,7 +1458,7 @@ struct Impl {
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ps, c->pev[0], 0);
     if (e != cudaSuccess) return cuda_err(c, e, "pipeline fork");
     cplx<R>* rec = (cplx<R>*)L.rec;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     const long CS = std::max(1L, std::min(16L, ci / 4));   // steps per chunk (their items fit one regeneration)
     const long nch = (steps + CS - 1) / CS;
     auto primal_chunk = [&](long k) -> cudaError_t {
@@ -1465,7 +1576,7 @@ struct Impl {
     // stream, into alternating halves of the regeneration buffer when two
     // chunks fit.
     L.acc.clear(); L.hs.clear();
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     const int ngrp = std::max(1, std::min(c->tgroups, B / 16));
     int bsplit[ecs_ctx::MAXG + 1];
     for (int g = 0; g <= ngrp; ++g) bsplit[g] = (int)((long)B * g / ngrp);
@@ -1612,7 +1723,7 @@ struct Impl {
     int st = grow(c, &c->Gx, &c->Gx_bytes, (size_t)B * NHA * K * N * sizeof(cplx<R>));
     if (st) return st;
     const long steps = L.nrec;
-    const long ci = (long)chunk_items();
+    const long ci = (long)chunk_items(c);
     const long CS = std::max(1L, std::min(64L, ci / 4));
     std::vector<long> items;
     items.reserve((size_t)(4 * steps));
@@ -1723,7 +1834,7 @@ struct Impl {
       }
       st = upload_items(c, items, s);
       if (st) return st;
-      const long ci = (long)chunk_items();
+      const long ci = (long)chunk_items(c);
       long chunk_lo = -1;
       auto phys_of = [&](long item) -> const R* {   // chunks end at the requested item (reverse sweep)
         if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {

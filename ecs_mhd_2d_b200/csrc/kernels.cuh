@@ -212,19 +212,25 @@ struct ColParams {
   int use_done;          // skip batch elements whose ctl.done is set (slot pool)
 };
 
+// Rows of F (and A1, K2) and of the factor e that a stage stages per warp (n <= 128).
+template <int N, int STAGE> __host__ __device__ constexpr bool col_rk4_stg() {
+  return N <= 128 && STAGE >= COL_RK4_S1 && STAGE <= COL_RK4_S4;
+}
+template <int N, int STAGE> __host__ __device__ constexpr int col_rk4_nc() {
+  return !col_rk4_stg<N, STAGE>() ? 0 : STAGE == COL_RK4_S3 ? 3 : 1;
+}
+template <int N, int STAGE> __host__ __device__ constexpr int col_rk4_nrl() {
+  return (col_rk4_stg<N, STAGE>() && (STAGE == COL_RK4_S1 || STAGE == COL_RK4_S3)) ? 1 : 0;
+}
+
+// One warp's column `colid` of a Lawson-RK4 column stage; my_c / my_e are the
+// warp's staging rows (col_rk4_nc complex and col_rk4_nrl real rows of M).
 template <typename R, int N, int STAGE>
-__global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
+__device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
+                                             cplx<R>* my_c, R* my_e) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (colid >= p.B * K * 2) return;
   const int c = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
 
   if (p.use_done && p.ctl[b].done) return;
@@ -232,13 +238,9 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   // The rows of F (and A1, K2, the factor e) that the stage algebra reads,
   // copied into the warp's shared buffers with cp.async before the forward
   // transform, so that their latency overlaps it (n <= 128).
-  constexpr bool STG = N <= 128 && STAGE >= COL_RK4_S1 && STAGE <= COL_RK4_S4;
-  constexpr int NC = !STG ? 0 : STAGE == COL_RK4_S3 ? 3 : 1;                    // F (A1, K2)
-  constexpr int NRL = (STG && (STAGE == COL_RK4_S1 || STAGE == COL_RK4_S3)) ? 1 : 0;   // e
-  __shared__ __align__(16) cplx<R> s_rc[(NC > 0 ? NC : 1) * 4 * M];   // 4 warps per CTA
-  __shared__ __align__(16) R s_rr[(NRL > 0 ? NRL : 1) * 4 * M];
-  cplx<R>* my_c = s_rc + (threadIdx.x >> 5) * NC * M;
-  R* my_e = s_rr + (threadIdx.x >> 5) * NRL * M;
+  constexpr bool STG = col_rk4_stg<N, STAGE>();
+  constexpr int NC = col_rk4_nc<N, STAGE>();     // F (A1, K2)
+  constexpr int NRL = col_rk4_nrl<N, STAGE>();   // e
   if constexpr (STG) {
     for (int s2 = lane; s2 < M; s2 += 32) {
       cp_async_v(my_c + s2, p.F + base + s2);
@@ -319,6 +321,23 @@ __global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
   }
   if (!p.produce) return;
   col_inverse_uv<R, N>(x, p.G, b, c, ky, lane, s_tw);
+}
+
+template <typename R, int N, int STAGE>
+__global__ void __launch_bounds__(128) k_col_rk4(ColParams<R> p) {
+  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr int NC = col_rk4_nc<N, STAGE>(), NRL = col_rk4_nrl<N, STAGE>();
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
+  __shared__ __align__(16) cplx<R> s_rc[(NC > 0 ? NC : 1) * 4 * M];   // 4 warps per CTA
+  __shared__ __align__(16) R s_rr[(NRL > 0 ? NRL : 1) * 4 * M];
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  col_rk4_body<R, N, STAGE>(p, colid, lane, s_tw, s_rc + (threadIdx.x >> 5) * NC * M, s_rr + (threadIdx.x >> 5) * NRL * M);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,20 +450,13 @@ __device__ __forceinline__ void split_store(const cplx<R> (&W)[N / 32], cplx<R>*
   }
 }
 
+// Rows x0 .. x0 + XT - 1 of state b, one warp per row (the CTA's XT warps);
+// s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
 template <typename R, int N, int XT>
-__global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
+__device__ __forceinline__ void row_rhs_body(const RowParams<R>& p, int b, int x0, const cplx<R>* s_tw, cplx<R>* s_G,
+                                             cplx<R>* s_H) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + fft_smem(N, XT);
-  cplx<R>* s_H = s_G + NG * K * (XT + 1);
-  const int tiles = N / XT;
-  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  if (p.ctl && p.ctl[b].done) return;   // whole block belongs to one batch element
   load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -476,6 +488,21 @@ __global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
   store_one<R, N, XT>(bb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
+}
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_rhs(RowParams<R> p) {
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  if (p.ctl && p.ctl[b].done) return;   // whole block belongs to one batch element
+  row_rhs_body<R, N, XT>(p, b, x0, s_tw, s_G, s_G + NG * K * (XT + 1));
 }
 
 // ---------------------------------------------------------------------------

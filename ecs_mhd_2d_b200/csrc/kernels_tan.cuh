@@ -107,22 +107,15 @@ struct RowTanParams {
   int B;
 };
 
+// Rows x0 .. x0 + XT - 1 of tangent b, one warp per row (the CTA's XT warps);
+// s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
 template <typename R, int N, int XT>
-__global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
+__device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, int x0, const cplx<R>* s_tw,
+                                             cplx<R>* s_G, cplx<R>* s_H) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + fft_smem(N, XT);
-  cplx<R>* s_H = s_G + NG * K * (XT + 1);
-  const int tiles = N / XT;
-  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x = x0 + w;
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  if (p.ctl && p.ctl[b].done) return;   // the whole CTA belongs to batch element b
   // primal u, v, B_x, B_y of this row, loaded first so that the loads overlap
   // the tile load and the inverse transforms (n <= 128); at n = 256 they would
   // hold 4 E = 32 registers across the transform, so they are loaded after it
@@ -160,6 +153,21 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   store_one<R, N, XT>(dbb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
+}
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  if (p.ctl && p.ctl[b].done) return;   // the whole CTA belongs to batch element b
+  row_tan_body<R, N, XT>(p, b, x0, s_tw, s_G, s_G + NG * K * (XT + 1));
 }
 
 // ---------------------------------------------------------------------------
@@ -225,19 +233,19 @@ __host__ __device__ constexpr unsigned tan_dmask(int stage) {
 }
 __host__ __device__ constexpr int popc_c(unsigned m) { return m ? (int)(m & 1u) + popc_c(m >> 1) : 0; }
 
+// Operand rows staged per warp by a tangent column stage (shared memory, M entries each).
+template <int N, int STAGE> __host__ __device__ constexpr int col_tan_nop() {
+  return N <= 128 ? popc_c(tan_qmask(STAGE)) + popc_c(tan_qmask2(STAGE)) + popc_c(tan_dmask(STAGE)) : 0;
+}
+
+// One warp's column `colid` of a tangent column stage; `my_op` is the warp's
+// staging buffer (col_tan_nop rows of M entries), `s_tw` the twiddle image.
 template <typename R, int N, int STAGE>
-__global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
+__device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
+                                             cplx<R>* my_op) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (colid >= p.B * K * 2) return;
   const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
   if (p.ctl && p.ctl[b].done) return;
   cplx<R>* D = p.D + (size_t)b * p.nslot * VEC;
@@ -254,8 +262,6 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   constexpr unsigned QM2 = N <= 128 ? tan_qmask2(STAGE) : 0u;
   constexpr int NQ = popc_c(QM), NQ2 = popc_c(QM2), NOP = NQ + NQ2 + popc_c(DM);
   const cplx<R>* Q2 = p.rec2;
-  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
-  cplx<R>* my_op = s_op + (threadIdx.x >> 5) * NOP * M;
   if constexpr (NOP > 0) {
     const size_t row = ((size_t)ch * K + ky) * M;
     int v = 0;
@@ -411,8 +417,36 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
   col_inverse_uv<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
+template <typename R, int N, int STAGE>
+__global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
+  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr int NOP = col_tan_nop<N, STAGE>();
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
+  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  col_tan_body<R, N, STAGE>(p, colid, lane, s_tw, s_op + (threadIdx.x >> 5) * NOP * M);
+}
+
 // Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);
 // its tangent is d(e (e k1)) with e' = e L h/2 dt ((e, e L h/2) from the attempt's record).
+// Entry o of tangent Db (slots of one tangent), dpar = dT * dscale.
+template <typename R>
+__device__ __forceinline__ void tan_reject_at(cplx<R>* Db, const cplx<R>* rec, size_t VEC, size_t o, R dpar) {
+  const cplx<R> eg = rec[RR_E * VEC + o];   // (e, e L h/2) of the attempt
+  const R e = eg.x;
+  const R de = eg.y * dpar;
+  const cplx<R> k1 = rec[RR_K1 * VEC + o];
+  const cplx<R> k1e = cscale(k1, e);
+  const cplx<R> dk1e = cadd(cscale(k1, de), cscale(Db[S_K1 * VEC + o], e));
+  Db[S_K1 * VEC + o] = cadd(cscale(k1e, de), cscale(dk1e, e));
+}
+
 template <typename R>
 __global__ void k_tan_reject(cplx<R>* D, int nslot, const cplx<R>* rec, const double* dT, double dscale, int n,
                              int B) {
@@ -422,14 +456,7 @@ __global__ void k_tan_reject(cplx<R>* D, int nslot, const cplx<R>* rec, const do
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
     const int b = (int)(i / VEC);
     const size_t o = i - (size_t)b * VEC;
-    const cplx<R> eg = rec[RR_E * VEC + o];   // (e, e L h/2) of the attempt
-    const R e = eg.x;
-    const R de = eg.y * (R)(dT[b] * dscale);
-    cplx<R>* Db = D + (size_t)b * nslot * VEC;
-    const cplx<R> k1 = rec[RR_K1 * VEC + o];
-    const cplx<R> k1e = cscale(k1, e);
-    const cplx<R> dk1e = cadd(cscale(k1, de), cscale(Db[S_K1 * VEC + o], e));
-    Db[S_K1 * VEC + o] = cadd(cscale(k1e, de), cscale(dk1e, e));
+    tan_reject_at<R>(D + (size_t)b * nslot * VEC, rec, VEC, o, (R)(dT[b] * dscale));
   }
 }
 

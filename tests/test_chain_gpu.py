@@ -1,0 +1,119 @@
+"""The cluster-resident tangent sweep (k_tan_chain: one launch runs the pass
+list of the adaptive Lawson-RK4(3) JVP -- column stages, row passes, updates of
+rejected attempts) against the launch-per-pass sweep (ECS_CHAIN_MAXB=0).  Both
+run the same per-column and per-row bodies in the same order, so the JVP of
+objective_RPO (jax.jvp at jax_scripts/lib/utils.py:108) is equal bit for bit:
+with rejected attempts, with regeneration-chunk boundaries inside the list
+(ECS_REGEN_ITEMS), for one and for several tangents, at n = 64 and 128."""
+import numpy as np
+import pytest
+import torch
+
+import ecs_mhd_2d_b200 as E
+from ecs_mhd_2d_b200 import context
+from ecs_mhd_2d_b200.synthetic import initial_condition
+
+pytestmark = pytest.mark.gpu
+
+CASES = [   # (n, B, T, atol, amp, env)
+    (64, 1, 0.3, 1e-6, 6.0, {}),
+    (64, 3, 0.3, 1e-6, 6.0, {"ECS_REGEN_ITEMS": "8"}),
+    (64, 64, 0.2, 1e-7, 6.0, {"ECS_REGEN_ITEMS": "24"}),
+    (128, 1, 0.15, 1e-8, 2.0, {}),
+    (128, 5, 0.15, 1e-8, 2.0, {"ECS_REGEN_ITEMS": "16"}),
+    # the 128^2 matvec workload's trajectory (initial condition seed 0, 64 x 64
+    # attempt cap) over T = 0.5: 145 accepted and 6 rejected attempts
+    (128, 2, 0.5, 1e-8, 2.0, {"ECS_REGEN_ITEMS": "64", "seed": 0}),
+]
+
+
+def _run(n, B, T, atol, amp, env, monkeypatch, chain):
+    env = dict(env)
+    seed = env.pop("seed", 4)
+    cap = (64, 64) if seed == 0 else (4, 64)
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    if chain:
+        monkeypatch.delenv("ECS_CHAIN_MAXB", raising=False)
+    else:
+        monkeypatch.setenv("ECS_CHAIN_MAXB", "0")
+    context.clear_cache()
+    try:
+        pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", shift_reflect_ny=1, rot=False,
+                               adaptive_dict={"atol": atol, "checkpoints": cap[0], "max_steps_per_checkpoint": cap[1]})
+        rng = np.random.default_rng(3)
+        prim = {"fields": torch.as_tensor(initial_condition(seed, n, amp=amp), device="cuda"), "T": T, "sx": 0.2}
+        du = np.stack([initial_condition(60 + i, n) * 0.1 + 0.01 * rng.standard_normal((2, n, n)) for i in range(B)])
+        tan = {"fields": torch.as_tensor(du, device="cuda"), "T": torch.linspace(-0.7, 1.1, B, dtype=torch.float64),
+               "sx": torch.linspace(0.4, -0.3, B, dtype=torch.float64)}
+        obj = E.Objective(pd, "Lawson_RK43")
+        obj.linearize(prim, force=True, batch=B)
+        ctx = context.get_context(pd, n, torch.float64, B)
+        torch.cuda.synchronize()
+        c0 = ctx.lib.ecs_launch_count(ctx.handle)
+        out = obj.jvp(prim, tan)
+        torch.cuda.synchronize()
+        launches = ctx.lib.ecs_launch_count(ctx.handle) - c0
+        res = {k: v.detach().cpu().clone() for k, v in out.items()}
+        return res, dict(obj.last_info), launches
+    finally:
+        monkeypatch.undo()
+        context.clear_cache()
+
+
+@pytest.mark.parametrize("n,B,T,atol,amp,env", CASES)
+def test_chain_equals_launch_per_pass(cuda, monkeypatch, n, B, T, atol, amp, env):
+    want, info, per_pass = _run(n, B, T, atol, amp, env, monkeypatch, chain=False)
+    got, info2, chained = _run(n, B, T, atol, amp, env, monkeypatch, chain=True)
+    assert info == info2
+    for k in ("fields", "T", "sx"):
+        assert torch.equal(got[k], want[k]), k
+    # the pass list ran as a handful of launches instead of one per pass
+    assert chained < per_pass // 4, (chained, per_pass)
+
+
+def test_chain_covers_rejected_attempts(cuda, monkeypatch):
+    """The last case's trajectory rejects attempts, so the list's reject
+    updates are part of the comparison."""
+    _, info, _ = _run(*CASES[-1], monkeypatch, chain=True)
+    assert info["rejected"] > 0, info
+
+
+RK4_CASES = [(64, 1, 5), (64, 8, 40), (128, 1, 37), (128, 3, 16)]   # (n, B, steps)
+
+
+def _rk4(n, B, steps, monkeypatch, chain):
+    if chain:
+        monkeypatch.delenv("ECS_RK4CHAIN_MAXB", raising=False)
+    else:
+        monkeypatch.setenv("ECS_RK4CHAIN_MAXB", "0")
+    context.clear_cache()
+    try:
+        pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+")
+        f = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(80 + b, n, amp=3.0) for b in range(B)])),
+                            device="cuda")
+        ctx = context.get_context(pd, n, torch.float64, B)
+        torch.cuda.synchronize()
+        c0 = ctx.lib.ecs_launch_count(ctx.handle)
+        out = E.lawson_rk4(f, 0.004 * steps, steps, pd).cpu().clone()
+        torch.cuda.synchronize()
+        # objective_RPO in Lawson_RK4 mode shoots through the same stepping
+        pdo = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", num_checkpoints=2, ministeps=steps,
+                                shift_reflect_ny=1, rot=False)
+        obj = E.objective_RPO({"fields": torch.as_tensor(initial_condition(5, n), device="cuda"), "T": 0.1,
+                               "sx": 0.3}, pdo, "Lawson_RK4")
+        return out, obj["fields"].cpu().clone(), ctx.lib.ecs_launch_count(ctx.handle) - c0
+    finally:
+        monkeypatch.undo()
+        context.clear_cache()
+
+
+@pytest.mark.parametrize("n,B,steps", RK4_CASES)
+def test_rk4_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, steps):
+    """Lawson-RK4 stepping as one cluster-resident launch (k_rk4_chain) equals
+    the launch-per-stage stepping (graphs of k_row_rhs / k_col_rk4) bit for bit."""
+    want, want_obj, per_stage = _rk4(n, B, steps, monkeypatch, chain=False)
+    got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True)
+    assert torch.equal(got, want)
+    assert torch.equal(got_obj, want_obj)
+    assert chained < per_stage
