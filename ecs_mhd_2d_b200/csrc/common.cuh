@@ -29,9 +29,6 @@ template <typename R> using cplx = typename CplxT<R>::type;
 template <typename R> __host__ __device__ __forceinline__ cplx<R> mk(R x, R y) { cplx<R> c; c.x = x; c.y = y; return c; }
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
-  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
-}
 template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
 template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { a.x *= s; a.y *= s; return a; }
 // (i*mu) * z for real mu, written exactly as the reference's `1j * mu * z`.
@@ -74,6 +71,24 @@ template <typename C, typename R> __device__ __forceinline__ C lin2_rn(C a, R sa
   return r;
 }
 template <int D, typename C> __device__ __forceinline__ C cdiv_k(C a) { a.x = div_k<D>(a.x); a.y = div_k<D>(a.y); return a; }
+// a b + c d and a b - c d with the rounding fixed: the second product rounded,
+// then one FMA.  Written out so that no kernel's compilation chooses another
+// contraction: the same formula gives the same bits in every kernel (the
+// cluster-resident passes reuse the per-pass kernels' bodies and must agree
+// with them bit for bit).
+template <typename R> __device__ __forceinline__ R fpp(R a, R b, R c, R d) { return fma(a, b, mul_rn(c, d)); }
+template <typename R> __device__ __forceinline__ R fpm(R a, R b, R c, R d) { return fma(a, b, -mul_rn(c, d)); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = fpm(a.x, b.x, a.y, b.y); r.y = fpp(a.x, b.y, a.y, b.x); return r;
+}
+// s a with each component product rounded on its own (no contraction with a later sum).
+template <typename C, typename R> __device__ __forceinline__ C cscale_rn(C a, R s) {
+  a.x = mul_rn(a.x, s); a.y = mul_rn(a.y, s); return a;
+}
+// a + b s, the product rounded on its own.
+template <typename C, typename R> __device__ __forceinline__ C cadd_scaled_rn(C a, C b, R s) {
+  a.x = add_rn(a.x, mul_rn(b.x, s)); a.y = add_rn(a.y, mul_rn(b.y, s)); return a;
+}
 
 template <typename R> __device__ __forceinline__ cplx<R> shfl_xor_c(cplx<R> v, int m) {
   v.x = __shfl_xor_sync(0xffffffffu, v.x, m);

@@ -62,7 +62,8 @@ __device__ __forceinline__ cplx<R> mul_mi(cplx<R> a) {
 template <typename R, bool INV>
 __device__ __forceinline__ cplx<R> mul_w8(cplx<R> a) {
   const R c = R(0.70710678118654752440084436210484904);
-  return INV ? mk<R>((a.x - a.y) * c, (a.x + a.y) * c) : mk<R>((a.x + a.y) * c, (a.y - a.x) * c);
+  // products rounded on their own (no contraction with the following sums)
+  return INV ? mk<R>(mul_rn(a.x - a.y, c), mul_rn(a.x + a.y, c)) : mk<R>(mul_rn(a.x + a.y, c), mul_rn(a.y - a.x, c));
 }
 
 // ---------------------------------------------------------------------------

@@ -92,10 +92,14 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, 4>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
-  if constexpr (N <= 128)
-    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N>());
-  if constexpr (N <= 128)
-    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N>());
+  if constexpr (N <= 128) {
+    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N, false>());
+    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N, true>());
+  }
+  if constexpr (N <= 128) {
+    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N, false>());
+    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N, true>());
+  }
   if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
   return ECS_OK;
 }
@@ -425,7 +429,10 @@ struct Impl {
       q.G = (const cplx<R>*)c->G; q.H = (cplx<R>*)c->H; q.tw = (const cplx<R>*)c->tw;
       q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.B = B;
       P.steps = steps; P.last_produce = 0;
-      launch_step(c, B, k_rk4_chain<R, N>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N>(), s, P);
+      if (c->chain_dsm)
+        launch_step(c, B, k_rk4_chain<R, N, true>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N, true>(), s, P);
+      else
+        launch_step(c, B, k_rk4_chain<R, N, false>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N, false>(), s, P);
       return cuda_err(c, cudaGetLastError(), "rk4 chain");
     } else {
       (void)B; (void)steps; (void)s;
@@ -1335,7 +1342,10 @@ struct Impl {
         if (end <= start) return;
         P.op0 = (int)start; P.op1 = (int)end;
         P.phys = (const R*)c->Phys; P.item0 = chunk_lo < 0 ? 0 : chunk_lo;
-        launch_step(c, B, k_tan_chain<R, N>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N>(), s, P);
+        if (c->chain_dsm)
+          launch_step(c, B, k_tan_chain<R, N, true>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N, true>(), s, P);
+        else
+          launch_step(c, B, k_tan_chain<R, N, false>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N, false>(), s, P);
         start = end;
       };
       for (size_t i = 0; i < ops.size(); ++i) {

@@ -34,6 +34,8 @@
 #include "common.cuh"
 #include "fft.cuh"
 
+#include <cooperative_groups.h>
+
 namespace ecs {
 
 // Field counts of the intermediate arrays (per batch element).
@@ -88,31 +90,17 @@ __device__ __forceinline__ R prod_mult(int f, int kx, int ky) {
 // column-pass building blocks (one warp per (batch, ky, channel))
 // ---------------------------------------------------------------------------
 
-// Load column H[b][f][ky][:] (nf fields per batch element) and transform it
-// along x (forward, natural -> bit-reversed order).
-template <typename R, int N>
-__device__ __forceinline__ void col_load_fwd1(const cplx<R>* __restrict__ H, int nf, int b, int f, int ky, int lane,
-                                              const cplx<R>* s_tw, cplx<R> (&r)[N / 32]) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
-  const cplx<R>* h = H + ((size_t)(b * nf + f) * K + ky) * N;
-#pragma unroll
-  for (int j = 0; j < E; ++j) r[j] = h[lane + 32 * j];
-  fft_dif<R, N, false>(r, s_tw, lane);
-}
-
 // Nonlinear time derivative of channel ch (without forcing) at every position
 // of the column ky, bit-reversed slot order, from the product rows in H:
 //   ch 0: -kx ky rfft2(P1) + (ky^2 - kx^2) rfft2(P2)  (two transforms in lockstep),
 //   ch 1: k^2 rfft2(P3).
+// The same from the product rows given directly: h0, h1 = the P1, P2 rows of
+// column ky (ch 0), or h0 = its P3 row (ch 1); global or shared memory.
 template <typename R, int N>
-__device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int b, int ch, int ky, int lane,
+__device__ __forceinline__ void col_rhs_rows(const cplx<R>* h0, const cplx<R>* h1, int ch, int ky, int lane,
                                              const cplx<R>* s_tw, cplx<R> (&v)[N / 32]) {
   constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
   if (ch == 0) {
-    const cplx<R>* h0 = H + ((size_t)(b * NH + 0) * K + ky) * N;
-    const cplx<R>* h1 = H + ((size_t)(b * NH + 1) * K + ky) * N;
     cplx<R> r[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) { v[j] = h0[lane + 32 * j]; r[j] = h1[lane + 32 * j]; }
@@ -121,10 +109,12 @@ __device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int 
     for (int j = 0; j < E; ++j) {
       const int kx = pos_to_k(spec_pos<N>(lane, j), N);
       const R m0 = prod_mult<R>(0, kx, ky), m1 = prod_mult<R>(1, kx, ky);
-      v[j] = mk<R>(m0 * v[j].x + m1 * r[j].x, m0 * v[j].y + m1 * r[j].y);
+      v[j] = mk<R>(fpp(m0, v[j].x, m1, r[j].x), fpp(m0, v[j].y, m1, r[j].y));
     }
   } else {
-    col_load_fwd1<R, N>(H, NH, b, 2, ky, lane, s_tw, v);
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = h0[lane + 32 * j];
+    fft_dif<R, N, false>(v, s_tw, lane);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int kx = pos_to_k(spec_pos<N>(lane, j), N);
@@ -133,16 +123,22 @@ __device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int 
   }
 }
 
+template <typename R, int N>
+__device__ __forceinline__ void col_load_rhs(const cplx<R>* __restrict__ H, int b, int ch, int ky, int lane,
+                                             const cplx<R>* s_tw, cplx<R> (&v)[N / 32]) {
+  constexpr int K = (N - 1) / 3 + 1;
+  const cplx<R>* h0 = H + ((size_t)(b * NH + (ch == 0 ? 0 : 2)) * K + ky) * N;
+  col_rhs_rows<R, N>(h0, h0 + (size_t)K * N, ch, ky, lane, s_tw, v);
+}
+
 // Stage input x of channel c (bit-reversed slot order) -> its two uncurled
 // fields i (ky/k^2) x and i (-kx/k^2) x (mhd_jax.py:140-141) transformed along
 // x in lockstep, scaled by 1/n^2, to G fields 2c and 2c+1.
 template <typename R, int N>
-__device__ __forceinline__ void col_inverse_uv(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int b, int c,
-                                               int ky, int lane, const cplx<R>* s_tw) {
+__device__ __forceinline__ void col_uv_transform(const cplx<R> (&x)[N / 32], int ky, int lane, const cplx<R>* s_tw,
+                                                 cplx<R> (&wu)[N / 32], cplx<R> (&wv)[N / 32]) {
   constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
   const R inv_n2 = R(1) / (R(N) * R(N));
-  cplx<R> wu[E], wv[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const int kx = pos_to_k(spec_pos<N>(lane, j), N);
@@ -150,6 +146,57 @@ __device__ __forceinline__ void col_inverse_uv(const cplx<R> (&x)[N / 32], cplx<
     wv[j] = cscale(cimul(x[j], spectral_mu<R>(3, kx, ky)), inv_n2);
   }
   fft_dit2<R, N, true>(wu, wv, s_tw, lane);
+}
+
+// Cluster-resident passes (kernels_chain.cuh): a cluster of N / CX_XT CTAs holds
+// one state; CTA r keeps the G tile of physical rows x in [CX_XT r, CX_XT r + CX_XT)
+// (NG K rows of pitch CX_XT + 1, at the same shared-memory offset in every CTA).
+constexpr int CX_XT = 16;
+
+// The two G rows of col_inverse_uv written into the cluster's G tiles instead of
+// global memory: position x goes to CTA x / CX_XT, tile rows (2c) K + ky (u) and
+// (2c + 1) K + ky (v), column x % CX_XT.  `tile` is this CTA's tile.
+template <typename R, int N>
+__device__ __forceinline__ void col_uv_to_tiles(const cplx<R> (&wu)[N / 32], const cplx<R> (&wv)[N / 32],
+                                                cplx<R>* tile, int c, int ky, int lane) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int x = lane + 32 * j;
+    cplx<R>* t = cl.map_shared_rank(tile, (unsigned)(x / CX_XT));
+    t[((2 * c) * K + ky) * (CX_XT + 1) + x % CX_XT] = wu[j];
+    t[((2 * c + 1) * K + ky) * (CX_XT + 1) + x % CX_XT] = wv[j];
+  }
+}
+
+// The NH K rows of a row pass's H tile (pitch CX_XT + 1, physical rows x0 ..
+// x0 + CX_XT - 1) sent to the warps of the cluster that transform them: row
+// (f, ky) feeds column c = 2 ky + (f == 2) of the column passes, which warp
+// c / CL of CTA c % CL holds (CL = N / CX_XT CTAs) in its two rows of N at
+// hcols + (c / CL) 2 N: P1, P2 (channel 0), or P3 in the first (channel 1).
+template <typename R, int N>
+__device__ __forceinline__ void scatter_h_tile(const cplx<R>* s_H, cplx<R>* hcols, int x0) {
+  constexpr int K = (N - 1) / 3 + 1;
+  constexpr int CL = N / CX_XT;
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  for (int i = threadIdx.x; i < NH * K * CX_XT; i += blockDim.x) {
+    const int rr = i / CX_XT, xt = i - rr * CX_XT;
+    const int f = rr / K, ky = rr - f * K;
+    const int c = 2 * ky + (f == 2 ? 1 : 0);
+    cplx<R>* dst = cl.map_shared_rank(hcols, (unsigned)(c % CL));
+    dst[((c / CL) * 2 + (f == 2 ? 0 : f)) * N + x0 + xt] = s_H[rr * (CX_XT + 1) + xt];
+  }
+}
+
+template <typename R, int N>
+__device__ __forceinline__ void col_inverse_uv(const cplx<R> (&x)[N / 32], cplx<R>* __restrict__ G, int b, int c,
+                                               int ky, int lane, const cplx<R>* s_tw) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  cplx<R> wu[E], wv[E];
+  col_uv_transform<R, N>(x, ky, lane, s_tw, wu, wv);
   cplx<R>* gu = G + ((size_t)(b * NG + 2 * c) * K + ky) * N;
   cplx<R>* gv = gu + (size_t)K * N;
 #pragma unroll
@@ -225,9 +272,12 @@ template <int N, int STAGE> __host__ __device__ constexpr int col_rk4_nrl() {
 
 // One warp's column `colid` of a Lawson-RK4 column stage; my_c / my_e are the
 // warp's staging rows (col_rk4_nc complex and col_rk4_nrl real rows of M).
-template <typename R, int N, int STAGE>
+// CX (cluster-resident passes): product rows from `hrows`, inverse transforms
+// to the cluster's G tiles at `gtile` (null: global H / G), as col_tan_body.
+template <typename R, int N, int STAGE, bool CX = false>
 __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
-                                             cplx<R>* my_c, R* my_e) {
+                                             cplx<R>* my_c, R* my_e, const cplx<R>* hrows = nullptr,
+                                             cplx<R>* gtile = nullptr) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
@@ -249,7 +299,10 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
     }
   }
   cplx<R> r[E];
-  if (STAGE != COL_START) col_load_rhs<R, N>(p.H, b, c, ky, lane, s_tw, r);
+  if (STAGE != COL_START) {
+    if (CX && hrows) col_rhs_rows<R, N>(hrows, hrows + N, c, ky, lane, s_tw, r);
+    else col_load_rhs<R, N>(p.H, b, c, ky, lane, s_tw, r);
+  }
   if constexpr (STG) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
@@ -284,8 +337,8 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
         const R e = EV;
         cplx<R> k1 = cscale(v, h);
         put(Q_F, FV); put(Q_K1, k1);
-        const cplx<R> f = cscale(FV, e);
-        k1 = cscale(k1, e);
+        const cplx<R> f = cscale_rn(FV, e);
+        k1 = cscale_rn(k1, e);
         p.F[i] = f; p.A1[i] = k1;
         x[j] = cadd(f, cscale(k1, R(0.5)));
         put(Q_X2, x[j]);
@@ -300,8 +353,8 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
         const R e = EV;
         cplx<R> k3 = cscale(v, h);
         put(Q_K3, k3);
-        const cplx<R> f = cscale(FV, e), a = cscale(A1V, e), q2 = cscale(K2V, e);
-        k3 = cscale(k3, e);
+        const cplx<R> f = cscale_rn(FV, e), a = cscale_rn(A1V, e), q2 = cscale_rn(K2V, e);
+        k3 = cscale_rn(k3, e);
         x[j] = cadd(f, k3);
         put(Q_X4, x[j]);
         p.F[i] = cadd(cadd(cadd(f, cdiv_k<6>(a)), cdiv_k<3>(q2)), cdiv_k<3>(k3));
@@ -320,6 +373,14 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
     }
   }
   if (!p.produce) return;
+  if constexpr (CX) {
+    if (gtile) {
+      cplx<R> wu[E], wv[E];
+      col_uv_transform<R, N>(x, ky, lane, s_tw, wu, wv);
+      col_uv_to_tiles<R, N>(wu, wv, gtile, c, ky, lane);
+      return;
+    }
+  }
   col_inverse_uv<R, N>(x, p.G, b, c, ky, lane, s_tw);
 }
 
@@ -452,12 +513,14 @@ __device__ __forceinline__ void split_store(const cplx<R> (&W)[N / 32], cplx<R>*
 
 // Rows x0 .. x0 + XT - 1 of state b, one warp per row (the CTA's XT warps);
 // s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
-template <typename R, int N, int XT>
+// CX (cluster-resident passes, XT = CX_XT): s_G holds the tile unless load_g;
+// the H tile goes to the column warps' rows at `hcols` unless that is null.
+template <typename R, int N, int XT, bool CX = false>
 __device__ __forceinline__ void row_rhs_body(const RowParams<R>& p, int b, int x0, const cplx<R>* s_tw, cplx<R>* s_G,
-                                             cplx<R>* s_H) {
+                                             cplx<R>* s_H, bool load_g = true, cplx<R>* hcols = nullptr) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
+  if (!CX || load_g) load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 
@@ -480,13 +543,17 @@ __device__ __forceinline__ void row_rhs_body(const RowParams<R>& p, int b, int x
       const int e = lane + 32 * j;
       ph[e] = u; ph[N + e] = v; ph[2 * N + e] = bx; ph[3 * N + e] = by;
     }
-    W[j] = mk<R>((u - v) * (u + v) - (bx - by) * (bx + by), bx * by - u * v);   // (P1, P2)
-    bb[j] = mk<R>(u * by - v * bx, R(0));                                       // (P3, 0), mhd_jax.py:163
+    W[j] = mk<R>(fpm(u - v, u + v, bx - by, bx + by), fpm(bx, by, u, v));   // (P1, P2)
+    bb[j] = mk<R>(fpm(u, by, v, bx), R(0));                                // (P3, 0), mhd_jax.py:163
   }
   fft_dit2<R, N, false>(W, bb, s_tw, lane);
   split_store<R, N, XT>(W, s_H, s_H + K * (XT + 1), w, lane);
   store_one<R, N, XT>(bb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
+  if constexpr (CX) {
+    static_assert(!CX || XT == CX_XT, "cluster tiles are CX_XT rows");
+    if (hcols) { scatter_h_tile<R, N>(s_H, hcols, x0); return; }
+  }
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }
 

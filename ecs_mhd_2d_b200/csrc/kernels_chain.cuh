@@ -19,12 +19,22 @@
 // the warp's own box rows, so they follow each other without a barrier (a
 // __syncwarp orders the lanes' writes before the next pass's staged reads).
 // Between a column pass and a row pass the cluster synchronises with the
-// hardware cluster barrier (arrive.release / wait.acquire): the G and H
-// intermediate arrays stay in global memory (L2-resident at these sizes), and
-// the barrier's release/acquire makes one pass's writes visible to the next
-// pass's readers on the other SMs of the cluster.  The barrier is a hardware
-// barrier over CTAs that are co-scheduled by construction (a cluster), so no
-// wait in this kernel spins on memory.
+// hardware cluster barrier (arrive.release / wait.acquire), whose
+// release/acquire makes one pass's writes visible to the next pass's readers on
+// the other SMs of the cluster.  The barrier is a hardware barrier over CTAs
+// that are co-scheduled by construction (a cluster), so no wait in this kernel
+// spins on memory.
+//
+// The intermediate arrays between the passes travel one of two ways (template
+// flag DSM):
+//   * DSM = false: through global memory (G, H; L2-resident at these sizes);
+//   * DSM = true: through distributed shared memory -- a column pass writes its
+//     inverse transforms straight into the G tiles of the CTAs that own those
+//     physical rows (col_uv_to_tiles), and a row pass sends its H tile to the
+//     shared rows of the warps that transform those columns (scatter_h_tile),
+//     so neither array leaves the cluster.  The first pass of a launch reads and
+//     the last one writes global G / H, which carries the state from one launch
+//     to the next (a launch ends before a row pass, at a regeneration chunk).
 #pragma once
 
 #include "kernels_tan.cuh"
@@ -50,12 +60,28 @@ template <int N> __host__ __device__ constexpr int chain_colwarps() {
 }
 // Operand rows staged per column warp: the largest col_tan_nop over the adaptive stages.
 constexpr int CH_NOP = 8;
-template <typename R, int N> __host__ __device__ constexpr size_t chain_smem() {
-  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
-  constexpr size_t col = (size_t)chain_colwarps<N>() * CH_NOP * M;
-  constexpr size_t row = (size_t)(NG + NH) * K * (CH_WARPS + 1);
-  return (fft_smem(N, CH_WARPS) + (col > row ? col : row)) * sizeof(cplx<R>);
+static_assert(CH_WARPS == CX_XT, "row tiles of the cluster exchange");
+// Shared memory of a chain kernel with `stage` complex entries of column
+// staging per column warp: twiddles, then with DSM the G tile and the column
+// warps' H rows, then the column staging overlaid with the row tiles.
+template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t chain_smem_for(int stage) {
+  constexpr int K = (N - 1) / 3 + 1;
+  const size_t col = (size_t)chain_colwarps<N>() * stage;
+  const size_t row = (size_t)(DSM ? NH : NG + NH) * K * (CH_WARPS + 1);
+  const size_t xch = DSM ? (size_t)NG * K * (CH_WARPS + 1) + (size_t)chain_colwarps<N>() * 2 * N : 0;
+  return (fft_smem(N, CH_WARPS) + xch + (col > row ? col : row)) * sizeof(cplx<R>);
 }
+template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t chain_smem() {
+  return chain_smem_for<R, N, DSM>(CH_NOP * (2 * ((N - 1) / 3) + 1));
+}
+// Shared-memory regions of a chain kernel (offsets in complex entries).
+template <int N, bool DSM> struct ChainSmem {
+  static constexpr int K = (N - 1) / 3 + 1;
+  static constexpr int tw = 0;
+  static constexpr int gt = fft_smem(N, CH_WARPS);                               // G tile (DSM)
+  static constexpr int hc = gt + (DSM ? NG * K * (CH_WARPS + 1) : 0);            // column warps' H rows (DSM)
+  static constexpr int work = hc + (DSM ? chain_colwarps<N>() * 2 * N : 0);      // staging / row tiles
+};
 
 template <typename R>
 struct ChainParams {
@@ -72,9 +98,10 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;\n" ::: "memory");
 }
 
-template <typename R, int N>
+template <typename R, int N, bool DSM>
 __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp& op, int b, int rank, int w,
-                                          int lane, const cplx<R>* s_tw, cplx<R>* my_op) {
+                                          int lane, const cplx<R>* s_tw, cplx<R>* my_op, const cplx<R>* hrows,
+                                          cplx<R>* gtile) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
   constexpr int CL = chain_cl<N>();
@@ -95,19 +122,19 @@ __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp
     return;
   }
   switch (op.stage) {
-    case T43_START: col_tan_body<R, N, T43_START>(p, colid, lane, s_tw, my_op); break;
-    case T43_INIT: col_tan_body<R, N, T43_INIT>(p, colid, lane, s_tw, my_op); break;
-    case T43_A: col_tan_body<R, N, T43_A>(p, colid, lane, s_tw, my_op); break;
-    case T43_B: col_tan_body<R, N, T43_B>(p, colid, lane, s_tw, my_op); break;
-    case T43_C: col_tan_body<R, N, T43_C>(p, colid, lane, s_tw, my_op); break;
-    case T43_D: col_tan_body<R, N, T43_D>(p, colid, lane, s_tw, my_op); break;
-    case T43_EA: col_tan_body<R, N, T43_EA>(p, colid, lane, s_tw, my_op); break;
-    default: col_tan_body<R, N, T43_E>(p, colid, lane, s_tw, my_op); break;
+    case T43_START: col_tan_body<R, N, T43_START, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_INIT: col_tan_body<R, N, T43_INIT, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_A: col_tan_body<R, N, T43_A, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_B: col_tan_body<R, N, T43_B, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_C: col_tan_body<R, N, T43_C, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_D: col_tan_body<R, N, T43_D, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_EA: col_tan_body<R, N, T43_EA, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    default: col_tan_body<R, N, T43_E, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
   }
 }
 
 // Grid: B clusters of CL CTAs (cluster b = tangent b), CH_WARPS * 32 threads each.
-template <typename R, int N>
+template <typename R, int N, bool DSM>
 __global__ void __cluster_dims__(chain_cl<N>(), 1, 1) __launch_bounds__(CH_WARPS * 32, 1)
 k_tan_chain(ChainParams<R> P) {
   constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
@@ -115,15 +142,20 @@ k_tan_chain(ChainParams<R> P) {
   static_assert(N <= 128, "staged column operands need n <= 128");
   static_assert(col_tan_nop<N, T43_C>() <= CH_NOP && col_tan_nop<N, T43_EA>() <= CH_NOP &&
                 col_tan_nop<N, T43_A>() <= CH_NOP && col_tan_nop<N, T43_D>() <= CH_NOP, "staging rows");
+  using SM = ChainSmem<N, DSM>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_work = s_tw + fft_smem(N, CH_WARPS);
+  cplx<R>* s_base = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_tw = s_base + SM::tw;
+  cplx<R>* s_gt = s_base + SM::gt;
+  cplx<R>* s_hc = s_base + SM::hc;
+  cplx<R>* s_work = s_base + SM::work;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
+  const int wc = w < chain_colwarps<N>() ? w : 0;
   load_twiddles<R, N>(s_tw, P.col.tw);
   pdl_wait();   // launched with programmatic serialization: the predecessor's writes are visible past here
   __syncthreads();
-  cplx<R>* my_op = s_work + (size_t)(w < chain_colwarps<N>() ? w : 0) * CH_NOP * M;
+  cplx<R>* my_op = s_work + (size_t)wc * CH_NOP * M;
   int prev = -1;   // kind class of the previous pass: 0 column-like, 1 row
   for (int i = P.op0; i < P.op1; ++i) {
     const ChainOp op = P.ops[i];
@@ -131,14 +163,20 @@ k_tan_chain(ChainParams<R> P) {
     if (prev >= 0 && (cls != prev || cls == 1)) cluster_barrier();
     else if (prev >= 0) __syncwarp();
     prev = cls;
+    const bool first = i == P.op0, last = i == P.op1 - 1;   // global G / H at the launch's ends
     if (cls) {
       RowTanParams<R> rp = P.row;
       rp.phys = P.phys + (size_t)(op.item - P.item0) * N * NPH * N;
-      row_tan_body<R, N, CH_WARPS>(rp, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
+      if constexpr (DSM)
+        row_tan_body<R, N, CH_WARPS, true>(rp, b, rank * CH_WARPS, s_tw, s_gt, s_work, first, last ? nullptr : s_hc);
+      else
+        row_tan_body<R, N, CH_WARPS>(rp, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
     } else {
-      chain_col<R, N>(P, op, b, rank, w, lane, s_tw, my_op);
+      chain_col<R, N, DSM>(P, op, b, rank, w, lane, s_tw, my_op,
+                           (DSM && !first) ? s_hc + (size_t)wc * 2 * N : nullptr, (DSM && !last) ? s_gt : nullptr);
     }
   }
+  if constexpr (DSM) cluster_barrier();   // no CTA leaves while a peer may still write its shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -157,23 +195,24 @@ struct Rk4ChainParams {
   int last_produce;   // inverse transforms after the last stage (the next stage input)
 };
 
-template <typename R, int N> __host__ __device__ constexpr size_t rk4_chain_smem() {
-  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
-  // per column warp: 3 complex rows (F, A1, K2) and one real row (e), in complex units
-  constexpr size_t col = (size_t)chain_colwarps<N>() * 4 * M;
-  constexpr size_t row = (size_t)(NG + NH) * K * (CH_WARPS + 1);
-  return (fft_smem(N, CH_WARPS) + (col > row ? col : row)) * sizeof(cplx<R>);
+// per column warp: 3 complex rows (F, A1, K2) and one real row (e), in complex units
+template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t rk4_chain_smem() {
+  return chain_smem_for<R, N, DSM>(4 * (2 * ((N - 1) / 3) + 1));
 }
 
-template <typename R, int N>
+template <typename R, int N, bool DSM>
 __global__ void __cluster_dims__(chain_cl<N>(), 1, 1) __launch_bounds__(CH_WARPS * 32, 1)
 k_rk4_chain(Rk4ChainParams<R> P) {
   constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
   constexpr int CL = chain_cl<N>();
   static_assert(N <= 128, "staged column operands need n <= 128");
+  using SM = ChainSmem<N, DSM>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_work = s_tw + fft_smem(N, CH_WARPS);
+  cplx<R>* s_base = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_tw = s_base + SM::tw;
+  cplx<R>* s_gt = s_base + SM::gt;
+  cplx<R>* s_hc = s_base + SM::hc;
+  cplx<R>* s_work = s_base + SM::work;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
   const int cidx = w * CL + rank;   // this warp's column of the state
@@ -181,26 +220,33 @@ k_rk4_chain(Rk4ChainParams<R> P) {
   const int colid = b * 2 * K + cidx;
   cplx<R>* my_c = s_work + (size_t)(has_col ? w : 0) * 4 * M;
   R* my_e = reinterpret_cast<R*>(my_c + 3 * M);
+  const cplx<R>* my_h = DSM ? s_hc + (size_t)(has_col ? w : 0) * 2 * N : nullptr;
   load_twiddles<R, N>(s_tw, P.col.tw);
   pdl_wait();   // launched with programmatic serialization: the predecessor's writes are visible past here
   __syncthreads();
   for (long step = 0; step < P.steps; ++step) {
     for (int st = COL_RK4_S1; st <= COL_RK4_S4; ++st) {
       if (step > 0 || st > COL_RK4_S1) cluster_barrier();   // column pass -> row pass
-      row_rhs_body<R, N, CH_WARPS>(P.row, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
+      const bool first = step == 0 && st == COL_RK4_S1, last = step == P.steps - 1 && st == COL_RK4_S4;
+      if constexpr (DSM)
+        row_rhs_body<R, N, CH_WARPS, true>(P.row, b, rank * CH_WARPS, s_tw, s_gt, s_work, first, s_hc);
+      else
+        row_rhs_body<R, N, CH_WARPS>(P.row, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
       cluster_barrier();                                     // row pass -> column pass
       if (!has_col) continue;
       ColParams<R> p = P.col;
       p.stage = st;
-      p.produce = (st == COL_RK4_S4 && step == P.steps - 1) ? P.last_produce : 1;
+      p.produce = last ? P.last_produce : 1;
+      cplx<R>* gt = (DSM && !last) ? s_gt : nullptr;
       switch (st) {
-        case COL_RK4_S1: col_rk4_body<R, N, COL_RK4_S1>(p, colid, lane, s_tw, my_c, my_e); break;
-        case COL_RK4_S2: col_rk4_body<R, N, COL_RK4_S2>(p, colid, lane, s_tw, my_c, my_e); break;
-        case COL_RK4_S3: col_rk4_body<R, N, COL_RK4_S3>(p, colid, lane, s_tw, my_c, my_e); break;
-        default: col_rk4_body<R, N, COL_RK4_S4>(p, colid, lane, s_tw, my_c, my_e); break;
+        case COL_RK4_S1: col_rk4_body<R, N, COL_RK4_S1, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        case COL_RK4_S2: col_rk4_body<R, N, COL_RK4_S2, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        case COL_RK4_S3: col_rk4_body<R, N, COL_RK4_S3, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        default: col_rk4_body<R, N, COL_RK4_S4, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
       }
     }
   }
+  if constexpr (DSM) cluster_barrier();   // no CTA leaves while a peer may still write its shared memory
 }
 
 }  // namespace ecs

@@ -109,9 +109,13 @@ struct RowTanParams {
 
 // Rows x0 .. x0 + XT - 1 of tangent b, one warp per row (the CTA's XT warps);
 // s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
-template <typename R, int N, int XT>
+// CX (cluster-resident passes, XT = CX_XT): s_G already holds the tile (written
+// by the column pass) unless load_g, and the H tile goes to the column warps'
+// rows at `hcols` (scatter_h_tile) unless that is null (global H).
+template <typename R, int N, int XT, bool CX = false>
 __device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, int x0, const cplx<R>* s_tw,
-                                             cplx<R>* s_G, cplx<R>* s_H) {
+                                             cplx<R>* s_G, cplx<R>* s_H, bool load_g = true,
+                                             cplx<R>* hcols = nullptr) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -129,7 +133,7 @@ __device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, in
     }
   };
   if constexpr (N <= 128) load_phys();
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
+  if (!CX || load_g) load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, NG * K, x0);
   __syncthreads();
   cplx<R> duv[E], dbb[E];
 #pragma unroll
@@ -144,14 +148,18 @@ __device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, in
   for (int j = 0; j < E; ++j) {
     const R du = duv[j].x, dv = duv[j].y, dbx = dbb[j].x, dby = dbb[j].y;
     const R u = pu[j], v = pv[j], bx = pbx[j], by = pby[j];
-    duv[j] = mk<R>(R(2) * ((u * du - v * dv) - (bx * dbx - by * dby)),     // dP1
-                   (bx * dby + by * dbx) - (u * dv + v * du));              // dP2
-    dbb[j] = mk<R>((u * dby + by * du) - (v * dbx + bx * dv), R(0));        // dP3
+    duv[j] = mk<R>(R(2) * (fpm(u, du, v, dv) - fpm(bx, dbx, by, dby)),     // dP1
+                   fpp(bx, dby, by, dbx) - fpp(u, dv, v, du));              // dP2
+    dbb[j] = mk<R>(fpp(u, dby, by, du) - fpp(v, dbx, bx, dv), R(0));        // dP3
   }
   fft_dit2<R, N, false>(duv, dbb, s_tw, lane);
   split_store<R, N, XT>(duv, s_H, s_H + K * (XT + 1), w, lane);
   store_one<R, N, XT>(dbb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
+  if constexpr (CX) {
+    static_assert(!CX || XT == CX_XT, "cluster tiles are CX_XT rows");
+    if (hcols) { scatter_h_tile<R, N>(s_H, hcols, x0); return; }
+  }
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }
 
@@ -240,9 +248,14 @@ template <int N, int STAGE> __host__ __device__ constexpr int col_tan_nop() {
 
 // One warp's column `colid` of a tangent column stage; `my_op` is the warp's
 // staging buffer (col_tan_nop rows of M entries), `s_tw` the twiddle image.
-template <typename R, int N, int STAGE>
+// CX (cluster-resident passes): the product rows come from `hrows` (the warp's
+// rows in shared memory, see scatter_h_tile) and the inverse transforms go to
+// the cluster's G tiles at `gtile` (col_uv_to_tiles); a null pointer selects
+// global H / G instead.
+template <typename R, int N, int STAGE, bool CX = false>
 __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
-                                             cplx<R>* my_op) {
+                                             cplx<R>* my_op, const cplx<R>* hrows = nullptr,
+                                             cplx<R>* gtile = nullptr) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
@@ -288,7 +301,10 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
     }
   }
   cplx<R> r[E];
-  if (has_rhs) col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
+  if (has_rhs) {
+    if (CX && hrows) col_rhs_rows<R, N>(hrows, hrows + N, ch, ky, lane, s_tw, r);
+    else col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
+  }
   if constexpr (NOP > 0) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
@@ -311,13 +327,13 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
       // Lawson-RK4: e = exp(h/2 L) mask, de = e L dh/2; dk = dh v + h dv with v = k/h
       const R e = p.etab ? p.etab[(size_t)b * VEC + o] : in_mask ? exp(h / R(2) * L) : R(0);
       const R de = e * L * (dpar / R(2));
-      auto dk_of = [&](int q) { return cadd(cscale(Q[q * VEC + o], dpar / h), cscale(dv, h)); };
+      auto dk_of = [&](int q) { return lin2_rn(Q[q * VEC + o], dpar / h, dv, h); };
       switch (STAGE) {
         case TS_START: xin = D[D_F * VEC + o]; break;
         case T4_S1: {
           const cplx<R> dk1 = dk_of(Q_K1);
-          const cplx<R> df1 = cadd(cscale(Q[Q_F * VEC + o], de), cscale(D[D_F * VEC + o], e));
-          const cplx<R> da1 = cadd(cscale(Q[Q_K1 * VEC + o], de), cscale(dk1, e));
+          const cplx<R> df1 = lin2_rn(Q[Q_F * VEC + o], de, D[D_F * VEC + o], e);
+          const cplx<R> da1 = lin2_rn(Q[Q_K1 * VEC + o], de, dk1, e);
           D[D_F * VEC + o] = df1; D[D_A1 * VEC + o] = da1;
           xin = cadd(df1, cscale(da1, R(0.5)));
         } break;
@@ -328,11 +344,11 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
         } break;
         case T4_S3: {
           const cplx<R> dk3 = dk_of(Q_K3);
-          const cplx<R> f1 = cscale(Q[Q_F * VEC + o], e), a1 = cscale(Q[Q_K1 * VEC + o], e);
-          const cplx<R> df2 = cadd(cscale(f1, de), cscale(D[D_F * VEC + o], e));
-          const cplx<R> db1 = cadd(cscale(a1, de), cscale(D[D_A1 * VEC + o], e));
-          const cplx<R> db2 = cadd(cscale(Q[Q_K2 * VEC + o], de), cscale(D[D_K2 * VEC + o], e));
-          const cplx<R> db3 = cadd(cscale(Q[Q_K3 * VEC + o], de), cscale(dk3, e));
+          const cplx<R> f1 = cscale_rn(Q[Q_F * VEC + o], e), a1 = cscale_rn(Q[Q_K1 * VEC + o], e);
+          const cplx<R> df2 = lin2_rn(f1, de, D[D_F * VEC + o], e);
+          const cplx<R> db1 = lin2_rn(a1, de, D[D_A1 * VEC + o], e);
+          const cplx<R> db2 = lin2_rn(Q[Q_K2 * VEC + o], de, D[D_K2 * VEC + o], e);
+          const cplx<R> db3 = lin2_rn(Q[Q_K3 * VEC + o], de, dk3, e);
           xin = cadd(df2, db3);
           D[D_F * VEC + o] = cadd(cadd(cadd(df2, cdiv_k<6>(db1)), cdiv_k<3>(db2)), cdiv_k<3>(db3));
         } break;
@@ -361,7 +377,7 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
         if constexpr (NOP > 0) return my_op[(NQ + NQ2 + popc_c(DM & ((1u << d) - 1u))) * M + slot];
         else return D[d * VEC + o];
       };
-      auto dk_of = [&](int q) { return cadd(cscale(QV(q), dpar / t), cscale(dv, t)); };
+      auto dk_of = [&](int q) { return lin2_rn(QV(q), dpar / t, dv, t); };
       // the A and E algebra, written with explicitly rounded operations: the
       // merged pass T43_EA computes exactly what T43_E followed by T43_A does
       auto stage_e = [&]() { return lin2_rn(QV(RR_K5), dpar / t, dv, t); };   // dk5
@@ -384,19 +400,19 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
         } break;
         case T43_C: {
           const cplx<R> dk3 = dk_of(RR_K3);
-          const cplx<R> xe = cscale(QV(RR_X0), e), k1e = cscale(QV(RR_K1), e);
-          const cplx<R> dx2 = cadd(cscale(xe, de), cscale(DV(S_XE), e));
-          const cplx<R> dk1ee = cadd(cscale(k1e, de), cscale(DV(S_K1E), e));
-          const cplx<R> dk2e = cadd(cscale(QV(RR_K2), de), cscale(DV(S_K2), e));
-          const cplx<R> dk3e = cadd(cscale(QV(RR_K3), de), cscale(dk3, e));
+          const cplx<R> xe = cscale_rn(QV(RR_X0), e), k1e = cscale_rn(QV(RR_K1), e);
+          const cplx<R> dx2 = lin2_rn(xe, de, DV(S_XE), e);
+          const cplx<R> dk1ee = lin2_rn(k1e, de, DV(S_K1E), e);
+          const cplx<R> dk2e = lin2_rn(QV(RR_K2), de, DV(S_K2), e);
+          const cplx<R> dk3e = lin2_rn(QV(RR_K3), de, dk3, e);
           D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
-          xin = cadd(dx2, cscale(dk3e, h));
+          xin = cadd_scaled_rn(dx2, dk3e, h);
         } break;
         case T43_D: {
           const cplx<R> dk4 = dk_of(RR_K4);
           const cplx<R> acc = cadd(cadd(cadd(cdiv_k<6>(DV(S_K1)), cdiv_k<3>(DV(S_K2))),
                                         cdiv_k<3>(DV(S_K3))), cdiv_k<6>(dk4));
-          xin = cadd(DV(S_X2), cscale(acc, h));
+          xin = cadd_scaled_rn(DV(S_X2), acc, h);
           D[S_XF * VEC + o] = xin;
         } break;
         case T43_E: {   // accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
@@ -414,6 +430,14 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
     x[j] = xin;
   }
   if (!p.produce || STAGE == T43_INIT || STAGE == T43_E) return;
+  if constexpr (CX) {
+    if (gtile) {
+      cplx<R> wu[E], wv[E];
+      col_uv_transform<R, N>(x, ky, lane, s_tw, wu, wv);
+      col_uv_to_tiles<R, N>(wu, wv, gtile, ch, ky, lane);
+      return;
+    }
+  }
   col_inverse_uv<R, N>(x, p.G, b, ch, ky, lane, s_tw);
 }
 
@@ -442,9 +466,9 @@ __device__ __forceinline__ void tan_reject_at(cplx<R>* Db, const cplx<R>* rec, s
   const R e = eg.x;
   const R de = eg.y * dpar;
   const cplx<R> k1 = rec[RR_K1 * VEC + o];
-  const cplx<R> k1e = cscale(k1, e);
-  const cplx<R> dk1e = cadd(cscale(k1, de), cscale(Db[S_K1 * VEC + o], e));
-  Db[S_K1 * VEC + o] = cadd(cscale(k1e, de), cscale(dk1e, e));
+  const cplx<R> k1e = cscale_rn(k1, e);
+  const cplx<R> dk1e = lin2_rn(k1, de, Db[S_K1 * VEC + o], e);
+  Db[S_K1 * VEC + o] = lin2_rn(k1e, de, dk1e, e);
 }
 
 template <typename R>

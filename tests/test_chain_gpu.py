@@ -4,7 +4,9 @@ rejected attempts) against the launch-per-pass sweep (ECS_CHAIN_MAXB=0).  Both
 run the same per-column and per-row bodies in the same order, so the JVP of
 objective_RPO (jax.jvp at jax_scripts/lib/utils.py:108) is equal bit for bit:
 with rejected attempts, with regeneration-chunk boundaries inside the list
-(ECS_REGEN_ITEMS), for one and for several tangents, at n = 64 and 128."""
+(ECS_REGEN_ITEMS), for one and for several tangents, at n = 64 and 128, with
+the passes exchanging their intermediate arrays through distributed shared
+memory (the default) and through global memory (ECS_CHAIN_DSMEM=0)."""
 import numpy as np
 import pytest
 import torch
@@ -27,8 +29,8 @@ CASES = [   # (n, B, T, atol, amp, env)
 ]
 
 
-def _run(n, B, T, atol, amp, env, monkeypatch, chain):
-    env = dict(env)
+def _run(n, B, T, atol, amp, env, monkeypatch, chain, dsm=1):
+    env = dict(env, ECS_CHAIN_DSMEM=str(dsm))
     seed = env.pop("seed", 4)
     cap = (64, 64) if seed == 0 else (4, 64)
     for k, v in env.items():
@@ -64,12 +66,13 @@ def _run(n, B, T, atol, amp, env, monkeypatch, chain):
 @pytest.mark.parametrize("n,B,T,atol,amp,env", CASES)
 def test_chain_equals_launch_per_pass(cuda, monkeypatch, n, B, T, atol, amp, env):
     want, info, per_pass = _run(n, B, T, atol, amp, env, monkeypatch, chain=False)
-    got, info2, chained = _run(n, B, T, atol, amp, env, monkeypatch, chain=True)
-    assert info == info2
-    for k in ("fields", "T", "sx"):
-        assert torch.equal(got[k], want[k]), k
-    # the pass list ran as a handful of launches instead of one per pass
-    assert chained < per_pass // 4, (chained, per_pass)
+    for dsm in (1, 0):
+        got, info2, chained = _run(n, B, T, atol, amp, env, monkeypatch, chain=True, dsm=dsm)
+        assert info == info2
+        for k in ("fields", "T", "sx"):
+            assert torch.equal(got[k], want[k]), (k, dsm)
+        # the pass list ran as a handful of launches instead of one per pass
+        assert chained < per_pass // 4, (chained, per_pass)
 
 
 def test_chain_covers_rejected_attempts(cuda, monkeypatch):
@@ -82,7 +85,8 @@ def test_chain_covers_rejected_attempts(cuda, monkeypatch):
 RK4_CASES = [(64, 1, 5), (64, 8, 40), (128, 1, 37), (128, 3, 16)]   # (n, B, steps)
 
 
-def _rk4(n, B, steps, monkeypatch, chain):
+def _rk4(n, B, steps, monkeypatch, chain, dsm=1):
+    monkeypatch.setenv("ECS_CHAIN_DSMEM", str(dsm))
     if chain:
         monkeypatch.delenv("ECS_RK4CHAIN_MAXB", raising=False)
     else:
@@ -113,7 +117,8 @@ def test_rk4_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, steps):
     """Lawson-RK4 stepping as one cluster-resident launch (k_rk4_chain) equals
     the launch-per-stage stepping (graphs of k_row_rhs / k_col_rk4) bit for bit."""
     want, want_obj, per_stage = _rk4(n, B, steps, monkeypatch, chain=False)
-    got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True)
-    assert torch.equal(got, want)
-    assert torch.equal(got_obj, want_obj)
-    assert chained < per_stage
+    for dsm in (1, 0):
+        got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True, dsm=dsm)
+        assert torch.equal(got, want), dsm
+        assert torch.equal(got_obj, want_obj), dsm
+        assert chained < per_stage
