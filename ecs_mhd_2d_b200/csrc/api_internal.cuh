@@ -41,8 +41,12 @@ struct ecs_ctx {
   int plain_order = 0;              // depth of PlainOrder scopes (no programmatic launch below batch 8)
   int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)
   int regen_items = 0;              // stage inputs per regeneration chunk (ECS_REGEN_ITEMS, at least 8; 0: about 384 MiB)
+  int rk4chain_minb = 1;            // smallest batch of Lawson-RK4 stepping run as one cluster-resident launch (ECS_RK4CHAIN_MINB)
   int rk4chain_maxb = 8;            // largest batch of Lawson-RK4 stepping run as one cluster-resident launch (ECS_RK4CHAIN_MAXB; 0: graphs of launches)
+  int chain_w = 8;                  // warps per CTA of the chain kernels: 8 (clusters of n / 8 CTAs) or 16 (ECS_CHAIN_WARPS; 16 where 8 does not fit)
+  int chain_resident = 0;           // clusters of the chain kernel the device holds at once
   int chain_dsm = 1;                // the cluster-resident passes exchange G / H through distributed shared memory (ECS_CHAIN_DSMEM=0: through global memory)
+  int chain_minb = 1;               // smallest batch of the adaptive tangent sweep run as one cluster-resident pass list (ECS_CHAIN_MINB)
   int chain_maxb = 64;              // largest batch of the adaptive tangent sweep run as one cluster-resident pass list (ECS_CHAIN_MAXB; 0: launch per pass)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {

@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 #include <utility>
+#include <type_traits>
 #include <mutex>
 
 // ---------------------------------------------------------------------------
@@ -62,6 +63,23 @@ inline void launch_step(ecs_ctx* c, int B, void (*k)(P...), dim3 grid, dim3 bloc
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+// launch_step for a kernel launched as clusters of `cl` CTAs along x.
+template <typename... P, typename... A>
+inline void launch_cluster(ecs_ctx* c, int B, int cl, void (*k)(P...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t s, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  const bool plain = c->plain_order > 0 && B < 8;
+  cfg.attrs = at; cfg.numAttrs = (c->pdl && B >= c->pdl_minb && !plain) ? 2 : 1;
+  ++c->launches;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Scope in which batches below 8 launch without programmatic dependent launch:
 // the adaptive Lawson-RK4(3) solve and the fixed-step integrations measured
 // 5-10% slower with it at batch 1, and the batch-1 primal that runs beside the
@@ -74,6 +92,38 @@ struct PlainOrder {
   PlainOrder(const PlainOrder&) = delete;
   PlainOrder& operator=(const PlainOrder&) = delete;
 };
+
+template <typename R, int N, int W>
+int configure_chain() {
+  int st = 0;
+  auto attrs = [&](auto* k, size_t smem) {
+    st |= (int)cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (chain_cl<N, W>() > 8) st |= (int)cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  };
+  attrs(k_tan_chain<R, N, W, false>, chain_smem<R, N, W, false>());
+  attrs(k_tan_chain<R, N, W, true>, chain_smem<R, N, W, true>());
+  attrs(k_rk4_chain<R, N, W, false>, rk4_chain_smem<R, N, W, false>());
+  attrs(k_rk4_chain<R, N, W, true>, rk4_chain_smem<R, N, W, true>());
+  return st;
+}
+
+// Clusters of the W-warp tangent chain kernel (DSMEM exchange, its largest
+// shared memory) that the device holds at once; 0 if it cannot hold one.
+template <typename R, int N, int W>
+int chain_clusters() {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(chain_cl<N, W>()); cfg.blockDim = dim3(W * 32); cfg.dynamicSmemBytes = chain_smem<R, N, W, true>();
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)chain_cl<N, W>(); at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  cfg.attrs = at; cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_tan_chain<R, N, W, true>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 
 template <typename R, int N>
 int configure_kernels(ecs_ctx* c) {
@@ -93,16 +143,20 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, 4>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   if constexpr (N <= 128) {
-    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N, false>());
-    st |= (int)cudaFuncSetAttribute(k_tan_chain<R, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chain_smem<R, N, true>());
-  }
-  if constexpr (N <= 128) {
-    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N, false>());
-    st |= (int)cudaFuncSetAttribute(k_rk4_chain<R, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk4_chain_smem<R, N, true>());
+    st |= configure_chain<R, N, 8>();
+    st |= configure_chain<R, N, 16>();
   }
   if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
+  if constexpr (N <= 128) {
+    // the chain kernels' CTA shape: 8 warps (clusters of N / 8 CTAs, non-portable
+    // above 8) when the device can hold such a cluster, else 16 warps
+    if (c->chain_w == 8 && chain_clusters<R, N, 8>() < 1) c->chain_w = 16;
+    c->chain_resident = c->chain_w == 8 ? chain_clusters<R, N, 8>() : chain_clusters<R, N, 16>();
+  }
   return ECS_OK;
 }
+
+
 
 template <typename R, int N>
 void launch_row_to_box(ecs_ctx* c, const R* fields, cplx<R>* H, int B, cudaStream_t s) {
@@ -415,6 +469,17 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "state_vel");
   }
 
+  // Calls go(W, DSM) with the context's chain shape and exchange as constants.
+  template <typename F> static void chain_dispatch(const ecs_ctx* c, F&& go) {
+    using W8 = std::integral_constant<int, 8>;
+    using W16 = std::integral_constant<int, 16>;
+    if (c->chain_w == 8) {
+      if (c->chain_dsm) go(W8{}, std::true_type{}); else go(W8{}, std::false_type{});
+    } else {
+      if (c->chain_dsm) go(W16{}, std::true_type{}); else go(W16{}, std::false_type{});
+    }
+  }
+
   // Lawson-RK4 steps of the box states in c->F as one cluster-resident launch
   // (k_rk4_chain), after the COL_START pass; no inverse transforms after the last stage.
   static int rk4_chain(ecs_ctx* c, int B, long steps, cudaStream_t s) {
@@ -429,10 +494,13 @@ struct Impl {
       q.G = (const cplx<R>*)c->G; q.H = (cplx<R>*)c->H; q.tw = (const cplx<R>*)c->tw;
       q.b0x = (R)c->b0x; q.b0y = (R)c->b0y; q.B = B;
       P.steps = steps; P.last_produce = 0;
-      if (c->chain_dsm)
-        launch_step(c, B, k_rk4_chain<R, N, true>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N, true>(), s, P);
-      else
-        launch_step(c, B, k_rk4_chain<R, N, false>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), rk4_chain_smem<R, N, false>(), s, P);
+      auto go = [&](auto w, auto dsm) {
+        constexpr int W = decltype(w)::value;
+        constexpr bool DSM = decltype(dsm)::value;
+        launch_cluster(c, B, chain_cl<N, W>(), k_rk4_chain<R, N, W, DSM>, dim3(B * chain_cl<N, W>()), dim3(W * 32),
+                       rk4_chain_smem<R, N, W, DSM>(), s, P);
+      };
+      chain_dispatch(c, go);
       return cuda_err(c, cudaGetLastError(), "rk4 chain");
     } else {
       (void)B; (void)steps; (void)s;
@@ -442,7 +510,7 @@ struct Impl {
 
   // Lawson-RK4 over `steps` steps of the box state in c->F (ctl/Etab prepared).
   // Chunks of GS steps are captured once into a CUDA graph and replayed; batches
-  // up to c->rk4chain_maxb at n <= 128 run as one cluster-resident launch.
+  // from c->rk4chain_minb to c->rk4chain_maxb at n <= 128 run as one cluster-resident launch.
   static int integrate_rk4(ecs_ctx* c, int B, long steps, cudaStream_t s) {
     if (steps <= 0) return ECS_OK;
     constexpr int GS = 16;
@@ -471,7 +539,7 @@ struct Impl {
       gk.B = B;
     }
     launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
-    if (N <= 128 && B <= c->rk4chain_maxb) return rk4_chain(c, B, steps, s);
+    if (N <= 128 && B >= c->rk4chain_minb && B <= c->rk4chain_maxb) return rk4_chain(c, B, steps, s);
     long it = 0;
     while (steps - it > GS) {   // the final step (no inverse transforms) is launched directly
       cudaError_t e = cudaGraphLaunch(gk.exec, s);
@@ -1313,8 +1381,8 @@ struct Impl {
   }
 
   // Batches that the adaptive tangent sweep runs through the cluster-resident
-  // pass list (k_tan_chain): n <= 128, batch up to c->chain_maxb.
-  static bool use_chain(const ecs_ctx* c, int B) { return N <= 128 && B <= c->chain_maxb; }
+  // pass list (k_tan_chain): n <= 128, batch from c->chain_minb to c->chain_maxb.
+  static bool use_chain(const ecs_ctx* c, int B) { return N <= 128 && B >= c->chain_minb && B <= c->chain_maxb; }
 
   // The pass list through k_tan_chain: one launch per regeneration chunk (the
   // row passes of a launch read the chunk's physical fields), with the chunk's
@@ -1342,10 +1410,13 @@ struct Impl {
         if (end <= start) return;
         P.op0 = (int)start; P.op1 = (int)end;
         P.phys = (const R*)c->Phys; P.item0 = chunk_lo < 0 ? 0 : chunk_lo;
-        if (c->chain_dsm)
-          launch_step(c, B, k_tan_chain<R, N, true>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N, true>(), s, P);
-        else
-          launch_step(c, B, k_tan_chain<R, N, false>, dim3(B * chain_cl<N>()), dim3(CH_WARPS * 32), chain_smem<R, N, false>(), s, P);
+        auto go = [&](auto w, auto dsm) {
+          constexpr int W = decltype(w)::value;
+          constexpr bool DSM = decltype(dsm)::value;
+          launch_cluster(c, B, chain_cl<N, W>(), k_tan_chain<R, N, W, DSM>, dim3(B * chain_cl<N, W>()), dim3(W * 32),
+                         chain_smem<R, N, W, DSM>(), s, P);
+        };
+        chain_dispatch(c, go);
         start = end;
       };
       for (size_t i = 0; i < ops.size(); ++i) {

@@ -148,15 +148,14 @@ __device__ __forceinline__ void col_uv_transform(const cplx<R> (&x)[N / 32], int
   fft_dit2<R, N, true>(wu, wv, s_tw, lane);
 }
 
-// Cluster-resident passes (kernels_chain.cuh): a cluster of N / CX_XT CTAs holds
-// one state; CTA r keeps the G tile of physical rows x in [CX_XT r, CX_XT r + CX_XT)
-// (NG K rows of pitch CX_XT + 1, at the same shared-memory offset in every CTA).
-constexpr int CX_XT = 16;
+// Cluster-resident passes (kernels_chain.cuh): a cluster of N / XT CTAs holds
+// one state; CTA r keeps the G tile of physical rows x in [XT r, XT r + XT)
+// (NG K rows of pitch XT + 1, at the same shared-memory offset in every CTA).
 
 // The two G rows of col_inverse_uv written into the cluster's G tiles instead of
-// global memory: position x goes to CTA x / CX_XT, tile rows (2c) K + ky (u) and
-// (2c + 1) K + ky (v), column x % CX_XT.  `tile` is this CTA's tile.
-template <typename R, int N>
+// global memory: position x goes to CTA x / XT, tile rows (2c) K + ky (u) and
+// (2c + 1) K + ky (v), column x % XT.  `tile` is this CTA's tile.
+template <typename R, int N, int XT>
 __device__ __forceinline__ void col_uv_to_tiles(const cplx<R> (&wu)[N / 32], const cplx<R> (&wv)[N / 32],
                                                 cplx<R>* tile, int c, int ky, int lane) {
   constexpr int E = N / 32;
@@ -165,28 +164,28 @@ __device__ __forceinline__ void col_uv_to_tiles(const cplx<R> (&wu)[N / 32], con
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     const int x = lane + 32 * j;
-    cplx<R>* t = cl.map_shared_rank(tile, (unsigned)(x / CX_XT));
-    t[((2 * c) * K + ky) * (CX_XT + 1) + x % CX_XT] = wu[j];
-    t[((2 * c + 1) * K + ky) * (CX_XT + 1) + x % CX_XT] = wv[j];
+    cplx<R>* t = cl.map_shared_rank(tile, (unsigned)(x / XT));
+    t[((2 * c) * K + ky) * (XT + 1) + x % XT] = wu[j];
+    t[((2 * c + 1) * K + ky) * (XT + 1) + x % XT] = wv[j];
   }
 }
 
-// The NH K rows of a row pass's H tile (pitch CX_XT + 1, physical rows x0 ..
-// x0 + CX_XT - 1) sent to the warps of the cluster that transform them: row
+// The NH K rows of a row pass's H tile (pitch XT + 1, physical rows x0 ..
+// x0 + XT - 1) sent to the warps of the cluster that transform them: row
 // (f, ky) feeds column c = 2 ky + (f == 2) of the column passes, which warp
-// c / CL of CTA c % CL holds (CL = N / CX_XT CTAs) in its two rows of N at
+// c / CL of CTA c % CL holds (CL = N / XT CTAs) in its two rows of N at
 // hcols + (c / CL) 2 N: P1, P2 (channel 0), or P3 in the first (channel 1).
-template <typename R, int N>
+template <typename R, int N, int XT>
 __device__ __forceinline__ void scatter_h_tile(const cplx<R>* s_H, cplx<R>* hcols, int x0) {
   constexpr int K = (N - 1) / 3 + 1;
-  constexpr int CL = N / CX_XT;
+  constexpr int CL = N / XT;
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-  for (int i = threadIdx.x; i < NH * K * CX_XT; i += blockDim.x) {
-    const int rr = i / CX_XT, xt = i - rr * CX_XT;
+  for (int i = threadIdx.x; i < NH * K * XT; i += blockDim.x) {
+    const int rr = i / XT, xt = i - rr * XT;
     const int f = rr / K, ky = rr - f * K;
     const int c = 2 * ky + (f == 2 ? 1 : 0);
     cplx<R>* dst = cl.map_shared_rank(hcols, (unsigned)(c % CL));
-    dst[((c / CL) * 2 + (f == 2 ? 0 : f)) * N + x0 + xt] = s_H[rr * (CX_XT + 1) + xt];
+    dst[((c / CL) * 2 + (f == 2 ? 0 : f)) * N + x0 + xt] = s_H[rr * (XT + 1) + xt];
   }
 }
 
@@ -272,9 +271,10 @@ template <int N, int STAGE> __host__ __device__ constexpr int col_rk4_nrl() {
 
 // One warp's column `colid` of a Lawson-RK4 column stage; my_c / my_e are the
 // warp's staging rows (col_rk4_nc complex and col_rk4_nrl real rows of M).
-// CX (cluster-resident passes): product rows from `hrows`, inverse transforms
-// to the cluster's G tiles at `gtile` (null: global H / G), as col_tan_body.
-template <typename R, int N, int STAGE, bool CX = false>
+// CX > 0 (cluster-resident passes with CX-row tiles): product rows from
+// `hrows`, inverse transforms to the cluster's G tiles at `gtile` (null:
+// global H / G), as col_tan_body.
+template <typename R, int N, int STAGE, int CX = 0>
 __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
                                              cplx<R>* my_c, R* my_e, const cplx<R>* hrows = nullptr,
                                              cplx<R>* gtile = nullptr) {
@@ -300,7 +300,7 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
   }
   cplx<R> r[E];
   if (STAGE != COL_START) {
-    if (CX && hrows) col_rhs_rows<R, N>(hrows, hrows + N, c, ky, lane, s_tw, r);
+    if (CX > 0 && hrows) col_rhs_rows<R, N>(hrows, hrows + N, c, ky, lane, s_tw, r);
     else col_load_rhs<R, N>(p.H, b, c, ky, lane, s_tw, r);
   }
   if constexpr (STG) {
@@ -373,11 +373,11 @@ __device__ __forceinline__ void col_rk4_body(const ColParams<R>& p, int colid, i
     }
   }
   if (!p.produce) return;
-  if constexpr (CX) {
+  if constexpr (CX > 0) {
     if (gtile) {
       cplx<R> wu[E], wv[E];
       col_uv_transform<R, N>(x, ky, lane, s_tw, wu, wv);
-      col_uv_to_tiles<R, N>(wu, wv, gtile, c, ky, lane);
+      col_uv_to_tiles<R, N, CX>(wu, wv, gtile, c, ky, lane);
       return;
     }
   }
@@ -513,8 +513,8 @@ __device__ __forceinline__ void split_store(const cplx<R> (&W)[N / 32], cplx<R>*
 
 // Rows x0 .. x0 + XT - 1 of state b, one warp per row (the CTA's XT warps);
 // s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
-// CX (cluster-resident passes, XT = CX_XT): s_G holds the tile unless load_g;
-// the H tile goes to the column warps' rows at `hcols` unless that is null.
+// CX (cluster-resident passes): s_G holds the tile unless load_g; the H tile
+// goes to the column warps' rows at `hcols` unless that is null.
 template <typename R, int N, int XT, bool CX = false>
 __device__ __forceinline__ void row_rhs_body(const RowParams<R>& p, int b, int x0, const cplx<R>* s_tw, cplx<R>* s_G,
                                              cplx<R>* s_H, bool load_g = true, cplx<R>* hcols = nullptr) {
@@ -551,8 +551,7 @@ __device__ __forceinline__ void row_rhs_body(const RowParams<R>& p, int b, int x
   store_one<R, N, XT>(bb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
   if constexpr (CX) {
-    static_assert(!CX || XT == CX_XT, "cluster tiles are CX_XT rows");
-    if (hcols) { scatter_h_tile<R, N>(s_H, hcols, x0); return; }
+    if (hcols) { scatter_h_tile<R, N, XT>(s_H, hcols, x0); return; }
   }
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }

@@ -6,13 +6,15 @@
 // (reference: jax.jvp of objective_RPO, jax_scripts/lib/utils.py:108, through
 // the adaptive stepper of jax_scripts/lib/timestepping.py:151-335).
 //
-// One thread-block cluster of CL = N / 16 CTAs of 16 warps serves one tangent:
+// One thread-block cluster of CL = N / W CTAs of W warps serves one tangent
+// (W = 16: 8 CTAs at n = 128, a portable cluster; W = 8: 16 CTAs, half the
+// warps per SM and no register cap below 255):
 //   * a column pass gives each warp fixed columns (ky, channel) of the box --
 //     column c of tangent b on warp c / CL of CTA c % CL -- and runs the same
 //     per-column body as k_col_tan (col_tan_body), so the arithmetic and the
 //     rounding are those of the launch-per-pass sweep;
-//   * a row pass gives CTA r the 16 physical rows 16 r .. 16 r + 15, one warp
-//     per row, and runs k_row_tan's body (row_tan_body) with 16-row tiles;
+//   * a row pass gives CTA r the W physical rows W r .. W r + W - 1, one warp
+//     per row, and runs k_row_tan's body (row_tan_body) with W-row tiles;
 //   * a rejected attempt updates the tangent's carried k1 column by column on
 //     the same warps as the column passes (tan_reject_at).
 // Consecutive passes of the same kind (column stages and rejects) touch only
@@ -52,35 +54,34 @@ struct ChainOp {
   double h;
 };
 
-constexpr int CH_WARPS = 16;   // warps per CTA = physical rows per CTA in a row pass
-template <int N> __host__ __device__ constexpr int chain_cl() { return N / CH_WARPS; }
+// W warps per CTA = physical rows per CTA in a row pass; CL = N / W CTAs per cluster.
+template <int N, int W> __host__ __device__ constexpr int chain_cl() { return N / W; }
 // Warps per CTA that own columns in the column passes (2 K columns over CL CTAs).
-template <int N> __host__ __device__ constexpr int chain_colwarps() {
-  return (2 * ((N - 1) / 3 + 1) + chain_cl<N>() - 1) / chain_cl<N>();
+template <int N, int W> __host__ __device__ constexpr int chain_colwarps() {
+  return (2 * ((N - 1) / 3 + 1) + chain_cl<N, W>() - 1) / chain_cl<N, W>();
 }
 // Operand rows staged per column warp: the largest col_tan_nop over the adaptive stages.
 constexpr int CH_NOP = 8;
-static_assert(CH_WARPS == CX_XT, "row tiles of the cluster exchange");
 // Shared memory of a chain kernel with `stage` complex entries of column
 // staging per column warp: twiddles, then with DSM the G tile and the column
 // warps' H rows, then the column staging overlaid with the row tiles.
-template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t chain_smem_for(int stage) {
+template <typename R, int N, int W, bool DSM> __host__ __device__ constexpr size_t chain_smem_for(int stage) {
   constexpr int K = (N - 1) / 3 + 1;
-  const size_t col = (size_t)chain_colwarps<N>() * stage;
-  const size_t row = (size_t)(DSM ? NH : NG + NH) * K * (CH_WARPS + 1);
-  const size_t xch = DSM ? (size_t)NG * K * (CH_WARPS + 1) + (size_t)chain_colwarps<N>() * 2 * N : 0;
-  return (fft_smem(N, CH_WARPS) + xch + (col > row ? col : row)) * sizeof(cplx<R>);
+  const size_t col = (size_t)chain_colwarps<N, W>() * stage;
+  const size_t row = (size_t)(DSM ? NH : NG + NH) * K * (W + 1);
+  const size_t xch = DSM ? (size_t)NG * K * (W + 1) + (size_t)chain_colwarps<N, W>() * 2 * N : 0;
+  return (fft_smem(N, W) + xch + (col > row ? col : row)) * sizeof(cplx<R>);
 }
-template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t chain_smem() {
-  return chain_smem_for<R, N, DSM>(CH_NOP * (2 * ((N - 1) / 3) + 1));
+template <typename R, int N, int W, bool DSM> __host__ __device__ constexpr size_t chain_smem() {
+  return chain_smem_for<R, N, W, DSM>(CH_NOP * (2 * ((N - 1) / 3) + 1));
 }
 // Shared-memory regions of a chain kernel (offsets in complex entries).
-template <int N, bool DSM> struct ChainSmem {
+template <int N, int W, bool DSM> struct ChainSmem {
   static constexpr int K = (N - 1) / 3 + 1;
   static constexpr int tw = 0;
-  static constexpr int gt = fft_smem(N, CH_WARPS);                               // G tile (DSM)
-  static constexpr int hc = gt + (DSM ? NG * K * (CH_WARPS + 1) : 0);            // column warps' H rows (DSM)
-  static constexpr int work = hc + (DSM ? chain_colwarps<N>() * 2 * N : 0);      // staging / row tiles
+  static constexpr int gt = fft_smem(N, W);                                     // G tile (DSM)
+  static constexpr int hc = gt + (DSM ? NG * K * (W + 1) : 0);                  // column warps' H rows (DSM)
+  static constexpr int work = hc + (DSM ? chain_colwarps<N, W>() * 2 * N : 0);  // staging / row tiles
 };
 
 template <typename R>
@@ -98,15 +99,15 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;\n" ::: "memory");
 }
 
-template <typename R, int N, bool DSM>
+template <typename R, int N, int W, bool DSM>
 __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp& op, int b, int rank, int w,
                                           int lane, const cplx<R>* s_tw, cplx<R>* my_op, const cplx<R>* hrows,
                                           cplx<R>* gtile) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  constexpr int CL = chain_cl<N>();
+  constexpr int CL = chain_cl<N, W>();
   const int c = w * CL + rank;   // this warp's column of the tangent
-  if (w >= chain_colwarps<N>() || c >= 2 * K) return;
+  if (w >= chain_colwarps<N, W>() || c >= 2 * K) return;
   const int colid = b * 2 * K + c;
   ColTanParams<R> p = P.col;
   p.rec = P.rec + (size_t)op.rec * VEC;
@@ -122,27 +123,27 @@ __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp
     return;
   }
   switch (op.stage) {
-    case T43_START: col_tan_body<R, N, T43_START, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_INIT: col_tan_body<R, N, T43_INIT, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_A: col_tan_body<R, N, T43_A, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_B: col_tan_body<R, N, T43_B, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_C: col_tan_body<R, N, T43_C, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_D: col_tan_body<R, N, T43_D, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_EA: col_tan_body<R, N, T43_EA, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    default: col_tan_body<R, N, T43_E, DSM>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_START: col_tan_body<R, N, T43_START, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_INIT: col_tan_body<R, N, T43_INIT, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_A: col_tan_body<R, N, T43_A, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_B: col_tan_body<R, N, T43_B, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_C: col_tan_body<R, N, T43_C, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_D: col_tan_body<R, N, T43_D, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_EA: col_tan_body<R, N, T43_EA, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    default: col_tan_body<R, N, T43_E, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
   }
 }
 
-// Grid: B clusters of CL CTAs (cluster b = tangent b), CH_WARPS * 32 threads each.
-template <typename R, int N, bool DSM>
-__global__ void __cluster_dims__(chain_cl<N>(), 1, 1) __launch_bounds__(CH_WARPS * 32, 1)
-k_tan_chain(ChainParams<R> P) {
+// Grid: B clusters of CL CTAs (cluster b = tangent b; the cluster shape is a
+// launch attribute), W * 32 threads each.
+template <typename R, int N, int W, bool DSM>
+__global__ void __launch_bounds__(W * 32, 1) k_tan_chain(ChainParams<R> P) {
   constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
-  constexpr int CL = chain_cl<N>();
+  constexpr int CL = chain_cl<N, W>();
   static_assert(N <= 128, "staged column operands need n <= 128");
   static_assert(col_tan_nop<N, T43_C>() <= CH_NOP && col_tan_nop<N, T43_EA>() <= CH_NOP &&
                 col_tan_nop<N, T43_A>() <= CH_NOP && col_tan_nop<N, T43_D>() <= CH_NOP, "staging rows");
-  using SM = ChainSmem<N, DSM>;
+  using SM = ChainSmem<N, W, DSM>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_base = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* s_tw = s_base + SM::tw;
@@ -151,7 +152,7 @@ k_tan_chain(ChainParams<R> P) {
   cplx<R>* s_work = s_base + SM::work;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
-  const int wc = w < chain_colwarps<N>() ? w : 0;
+  const int wc = w < chain_colwarps<N, W>() ? w : 0;
   load_twiddles<R, N>(s_tw, P.col.tw);
   pdl_wait();   // launched with programmatic serialization: the predecessor's writes are visible past here
   __syncthreads();
@@ -168,11 +169,11 @@ k_tan_chain(ChainParams<R> P) {
       RowTanParams<R> rp = P.row;
       rp.phys = P.phys + (size_t)(op.item - P.item0) * N * NPH * N;
       if constexpr (DSM)
-        row_tan_body<R, N, CH_WARPS, true>(rp, b, rank * CH_WARPS, s_tw, s_gt, s_work, first, last ? nullptr : s_hc);
+        row_tan_body<R, N, W, true>(rp, b, rank * W, s_tw, s_gt, s_work, first, last ? nullptr : s_hc);
       else
-        row_tan_body<R, N, CH_WARPS>(rp, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
+        row_tan_body<R, N, W>(rp, b, rank * W, s_tw, s_work, s_work + NG * K * (W + 1));
     } else {
-      chain_col<R, N, DSM>(P, op, b, rank, w, lane, s_tw, my_op,
+      chain_col<R, N, W, DSM>(P, op, b, rank, w, lane, s_tw, my_op,
                            (DSM && !first) ? s_hc + (size_t)wc * 2 * N : nullptr, (DSM && !last) ? s_gt : nullptr);
     }
   }
@@ -183,7 +184,7 @@ k_tan_chain(ChainParams<R> P) {
 // Lawson-RK4 steps of the primal (timestepping.lawson_rk4,
 // jax_scripts/lib/timestepping.py:69-80) in one launch: cluster b advances
 // state b through `steps` steps, each stage a row pass (k_row_rhs's body,
-// 16-row tiles) and a column pass (k_col_rk4's body), with the same layout and
+// W-row tiles) and a column pass (k_col_rk4's body), with the same layout and
 // barriers as k_tan_chain.  The stage input of the first stage is in G (from a
 // COL_START column pass before the launch).
 // ---------------------------------------------------------------------------
@@ -196,17 +197,16 @@ struct Rk4ChainParams {
 };
 
 // per column warp: 3 complex rows (F, A1, K2) and one real row (e), in complex units
-template <typename R, int N, bool DSM> __host__ __device__ constexpr size_t rk4_chain_smem() {
-  return chain_smem_for<R, N, DSM>(4 * (2 * ((N - 1) / 3) + 1));
+template <typename R, int N, int W, bool DSM> __host__ __device__ constexpr size_t rk4_chain_smem() {
+  return chain_smem_for<R, N, W, DSM>(4 * (2 * ((N - 1) / 3) + 1));
 }
 
-template <typename R, int N, bool DSM>
-__global__ void __cluster_dims__(chain_cl<N>(), 1, 1) __launch_bounds__(CH_WARPS * 32, 1)
-k_rk4_chain(Rk4ChainParams<R> P) {
+template <typename R, int N, int W, bool DSM>
+__global__ void __launch_bounds__(W * 32, 1) k_rk4_chain(Rk4ChainParams<R> P) {
   constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
-  constexpr int CL = chain_cl<N>();
+  constexpr int CL = chain_cl<N, W>();
   static_assert(N <= 128, "staged column operands need n <= 128");
-  using SM = ChainSmem<N, DSM>;
+  using SM = ChainSmem<N, W, DSM>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_base = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* s_tw = s_base + SM::tw;
@@ -216,7 +216,7 @@ k_rk4_chain(Rk4ChainParams<R> P) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
   const int cidx = w * CL + rank;   // this warp's column of the state
-  const bool has_col = w < chain_colwarps<N>() && cidx < 2 * K;
+  const bool has_col = w < chain_colwarps<N, W>() && cidx < 2 * K;
   const int colid = b * 2 * K + cidx;
   cplx<R>* my_c = s_work + (size_t)(has_col ? w : 0) * 4 * M;
   R* my_e = reinterpret_cast<R*>(my_c + 3 * M);
@@ -229,9 +229,9 @@ k_rk4_chain(Rk4ChainParams<R> P) {
       if (step > 0 || st > COL_RK4_S1) cluster_barrier();   // column pass -> row pass
       const bool first = step == 0 && st == COL_RK4_S1, last = step == P.steps - 1 && st == COL_RK4_S4;
       if constexpr (DSM)
-        row_rhs_body<R, N, CH_WARPS, true>(P.row, b, rank * CH_WARPS, s_tw, s_gt, s_work, first, s_hc);
+        row_rhs_body<R, N, W, true>(P.row, b, rank * W, s_tw, s_gt, s_work, first, s_hc);
       else
-        row_rhs_body<R, N, CH_WARPS>(P.row, b, rank * CH_WARPS, s_tw, s_work, s_work + NG * K * (CH_WARPS + 1));
+        row_rhs_body<R, N, W>(P.row, b, rank * W, s_tw, s_work, s_work + NG * K * (W + 1));
       cluster_barrier();                                     // row pass -> column pass
       if (!has_col) continue;
       ColParams<R> p = P.col;
@@ -239,10 +239,10 @@ k_rk4_chain(Rk4ChainParams<R> P) {
       p.produce = last ? P.last_produce : 1;
       cplx<R>* gt = (DSM && !last) ? s_gt : nullptr;
       switch (st) {
-        case COL_RK4_S1: col_rk4_body<R, N, COL_RK4_S1, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
-        case COL_RK4_S2: col_rk4_body<R, N, COL_RK4_S2, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
-        case COL_RK4_S3: col_rk4_body<R, N, COL_RK4_S3, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
-        default: col_rk4_body<R, N, COL_RK4_S4, DSM>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        case COL_RK4_S1: col_rk4_body<R, N, COL_RK4_S1, DSM ? W : 0>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        case COL_RK4_S2: col_rk4_body<R, N, COL_RK4_S2, DSM ? W : 0>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        case COL_RK4_S3: col_rk4_body<R, N, COL_RK4_S3, DSM ? W : 0>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
+        default: col_rk4_body<R, N, COL_RK4_S4, DSM ? W : 0>(p, colid, lane, s_tw, my_c, my_e, my_h, gt); break;
       }
     }
   }

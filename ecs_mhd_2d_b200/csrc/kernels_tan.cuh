@@ -109,7 +109,7 @@ struct RowTanParams {
 
 // Rows x0 .. x0 + XT - 1 of tangent b, one warp per row (the CTA's XT warps);
 // s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
-// CX (cluster-resident passes, XT = CX_XT): s_G already holds the tile (written
+// CX (cluster-resident passes): s_G already holds the tile (written
 // by the column pass) unless load_g, and the H tile goes to the column warps'
 // rows at `hcols` (scatter_h_tile) unless that is null (global H).
 template <typename R, int N, int XT, bool CX = false>
@@ -157,8 +157,7 @@ __device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, in
   store_one<R, N, XT>(dbb, s_H + 2 * K * (XT + 1), w, lane);
   __syncthreads();
   if constexpr (CX) {
-    static_assert(!CX || XT == CX_XT, "cluster tiles are CX_XT rows");
-    if (hcols) { scatter_h_tile<R, N>(s_H, hcols, x0); return; }
+    if (hcols) { scatter_h_tile<R, N, XT>(s_H, hcols, x0); return; }
   }
   store_tile<R, N, XT>(p.H + (size_t)b * NH * K * N, s_H, NH * K, x0);
 }
@@ -248,11 +247,11 @@ template <int N, int STAGE> __host__ __device__ constexpr int col_tan_nop() {
 
 // One warp's column `colid` of a tangent column stage; `my_op` is the warp's
 // staging buffer (col_tan_nop rows of M entries), `s_tw` the twiddle image.
-// CX (cluster-resident passes): the product rows come from `hrows` (the warp's
-// rows in shared memory, see scatter_h_tile) and the inverse transforms go to
-// the cluster's G tiles at `gtile` (col_uv_to_tiles); a null pointer selects
-// global H / G instead.
-template <typename R, int N, int STAGE, bool CX = false>
+// CX > 0 (cluster-resident passes with CX-row tiles): the product rows come from
+// `hrows` (the warp's rows in shared memory, see scatter_h_tile) and the
+// inverse transforms go to the cluster's G tiles at `gtile` (col_uv_to_tiles);
+// a null pointer selects global H / G instead.
+template <typename R, int N, int STAGE, int CX = 0>
 __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
                                              cplx<R>* my_op, const cplx<R>* hrows = nullptr,
                                              cplx<R>* gtile = nullptr) {
@@ -302,7 +301,7 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
   }
   cplx<R> r[E];
   if (has_rhs) {
-    if (CX && hrows) col_rhs_rows<R, N>(hrows, hrows + N, ch, ky, lane, s_tw, r);
+    if (CX > 0 && hrows) col_rhs_rows<R, N>(hrows, hrows + N, ch, ky, lane, s_tw, r);
     else col_load_rhs<R, N>(p.H, b, ch, ky, lane, s_tw, r);
   }
   if constexpr (NOP > 0) {
@@ -430,11 +429,11 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
     x[j] = xin;
   }
   if (!p.produce || STAGE == T43_INIT || STAGE == T43_E) return;
-  if constexpr (CX) {
+  if constexpr (CX > 0) {
     if (gtile) {
       cplx<R> wu[E], wv[E];
       col_uv_transform<R, N>(x, ky, lane, s_tw, wu, wv);
-      col_uv_to_tiles<R, N>(wu, wv, gtile, ch, ky, lane);
+      col_uv_to_tiles<R, N, CX>(wu, wv, gtile, ch, ky, lane);
       return;
     }
   }

@@ -6,7 +6,8 @@ objective_RPO (jax.jvp at jax_scripts/lib/utils.py:108) is equal bit for bit:
 with rejected attempts, with regeneration-chunk boundaries inside the list
 (ECS_REGEN_ITEMS), for one and for several tangents, at n = 64 and 128, with
 the passes exchanging their intermediate arrays through distributed shared
-memory (the default) and through global memory (ECS_CHAIN_DSMEM=0)."""
+memory (the default) and through global memory (ECS_CHAIN_DSMEM=0), and with
+8- and 16-warp CTAs (ECS_CHAIN_WARPS)."""
 import numpy as np
 import pytest
 import torch
@@ -29,14 +30,18 @@ CASES = [   # (n, B, T, atol, amp, env)
 ]
 
 
-def _run(n, B, T, atol, amp, env, monkeypatch, chain, dsm=1):
-    env = dict(env, ECS_CHAIN_DSMEM=str(dsm))
+VARIANTS = [(8, 1), (8, 0), (16, 1), (16, 0)]   # (warps per CTA, exchange through distributed shared memory)
+
+
+def _run(n, B, T, atol, amp, env, monkeypatch, chain, variant=(8, 1)):
+    env = dict(env, ECS_CHAIN_WARPS=str(variant[0]), ECS_CHAIN_DSMEM=str(variant[1]))
     seed = env.pop("seed", 4)
     cap = (64, 64) if seed == 0 else (4, 64)
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     if chain:
-        monkeypatch.delenv("ECS_CHAIN_MAXB", raising=False)
+        monkeypatch.setenv("ECS_CHAIN_MINB", "1")
+        monkeypatch.setenv("ECS_CHAIN_MAXB", "64")
     else:
         monkeypatch.setenv("ECS_CHAIN_MAXB", "0")
     context.clear_cache()
@@ -66,11 +71,11 @@ def _run(n, B, T, atol, amp, env, monkeypatch, chain, dsm=1):
 @pytest.mark.parametrize("n,B,T,atol,amp,env", CASES)
 def test_chain_equals_launch_per_pass(cuda, monkeypatch, n, B, T, atol, amp, env):
     want, info, per_pass = _run(n, B, T, atol, amp, env, monkeypatch, chain=False)
-    for dsm in (1, 0):
-        got, info2, chained = _run(n, B, T, atol, amp, env, monkeypatch, chain=True, dsm=dsm)
+    for v in VARIANTS:
+        got, info2, chained = _run(n, B, T, atol, amp, env, monkeypatch, chain=True, variant=v)
         assert info == info2
         for k in ("fields", "T", "sx"):
-            assert torch.equal(got[k], want[k]), (k, dsm)
+            assert torch.equal(got[k], want[k]), (k, v)
         # the pass list ran as a handful of launches instead of one per pass
         assert chained < per_pass // 4, (chained, per_pass)
 
@@ -85,10 +90,12 @@ def test_chain_covers_rejected_attempts(cuda, monkeypatch):
 RK4_CASES = [(64, 1, 5), (64, 8, 40), (128, 1, 37), (128, 3, 16)]   # (n, B, steps)
 
 
-def _rk4(n, B, steps, monkeypatch, chain, dsm=1):
-    monkeypatch.setenv("ECS_CHAIN_DSMEM", str(dsm))
+def _rk4(n, B, steps, monkeypatch, chain, variant=(8, 1)):
+    monkeypatch.setenv("ECS_CHAIN_WARPS", str(variant[0]))
+    monkeypatch.setenv("ECS_CHAIN_DSMEM", str(variant[1]))
     if chain:
-        monkeypatch.delenv("ECS_RK4CHAIN_MAXB", raising=False)
+        monkeypatch.setenv("ECS_RK4CHAIN_MINB", "1")
+        monkeypatch.setenv("ECS_RK4CHAIN_MAXB", "64")
     else:
         monkeypatch.setenv("ECS_RK4CHAIN_MAXB", "0")
     context.clear_cache()
@@ -117,8 +124,8 @@ def test_rk4_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, steps):
     """Lawson-RK4 stepping as one cluster-resident launch (k_rk4_chain) equals
     the launch-per-stage stepping (graphs of k_row_rhs / k_col_rk4) bit for bit."""
     want, want_obj, per_stage = _rk4(n, B, steps, monkeypatch, chain=False)
-    for dsm in (1, 0):
-        got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True, dsm=dsm)
-        assert torch.equal(got, want), dsm
-        assert torch.equal(got_obj, want_obj), dsm
+    for v in VARIANTS:
+        got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True, variant=v)
+        assert torch.equal(got, want), v
+        assert torch.equal(got_obj, want_obj), v
         assert chained < per_stage
