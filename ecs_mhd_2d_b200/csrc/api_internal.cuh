@@ -41,13 +41,18 @@ struct ecs_ctx {
   int plain_order = 0;              // depth of PlainOrder scopes (no programmatic launch below batch 8)
   int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)
   int regen_items = 0;              // stage inputs per regeneration chunk (ECS_REGEN_ITEMS, at least 8; 0: about 384 MiB)
-  int rk4chain_minb = 1;            // smallest batch of Lawson-RK4 stepping run as one cluster-resident launch (ECS_RK4CHAIN_MINB)
-  int rk4chain_maxb = 8;            // largest batch of Lawson-RK4 stepping run as one cluster-resident launch (ECS_RK4CHAIN_MAXB; 0: graphs of launches)
-  int chain_w = 8;                  // warps per CTA of the chain kernels: 8 (clusters of n / 8 CTAs) or 16 (ECS_CHAIN_WARPS; 16 where 8 does not fit)
-  int chain_resident = 0;           // clusters of the chain kernel the device holds at once
-  int chain_dsm = 1;                // the cluster-resident passes exchange G / H through distributed shared memory (ECS_CHAIN_DSMEM=0: through global memory)
-  int chain_minb = 1;               // smallest batch of the adaptive tangent sweep run as one cluster-resident pass list (ECS_CHAIN_MINB)
-  int chain_maxb = 64;              // largest batch of the adaptive tangent sweep run as one cluster-resident pass list (ECS_CHAIN_MAXB; 0: launch per pass)
+  // Cluster-resident chains (k_tan_chain for the adaptive tangent sweep,
+  // k_rk4_chain for Lawson-RK4 stepping) run batches up to the number of
+  // 16-warp clusters the device holds at once; batches up to the number of
+  // 8-warp clusters (16 CTAs each at n = 128) use those.  Measured at n = 128
+  // FP64 (matvecs/s, state-steps/s; launch per pass -> chain): batch 1 11.2 ->
+  // 12.5 and 23.4k -> 30.1k, batch 4 30.3 -> 50.5 and 67.5k -> 120k, batch 8
+  // 59.4 -> 68.7 and 111k -> 165k; at batch 16 the launch-per-pass path is ahead.
+  int chain_res8 = 0, chain_res16 = 0;   // clusters of each shape the device holds at once (set at creation)
+  int chain_w = 0;                  // warps per CTA forced for the chains (ECS_CHAIN_WARPS=8 or 16; 0: by batch as above)
+  int chain_dsm = -1;               // G / H exchange of the chains: 1 distributed shared memory, 0 global memory (ECS_CHAIN_DSMEM; -1: global for the tangent chain, shared for Lawson-RK4, as measured)
+  int chain_minb = 1, chain_maxb = -1;         // batch range of the tangent chain (ECS_CHAIN_MINB / ECS_CHAIN_MAXB; -1: chain_res16; 0: off)
+  int rk4chain_minb = 1, rk4chain_maxb = -1;   // batch range of the Lawson-RK4 chain (ECS_RK4CHAIN_MINB / ECS_RK4CHAIN_MAXB)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;

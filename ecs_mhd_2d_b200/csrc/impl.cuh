@@ -148,10 +148,10 @@ int configure_kernels(ecs_ctx* c) {
   }
   if (st) return cuda_err(c, cudaGetLastError(), "cudaFuncSetAttribute");
   if constexpr (N <= 128) {
-    // the chain kernels' CTA shape: 8 warps (clusters of N / 8 CTAs, non-portable
-    // above 8) when the device can hold such a cluster, else 16 warps
-    if (c->chain_w == 8 && chain_clusters<R, N, 8>() < 1) c->chain_w = 16;
-    c->chain_resident = c->chain_w == 8 ? chain_clusters<R, N, 8>() : chain_clusters<R, N, 16>();
+    // clusters of each chain shape that the device holds at once (8 warps:
+    // clusters of N / 8 CTAs, non-portable above 8; 16 warps: N / 16 CTAs)
+    c->chain_res8 = chain_clusters<R, N, 8>();
+    c->chain_res16 = chain_clusters<R, N, 16>();
   }
   return ECS_OK;
 }
@@ -469,15 +469,26 @@ struct Impl {
     return cuda_err(c, cudaGetLastError(), "state_vel");
   }
 
-  // Calls go(W, DSM) with the context's chain shape and exchange as constants.
-  template <typename F> static void chain_dispatch(const ecs_ctx* c, F&& go) {
+  // Calls go(W, DSM) with the chain shape for batch B and the exchange (dsm_default
+  // unless ECS_CHAIN_DSMEM set it) as constants: 8 warps while B such clusters
+  // fit on the device at once, else 16.
+  template <typename F> static void chain_dispatch(const ecs_ctx* c, int B, bool dsm_default, F&& go) {
     using W8 = std::integral_constant<int, 8>;
     using W16 = std::integral_constant<int, 16>;
-    if (c->chain_w == 8) {
-      if (c->chain_dsm) go(W8{}, std::true_type{}); else go(W8{}, std::false_type{});
+    const int w = c->chain_w ? c->chain_w : (B <= c->chain_res8 ? 8 : 16);
+    const bool dsm = c->chain_dsm < 0 ? dsm_default : c->chain_dsm != 0;
+    if (w == 8) {
+      if (dsm) go(W8{}, std::true_type{}); else go(W8{}, std::false_type{});
     } else {
-      if (c->chain_dsm) go(W16{}, std::true_type{}); else go(W16{}, std::false_type{});
+      if (dsm) go(W16{}, std::true_type{}); else go(W16{}, std::false_type{});
     }
+  }
+  // Whether a batch of B runs through a chain with batch range [minb, maxb] (maxb -1: the
+  // 16-warp clusters the device holds at once).
+  static bool chain_batch(const ecs_ctx* c, int B, int minb, int maxb) {
+    if (N > 128) return false;
+    const int hi = maxb < 0 ? c->chain_res16 : maxb;
+    return B >= minb && B <= hi && (c->chain_res8 > 0 || c->chain_res16 > 0);
   }
 
   // Lawson-RK4 steps of the box states in c->F as one cluster-resident launch
@@ -500,7 +511,7 @@ struct Impl {
         launch_cluster(c, B, chain_cl<N, W>(), k_rk4_chain<R, N, W, DSM>, dim3(B * chain_cl<N, W>()), dim3(W * 32),
                        rk4_chain_smem<R, N, W, DSM>(), s, P);
       };
-      chain_dispatch(c, go);
+      chain_dispatch(c, B, true, go);
       return cuda_err(c, cudaGetLastError(), "rk4 chain");
     } else {
       (void)B; (void)steps; (void)s;
@@ -510,7 +521,7 @@ struct Impl {
 
   // Lawson-RK4 over `steps` steps of the box state in c->F (ctl/Etab prepared).
   // Chunks of GS steps are captured once into a CUDA graph and replayed; batches
-  // from c->rk4chain_minb to c->rk4chain_maxb at n <= 128 run as one cluster-resident launch.
+  // in the Lawson-RK4 chain range (chain_batch) run as one cluster-resident launch.
   static int integrate_rk4(ecs_ctx* c, int B, long steps, cudaStream_t s) {
     if (steps <= 0) return ECS_OK;
     constexpr int GS = 16;
@@ -539,7 +550,7 @@ struct Impl {
       gk.B = B;
     }
     launch_col_rk4<R, N>(c, B, COL_START, 1, 0, s);
-    if (N <= 128 && B >= c->rk4chain_minb && B <= c->rk4chain_maxb) return rk4_chain(c, B, steps, s);
+    if (chain_batch(c, B, c->rk4chain_minb, c->rk4chain_maxb)) return rk4_chain(c, B, steps, s);
     long it = 0;
     while (steps - it > GS) {   // the final step (no inverse transforms) is launched directly
       cudaError_t e = cudaGraphLaunch(gk.exec, s);
@@ -1381,8 +1392,8 @@ struct Impl {
   }
 
   // Batches that the adaptive tangent sweep runs through the cluster-resident
-  // pass list (k_tan_chain): n <= 128, batch from c->chain_minb to c->chain_maxb.
-  static bool use_chain(const ecs_ctx* c, int B) { return N <= 128 && B >= c->chain_minb && B <= c->chain_maxb; }
+  // pass list (k_tan_chain): see chain_batch.
+  static bool use_chain(const ecs_ctx* c, int B) { return chain_batch(c, B, c->chain_minb, c->chain_maxb); }
 
   // The pass list through k_tan_chain: one launch per regeneration chunk (the
   // row passes of a launch read the chunk's physical fields), with the chunk's
@@ -1416,7 +1427,7 @@ struct Impl {
           launch_cluster(c, B, chain_cl<N, W>(), k_tan_chain<R, N, W, DSM>, dim3(B * chain_cl<N, W>()), dim3(W * 32),
                          chain_smem<R, N, W, DSM>(), s, P);
         };
-        chain_dispatch(c, go);
+        chain_dispatch(c, B, false, go);
         start = end;
       };
       for (size_t i = 0; i < ops.size(); ++i) {

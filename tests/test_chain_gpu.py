@@ -129,3 +129,34 @@ def test_rk4_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, steps):
         assert torch.equal(got, want), v
         assert torch.equal(got_obj, want_obj), v
         assert chained < per_stage
+
+
+def test_default_batch_ranges(cuda, monkeypatch):
+    """With no switches set, one tangent at 128^2 runs through the chain (a few
+    launches) and 64 tangents through the launch-per-pass sweep (the chain's
+    clusters would not all fit on the device at once)."""
+    for k in ("ECS_CHAIN_MINB", "ECS_CHAIN_MAXB", "ECS_CHAIN_WARPS", "ECS_CHAIN_DSMEM", "ECS_REGEN_ITEMS"):
+        monkeypatch.delenv(k, raising=False)
+    n, T = 128, 0.15
+    pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", shift_reflect_ny=1, rot=False,
+                           adaptive_dict={"atol": 1e-8, "checkpoints": 4, "max_steps_per_checkpoint": 64})
+    prim = {"fields": torch.as_tensor(initial_condition(4, n, amp=2.0), device="cuda"), "T": T, "sx": 0.2}
+    context.clear_cache()
+    try:
+        counts = {}
+        for B in (1, 64):
+            du = np.stack([initial_condition(60 + i, n) * 0.1 for i in range(B)])
+            tan = {"fields": torch.as_tensor(du, device="cuda"), "T": torch.zeros(B, dtype=torch.float64),
+                   "sx": torch.zeros(B, dtype=torch.float64)}
+            obj = E.Objective(pd, "Lawson_RK43")
+            obj.linearize(prim, force=True, batch=B)
+            ctx = context.get_context(pd, n, torch.float64, B)
+            torch.cuda.synchronize()
+            c0 = ctx.lib.ecs_launch_count(ctx.handle)
+            obj.jvp(prim, tan)
+            torch.cuda.synchronize()
+            counts[B] = (ctx.lib.ecs_launch_count(ctx.handle) - c0, obj.last_info["accepted"])
+        assert counts[1][0] < 20, counts
+        assert counts[64][0] > 4 * counts[64][1], counts
+    finally:
+        context.clear_cache()
