@@ -463,8 +463,8 @@ def run_kernels(rank, local, B=64):
     Lawson-RK4 stepping (k_col_rk4, k_row_rhs), the adaptive solve (k_col_rk43,
     k_row_err), linearisation + JVP batch (k_col_regen, k_row_phys, k_col_tan,
     k_row_tan), VJP batch (k_col_adj, k_row_adj), an Arnoldi step
-    (k_arnoldi_mgs) and a multi-candidate matvec sweep.  Prints one JSON line
-    with the seconds taken."""
+    (k_arnoldi_mgs), a multi-candidate matvec sweep, and the batch-1 chains
+    (k_tan_chain, k_rk4_chain).  Prints one JSON line with the seconds taken."""
     import torch
     import ecs_mhd_2d_b200 as E
     from ecs_mhd_2d_b200 import build as _build, linalg
@@ -496,6 +496,11 @@ def run_kernels(rank, local, B=64):
     prims = [{"fields": fields[b], "T": 0.03, "sx": 0.1} for b in range(16)]
     tans = [{"fields": tan["fields"][b], "T": 0.1, "sx": 0.2} for b in range(16)]
     E.jvp_multi(prims, tans, pds)
+    # batch-1 chains: the tangent pass list at the fixed linearisation (k_tan_chain)
+    # and Lawson-RK4 stepping of one state (k_rk4_chain)
+    obj.linearize(prim, force=True, batch=1)
+    obj.jvp(prim, {"fields": tan["fields"][:1].contiguous(), "T": tan["T"][:1], "sx": tan["sx"][:1]})
+    E.lawson_rk4(f[:1].contiguous(), 0.016, 8, pd)
     torch.cuda.synchronize()
     print(json.dumps({"workload": "kernels", "seconds": time.perf_counter() - t0}), flush=True)
 

@@ -37,6 +37,7 @@ struct ecs_ctx {
   long long launches = 0;           // kernels launched through this context
   int pdl = 1;                      // stepping kernels use programmatic dependent launch (ECS_PDL=0 disables)
   int rowtan_xt = 4;                // rows per CTA of the batched tangent row pass at n = 128 (ECS_ROWTAN_XT=4 or 8; 4 measured best)
+  int rowtan_pair = 0;              // the 4-row tangent row pass takes two tangents per warp (ECS_ROWTAN_PAIR=1)
   int pdl_minb = 1;                 // smallest batch launched with programmatic dependent launch (ECS_PDL_MINB)
   int plain_order = 0;              // depth of PlainOrder scopes (no programmatic launch below batch 8)
   int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)

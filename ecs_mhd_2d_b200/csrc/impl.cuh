@@ -38,6 +38,7 @@ template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (fft_sme
 // Small batches use 2-row tiles: 4x more CTAs for the same rows.
 constexpr int XTS = 2;
 template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
+template <typename R, int N, int X> size_t smem_row_tan_pair() { return (fft_smem(N, X) + 14 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 template <typename R, int N> size_t smem_row_tan2() { return (fft_smem(N, XT) + 11 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N> size_t smem_row_phys() { return (fft_smem(N, XT) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N, int X = XT> size_t smem_row_2f() { return (fft_smem(N, X) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
@@ -141,6 +142,7 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, 4>());
+  st |= (int)cudaFuncSetAttribute(k_row_tan_pair<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_tan_pair<R, N, 4>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   if constexpr (N <= 128) {
     st |= configure_chain<R, N, 8>();
@@ -267,6 +269,8 @@ void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_
   RowTanParams<R> p{}; p.ctl = ctl; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B; p.phys_bstride = phys_bstride;
   if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
+  else if (N == 128 && c->rowtan_xt == 4 && c->rowtan_pair && phys_bstride == 0 && !ctl)   // two tangents per warp
+    launch_step(c, B, k_row_tan_pair<R, N, 4>, dim3((B + 1) / 2 * (N / 4)), dim3(4 * 32), smem_row_tan_pair<R, N, 4>(), s, p);
   else if (N == 128 && c->rowtan_xt == 4)   // 4-row tiles measured faster at n = 128 only
     launch_step(c, B, k_row_tan<R, N, 4>, dim3(B * (N / 4)), dim3(4 * 32), smem_row_rhs<R, N, 4>(), s, p);
   else launch_step(c, B, k_row_tan<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
@@ -1434,7 +1438,7 @@ struct Impl {
         if (ops[i].kind != CH_ROW) continue;
         const long item = ops[i].item;
         if (chunk_lo < 0 || item < chunk_lo || item >= chunk_lo + ci) {
-          flush(i);
+          if (chunk_lo >= 0) flush(i);   // the passes before the first row pass read no physical fields
           chunk_lo = item;
           const long cnt = std::min<long>(ci, nitems - item);
           launch_regen<R, N>(c, (const cplx<R>*)L.rec, c->items + item, (int)cnt, s);

@@ -107,6 +107,20 @@ struct RowTanParams {
   int B;
 };
 
+// The linearised products of one row in physical space (dP1, dP2 in duv, dP3 in dbb).
+template <typename R, int E>
+__device__ __forceinline__ void row_tan_products(cplx<R> (&duv)[E], cplx<R> (&dbb)[E], const R (&pu)[E],
+                                                 const R (&pv)[E], const R (&pbx)[E], const R (&pby)[E]) {
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const R du = duv[j].x, dv = duv[j].y, dbx = dbb[j].x, dby = dbb[j].y;
+    const R u = pu[j], v = pv[j], bx = pbx[j], by = pby[j];
+    duv[j] = mk<R>(R(2) * (fpm(u, du, v, dv) - fpm(bx, dbx, by, dby)),     // dP1
+                   fpp(bx, dby, by, dbx) - fpp(u, dv, v, du));              // dP2
+    dbb[j] = mk<R>(fpp(u, dby, by, du) - fpp(v, dbx, bx, dv), R(0));        // dP3
+  }
+}
+
 // Rows x0 .. x0 + XT - 1 of tangent b, one warp per row (the CTA's XT warps);
 // s_G and s_H are the tile buffers (NG and NH rows of K x (XT + 1)).
 // CX (cluster-resident passes): s_G already holds the tile (written
@@ -144,14 +158,7 @@ __device__ __forceinline__ void row_tan_body(const RowTanParams<R>& p, int b, in
   }
   fft_dif2<R, N, true>(duv, dbb, s_tw, lane);
   if constexpr (N > 128) load_phys();
-#pragma unroll
-  for (int j = 0; j < E; ++j) {
-    const R du = duv[j].x, dv = duv[j].y, dbx = dbb[j].x, dby = dbb[j].y;
-    const R u = pu[j], v = pv[j], bx = pbx[j], by = pby[j];
-    duv[j] = mk<R>(R(2) * (fpm(u, du, v, dv) - fpm(bx, dbx, by, dby)),     // dP1
-                   fpp(bx, dby, by, dbx) - fpp(u, dv, v, du));              // dP2
-    dbb[j] = mk<R>(fpp(u, dby, by, du) - fpp(v, dbx, bx, dv), R(0));        // dP3
-  }
+  row_tan_products<R, E>(duv, dbb, pu, pv, pbx, pby);
   fft_dit2<R, N, false>(duv, dbb, s_tw, lane);
   split_store<R, N, XT>(duv, s_H, s_H + K * (XT + 1), w, lane);
   store_one<R, N, XT>(dbb, s_H + 2 * K * (XT + 1), w, lane);
@@ -175,6 +182,66 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   pdl_wait();
   if (p.ctl && p.ctl[b].done) return;   // the whole CTA belongs to batch element b
   row_tan_body<R, N, XT>(p, b, x0, s_tw, s_G, s_G + NG * K * (XT + 1));
+}
+
+// The row pass for two tangents per warp (b0 = 2 (blockIdx / tiles), b0 + 1; the
+// second repeats the first, without its store, when B is odd): one primal shared
+// by the batch, whose row is loaded once, and four transforms in lockstep.  The
+// same arithmetic per tangent as k_row_tan.
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32, 2) k_row_tan_pair(RowTanParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  constexpr int TG = NG * K * (XT + 1), TH = NH * K * (XT + 1);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G0 = s_tw + fft_smem(N, XT);
+  cplx<R>* s_G1 = s_G0 + TG;
+  cplx<R>* s_H0 = s_G1 + TG;
+  cplx<R>* s_H1 = s_H0 + TH;
+  const int tiles = N / XT;
+  const int pair = blockIdx.x / tiles, x0 = (blockIdx.x - pair * tiles) * XT;
+  const int b0 = 2 * pair, b1 = b0 + 1 < p.B ? b0 + 1 : b0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  const R* ph = phys_row<R, N>(p.phys, x0 + w);
+  R pu[E], pv[E], pbx[E], pby[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int e = lane + 32 * j;
+    pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
+  }
+  load_tile<R, N, XT>(s_G0, p.G + (size_t)b0 * NG * K * N, NG * K, x0);
+  load_tile<R, N, XT>(s_G1, p.G + (size_t)b1 * NG * K * N, NG * K, x0);
+  __syncthreads();
+  cplx<R> duv0[E], dbb0[E], duv1[E], dbb1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int q = lane + 32 * j;
+    duv0[j] = packed_pair<R, N, XT>(s_G0, s_G0 + K * (XT + 1), q, w);
+    dbb0[j] = packed_pair<R, N, XT>(s_G0 + 2 * K * (XT + 1), s_G0 + 3 * K * (XT + 1), q, w);
+    duv1[j] = packed_pair<R, N, XT>(s_G1, s_G1 + K * (XT + 1), q, w);
+    dbb1[j] = packed_pair<R, N, XT>(s_G1 + 2 * K * (XT + 1), s_G1 + 3 * K * (XT + 1), q, w);
+  }
+  {
+    cplx<R>(*const v[4])[E] = {&duv0, &dbb0, &duv1, &dbb1};
+    fft_dif_n<R, true, 4, N>(v, s_tw, lane);
+  }
+  row_tan_products<R, E>(duv0, dbb0, pu, pv, pbx, pby);
+  row_tan_products<R, E>(duv1, dbb1, pu, pv, pbx, pby);
+  {
+    cplx<R>(*const v[4])[E] = {&duv0, &dbb0, &duv1, &dbb1};
+    fft_dit_n<R, false, 4, N>(v, s_tw, lane);
+  }
+  split_store<R, N, XT>(duv0, s_H0, s_H0 + K * (XT + 1), w, lane);
+  store_one<R, N, XT>(dbb0, s_H0 + 2 * K * (XT + 1), w, lane);
+  split_store<R, N, XT>(duv1, s_H1, s_H1 + K * (XT + 1), w, lane);
+  store_one<R, N, XT>(dbb1, s_H1 + 2 * K * (XT + 1), w, lane);
+  __syncthreads();
+  store_tile<R, N, XT>(p.H + (size_t)b0 * NH * K * N, s_H0, NH * K, x0);
+  if (b1 != b0) store_tile<R, N, XT>(p.H + (size_t)b1 * NH * K * N, s_H1, NH * K, x0);
 }
 
 // ---------------------------------------------------------------------------
