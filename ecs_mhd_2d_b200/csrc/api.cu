@@ -96,10 +96,10 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   if (const char* v = getenv("ECS_TGROUPS")) c->tgroups = std::max(1, std::min(ecs_ctx::MAXG, atoi(v)));
   if (const char* v = getenv("ECS_ROWTAN_XT")) c->rowtan_xt = atoi(v) == 4 ? 4 : 8;
   if (const char* v = getenv("ECS_PDL_MINB")) c->pdl_minb = std::max(1, atoi(v));
-  if (const char* v = getenv("ECS_ROWTAN_PAIR")) c->rowtan_pair = atoi(v) != 0 ? 1 : 0;
   if (const char* v = getenv("ECS_CHAIN_MAXB")) c->chain_maxb = std::max(0, atoi(v));
   if (const char* v = getenv("ECS_RK4CHAIN_MAXB")) c->rk4chain_maxb = std::max(0, atoi(v));
   if (const char* v = getenv("ECS_CHAIN_DSMEM")) c->chain_dsm = atoi(v) != 0 ? 1 : 0;
+  if (const char* v = getenv("ECS_CHAIN_DSLOTS")) c->chain_dsh = atoi(v) != 0 ? 1 : 0;
   if (const char* v = getenv("ECS_CHAIN_WARPS")) c->chain_w = atoi(v) == 16 ? 16 : atoi(v) == 8 ? 8 : 0;
   if (const char* v = getenv("ECS_CHAIN_MINB")) c->chain_minb = std::max(1, atoi(v));
   if (const char* v = getenv("ECS_RK4CHAIN_MINB")) c->rk4chain_minb = std::max(1, atoi(v));

@@ -37,7 +37,6 @@ struct ecs_ctx {
   long long launches = 0;           // kernels launched through this context
   int pdl = 1;                      // stepping kernels use programmatic dependent launch (ECS_PDL=0 disables)
   int rowtan_xt = 4;                // rows per CTA of the batched tangent row pass at n = 128 (ECS_ROWTAN_XT=4 or 8; 4 measured best)
-  int rowtan_pair = 0;              // the 4-row tangent row pass takes two tangents per warp (ECS_ROWTAN_PAIR=1)
   int pdl_minb = 1;                 // smallest batch launched with programmatic dependent launch (ECS_PDL_MINB)
   int plain_order = 0;              // depth of PlainOrder scopes (no programmatic launch below batch 8)
   int tgroups = 3;                  // tangent groups of ecs_linearize_jvp (ECS_TGROUPS=1..4; 3 measured best at B=64)
@@ -51,6 +50,7 @@ struct ecs_ctx {
   // 59.4 -> 68.7 and 111k -> 165k; at batch 16 the launch-per-pass path is ahead.
   int chain_res8 = 0, chain_res16 = 0;   // clusters of each shape the device holds at once (set at creation)
   int chain_w = 0;                  // warps per CTA forced for the chains (ECS_CHAIN_WARPS=8 or 16; 0: by batch as above)
+  int chain_dsh = 1;                // the 8-warp tangent chain keeps each column's tangent slots in shared memory (ECS_CHAIN_DSLOTS=0: global)
   int chain_dsm = -1;               // G / H exchange of the chains: 1 distributed shared memory, 0 global memory (ECS_CHAIN_DSMEM; -1: global for the tangent chain, shared for Lawson-RK4, as measured)
   int chain_minb = 1, chain_maxb = -1;         // batch range of the tangent chain (ECS_CHAIN_MINB / ECS_CHAIN_MAXB; -1: chain_res16; 0: off)
   int rk4chain_minb = 1, rk4chain_maxb = -1;   // batch range of the Lawson-RK4 chain (ECS_RK4CHAIN_MINB / ECS_RK4CHAIN_MAXB)

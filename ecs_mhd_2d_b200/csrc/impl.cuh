@@ -38,7 +38,6 @@ template <typename R, int N, int X = XT> size_t smem_row_rhs() { return (fft_sme
 // Small batches use 2-row tiles: 4x more CTAs for the same rows.
 constexpr int XTS = 2;
 template <int N> bool small_rows(int B) { return (long)B * (N / XT) < 2L * 148; }
-template <typename R, int N, int X> size_t smem_row_tan_pair() { return (fft_smem(N, X) + 14 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
 template <typename R, int N> size_t smem_row_tan2() { return (fft_smem(N, XT) + 11 * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N> size_t smem_row_phys() { return (fft_smem(N, XT) + NG * Geomc<N>::K * (XT + 1)) * sizeof(cplx<R>); }
 template <typename R, int N, int X = XT> size_t smem_row_2f() { return (fft_smem(N, X) + 2 * Geomc<N>::K * (X + 1)) * sizeof(cplx<R>); }
@@ -101,25 +100,30 @@ int configure_chain() {
     st |= (int)cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (chain_cl<N, W>() > 8) st |= (int)cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   };
-  attrs(k_tan_chain<R, N, W, false>, chain_smem<R, N, W, false>());
-  attrs(k_tan_chain<R, N, W, true>, chain_smem<R, N, W, true>());
+  attrs(k_tan_chain<R, N, W, false, false>, chain_smem<R, N, W, false, false>());
+  attrs(k_tan_chain<R, N, W, true, false>, chain_smem<R, N, W, true, false>());
+  if constexpr (W == 8) {   // tangent slots in shared memory: the 8-warp shape only (smem)
+    attrs(k_tan_chain<R, N, W, false, true>, chain_smem<R, N, W, false, true>());
+    attrs(k_tan_chain<R, N, W, true, true>, chain_smem<R, N, W, true, true>());
+  }
   attrs(k_rk4_chain<R, N, W, false>, rk4_chain_smem<R, N, W, false>());
   attrs(k_rk4_chain<R, N, W, true>, rk4_chain_smem<R, N, W, true>());
   return st;
 }
 
-// Clusters of the W-warp tangent chain kernel (DSMEM exchange, its largest
+// Clusters of the W-warp tangent chain kernel (its variant with the largest
 // shared memory) that the device holds at once; 0 if it cannot hold one.
 template <typename R, int N, int W>
 int chain_clusters() {
+  constexpr bool DSH = W == 8;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(chain_cl<N, W>()); cfg.blockDim = dim3(W * 32); cfg.dynamicSmemBytes = chain_smem<R, N, W, true>();
+  cfg.gridDim = dim3(chain_cl<N, W>()); cfg.blockDim = dim3(W * 32); cfg.dynamicSmemBytes = chain_smem<R, N, W, true, DSH>();
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = (unsigned)chain_cl<N, W>(); at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
   cfg.attrs = at; cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_tan_chain<R, N, W, true>, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, k_tan_chain<R, N, W, true, DSH>, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -142,7 +146,6 @@ int configure_kernels(ecs_ctx* c) {
   st |= (int)cudaFuncSetAttribute(k_row_err<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_2f<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   st |= (int)cudaFuncSetAttribute(k_row_tan<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, 4>());
-  st |= (int)cudaFuncSetAttribute(k_row_tan_pair<R, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_tan_pair<R, N, 4>());
   st |= (int)cudaFuncSetAttribute(k_row_adj<R, N, XTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row_rhs<R, N, XTS>());
   if constexpr (N <= 128) {
     st |= configure_chain<R, N, 8>();
@@ -269,8 +272,6 @@ void launch_row_tan(ecs_ctx* c, int B, const R* phys, cudaStream_t s, long phys_
   RowTanParams<R> p{}; p.ctl = ctl; p.G = (const cplx<R>*)c->G; p.H = (cplx<R>*)c->H; p.phys = phys; p.tw = (const cplx<R>*)c->tw;
   p.B = B; p.phys_bstride = phys_bstride;
   if (small_rows<N>(B)) launch_step(c, B, k_row_tan<R, N, XTS>, dim3(B * (N / XTS)), dim3(XTS * 32), smem_row_rhs<R, N, XTS>(), s, p);
-  else if (N == 128 && c->rowtan_xt == 4 && c->rowtan_pair && phys_bstride == 0 && !ctl)   // two tangents per warp
-    launch_step(c, B, k_row_tan_pair<R, N, 4>, dim3((B + 1) / 2 * (N / 4)), dim3(4 * 32), smem_row_tan_pair<R, N, 4>(), s, p);
   else if (N == 128 && c->rowtan_xt == 4)   // 4-row tiles measured faster at n = 128 only
     launch_step(c, B, k_row_tan<R, N, 4>, dim3(B * (N / 4)), dim3(4 * 32), smem_row_rhs<R, N, 4>(), s, p);
   else launch_step(c, B, k_row_tan<R, N, XT>, dim3(B * (N / XT)), dim3(XT * 32), smem_row_rhs<R, N>(), s, p);
@@ -1425,11 +1426,16 @@ struct Impl {
         if (end <= start) return;
         P.op0 = (int)start; P.op1 = (int)end;
         P.phys = (const R*)c->Phys; P.item0 = chunk_lo < 0 ? 0 : chunk_lo;
+        const bool dsh = c->chain_dsh != 0;
         auto go = [&](auto w, auto dsm) {
           constexpr int W = decltype(w)::value;
           constexpr bool DSM = decltype(dsm)::value;
-          launch_cluster(c, B, chain_cl<N, W>(), k_tan_chain<R, N, W, DSM>, dim3(B * chain_cl<N, W>()), dim3(W * 32),
-                         chain_smem<R, N, W, DSM>(), s, P);
+          if (W == 8 && dsh)
+            launch_cluster(c, B, chain_cl<N, W>(), k_tan_chain<R, N, W, DSM, W == 8>, dim3(B * chain_cl<N, W>()),
+                           dim3(W * 32), chain_smem<R, N, W, DSM, W == 8>(), s, P);
+          else
+            launch_cluster(c, B, chain_cl<N, W>(), k_tan_chain<R, N, W, DSM, false>, dim3(B * chain_cl<N, W>()),
+                           dim3(W * 32), chain_smem<R, N, W, DSM, false>(), s, P);
         };
         chain_dispatch(c, B, false, go);
         start = end;

@@ -60,29 +60,32 @@ template <int N, int W> __host__ __device__ constexpr int chain_cl() { return N 
 template <int N, int W> __host__ __device__ constexpr int chain_colwarps() {
   return (2 * ((N - 1) / 3 + 1) + chain_cl<N, W>() - 1) / chain_cl<N, W>();
 }
-// Operand rows staged per column warp: the largest col_tan_nop over the adaptive stages.
-constexpr int CH_NOP = 8;
-// Shared memory of a chain kernel with `stage` complex entries of column
-// staging per column warp: twiddles, then with DSM the G tile and the column
-// warps' H rows, then the column staging overlaid with the row tiles.
-template <typename R, int N, int W, bool DSM> __host__ __device__ constexpr size_t chain_smem_for(int stage) {
-  constexpr int K = (N - 1) / 3 + 1;
-  const size_t col = (size_t)chain_colwarps<N, W>() * stage;
-  const size_t row = (size_t)(DSM ? NH : NG + NH) * K * (W + 1);
-  const size_t xch = DSM ? (size_t)NG * K * (W + 1) + (size_t)chain_colwarps<N, W>() * 2 * N : 0;
-  return (fft_smem(N, W) + xch + (col > row ? col : row)) * sizeof(cplx<R>);
-}
-template <typename R, int N, int W, bool DSM> __host__ __device__ constexpr size_t chain_smem() {
-  return chain_smem_for<R, N, W, DSM>(CH_NOP * (2 * ((N - 1) / 3) + 1));
-}
-// Shared-memory regions of a chain kernel (offsets in complex entries).
-template <int N, int W, bool DSM> struct ChainSmem {
-  static constexpr int K = (N - 1) / 3 + 1;
+// Operand rows staged per column warp: the largest col_tan_nop over the adaptive
+// stages (8), or, with the tangent slots in shared memory (DSH), the largest
+// number of record rows a stage reads (5, stage C).
+constexpr int CH_NOP = 8, CH_NOP_DSH = 5;
+// Shared-memory regions of a chain kernel (offsets in complex entries), with
+// `stage` complex entries of column staging per column warp: twiddles; with
+// DSM the G tile and the column warps' H rows; the column staging overlaid
+// with the row tiles; with DSH the column warps' tangent slots [S_NSLOT][M].
+template <int N, int W, bool DSM, bool DSH = false> struct ChainSmem {
+  static constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  static constexpr int CW = chain_colwarps<N, W>();
   static constexpr int tw = 0;
-  static constexpr int gt = fft_smem(N, W);                                     // G tile (DSM)
-  static constexpr int hc = gt + (DSM ? NG * K * (W + 1) : 0);                  // column warps' H rows (DSM)
-  static constexpr int work = hc + (DSM ? chain_colwarps<N, W>() * 2 * N : 0);  // staging / row tiles
+  static constexpr int gt = fft_smem(N, W);                        // G tile (DSM)
+  static constexpr int hc = gt + (DSM ? NG * K * (W + 1) : 0);     // column warps' H rows (DSM)
+  static constexpr int work = hc + (DSM ? CW * 2 * N : 0);         // staging / row tiles
+  static constexpr int row = (DSM ? NH : NG + NH) * K * (W + 1);
+  static constexpr int ds_at(int stage) { return work + (CW * stage > row ? CW * stage : row); }
+  static constexpr int end_at(int stage) { return ds_at(stage) + (DSH ? CW * S_NSLOT * M : 0); }
 };
+template <typename R, int N, int W, bool DSM, bool DSH = false>
+__host__ __device__ constexpr size_t chain_smem_for(int stage) {
+  return (size_t)ChainSmem<N, W, DSM, DSH>::end_at(stage) * sizeof(cplx<R>);
+}
+template <typename R, int N, int W, bool DSM, bool DSH = false> __host__ __device__ constexpr size_t chain_smem() {
+  return chain_smem_for<R, N, W, DSM, DSH>((DSH ? CH_NOP_DSH : CH_NOP) * (2 * ((N - 1) / 3) + 1));
+}
 
 template <typename R>
 struct ChainParams {
@@ -99,10 +102,10 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;\n" ::: "memory");
 }
 
-template <typename R, int N, int W, bool DSM>
+template <typename R, int N, int W, bool DSM, bool DSH>
 __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp& op, int b, int rank, int w,
                                           int lane, const cplx<R>* s_tw, cplx<R>* my_op, const cplx<R>* hrows,
-                                          cplx<R>* gtile) {
+                                          cplx<R>* gtile, cplx<R>* dsh) {
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
   constexpr int CL = chain_cl<N, W>();
@@ -119,31 +122,39 @@ __device__ __forceinline__ void chain_col(const ChainParams<R>& P, const ChainOp
     const int ch = c & 1, ky = c >> 1;
     cplx<R>* Db = p.D + (size_t)b * p.nslot * VEC;
     const R dpar = (R)(p.dT[b] * p.dscale);
-    for (int s = lane; s < M; s += 32) tan_reject_at<R>(Db, p.rec, VEC, ((size_t)ch * K + ky) * M + s, dpar);
+    for (int s = lane; s < M; s += 32) {
+      const size_t o = ((size_t)ch * K + ky) * M + s;
+      if constexpr (DSH) dsh[S_K1 * M + s] = tan_reject_k1<R>(p.rec, VEC, o, dpar, dsh[S_K1 * M + s]);
+      else tan_reject_at<R>(Db, p.rec, VEC, o, dpar);
+    }
     return;
   }
   switch (op.stage) {
-    case T43_START: col_tan_body<R, N, T43_START, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_INIT: col_tan_body<R, N, T43_INIT, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_A: col_tan_body<R, N, T43_A, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_B: col_tan_body<R, N, T43_B, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_C: col_tan_body<R, N, T43_C, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_D: col_tan_body<R, N, T43_D, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    case T43_EA: col_tan_body<R, N, T43_EA, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
-    default: col_tan_body<R, N, T43_E, DSM ? W : 0>(p, colid, lane, s_tw, my_op, hrows, gtile); break;
+    case T43_START: col_tan_body<R, N, T43_START, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_INIT: col_tan_body<R, N, T43_INIT, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_A: col_tan_body<R, N, T43_A, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_B: col_tan_body<R, N, T43_B, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_C: col_tan_body<R, N, T43_C, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_D: col_tan_body<R, N, T43_D, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    case T43_EA: col_tan_body<R, N, T43_EA, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
+    default: col_tan_body<R, N, T43_E, DSM ? W : 0, DSH>(p, colid, lane, s_tw, my_op, hrows, gtile, dsh); break;
   }
 }
 
 // Grid: B clusters of CL CTAs (cluster b = tangent b; the cluster shape is a
 // launch attribute), W * 32 threads each.
-template <typename R, int N, int W, bool DSM>
+template <typename R, int N, int W, bool DSM, bool DSH>
 __global__ void __launch_bounds__(W * 32, 1) k_tan_chain(ChainParams<R> P) {
   constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr size_t VEC = (size_t)2 * K * M;
   constexpr int CL = chain_cl<N, W>();
+  constexpr int NOPW = DSH ? CH_NOP_DSH : CH_NOP;
   static_assert(N <= 128, "staged column operands need n <= 128");
   static_assert(col_tan_nop<N, T43_C>() <= CH_NOP && col_tan_nop<N, T43_EA>() <= CH_NOP &&
                 col_tan_nop<N, T43_A>() <= CH_NOP && col_tan_nop<N, T43_D>() <= CH_NOP, "staging rows");
-  using SM = ChainSmem<N, W, DSM>;
+  static_assert(popc_c(tan_qmask(T43_C)) <= CH_NOP_DSH && popc_c(tan_qmask(T43_EA)) + popc_c(tan_qmask2(T43_EA)) <= CH_NOP_DSH,
+                "record rows staged with the slots in shared memory");
+  using SM = ChainSmem<N, W, DSM, DSH>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_base = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* s_tw = s_base + SM::tw;
@@ -153,10 +164,19 @@ __global__ void __launch_bounds__(W * 32, 1) k_tan_chain(ChainParams<R> P) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
   const int wc = w < chain_colwarps<N, W>() ? w : 0;
+  const int cown = w * CL + rank;   // this warp's column (tangent slots in shared memory)
+  const bool owns = w < chain_colwarps<N, W>() && cown < 2 * K;
+  cplx<R>* dsh = s_base + SM::ds_at(NOPW * M) + (size_t)wc * S_NSLOT * M;
+  cplx<R>* dglob = P.col.D + (size_t)b * P.col.nslot * VEC + ((size_t)(cown & 1) * K + (cown >> 1)) * M;
   load_twiddles<R, N>(s_tw, P.col.tw);
   pdl_wait();   // launched with programmatic serialization: the predecessor's writes are visible past here
+  if constexpr (DSH) {
+    if (owns)
+      for (int d = 0; d < S_NSLOT; ++d)
+        for (int e = lane; e < M; e += 32) dsh[d * M + e] = dglob[d * VEC + e];
+  }
   __syncthreads();
-  cplx<R>* my_op = s_work + (size_t)wc * CH_NOP * M;
+  cplx<R>* my_op = s_work + (size_t)wc * NOPW * M;
   int prev = -1;   // kind class of the previous pass: 0 column-like, 1 row
   for (int i = P.op0; i < P.op1; ++i) {
     const ChainOp op = P.ops[i];
@@ -173,9 +193,16 @@ __global__ void __launch_bounds__(W * 32, 1) k_tan_chain(ChainParams<R> P) {
       else
         row_tan_body<R, N, W>(rp, b, rank * W, s_tw, s_work, s_work + NG * K * (W + 1));
     } else {
-      chain_col<R, N, W, DSM>(P, op, b, rank, w, lane, s_tw, my_op,
-                           (DSM && !first) ? s_hc + (size_t)wc * 2 * N : nullptr, (DSM && !last) ? s_gt : nullptr);
+      chain_col<R, N, W, DSM, DSH>(P, op, b, rank, w, lane, s_tw, my_op,
+                                   (DSM && !first) ? s_hc + (size_t)wc * 2 * N : nullptr,
+                                   (DSM && !last) ? s_gt : nullptr, dsh);
     }
+  }
+  if constexpr (DSH) {   // the slots back to global memory for the next launch and the JVP output
+    __syncwarp();
+    if (owns)
+      for (int d = 0; d < S_NSLOT; ++d)
+        for (int e = lane; e < M; e += 32) dglob[d * VEC + e] = dsh[d * M + e];
   }
   if constexpr (DSM) cluster_barrier();   // no CTA leaves while a peer may still write its shared memory
 }

@@ -184,66 +184,6 @@ __global__ void __launch_bounds__(XT * 32, 2) k_row_tan(RowTanParams<R> p) {
   row_tan_body<R, N, XT>(p, b, x0, s_tw, s_G, s_G + NG * K * (XT + 1));
 }
 
-// The row pass for two tangents per warp (b0 = 2 (blockIdx / tiles), b0 + 1; the
-// second repeats the first, without its store, when B is odd): one primal shared
-// by the batch, whose row is loaded once, and four transforms in lockstep.  The
-// same arithmetic per tangent as k_row_tan.
-template <typename R, int N, int XT>
-__global__ void __launch_bounds__(XT * 32, 2) k_row_tan_pair(RowTanParams<R> p) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
-  constexpr int TG = NG * K * (XT + 1), TH = NH * K * (XT + 1);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G0 = s_tw + fft_smem(N, XT);
-  cplx<R>* s_G1 = s_G0 + TG;
-  cplx<R>* s_H0 = s_G1 + TG;
-  cplx<R>* s_H1 = s_H0 + TH;
-  const int tiles = N / XT;
-  const int pair = blockIdx.x / tiles, x0 = (blockIdx.x - pair * tiles) * XT;
-  const int b0 = 2 * pair, b1 = b0 + 1 < p.B ? b0 + 1 : b0;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  const R* ph = phys_row<R, N>(p.phys, x0 + w);
-  R pu[E], pv[E], pbx[E], pby[E];
-#pragma unroll
-  for (int j = 0; j < E; ++j) {
-    const int e = lane + 32 * j;
-    pu[j] = ph[e]; pv[j] = ph[N + e]; pbx[j] = ph[2 * N + e]; pby[j] = ph[3 * N + e];
-  }
-  load_tile<R, N, XT>(s_G0, p.G + (size_t)b0 * NG * K * N, NG * K, x0);
-  load_tile<R, N, XT>(s_G1, p.G + (size_t)b1 * NG * K * N, NG * K, x0);
-  __syncthreads();
-  cplx<R> duv0[E], dbb0[E], duv1[E], dbb1[E];
-#pragma unroll
-  for (int j = 0; j < E; ++j) {
-    const int q = lane + 32 * j;
-    duv0[j] = packed_pair<R, N, XT>(s_G0, s_G0 + K * (XT + 1), q, w);
-    dbb0[j] = packed_pair<R, N, XT>(s_G0 + 2 * K * (XT + 1), s_G0 + 3 * K * (XT + 1), q, w);
-    duv1[j] = packed_pair<R, N, XT>(s_G1, s_G1 + K * (XT + 1), q, w);
-    dbb1[j] = packed_pair<R, N, XT>(s_G1 + 2 * K * (XT + 1), s_G1 + 3 * K * (XT + 1), q, w);
-  }
-  {
-    cplx<R>(*const v[4])[E] = {&duv0, &dbb0, &duv1, &dbb1};
-    fft_dif_n<R, true, 4, N>(v, s_tw, lane);
-  }
-  row_tan_products<R, E>(duv0, dbb0, pu, pv, pbx, pby);
-  row_tan_products<R, E>(duv1, dbb1, pu, pv, pbx, pby);
-  {
-    cplx<R>(*const v[4])[E] = {&duv0, &dbb0, &duv1, &dbb1};
-    fft_dit_n<R, false, 4, N>(v, s_tw, lane);
-  }
-  split_store<R, N, XT>(duv0, s_H0, s_H0 + K * (XT + 1), w, lane);
-  store_one<R, N, XT>(dbb0, s_H0 + 2 * K * (XT + 1), w, lane);
-  split_store<R, N, XT>(duv1, s_H1, s_H1 + K * (XT + 1), w, lane);
-  store_one<R, N, XT>(dbb1, s_H1 + 2 * K * (XT + 1), w, lane);
-  __syncthreads();
-  store_tile<R, N, XT>(p.H + (size_t)b0 * NH * K * N, s_H0, NH * K, x0);
-  if (b1 != b0) store_tile<R, N, XT>(p.H + (size_t)b1 * NH * K * N, s_H1, NH * K, x0);
-}
-
 // ---------------------------------------------------------------------------
 // Tangent column pass: forward transform of the linearised products and the
 // tangent of the stepper algebra.
@@ -318,10 +258,12 @@ template <int N, int STAGE> __host__ __device__ constexpr int col_tan_nop() {
 // `hrows` (the warp's rows in shared memory, see scatter_h_tile) and the
 // inverse transforms go to the cluster's G tiles at `gtile` (col_uv_to_tiles);
 // a null pointer selects global H / G instead.
-template <typename R, int N, int STAGE, int CX = 0>
+// DSH (cluster-resident adaptive passes): the tangent slots of this column live
+// in shared memory at `dsh` ([S_NSLOT][M]) instead of global D.
+template <typename R, int N, int STAGE, int CX = 0, bool DSH = false>
 __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid, int lane, const cplx<R>* s_tw,
                                              cplx<R>* my_op, const cplx<R>* hrows = nullptr,
-                                             cplx<R>* gtile = nullptr) {
+                                             cplx<R>* gtile = nullptr, cplx<R>* dsh = nullptr) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
@@ -337,7 +279,7 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
   // rows of them (M entries each), copied into the warp's shared buffer with
   // cp.async before the forward transform, so that their latency overlaps it
   // without holding registers (adaptive stages, n <= 128: static shared memory).
-  constexpr unsigned QM = N <= 128 ? tan_qmask(STAGE) : 0u, DM = N <= 128 ? tan_dmask(STAGE) : 0u;
+  constexpr unsigned QM = N <= 128 ? tan_qmask(STAGE) : 0u, DM = (N <= 128 && !DSH) ? tan_dmask(STAGE) : 0u;
   constexpr unsigned QM2 = N <= 128 ? tan_qmask2(STAGE) : 0u;
   constexpr int NQ = popc_c(QM), NQ2 = popc_c(QM2), NOP = NQ + NQ2 + popc_c(DM);
   const cplx<R>* Q2 = p.rec2;
@@ -440,8 +382,13 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
         else return Q2[q * VEC + o];
       };
       auto DV = [&](int d) -> cplx<R> {
-        if constexpr (NOP > 0) return my_op[(NQ + NQ2 + popc_c(DM & ((1u << d) - 1u))) * M + slot];
+        if constexpr (DSH) return dsh[d * M + slot];
+        else if constexpr (NOP > 0) return my_op[(NQ + NQ2 + popc_c(DM & ((1u << d) - 1u))) * M + slot];
         else return D[d * VEC + o];
+      };
+      auto DW = [&](int d, cplx<R> v) {
+        if constexpr (DSH) dsh[d * M + slot] = v;
+        else D[d * VEC + o] = v;
       };
       auto dk_of = [&](int q) { return lin2_rn(QV(q), dpar / t, dv, t); };
       // the A and E algebra, written with explicitly rounded operations: the
@@ -450,18 +397,18 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
       auto stage_a = [&](cplx<R> x0, cplx<R> k1, cplx<R> eg_, cplx<R> dx0, cplx<R> dk1, R h_) {
         const R e_ = eg_.x, de_ = mul_rn(eg_.y, dpar);
         const cplx<R> dxe = lin2_rn(x0, de_, dx0, e_), dk1e = lin2_rn(k1, de_, dk1, e_);
-        D[S_XE * VEC + o] = dxe; D[S_K1E * VEC + o] = dk1e;
+        DW(S_XE, dxe); DW(S_K1E, dk1e);
         cplx<R> half = cscale(dk1e, h_);
         half.x = mul_rn(half.x, R(0.5)); half.y = mul_rn(half.y, R(0.5));
         return mk<R>(add_rn(dxe.x, half.x), add_rn(dxe.y, half.y));
       };
       switch (STAGE) {
         case T43_START: xin = DV(S_X0); break;
-        case T43_INIT: D[S_K1 * VEC + o] = dk_of(RR_K1); break;
+        case T43_INIT: DW(S_K1, dk_of(RR_K1)); break;
         case T43_A: xin = stage_a(QV(RR_X0), QV(RR_K1), eg, DV(S_X0), DV(S_K1), h); break;
         case T43_B: {
           const cplx<R> dk2 = dk_of(RR_K2);
-          D[S_K2 * VEC + o] = dk2;
+          DW(S_K2, dk2);
           xin = cadd(DV(S_XE), cscale(cscale(dk2, h), R(0.5)));
         } break;
         case T43_C: {
@@ -471,7 +418,7 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
           const cplx<R> dk1ee = lin2_rn(k1e, de, DV(S_K1E), e);
           const cplx<R> dk2e = lin2_rn(QV(RR_K2), de, DV(S_K2), e);
           const cplx<R> dk3e = lin2_rn(QV(RR_K3), de, dk3, e);
-          D[S_X2 * VEC + o] = dx2; D[S_K1 * VEC + o] = dk1ee; D[S_K2 * VEC + o] = dk2e; D[S_K3 * VEC + o] = dk3e;
+          DW(S_X2, dx2); DW(S_K1, dk1ee); DW(S_K2, dk2e); DW(S_K3, dk3e);
           xin = cadd_scaled_rn(dx2, dk3e, h);
         } break;
         case T43_D: {
@@ -479,16 +426,16 @@ __device__ __forceinline__ void col_tan_body(const ColTanParams<R>& p, int colid
           const cplx<R> acc = cadd(cadd(cadd(cdiv_k<6>(DV(S_K1)), cdiv_k<3>(DV(S_K2))),
                                         cdiv_k<3>(DV(S_K3))), cdiv_k<6>(dk4));
           xin = cadd_scaled_rn(DV(S_X2), acc, h);
-          D[S_XF * VEC + o] = xin;
+          DW(S_XF, xin);
         } break;
         case T43_E: {   // accepted attempt, promote (dxf, dk5) -> (dx0, dk1)
-          D[S_K1 * VEC + o] = stage_e();
-          D[S_X0 * VEC + o] = DV(S_XF);
+          DW(S_K1, stage_e());
+          DW(S_X0, DV(S_XF));
         } break;
         default: {      // T43_EA: T43_E, then T43_A of the next attempt on the promoted values
           const cplx<R> dk1 = stage_e(), dx0 = DV(S_XF);
-          D[S_K1 * VEC + o] = dk1;
-          D[S_X0 * VEC + o] = dx0;
+          DW(S_K1, dk1);
+          DW(S_X0, dx0);
           xin = stage_a(Q2V(RR_X0), Q2V(RR_K1), Q2V(RR_E), dx0, dk1, h);
         } break;
       }
@@ -525,16 +472,21 @@ __global__ void __launch_bounds__(128) k_col_tan(ColTanParams<R> p) {
 
 // Rejected Lawson-RK4(3) attempt: the carried k1 becomes e^2 k1 (timestepping.py:267,275,297);
 // its tangent is d(e (e k1)) with e' = e L h/2 dt ((e, e L h/2) from the attempt's record).
-// Entry o of tangent Db (slots of one tangent), dpar = dT * dscale.
+// The carried dk1 at entry o after a rejected attempt (record rec), dpar = dT * dscale.
 template <typename R>
-__device__ __forceinline__ void tan_reject_at(cplx<R>* Db, const cplx<R>* rec, size_t VEC, size_t o, R dpar) {
+__device__ __forceinline__ cplx<R> tan_reject_k1(const cplx<R>* rec, size_t VEC, size_t o, R dpar, cplx<R> dk1) {
   const cplx<R> eg = rec[RR_E * VEC + o];   // (e, e L h/2) of the attempt
   const R e = eg.x;
   const R de = eg.y * dpar;
   const cplx<R> k1 = rec[RR_K1 * VEC + o];
   const cplx<R> k1e = cscale_rn(k1, e);
-  const cplx<R> dk1e = lin2_rn(k1, de, Db[S_K1 * VEC + o], e);
-  Db[S_K1 * VEC + o] = lin2_rn(k1e, de, dk1e, e);
+  const cplx<R> dk1e = lin2_rn(k1, de, dk1, e);
+  return lin2_rn(k1e, de, dk1e, e);
+}
+// Entry o of tangent Db (slots of one tangent).
+template <typename R>
+__device__ __forceinline__ void tan_reject_at(cplx<R>* Db, const cplx<R>* rec, size_t VEC, size_t o, R dpar) {
+  Db[S_K1 * VEC + o] = tan_reject_k1<R>(rec, VEC, o, dpar, Db[S_K1 * VEC + o]);
 }
 
 template <typename R>

@@ -6,8 +6,9 @@ objective_RPO (jax.jvp at jax_scripts/lib/utils.py:108) is equal bit for bit:
 with rejected attempts, with regeneration-chunk boundaries inside the list
 (ECS_REGEN_ITEMS), for one and for several tangents, at n = 64 and 128, with
 the passes exchanging their intermediate arrays through distributed shared
-memory (the default) and through global memory (ECS_CHAIN_DSMEM=0), and with
-8- and 16-warp CTAs (ECS_CHAIN_WARPS)."""
+memory and through global memory (ECS_CHAIN_DSMEM), with 8- and 16-warp CTAs
+(ECS_CHAIN_WARPS), and with the tangent slots in shared or global memory
+(ECS_CHAIN_DSLOTS)."""
 import numpy as np
 import pytest
 import torch
@@ -30,11 +31,12 @@ CASES = [   # (n, B, T, atol, amp, env)
 ]
 
 
-VARIANTS = [(8, 1), (8, 0), (16, 1), (16, 0)]   # (warps per CTA, exchange through distributed shared memory)
+# (warps per CTA, exchange through distributed shared memory, tangent slots in shared memory)
+VARIANTS = [(8, 1, 1), (8, 0, 1), (8, 1, 0), (8, 0, 0), (16, 1, 0), (16, 0, 0)]
 
 
-def _run(n, B, T, atol, amp, env, monkeypatch, chain, variant=(8, 1)):
-    env = dict(env, ECS_CHAIN_WARPS=str(variant[0]), ECS_CHAIN_DSMEM=str(variant[1]))
+def _run(n, B, T, atol, amp, env, monkeypatch, chain, variant=(8, 1, 1)):
+    env = dict(env, ECS_CHAIN_WARPS=str(variant[0]), ECS_CHAIN_DSMEM=str(variant[1]), ECS_CHAIN_DSLOTS=str(variant[2]))
     seed = env.pop("seed", 4)
     cap = (64, 64) if seed == 0 else (4, 64)
     for k, v in env.items():
@@ -90,7 +92,7 @@ def test_chain_covers_rejected_attempts(cuda, monkeypatch):
 RK4_CASES = [(64, 1, 5), (64, 8, 40), (128, 1, 37), (128, 3, 16)]   # (n, B, steps)
 
 
-def _rk4(n, B, steps, monkeypatch, chain, variant=(8, 1)):
+def _rk4(n, B, steps, monkeypatch, chain, variant=(8, 1, 1)):
     monkeypatch.setenv("ECS_CHAIN_WARPS", str(variant[0]))
     monkeypatch.setenv("ECS_CHAIN_DSMEM", str(variant[1]))
     if chain:
@@ -124,7 +126,7 @@ def test_rk4_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, steps):
     """Lawson-RK4 stepping as one cluster-resident launch (k_rk4_chain) equals
     the launch-per-stage stepping (graphs of k_row_rhs / k_col_rk4) bit for bit."""
     want, want_obj, per_stage = _rk4(n, B, steps, monkeypatch, chain=False)
-    for v in VARIANTS:
+    for v in [(8, 1, 0), (8, 0, 0), (16, 1, 0), (16, 0, 0)]:
         got, got_obj, chained = _rk4(n, B, steps, monkeypatch, chain=True, variant=v)
         assert torch.equal(got, want), v
         assert torch.equal(got_obj, want_obj), v
@@ -135,7 +137,7 @@ def test_default_batch_ranges(cuda, monkeypatch):
     """With no switches set, one tangent at 128^2 runs through the chain (a few
     launches) and 64 tangents through the launch-per-pass sweep (the chain's
     clusters would not all fit on the device at once)."""
-    for k in ("ECS_CHAIN_MINB", "ECS_CHAIN_MAXB", "ECS_CHAIN_WARPS", "ECS_CHAIN_DSMEM", "ECS_REGEN_ITEMS"):
+    for k in ("ECS_CHAIN_MINB", "ECS_CHAIN_MAXB", "ECS_CHAIN_WARPS", "ECS_CHAIN_DSMEM", "ECS_CHAIN_DSLOTS", "ECS_REGEN_ITEMS"):
         monkeypatch.delenv(k, raising=False)
     n, T = 128, 0.15
     pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", shift_reflect_ny=1, rot=False,

@@ -95,7 +95,7 @@ def test_linearize_jvp_repeated_calls(cuda):
 
 
 @pytest.mark.parametrize("env", [{"ECS_ROWTAN_XT": "8"}, {"ECS_PDL_MINB": "8"}, {"ECS_TGROUPS": "1"},
-                                 {"ECS_ROWTAN_PAIR": "1"}, {"ECS_ROWTAN_PAIR": "1", "ECS_TGROUPS": "2"}])
+                                 {"ECS_TGROUPS": "2"}])
 def test_tuning_switches_do_not_change_results(cuda, env, monkeypatch):
     """The tuning switches (read when a context is created) change launch
     shapes and ordering only: the objective and a batch of 64 tangents at
