@@ -103,6 +103,8 @@ int ecs_ctx_create(int n, int dtype, const ecs_params* params, int max_batch, ec
   if (const char* v = getenv("ECS_CHAIN_WARPS")) c->chain_w = atoi(v) == 16 ? 16 : atoi(v) == 8 ? 8 : 0;
   if (const char* v = getenv("ECS_CHAIN_MINB")) c->chain_minb = std::max(1, atoi(v));
   if (const char* v = getenv("ECS_RK4CHAIN_MINB")) c->rk4chain_minb = std::max(1, atoi(v));
+  if (const char* v = getenv("ECS_RK43CHAIN_MINB")) c->rk43chain_minb = std::max(1, atoi(v));
+  if (const char* v = getenv("ECS_RK43CHAIN_MAXB")) c->rk43chain_maxb = std::max(0, atoi(v));
   if (const char* v = getenv("ECS_REGEN_ITEMS")) c->regen_items = atoi(v) > 0 ? std::max(8, atoi(v)) : 0;
   int st;
   const ecs::ImplTable* t = ecs::impl_table(dtype, n);

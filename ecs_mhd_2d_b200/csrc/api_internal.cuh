@@ -54,6 +54,7 @@ struct ecs_ctx {
   int chain_dsm = -1;               // G / H exchange of the chains: 1 distributed shared memory, 0 global memory (ECS_CHAIN_DSMEM; -1: global for the tangent chain, shared for Lawson-RK4, as measured)
   int chain_minb = 1, chain_maxb = -1;         // batch range of the tangent chain (ECS_CHAIN_MINB / ECS_CHAIN_MAXB; -1: chain_res16; 0: off)
   int rk4chain_minb = 1, rk4chain_maxb = -1;   // batch range of the Lawson-RK4 chain (ECS_RK4CHAIN_MINB / ECS_RK4CHAIN_MAXB)
+  int rk43chain_minb = 1, rk43chain_maxb = -1; // batch range of the adaptive Lawson-RK4(3) solve's chain (ECS_RK43CHAIN_MINB / _MAXB)
   // linearisation (primal trajectory record) shared by JVP / VJP calls
   struct Lin {
     int valid = 0, mode = 0;

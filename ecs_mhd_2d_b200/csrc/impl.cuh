@@ -106,6 +106,7 @@ int configure_chain() {
     attrs(k_tan_chain<R, N, W, false, true>, chain_smem<R, N, W, false, true>());
     attrs(k_tan_chain<R, N, W, true, true>, chain_smem<R, N, W, true, true>());
   }
+  attrs(k_rk43_chain<R, N, W>, rk43_chain_smem<R, N, W>());
   attrs(k_rk4_chain<R, N, W, false>, rk4_chain_smem<R, N, W, false>());
   attrs(k_rk4_chain<R, N, W, true>, rk4_chain_smem<R, N, W, true>());
   return st;
@@ -692,6 +693,29 @@ struct Impl {
     launch_col_rk43<R, N>(c, B, R43_START, s);
     launch_row_rhs<R, N>(c, B, s, c->ctl);
     launch_col_rk43<R, N>(c, B, R43_INIT, s);
+    if (launch && chain_batch(c, B, c->rk43chain_minb, c->rk43chain_maxb)) {
+      // the attempts as one cluster-resident launch, no host round trip (k_rk43_chain)
+      if constexpr (N <= 128) {
+        Rk43ChainParams<R> P{};
+        Col43Params<R>& q = P.col;
+        q.H = (const cplx<R>*)c->H; q.G = (cplx<R>*)c->G; q.S = (cplx<R>*)c->S43; q.ctl = c->ctl;
+        q.fhat = (const cplx<R>*)c->fhat; q.tw = (const cplx<R>*)c->tw; q.rec = rec; q.cap = cap;
+        q.nu = (R)c->nu; q.eta = (R)c->eta; q.B = B;
+        RowParams<R>& r = P.row;
+        r.G = (const cplx<R>*)c->G; r.H = (cplx<R>*)c->H; r.tw = (const cplx<R>*)c->tw; r.ctl = c->ctl;
+        r.b0x = (R)c->b0x; r.b0y = (R)c->b0y; r.B = B;
+        P.atol = cfg->atol; P.rec_h = rec_h; P.rec_acc = rec_acc; P.amax = amax;
+        if (c->chain_w == 8 || (c->chain_w == 0 && B <= c->chain_res8))
+          launch_cluster(c, B, chain_cl<N, 8>(), k_rk43_chain<R, N, 8>, dim3(B * chain_cl<N, 8>()), dim3(8 * 32),
+                         rk43_chain_smem<R, N, 8>(), s, P);
+        else
+          launch_cluster(c, B, chain_cl<N, 16>(), k_rk43_chain<R, N, 16>, dim3(B * chain_cl<N, 16>()), dim3(16 * 32),
+                         rk43_chain_smem<R, N, 16>(), s, P);
+        const long nbox = (long)B * 2 * K * M;
+        ++c->launches; k_rk43_resolve<R><<<grid1d(nbox), 256, 0, s>>>((cplx<R>*)c->S43, c->ctl, (cplx<R>*)c->F, N, B);
+        return cuda_err(c, cudaGetLastError(), "rk43 chain");
+      }
+    }
     // one attempt = 5 column + 4 row + 1 error launches; a chunk of GA attempts is
     // captured once into a CUDA graph (all per-attempt data is read from the
     // device control block, so the same graph replays every chunk)

@@ -276,4 +276,92 @@ __global__ void __launch_bounds__(W * 32, 1) k_rk4_chain(Rk4ChainParams<R> P) {
   if constexpr (DSM) cluster_barrier();   // no CTA leaves while a peer may still write its shared memory
 }
 
+// ---------------------------------------------------------------------------
+// Adaptive Lawson-RK4(3) attempts of the primal (timestepping.lawson_rk43,
+// jax_scripts/lib/timestepping.py:151-335) in one launch: cluster b runs state
+// b's attempts until it completes or `amax` attempts were made -- the column
+// stages A..E (k_col_rk43's body), the four RHS row passes (k_row_rhs's body)
+// and the error norm (k_row_err's body); each CTA's maximum goes to the
+// cluster through distributed shared memory, CTA 0 makes the accept/reject
+// decision and the step-size update on the control block (rk43_control, as
+// the last block of k_row_err does), and every CTA reads it after the next
+// cluster barrier.  The G and H arrays go through global memory.  Set-up,
+// START and INIT passes run before the launch.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct Rk43ChainParams {
+  Col43Params<R> col;
+  RowParams<R> row;
+  double atol;
+  double* rec_h;   // optional [B][cap] attempted step sizes
+  int* rec_acc;    // optional [B][cap] accept flags
+  long amax;       // attempts at most
+};
+constexpr int CH_NOP43 = 5;   // rows staged per column warp by an attempt stage (slots + forcing)
+
+template <typename R, int N, int W> __host__ __device__ constexpr size_t rk43_chain_smem() {
+  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr size_t col = (size_t)chain_colwarps<N, W>() * CH_NOP43 * M;
+  constexpr size_t row = (size_t)(NG + NH) * K * (W + 1);
+  return (fft_smem(N, W) + (col > row ? col : row)) * sizeof(cplx<R>);
+}
+
+template <typename R, int N, int W>
+__global__ void __launch_bounds__(W * 32, 1) k_rk43_chain(Rk43ChainParams<R> P) {
+  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr int CL = chain_cl<N, W>();
+  static_assert(N <= 128, "staged column operands need n <= 128");
+  static_assert(col_rk43_nop<N, R43_C>() <= CH_NOP43 && col_rk43_nop<N, R43_D>() <= CH_NOP43 &&
+                col_rk43_nop<N, R43_B>() <= CH_NOP43 && col_rk43_nop<N, R43_E>() <= CH_NOP43, "staging rows");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_work = s_tw + fft_smem(N, W);
+  __shared__ double s_max[W];
+  __shared__ double s_part;   // this CTA's error maximum, read by CTA 0 of the cluster
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b = blockIdx.x / CL, rank = blockIdx.x - b * CL;
+  const int cidx = w * CL + rank;   // this warp's column of the state
+  const bool has_col = w < chain_colwarps<N, W>() && cidx < 2 * K;
+  const int colid = b * 2 * K + cidx;
+  cplx<R>* my_op = s_work + (size_t)(has_col ? w : 0) * CH_NOP43 * M;
+  StepCtl* ctl = P.col.ctl + b;
+  load_twiddles<R, N>(s_tw, P.col.tw);
+  pdl_wait();   // launched with programmatic serialization: the predecessor's writes are visible past here
+  __syncthreads();
+  for (long a = 0; a < P.amax; ++a) {
+    if (*(volatile int*)&ctl->done) break;   // written by CTA 0 before the last cluster barrier
+    if (has_col) col_rk43_body<R, N, R43_A>(P.col, colid, lane, s_tw, my_op);
+    cluster_barrier();
+#pragma unroll 1
+    for (int st = R43_B; st <= R43_E; ++st) {
+      row_rhs_body<R, N, W>(P.row, b, rank * W, s_tw, s_work, s_work + NG * K * (W + 1));
+      cluster_barrier();
+      if (has_col) {
+        switch (st) {
+          case R43_B: col_rk43_body<R, N, R43_B>(P.col, colid, lane, s_tw, my_op); break;
+          case R43_C: col_rk43_body<R, N, R43_C>(P.col, colid, lane, s_tw, my_op); break;
+          case R43_D: col_rk43_body<R, N, R43_D>(P.col, colid, lane, s_tw, my_op); break;
+          default: col_rk43_body<R, N, R43_E>(P.col, colid, lane, s_tw, my_op); break;
+        }
+      }
+      cluster_barrier();
+    }
+    const double bm = row_err_max<R, N, W>(P.col.G, b, rank * W, s_tw, s_work, s_max);
+    if (threadIdx.x == 0) s_part = bm;
+    cluster_barrier();
+    if (rank == 0 && threadIdx.x == 0) {
+      cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+      double err = 0.0;
+      for (int r = 0; r < CL; ++r) {
+        const double q = *cl.map_shared_rank(&s_part, (unsigned)r);
+        err = (q > err || isnan(q)) ? q : err;
+      }
+      const int at = ctl->attempts, cap = P.col.cap;
+      rk43_control(*ctl, P.atol, err, P.rec_h && at < cap ? P.rec_h + (size_t)b * cap : nullptr,
+                   P.rec_acc && at < cap ? P.rec_acc + (size_t)b * cap : nullptr);
+    }
+    cluster_barrier();
+  }
+}
+
 }  // namespace ecs

@@ -57,19 +57,19 @@ __host__ __device__ constexpr unsigned r43_smask(int stage) {
 }
 __host__ __device__ constexpr int popc_r43(unsigned m) { return m ? (int)(m & 1u) + popc_r43(m >> 1) : 0; }
 
+// Slot rows staged per warp by an attempt stage (+ the forcing row), n <= 128.
+template <int N, int STAGE> __host__ __device__ constexpr int col_rk43_nop() {
+  return (N <= 128 && popc_r43(r43_smask(STAGE)) > 0) ? popc_r43(r43_smask(STAGE)) + 1 : 0;
+}
+
+// One warp's column `colid` of an attempt stage; `my_op` is the warp's staging
+// buffer (col_rk43_nop rows of M entries).
 template <typename R, int N, int STAGE>
-__global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
+__device__ __forceinline__ void col_rk43_body(const Col43Params<R>& p, int colid, int lane, const cplx<R>* s_tw,
+                                              cplx<R>* my_op) {
   constexpr int E = N / 32;
   constexpr int KMAX = (N - 1) / 3, K = KMAX + 1, M = 2 * KMAX + 1;
   constexpr size_t VEC = (size_t)2 * K * M;
-  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (colid >= p.B * K * 2) return;
   const int ch = colid & 1, bk = colid >> 1, b = bk / K, ky = bk - b * K;   // one warp per (b, ky, channel)
   const StepCtl& c = p.ctl[b];
   if (c.done) return;
@@ -84,8 +84,6 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   // with cp.async before it, so that their latency overlaps it (n <= 128).
   constexpr unsigned SM = N <= 128 ? r43_smask(STAGE) : 0u;
   constexpr int NS = popc_r43(SM), NOP = NS > 0 ? NS + 1 : 0;   // + the forcing row
-  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
-  cplx<R>* my_op = s_op + (threadIdx.x >> 5) * NOP * M;
   if constexpr (NOP > 0) {
     const size_t row = ((size_t)ch * K + ky) * M;
     int v = 0;
@@ -128,7 +126,7 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
     }
     const size_t o = ((size_t)ch * K + ky) * M + slot;
     const R L = diss_L<R>(kx, ky, coeff);
-    const cplx<R> kv = cscale(v, t);                 // mod_vel_fn = t * vel_fn (timestepping.py:243)
+    const cplx<R> kv = cscale_rn(v, t);              // mod_vel_fn = t * vel_fn (timestepping.py:243)
     cplx<R> xin = mk<R>(0, 0);
     switch (STAGE) {
       case R43_START: xin = S[S_X0 * VEC + o]; break;
@@ -142,27 +140,27 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
         const cplx<R> eg = mk<R>(e, e * (L * h * R(0.5)));
         S[S_E * VEC + o] = eg;
         if (rec) rec[RR_E * VEC + o] = eg;
-        const cplx<R> xe = cscale(xs, e), k1e = cscale(ks, e);
+        const cplx<R> xe = cscale_rn(xs, e), k1e = cscale_rn(ks, e);
         S[S_XE * VEC + o] = xe; S[S_K1E * VEC + o] = k1e;
-        xin = cadd(xe, cscale(cscale(k1e, h), R(0.5)));
+        xin = cadd(xe, cscale(cscale_rn(k1e, h), R(0.5)));
         if (rec) rec[RR_Y2 * VEC + o] = xin;
       } break;
       case R43_B: {                                  // :270-271
         S[S_K2 * VEC + o] = kv;
         if (rec) rec[RR_K2 * VEC + o] = kv;
-        xin = cadd(SV(S_XE, o, slot), cscale(cscale(kv, h), R(0.5)));
+        xin = cadd(SV(S_XE, o, slot), cscale(cscale_rn(kv, h), R(0.5)));
         if (rec) rec[RR_Y3 * VEC + o] = xin;
       } break;
       case R43_C: {                                  // :271-280
         if (rec) rec[RR_K3 * VEC + o] = kv;
         const R e = SV(S_E, o, slot).x;
-        const cplx<R> x2 = cscale(SV(S_XE, o, slot), e);
-        const cplx<R> k1ee = cscale(SV(S_K1E, o, slot), e);
-        const cplx<R> k2e = cscale(SV(S_K2, o, slot), e);
-        const cplx<R> k3e = cscale(kv, e);
+        const cplx<R> x2 = cscale_rn(SV(S_XE, o, slot), e);
+        const cplx<R> k1ee = cscale_rn(SV(S_K1E, o, slot), e);
+        const cplx<R> k2e = cscale_rn(SV(S_K2, o, slot), e);
+        const cplx<R> k3e = cscale_rn(kv, e);
         S[S_X2 * VEC + o] = x2; S[S_K1 * VEC + o] = k1ee;   // k1 carried on rejection is e^2 k1 (:297)
         S[S_K2 * VEC + o] = k2e; S[S_K3 * VEC + o] = k3e;
-        xin = cadd(x2, cscale(k3e, h));
+        xin = cadd_scaled_rn(x2, k3e, h);
         if (rec) rec[RR_Y4 * VEC + o] = xin;
       } break;
       case R43_D: {                                  // :280-281
@@ -170,14 +168,14 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
         if (rec) rec[RR_K4 * VEC + o] = kv;
         const cplx<R> acc = cadd(cadd(cadd(cdiv_k<6>(SV(S_K1, o, slot)), cdiv_k<3>(SV(S_K2, o, slot))),
                                       cdiv_k<3>(SV(S_K3, o, slot))), cdiv_k<6>(kv));
-        xin = cadd(SV(S_X2, o, slot), cscale(acc, h));
+        xin = cadd_scaled_rn(SV(S_X2, o, slot), acc, h);
         S[S_XF * VEC + o] = xin;
         if (rec) rec[RR_XF * VEC + o] = xin;
       } break;
       default: {                                     // R43_E: :282, :288
         S[S_K5 * VEC + o] = kv;
         if (rec) rec[RR_K5 * VEC + o] = kv;
-        xin = cdiv_k<6>(cscale(csub(kv, SV(S_K4, o, slot)), h));
+        xin = cdiv_k<6>(cscale_rn(csub(kv, SV(S_K4, o, slot)), h));
       } break;
     }
     x[j] = xin;
@@ -185,6 +183,22 @@ __global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
   if (STAGE == R43_INIT) return;
   if (STAGE == R43_E) col_inverse1<R, N>(x, p.G, NG, b, ch, ky, lane, s_tw, R(1) / (R(N) * R(N)));
   else col_inverse_uv<R, N>(x, p.G, b, ch, ky, lane, s_tw);
+}
+
+template <typename R, int N, int STAGE>
+__global__ void __launch_bounds__(128) k_col_rk43(Col43Params<R> p) {
+  constexpr int K = (N - 1) / 3 + 1, M = 2 * ((N - 1) / 3) + 1;
+  constexpr int NOP = col_rk43_nop<N, STAGE>();
+  __shared__ __align__(16) cplx<R> s_tw[fft_smem(N, 4)];
+  __shared__ __align__(16) cplx<R> s_op[(NOP > 0 ? NOP : 1) * 4 * M];   // 4 warps per CTA
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int colid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (colid >= p.B * K * 2) return;
+  col_rk43_body<R, N, STAGE>(p, colid, lane, s_tw, s_op + (threadIdx.x >> 5) * NOP * M);
 }
 
 // Error norm max|irfft2(d)| of the two channels (timestepping.py:288-291) with
@@ -219,23 +233,14 @@ __device__ __forceinline__ void rk43_control(StepCtl& c, double atol, double err
   c.done = fabs(c.s - 1.0) < 1e-10 ? 1 : 0;                // :313
 }
 
+// max |irfft2(d)| over rows x0 .. x0 + XT - 1 of state b (the inverse column
+// transforms of d in G fields 0 and 1), one warp per row; valid in thread 0.
 template <typename R, int N, int XT>
-__global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
+__device__ __forceinline__ double row_err_max(const cplx<R>* G, int b, int x0, const cplx<R>* s_tw, cplx<R>* s_G,
+                                              double* s_max) {
   constexpr int E = N / 32;
   constexpr int K = (N - 1) / 3 + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
-  cplx<R>* s_G = s_tw + fft_smem(N, XT);
-  __shared__ double s_max[XT];
-  __shared__ int s_last;
-  const int tiles = N / XT;
-  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
-  pdl_trigger();
-  load_twiddles<R, N>(s_tw, p.tw);
-  pdl_wait();
-  StepCtl& c = p.ctl[b];
-  if (c.done) return;
-  load_tile<R, N, XT>(s_G, p.G + (size_t)b * NG * K * N, 2 * K, x0);
+  load_tile<R, N, XT>(s_G, G + (size_t)b * NG * K * N, 2 * K, x0);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   cplx<R> z[E];
@@ -256,9 +261,29 @@ __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
   }
   if (lane == 0) s_max[w] = m;
   __syncthreads();
+  double bm = s_max[0];
+  for (int i = 1; i < XT; ++i) bm = (s_max[i] > bm || isnan(s_max[i])) ? s_max[i] : bm;
+  return bm;
+}
+
+template <typename R, int N, int XT>
+__global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
+  constexpr int E = N / 32;
+  constexpr int K = (N - 1) / 3 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
+  cplx<R>* s_G = s_tw + fft_smem(N, XT);
+  __shared__ double s_max[XT];
+  __shared__ int s_last;
+  const int tiles = N / XT;
+  const int b = blockIdx.x / tiles, x0 = (blockIdx.x - b * tiles) * XT;
+  pdl_trigger();
+  load_twiddles<R, N>(s_tw, p.tw);
+  pdl_wait();
+  StepCtl& c = p.ctl[b];
+  if (c.done) return;
+  const double bm = row_err_max<R, N, XT>(p.G, b, x0, s_tw, s_G, s_max);
   if (threadIdx.x == 0) {
-    double bm = s_max[0];
-    for (int i = 1; i < XT; ++i) bm = (s_max[i] > bm || isnan(s_max[i])) ? s_max[i] : bm;
     // non-negative doubles (and NaN with the sign bit clear) order like their bit patterns
     atomicMax(&c.err_bits, (unsigned long long)__double_as_longlong(fabs(bm)));
     __threadfence();

@@ -162,3 +162,59 @@ def test_default_batch_ranges(cuda, monkeypatch):
         assert counts[64][0] > 4 * counts[64][1], counts
     finally:
         context.clear_cache()
+
+
+RK43_CASES = [   # (n, B, T, atol, amp, seed)
+    (64, 1, 0.3, 1e-6, 6.0, 4),
+    (64, 3, 0.3, 1e-6, 6.0, 4),
+    (128, 2, 0.2, 1e-8, 2.0, 4),
+    (128, 1, 0.5, 1e-8, 2.0, 0),   # the 128^2 matvec workload's trajectory: rejected attempts
+]
+
+
+def _rk43(n, B, T, atol, amp, seed, monkeypatch, chain, w=0):
+    monkeypatch.setenv("ECS_CHAIN_MAXB", "0")   # the tangent sweep launched per pass in both runs
+    if chain:
+        monkeypatch.setenv("ECS_RK43CHAIN_MINB", "1")
+        monkeypatch.setenv("ECS_RK43CHAIN_MAXB", "64")
+        monkeypatch.setenv("ECS_CHAIN_WARPS", str(w))
+    else:
+        monkeypatch.setenv("ECS_RK43CHAIN_MAXB", "0")
+    context.clear_cache()
+    try:
+        cap = (64, 64) if seed == 0 else (4, 64)
+        pd = E.make_param_dict(n, 1 / 50, 1 / 50, forcing="kolmogorov+", shift_reflect_ny=1, rot=False,
+                               adaptive_dict={"atol": atol, "checkpoints": cap[0], "max_steps_per_checkpoint": cap[1]})
+        fields = torch.as_tensor(np.stack([initial_condition(seed + i, n, amp=amp) for i in range(B)]), device="cuda")
+        batch = E.objective_RPO({"fields": fields, "T": torch.linspace(T, 1.2 * T, B, dtype=torch.float64),
+                                 "sx": 0.2}, pd, "Lawson_RK43")["fields"].cpu().clone()
+        # the recorded linearisation of candidate 0 and a JVP through it (launched per pass)
+        prim = {"fields": fields[0].contiguous(), "T": T, "sx": 0.2}
+        obj = E.Objective(pd, "Lawson_RK43")
+        obj.linearize(prim, force=True, batch=1)
+        info = dict(obj.last_info)
+        du = torch.as_tensor(initial_condition(70, n) * 0.1, device="cuda")[None]
+        jv = obj.jvp(prim, {"fields": du, "T": torch.tensor([0.3], dtype=torch.float64),
+                            "sx": torch.tensor([-0.2], dtype=torch.float64)})
+        return batch, info, {k: v.detach().cpu().clone() for k, v in jv.items()}
+    finally:
+        monkeypatch.undo()
+        context.clear_cache()
+
+
+@pytest.mark.parametrize("n,B,T,atol,amp,seed", RK43_CASES)
+def test_rk43_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, T, atol, amp, seed):
+    """The adaptive Lawson-RK4(3) solve as one cluster-resident launch
+    (k_rk43_chain: attempts, error norm and accept/reject decision on the
+    device) equals the per-stage launches (k_col_rk43 / k_row_rhs / k_row_err)
+    bit for bit: the batched objective, the step statistics and the recorded
+    trajectory (through a JVP at the linearisation), with either CTA shape."""
+    want, want_info, want_jv = _rk43(n, B, T, atol, amp, seed, monkeypatch, chain=False)
+    for w in (8, 16):
+        got, info, jv = _rk43(n, B, T, atol, amp, seed, monkeypatch, chain=True, w=w)
+        assert torch.equal(got, want), w
+        assert info == want_info, w
+        for k in ("fields", "T", "sx"):
+            assert torch.equal(jv[k], want_jv[k]), (k, w)
+    if seed == 0:
+        assert want_info["rejected"] > 0, want_info
