@@ -37,6 +37,13 @@
 //     so neither array leaves the cluster.  The first pass of a launch reads and
 //     the last one writes global G / H, which carries the state from one launch
 //     to the next (a launch ends before a row pass, at a regeneration chunk).
+// With DSH (8-warp CTAs only, for shared-memory room) each column warp keeps its
+// column's tangent slots ([S_NSLOT][M]) in shared memory for the whole launch:
+// loaded at the start, written back to global D at the end.
+//
+// The same layout runs the primal: k_rk4_chain (fixed-step Lawson-RK4 steps)
+// and k_rk43_chain (adaptive attempts with the error norm and the accept/reject
+// decision in the kernel), below.
 #pragma once
 
 #include "kernels_tan.cuh"
