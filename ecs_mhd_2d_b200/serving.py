@@ -244,7 +244,8 @@ class Batcher(threading.Thread):
         self.kind, self.n, self.dtype, self.Re, self.batch = kind, n, dtype, Re, batch
         self.inbox = queue.Queue()
         self.results, self.now_fn = results, now_fn
-        self.queued = 0
+        self.queued = 0                  # requests handed over and not yet finished
+        self.lock = threading.Lock()     # guards `queued` (the scheduler adds, this thread subtracts)
         self.bytes = context_bytes(n, dtype, batch) + multi_bytes(n, dtype, batch)
         if kind == "gradient":
             self.bytes += grad_multi_bytes(n, dtype, batch)
@@ -281,7 +282,8 @@ class Batcher(threading.Thread):
             except Exception as ex:   # surfaced by Server.run
                 self.error = ex
                 self.results.put(None)
-            self.queued -= len(items)
+            with self.lock:
+                self.queued -= len(items)
 
 
 def run_matvec_batch(reqs, ctx, stream):
@@ -407,9 +409,10 @@ class Server:
                 bt = self.batchers[bkey] = Batcher(r.kind, r.n, r.dtype, r.Re, self.results, self._now,
                                                    batch=self.slots)
                 bt.start()
-            if bt.queued >= 2 * bt.batch:   # bounded backlog: the rest waits for admission
-                return False
-            bt.queued += 1
+            with bt.lock:
+                if bt.queued >= 2 * bt.batch:   # bounded backlog: the rest waits for admission
+                    return False
+                bt.queued += 1
             bt.inbox.put((r, t))
             return True
         if r.kind == "forward" and r.mode == "Lawson_RK4":

@@ -218,3 +218,41 @@ def test_rk43_chain_equals_launch_per_stage(cuda, monkeypatch, n, B, T, atol, am
             assert torch.equal(jv[k], want_jv[k]), (k, w)
     if seed == 0:
         assert want_info["rejected"] > 0, want_info
+
+
+def test_fp32_chains_equal_launch_per_pass(cuda, monkeypatch):
+    """FP32 (the precision mode's stepping and JVPs) through the chains: Lawson-RK4
+    stepping and a batch-1 adaptive JVP at n = 64 equal the per-pass launches bit
+    for bit."""
+    n = 64
+
+    def run(chain):
+        monkeypatch.setenv("ECS_CHAIN_MAXB", "64" if chain else "0")
+        monkeypatch.setenv("ECS_RK4CHAIN_MAXB", "64" if chain else "0")
+        monkeypatch.setenv("ECS_RK43CHAIN_MAXB", "64" if chain else "0")
+        context.clear_cache()
+        try:
+            pd = E.make_param_dict(n, 1 / 40, 1 / 40, forcing="kolmogorov+", data_type=torch.float32,
+                                   shift_reflect_ny=1, rot=False,
+                                   adaptive_dict={"atol": 1e-5, "checkpoints": 4, "max_steps_per_checkpoint": 64})
+            f = torch.as_tensor(np.fft.rfft2(np.stack([initial_condition(80 + b, n, amp=3.0) for b in range(2)])),
+                                dtype=torch.complex64, device="cuda")
+            stepped = E.lawson_rk4(f, 0.1, 20, pd).cpu().clone()
+            prim = {"fields": torch.as_tensor(initial_condition(4, n, amp=4.0), dtype=torch.float32, device="cuda"),
+                    "T": 0.3, "sx": 0.2}
+            obj = E.Objective(pd, "Lawson_RK43")
+            obj.linearize(prim, force=True, batch=1)
+            du = torch.as_tensor(initial_condition(61, n) * 0.1, dtype=torch.float32, device="cuda")[None]
+            jv = obj.jvp(prim, {"fields": du, "T": torch.tensor([0.4], dtype=torch.float64),
+                                "sx": torch.tensor([0.1], dtype=torch.float64)})
+            return stepped, {k: v.detach().cpu().clone() for k, v in jv.items()}, dict(obj.last_info)
+        finally:
+            monkeypatch.undo()
+            context.clear_cache()
+
+    want = run(False)
+    got = run(True)
+    assert torch.equal(got[0], want[0])
+    for k in ("fields", "T", "sx"):
+        assert torch.equal(got[1][k], want[1][k]), k
+    assert got[2] == want[2]
