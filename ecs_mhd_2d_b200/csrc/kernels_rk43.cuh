@@ -268,8 +268,6 @@ __device__ __forceinline__ double row_err_max(const cplx<R>* G, int b, int x0, c
 
 template <typename R, int N, int XT>
 __global__ void __launch_bounds__(XT * 32) k_row_err(RowErrParams<R> p) {
-  constexpr int E = N / 32;
-  constexpr int K = (N - 1) / 3 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<R>* s_tw = reinterpret_cast<cplx<R>*>(smem_raw);
   cplx<R>* s_G = s_tw + fft_smem(N, XT);
