@@ -145,7 +145,10 @@ class ForwardPool:
         self.pd = make_param_dict(n, 1.0 / Re, 1.0 / Re, forcing="kolmogorov+", data_type=dtype)
         fk = C._forcing_key(self.pd["forcing"])
         self.ctx = C.Context(n, dtype, 1.0 / Re, 1.0 / Re, self.pd["b0"], fk[1], max_batch=slots)
-        self.stream = torch.cuda.Stream()
+        # high priority: the pool's small step launches run ahead of the batchers'
+        # and workers' large sweeps instead of queueing behind them (the scheduler
+        # waits for every pool's chunk before it admits and retires again)
+        self.stream = torch.cuda.Stream(priority=-1)
         self.req = [None] * slots
         self.t_admit = [0.0] * slots
         self.bytes = context_bytes(n, dtype, slots)
@@ -230,6 +233,7 @@ class Worker(threading.Thread):
                 self.error = ex
                 self.results.put(None)
             self.busy = False
+        self.ctx.close()   # in this thread, before the interpreter's shutdown
 
 
 class Batcher(threading.Thread):
@@ -284,6 +288,7 @@ class Batcher(threading.Thread):
                 self.results.put(None)
             with self.lock:
                 self.queued -= len(items)
+        ctx.close()   # in this thread, before the interpreter's shutdown
 
 
 def run_matvec_batch(reqs, ctx, stream):
@@ -388,19 +393,30 @@ class Server:
                 results[res.rid] = res
             if not any(p.active() for p in self.pools.values()) and len(results) < total:
                 time.sleep(0.0005)
-        for ws in self.workers.values():
-            for w in ws:
-                w.inbox.put(None)
-        for b in self.batchers.values():
-            b.inbox.put(None)
+        self.close()
         return [results[k] for k in sorted(results)]
+
+    def close(self):
+        """Stop the worker and batcher threads (each releases its context) and
+        release the pools' contexts, so that nothing is left to tear down at
+        interpreter exit.  The stopped batchers stay in `batchers` (their sweep
+        sizes); a later run starts new threads and pools."""
+        threads = [w for ws in self.workers.values() for w in ws] + list(self.batchers.values())
+        for t in threads:
+            if t.is_alive():
+                t.inbox.put(None)
+        for t in threads:
+            t.join(timeout=120)
+        for p in self.pools.values():
+            p.ctx.close()
+        self.workers, self.pools = {}, {}
 
     def _admit(self, r, t):
         key = (r.n, r.dtype, r.Re)
         if r.kind in ("matvec", "gradient") and r.mode == "Lawson_RK4":
             bkey = (r.kind,) + key
             bt = self.batchers.get(bkey)
-            if bt is None:
+            if bt is None or not bt.is_alive():   # (a batcher of an earlier run has stopped)
                 need = context_bytes(r.n, r.dtype, self.slots) + multi_bytes(r.n, r.dtype, self.slots)
                 if r.kind == "gradient":
                     need += grad_multi_bytes(r.n, r.dtype, self.slots)
