@@ -30,6 +30,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import queue
+import sys
 import threading
 import time
 
@@ -359,7 +360,20 @@ class Server:
                 + sum(w.bytes + w.req_bytes for ws in self.workers.values() for w in ws))
 
     def run(self, requests, time_scale=1.0):
-        """Serve `requests` (arrival times in seconds); returns results in rid order."""
+        """Serve `requests` (arrival times in seconds); returns results in rid order.
+        The interpreter's thread switch interval is 0.5 ms meanwhile (5 ms by
+        default): the scheduler loop shares the interpreter with the worker and
+        batcher threads, and each of its steps would otherwise wait up to 5 ms
+        for them (measured: admission waits and forward latencies fell by a
+        third)."""
+        old_switch = sys.getswitchinterval()
+        sys.setswitchinterval(min(old_switch, 0.0005))
+        try:
+            return self._run(requests, time_scale)
+        finally:
+            sys.setswitchinterval(old_switch)
+
+    def _run(self, requests, time_scale):
         t0 = time.perf_counter()
         now = lambda: (time.perf_counter() - t0) / time_scale
         self._now = now
